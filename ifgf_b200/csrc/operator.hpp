@@ -1,0 +1,86 @@
+// The IFGF operator object behind the C ABI: host planner + device tables +
+// the per-level CUDA pipeline.  No CUDA types appear in this header.
+#pragma once
+
+#include <cstdint>
+#include <functional>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "common.hpp"
+#include "plan.hpp"
+
+namespace ifgf
+{
+
+struct DeviceState; // device buffers, defined in operator.cu
+
+struct StageTimes
+{
+    double permute = 0, coarse = 0, c2f = 0, eval = 0, total = 0;
+};
+
+class Operator
+{
+  public:
+    // IfgfOperator ctor (ifgfoperator.hpp:36-59) + plug-in ctor
+    Operator(int kind, double k_re, double k_im, int64_t leaf_size, int64_t order, int64_t n_elem,
+             double tol);
+    ~Operator();
+
+    void set_dx(int dx);
+    void set_precision(int mode);
+    // IfgfOperator::init (ifgfoperator.hpp:65-106)
+    void init(const double* srcs, int64_t ns, const double* tgts, int64_t nt,
+              const double* normals, const std::function<bool(double)>& cutoff,
+              bool plan_only = false);
+    // IfgfOperator::mult on device buffers; stream is a cudaStream_t
+    void mult_device(const void* d_w, void* d_u, void* stream);
+    // host buffers, `batch` right-hand sides
+    void mult_host(const void* w, void* u, int64_t batch);
+
+    int kind() const { return kind_; }
+    bool is_real() const { return kind_ == K_LAPLACE; }
+    int64_t n_src() const { return plan_.src.n; }
+    int64_t n_tgt() const { return plan_.tgt.n; }
+    bool initialized() const { return initialized_; }
+    bool planned() const { return planned_; }
+    const Plan& plan() const { return plan_; }
+    void orders(int step, int* o) const;
+    void level_grid(int level, int step, int64_t* n) const;
+    std::vector<int64_t> box_cones(int level, int64_t box, int step) const;
+    std::string stats_json() const;
+
+  private:
+    void order_for_box(int step, int* out) const;
+    void elements_for_box(double H, int step, int64_t* out) const;
+    double cutoff_limit(double H) const;
+    void setup_device(const double* normals);
+    void launch_mult(const void* d_w, void* d_u, void* stream, bool timed);
+
+    int kind_;
+    double kr_, ki_;
+    int dx_ = -1;
+    double tol_;
+    int64_t leaf_;
+    int order0_;
+    int base_order_[3];
+    int64_t base_n_[3];
+    int precision_ = PREC_FP64;
+    bool initialized_ = false;
+    bool planned_ = false;
+    Plan plan_;
+    std::vector<LevelGeom> lv_;
+    int lo_[3], hi_[3];
+    int fct_[3];
+    std::unique_ptr<DeviceState> dev_;
+    // statistics
+    double init_ms_ = 0;
+    StageTimes last_;
+    int64_t n_coarse_total_ = 0, n_fine_total_ = 0;
+    double leaf_evals_ = 0, upward_evals_ = 0;
+    unsigned long long missing_ = 0;
+};
+
+} // namespace ifgf

@@ -1,0 +1,320 @@
+// Host-side planner: octrees and dual-tree interaction lists.
+#include "plan.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+
+#include "common.hpp"
+
+namespace ifgf
+{
+
+// Spread the low 21 bits of v to every third bit position.
+static inline uint64_t spread3(uint64_t v)
+{
+    v &= 0x1fffffull;
+    v = (v | (v << 32)) & 0x1f00000000ffffull;
+    v = (v | (v << 16)) & 0x1f0000ff0000ffull;
+    v = (v | (v << 8)) & 0x100f00f00f00f00full;
+    v = (v | (v << 4)) & 0x10c30c30c30c30c3ull;
+    v = (v | (v << 2)) & 0x1249249249249249ull;
+    return v;
+}
+
+// Order-preserving 42-bit code of a normalised coordinate p in (-0.5, 0.5):
+// the top bit is the sign test of zorder_less.hpp:230 (negative first), the
+// remaining 41 bits are |p| in fixed point, complemented for negative p so
+// that larger magnitudes sort first, as `p[k] < q[k]` does for negatives.
+static inline uint64_t coord_code(double p)
+{
+    const uint64_t top = 1ull << 41;
+    const bool neg = p < 0.0;
+    double a = std::fabs(p) * 4398046511104.0; // |p| * 2^42, exact scaling
+    uint64_t u = a >= (double)(top - 1) ? top - 1 : (uint64_t)a;
+    return neg ? (top - 1 - u) : (top | u);
+}
+
+void morton_key(const double* x, const double* c, const double* diam, uint64_t* hi,
+                uint64_t* lo)
+{
+    // normalisation exactly as zorder_less.hpp:226-227
+    uint64_t k[3];
+    for (int d = 0; d < 3; d++)
+        k[d] = coord_code((x[d] - c[d]) / diam[d]);
+    // equal bit levels: z beats y beats x (ties keep the higher dimension,
+    // zorder_less.hpp:229-240)
+    *hi = (spread3(k[2] >> 21) << 2) | (spread3(k[1] >> 21) << 1) | spread3(k[0] >> 21);
+    *lo = (spread3(k[2]) << 2) | (spread3(k[1]) << 1) | spread3(k[0]);
+}
+
+static bool box_contains(const double* mn, const double* mx, const double* p)
+{
+    for (int k = 0; k < 3; k++)
+        if (!(mn[k] <= p[k]) || !(p[k] <= mx[k]))
+            return false;
+    return true;
+}
+
+void Tree::build(const double* p, int64_t n_pts, int64_t leaf_size)
+{
+    n = n_pts;
+    max_leaf = leaf_size;
+    // bounding box, inflated as octree.hpp:207-218
+    double mn[3], mx[3];
+    for (int d = 0; d < 3; d++)
+        mn[d] = mx[d] = p[d];
+    for (int64_t i = 0; i < n; i++)
+        for (int d = 0; d < 3; d++)
+        {
+            mn[d] = std::min(mn[d], p[3 * i + d]);
+            mx[d] = std::max(mx[d], p[3 * i + d]);
+        }
+    const double nmn = std::sqrt(mn[0] * mn[0] + mn[1] * mn[1] + mn[2] * mn[2]);
+    const double nmx = std::sqrt(mx[0] * mx[0] + mx[1] * mx[1] + mx[2] * mx[2]);
+    for (int d = 0; d < 3; d++)
+    {
+        mn[d] -= 1e-8 * nmn;
+        mx[d] += 1e-8 * nmx;
+    }
+    double c[3], diam[3];
+    for (int d = 0; d < 3; d++)
+    {
+        c[d] = (mx[d] + mn[d]) / 2.0;
+        diam[d] = mx[d] - mn[d];
+    }
+    // Morton sort: keys, ties broken by the original index
+    struct K
+    {
+        uint64_t hi, lo;
+        int64_t idx;
+    };
+    std::vector<K> keys(n);
+    for (int64_t i = 0; i < n; i++)
+    {
+        morton_key(p + 3 * i, c, diam, &keys[i].hi, &keys[i].lo);
+        keys[i].idx = i;
+    }
+    std::sort(keys.begin(), keys.end(), [](const K& a, const K& b) {
+        if (a.hi != b.hi)
+            return a.hi < b.hi;
+        if (a.lo != b.lo)
+            return a.lo < b.lo;
+        return a.idx < b.idx;
+    });
+    perm.resize(n);
+    pts.resize(3 * n);
+    for (int64_t i = 0; i < n; i++)
+    {
+        perm[i] = keys[i].idx;
+        for (int d = 0; d < 3; d++)
+            pts[3 * i + d] = p[3 * keys[i].idx + d];
+    }
+    keys.clear();
+    keys.shrink_to_fit();
+
+    // Level-synchronous construction.  Visiting the boxes of a level in id
+    // order and their children in octant order hands out the same per-level
+    // ids as the depth-first construction of octree.hpp:1106-1184.
+    levels.clear();
+    auto push_box = [&](TreeLevel& L, int64_t f, int64_t l, int32_t par, const double* bmn,
+                        const double* bmx) {
+        L.first.push_back(f);
+        L.last.push_back(l);
+        L.parent.push_back(par);
+        L.leaf.push_back(1);
+        for (int j = 0; j < 8; j++)
+            L.child.push_back(-1);
+        double s = 0;
+        for (int d = 0; d < 3; d++)
+        {
+            L.bbmin.push_back(bmn[d]);
+            L.bbmax.push_back(bmx[d]);
+            L.center.push_back((bmx[d] + bmn[d]) / 2.0);
+            s = std::max(s, std::abs(bmx[d] - bmn[d]));
+        }
+        L.sides.push_back(s);
+    };
+    levels.emplace_back();
+    if (n > 0)
+        push_box(levels[0], 0, n, -1, mn, mx);
+    for (size_t l = 0; l < levels.size(); l++)
+    {
+        TreeLevel next;
+        TreeLevel& L = levels[l];
+        for (size_t b = 0; b < L.size(); b++)
+        {
+            const int64_t cnt = L.last[b] - L.first[b];
+            if (cnt <= max_leaf)
+                continue;
+            int64_t pidx = L.first[b];
+            for (int j = 0; j < 8; j++)
+            {
+                double cmn[3], cmx[3];
+                for (int d = 0; d < 3; d++)
+                {
+                    const double size = 0.5 * (L.bbmax[3 * b + d] - L.bbmin[3 * b + d]);
+                    cmn[d] = L.bbmin[3 * b + d] + size * (double)((j >> d) & 1);
+                    cmx[d] = cmn[d] + size;
+                }
+                int64_t end = pidx;
+                while (end < L.last[b] && box_contains(cmn, cmx, &pts[3 * end]))
+                    ++end;
+                if (end > pidx)
+                {
+                    L.child[8 * b + j] = (int32_t)next.size();
+                    L.leaf[b] = 0;
+                    push_box(next, pidx, end, (int32_t)b, cmn, cmx);
+                }
+                pidx = end;
+            }
+        }
+        if (next.size() == 0)
+            break;
+        levels.push_back(std::move(next));
+    }
+    level_off.assign(levels.size() + 1, 0);
+    for (size_t l = 0; l < levels.size(); l++)
+    {
+        levels[l].side = levels[l].size() ? levels[l].sides[0] : 0;
+        level_off[l + 1] = level_off[l] + (int64_t)levels[l].size();
+    }
+}
+
+namespace
+{
+struct Walker
+{
+    Plan& P;
+    const std::function<bool(double)>& cutoff;
+    const double eta = std::sqrt(3.0);
+
+    // Octree::buildInteractionList (octree.hpp:272-349)
+    void walk(int sl, int32_t s, int tl, int32_t t)
+    {
+        if (s < 0 || t < 0)
+            return;
+        const TreeLevel& SL = P.src.levels[sl];
+        const TreeLevel& TL = P.tgt.levels[tl];
+        if (SL.first[s] == SL.last[s] || TL.first[t] == TL.last[t])
+            return;
+        // admissibility (octree.hpp:189-198): exterior distance of the
+        // target box to the source centre >= sqrt(3) * source side length
+        double d2 = 0;
+        for (int k = 0; k < 3; k++)
+        {
+            const double p = SL.center[3 * s + k];
+            const double lo = TL.bbmin[3 * t + k], hi = TL.bbmax[3 * t + k];
+            if (lo > p)
+            {
+                const double a = lo - p;
+                d2 += a * a;
+            }
+            else if (p > hi)
+            {
+                const double a = p - hi;
+                d2 += a * a;
+            }
+        }
+        const double dist = std::sqrt(d2);
+        const int64_t sg = P.src.level_off[sl] + s, tg = P.tgt.level_off[tl] + t;
+        if (dist >= eta * SL.sides[s])
+        {
+            if (cutoff && cutoff(dist))
+            {
+                P.n_dropped++;
+                return;
+            }
+            P.far[sg].push_back(tg);
+            P.n_far_pairs++;
+            P.far_target_evals += TL.last[t] - TL.first[t];
+            return;
+        }
+        const bool sleaf = SL.leaf[s], tleaf = TL.leaf[t];
+        if (sleaf && tleaf)
+        {
+            P.near[sg].push_back(tg);
+            P.n_near_pairs++;
+            P.near_point_pairs += (SL.last[s] - SL.first[s]) * (TL.last[t] - TL.first[t]);
+            return;
+        }
+        if (sleaf && !tleaf)
+        {
+            for (int j = 0; j < 8; j++)
+                walk(sl, s, tl + 1, TL.child[8 * t + j]);
+            return;
+        }
+        if (tleaf && !sleaf)
+        {
+            for (int j = 0; j < 8; j++)
+                walk(sl + 1, SL.child[8 * s + j], tl, t);
+            return;
+        }
+        if (SL.sides[s] > TL.sides[t])
+            for (int j = 0; j < 8; j++)
+                walk(sl + 1, SL.child[8 * s + j], tl, t);
+        else
+            for (int j = 0; j < 8; j++)
+                walk(sl, s, tl + 1, TL.child[8 * t + j]);
+    }
+};
+} // namespace
+
+void Plan::build_lists(const std::function<bool(double)>& cutoff)
+{
+    const int64_t nb = src.num_boxes_total();
+    far.assign(nb, {});
+    near.assign(nb, {});
+    n_far_pairs = n_near_pairs = n_dropped = far_target_evals = near_point_pairs = 0;
+    if (src.n == 0 || tgt.n == 0)
+        return;
+    Walker w{*this, cutoff};
+    w.walk(0, 0, 0, 0);
+}
+
+void Plan::build_target_lists()
+{
+    const int64_t ntb = tgt.num_boxes_total();
+    std::vector<std::vector<int32_t>> far_in(ntb), near_in(ntb);
+    const int64_t nsb = src.num_boxes_total();
+    for (int64_t s = 0; s < nsb; s++)
+    {
+        for (int64_t t : far[s])
+            far_in[t].push_back((int32_t)s);
+        for (int64_t t : near[s])
+            near_in[t].push_back((int32_t)s);
+    }
+    tleaf_gid.clear();
+    tleaf_far_off.assign(1, 0);
+    tleaf_near_off.assign(1, 0);
+    tleaf_far_src.clear();
+    tleaf_near_src.clear();
+    for (int l = 0; l < tgt.num_levels(); l++)
+    {
+        const TreeLevel& L = tgt.levels[l];
+        for (size_t b = 0; b < L.size(); b++)
+        {
+            if (!L.leaf[b])
+                continue;
+            const int64_t g = tgt.level_off[l] + (int64_t)b;
+            tleaf_gid.push_back(g);
+            // far interactions of this leaf and of all its ancestors
+            int al = l;
+            int32_t ab = (int32_t)b;
+            while (al >= 0)
+            {
+                const int64_t ag = tgt.level_off[al] + ab;
+                for (int32_t s : far_in[ag])
+                    tleaf_far_src.push_back(s);
+                ab = tgt.levels[al].parent[ab];
+                al--;
+            }
+            tleaf_far_off.push_back((int64_t)tleaf_far_src.size());
+            for (int32_t s : near_in[g])
+                tleaf_near_src.push_back(s);
+            tleaf_near_off.push_back((int64_t)tleaf_near_src.size());
+        }
+    }
+}
+
+} // namespace ifgf

@@ -1,0 +1,69 @@
+// Host-side planner: octrees and dual-tree interaction lists.
+//
+// The trees reproduce the reference's box indexing: Morton order of the
+// points (zorder_less.hpp:212-248) realised with interleaved fixed-point keys,
+// greedy closed-interval child ranges (octree.hpp:1106-1184) and per-level
+// box ids in creation order.  The interaction lists follow the dual-tree walk
+// of octree.hpp:255-349 in the same visiting order.
+#pragma once
+
+#include <cstdint>
+#include <functional>
+#include <vector>
+
+namespace ifgf
+{
+
+struct TreeLevel
+{
+    std::vector<int64_t> first, last; // point range [first, last)
+    std::vector<int32_t> parent;      // index in level-1 (-1 at the root)
+    std::vector<uint8_t> leaf;
+    std::vector<int32_t> child;       // 8 per box, index in level+1 or -1
+    std::vector<double> bbmin, bbmax, center; // 3 per box
+    double side = 0;                  // sideLength() of the first box (all equal)
+    std::vector<double> sides;        // per box (identical up to rounding)
+    size_t size() const { return first.size(); }
+};
+
+struct Tree
+{
+    int64_t n = 0;
+    int64_t max_leaf = 100;
+    std::vector<int64_t> perm;  // sorted position -> original index
+    std::vector<double> pts;    // sorted points, AoS xyz
+    std::vector<TreeLevel> levels;
+    std::vector<int64_t> level_off; // global box id of the first box of a level
+
+    int num_levels() const { return (int)levels.size(); }
+    int64_t num_boxes_total() const { return level_off.empty() ? 0 : level_off.back(); }
+
+    // Octree::build (octree.hpp:202-238)
+    void build(const double* p, int64_t n_pts, int64_t leaf_size);
+};
+
+struct Plan
+{
+    Tree src, tgt;
+    // per source box (global id): target boxes (global ids) in discovery order
+    std::vector<std::vector<int64_t>> far, near;
+    // target-leaf-centric lists for the evaluation kernel
+    std::vector<int64_t> tleaf_gid;       // target leaves (global target box ids)
+    std::vector<int64_t> tleaf_far_off;   // CSR offsets into tleaf_far_src
+    std::vector<int32_t> tleaf_far_src;   // source global box ids
+    std::vector<int64_t> tleaf_near_off;
+    std::vector<int32_t> tleaf_near_src;  // source leaf global box ids
+    // counters (octree.hpp:265-268)
+    int64_t n_far_pairs = 0, n_near_pairs = 0, n_dropped = 0;
+    int64_t far_target_evals = 0, near_point_pairs = 0;
+
+    void build_lists(const std::function<bool(double)>& cutoff);
+    void build_target_lists();
+};
+
+// Morton key of a point normalised to the root box: 42 bits per dimension,
+// interleaved z,y,x most significant first, split in two 63-bit halves.
+void morton_key(const double* p, const double* center, const double* diam, uint64_t* hi,
+                uint64_t* lo);
+
+} // namespace ifgf

@@ -1,0 +1,146 @@
+/*
+ * ifgf_b200 -- C ABI of the B200 IFGF matvec library (libifgf_b200.so).
+ *
+ * The entry points below are the boundary a foreign-function binding of the
+ * reference's operator would bind.  The reference exposes its operators
+ * through pybind11 (py_ifgf.cpp:16-58); each function names the reference
+ * interface it replaces.  Plain pointers and sizes only; every call returns an
+ * int status (IFGF_OK == 0) and ifgf_last_error() gives a message for the
+ * calling thread's last failure.
+ *
+ * Point arrays are float64, 3 x N in column-major order (x0,y0,z0,x1,...),
+ * the memory layout of the reference's Eigen::Array<double, 3, Dynamic>.
+ * Densities and results are complex128 (interleaved re, im) for every kernel
+ * except Laplace, whose densities and results are float64 (the reference's
+ * T = double, laplace_ifgf.hpp:8).
+ *
+ * A handle owns all of its device memory.  Calls on one handle are not
+ * thread-safe; separate handles are independent.
+ */
+#ifndef IFGF_B200_H
+#define IFGF_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct ifgf_operator ifgf_operator;
+
+/* status codes */
+#define IFGF_OK 0
+#define IFGF_ERR_INVALID_ARG 1 /* bad size, order, kind, NaN/Inf input, ... */
+#define IFGF_ERR_CUDA 2        /* a CUDA runtime call failed                  */
+#define IFGF_ERR_STATE 3       /* e.g. mult before init                      */
+#define IFGF_ERR_OOM 4         /* device allocation failed                   */
+#define IFGF_ERR_TIMEOUT 5     /* a bounded device wait gave up              */
+#define IFGF_ERR_INTERNAL 6    /* consistency check failed (cone lookups)    */
+
+/* kernel plug-ins (one per reference Derived class) */
+#define IFGF_LAPLACE 0            /* laplace_ifgf.hpp                    */
+#define IFGF_HELMHOLTZ 1          /* helmholtz_ifgf.hpp                  */
+#define IFGF_MODIFIED_HELMHOLTZ 2 /* modified_helmholtz_ifgf.hpp         */
+#define IFGF_GRAD_HELMHOLTZ 3     /* grad_helmholtz_ifgf.hpp             */
+#define IFGF_DOUBLE_LAYER 4       /* double_layer_helmholtz_ifgf.hpp     */
+#define IFGF_COMBINED_FIELD 5     /* combined_field_helmholtz_ifgf.hpp   */
+
+/* precision modes */
+#define IFGF_PREC_FP64 0  /* FP64 throughout                                  */
+#define IFGF_PREC_MIXED 1 /* FP32 sums with FP64 phase / final accumulation   */
+
+/* Replaces the IfgfOperator constructor (ifgfoperator.hpp:36-59) together
+ * with the plug-in constructors (helmholtz_ifgf.hpp:13-20,
+ * laplace_ifgf.hpp:12-15, modified_helmholtz_ifgf.hpp:13-20,
+ * grad_helmholtz_ifgf.hpp:13-21, double_layer_helmholtz_ifgf.hpp:13-20,
+ * combined_field_helmholtz_ifgf.hpp:13-20) as bound at py_ifgf.cpp:19, :46.
+ * k = k_re + i k_im is the wavenumber (ignored by Laplace; the imaginary part
+ * is ignored by the real-wavenumber Helmholtz and combined-field kernels).
+ * tol <= 0 selects the fixed-order path (ifgfoperator.hpp:88-91); tol > 0 is
+ * accepted and, as in the reference, only changes the gradient kernel's
+ * cutoff (grad_helmholtz_ifgf.hpp:294-304) -- order estimation is not run. */
+int ifgf_create(int kind, double k_re, double k_im, long leaf_size, long order, long n_elem,
+                double tol, ifgf_operator** out);
+
+/* Replaces GradHelmholtzIfgfOperator::setDx (grad_helmholtz_ifgf.hpp:61,
+ * py_ifgf.cpp:40): dx in {-1, 0, 1, 2}. */
+int ifgf_set_dx(ifgf_operator* op, int dx);
+
+/* Selects FP64 (default) or the mixed-precision pipeline.  No reference
+ * counterpart (the reference is FP64 only). */
+int ifgf_set_precision(ifgf_operator* op, int mode);
+
+/* Far-interaction drop predicate of IfgfOperator::init
+ * (ifgfoperator.hpp:65-67, octree.hpp:282-297): return nonzero to drop an
+ * admissible pair at exterior distance `dist`.  May be NULL. */
+typedef int (*ifgf_cutoff_fn)(double dist, void* user);
+
+/* Replaces IfgfOperator::init (ifgfoperator.hpp:65-106) and the double-layer
+ * / combined-field init(srcs, targets, normals)
+ * (double_layer_helmholtz_ifgf.hpp:22-26,
+ * combined_field_helmholtz_ifgf.hpp:22-26).  normals: 3 x n_src, required for
+ * IFGF_DOUBLE_LAYER and IFGF_COMBINED_FIELD, ignored otherwise. */
+int ifgf_init(ifgf_operator* op, const double* srcs, long n_src, const double* tgts,
+              long n_tgt, const double* normals, ifgf_cutoff_fn cutoff, void* user);
+
+/* Host half of ifgf_init: builds the octrees and interaction lists only,
+ * touching no GPU (the tree and list accessors below work after it; mult
+ * does not).  For tests and tooling on machines without a GPU. */
+int ifgf_init_plan_only(ifgf_operator* op, const double* srcs, long n_src, const double* tgts,
+                        long n_tgt, ifgf_cutoff_fn cutoff, void* user);
+
+/* Replaces IfgfOperator::mult (ifgfoperator.hpp:246-867) with host buffers:
+ * w has n_src entries, u receives n_tgt entries (caller's original order). */
+int ifgf_mult(ifgf_operator* op, const void* w, void* u);
+
+/* Same as ifgf_mult for `batch` right-hand sides stored one after another
+ * (w: batch x n_src, u: batch x n_tgt).  No reference counterpart. */
+int ifgf_mult_batch(ifgf_operator* op, const void* w, void* u, long batch);
+
+/* ifgf_mult on device buffers (complex128 / float64 as above) enqueued on
+ * `stream` (a cudaStream_t, NULL = legacy default stream).  Returns after
+ * enqueueing.  No reference counterpart. */
+int ifgf_mult_device(ifgf_operator* op, const void* d_w, void* d_u, void* stream);
+
+int ifgf_num_sources(const ifgf_operator* op, long* n);
+int ifgf_num_targets(const ifgf_operator* op, long* n);
+
+/* Structured statistics of the last init/mult as JSON text (levels, boxes,
+ * active cones, near/far pairs, per-stage milliseconds, work counts).
+ * Writes at most cap bytes including the terminating NUL; *needed receives
+ * the full length.  No reference counterpart (it prints to stdout). */
+int ifgf_stats_json(const ifgf_operator* op, char* buf, long cap, long* needed);
+
+/* Tree and cone tables, for parity tests against the reference's octree.
+ * which: 0 = source tree, 1 = target tree. */
+int ifgf_tree_levels(const ifgf_operator* op, int which, int* levels);
+int ifgf_tree_num_boxes(const ifgf_operator* op, int which, int level, long* n);
+/* perm[i] = original index of the i-th point in Morton order
+ * (Octree::permutation, octree.hpp:225-226). */
+int ifgf_tree_permutation(const ifgf_operator* op, int which, long* perm);
+/* per box 12 longs: first, last, parent, is_leaf, child[8] (-1 = absent);
+ * bbox: 6 doubles per box (min xyz, max xyz) (octree.hpp:1106-1184). */
+int ifgf_tree_boxes(const ifgf_operator* op, int which, int level, long* ints, double* bbox);
+/* interaction list of one source box (Octree::OctreeNode::nearTargets /
+ * farTargets, octree.hpp:150-156): far = 0 near, 1 far; writes up to cap
+ * (first, last) target point ranges in discovery order. */
+int ifgf_box_list(const ifgf_operator* op, int level, long box, int far, long* out, long cap,
+                  long* n);
+/* active cone element ids of one source box, step 0 = fine, 1 = coarse,
+ * in increasing element order (octree.hpp:743-790 hands them out in first-
+ * insertion order; the set is the same). */
+int ifgf_box_cones(const ifgf_operator* op, int level, long box, int step, long* out, long cap,
+                   long* n);
+/* cone grid of a level: n[3] elements per dimension; orders of a step */
+int ifgf_level_grid(const ifgf_operator* op, int level, int step, long* n);
+int ifgf_orders(const ifgf_operator* op, int step, int* order);
+
+/* Destroys the handle and frees its device memory. */
+int ifgf_destroy(ifgf_operator* op);
+
+/* Message of the calling thread's last failed call ("" if none). */
+const char* ifgf_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* IFGF_B200_H */
