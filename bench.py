@@ -1,0 +1,390 @@
+#!/usr/bin/env python
+"""Benchmark of the IFGF matvec at the headline configuration.
+
+Workload: N = 1,000,000 points uniform on the ellipsoid with semi-axes
+(1, 1, 0.5) (normalised Gaussian directions projected radially, seed 0),
+sources = targets, Helmholtz kernel e^{ikr}/(4 pi r) with k = 100, complex
+densities Re, Im ~ N(0, 1) (seed 1), leaf boxes <= 100 points, order p
+(high-order cones (p-3, p, p), low-order cones (p-3, p-3, p-3) clamped at 2).
+A step is one matvec u = A w.  The metric is milliseconds per matvec (lower
+is better) at relative error <= 1e-4 against the FP64 direct sum at 1,000
+sampled targets.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--impl reference times the CPU restatement of the reference's mult (the
+reference itself needs Eigen and oneTBB, which this image lacks) on the
+host cores, on a bounded sample of the same workload (whole level-2 source
+subtrees), scaled to the full matvec by the modelled work.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from ifgf_b200 import workloads as W  # noqa: E402
+
+METRIC = "IFGF matvec ms at N=1e6, k=100, rel err<=1e-4 vs FP64; mixed/batched vs FP64"
+UNIT = "ms"
+TOL = 1e-4
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--precision", choices=["mixed", "fp64"], default=None)
+    ap.add_argument("--n", type=int, default=1_000_000)
+    ap.add_argument("--k", type=float, default=100.0)
+    ap.add_argument("--order", type=int, default=9)
+    ap.add_argument("--leaf", type=int, default=100)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--sample-boxes", type=int, default=0,
+                    help="source subtrees in the CPU sample (0: one per host thread)")
+    return ap.parse_args()
+
+
+def workload_config(a, precision):
+    return {
+        "workload": f"helmholtz k={a.k:g}, N={a.n} ellipsoid (1,1,0.5), sources=targets",
+        "kernel": "helmholtz",
+        "n_points": a.n,
+        "wavenumber": a.k,
+        "leaf_size": a.leaf,
+        "order_p": a.order,
+        "precision": precision,
+        "l2": "inputs and per-matvec working set larger than L2 (126 MB)",
+    }
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class Clocks:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.2)
+        self.proc.terminate()
+        self.proc.wait()
+        rows = []
+        for line in open(self.path):
+            p = [x.strip() for x in line.split(",")]
+            if len(p) >= 9:
+                rows.append(p)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing
+# ---------------------------------------------------------------------------
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return ws, rank, local
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(ws, x):
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------
+# flop model (per unit; transcendental = 1, FMA = 2, complex mul = 6)
+# ---------------------------------------------------------------------------
+def model(stats):
+    lo = stats["order_low"]
+    hi = stats["order_high"]
+    plo = lo[0] * lo[1] * lo[2]
+    cheb = 3 * (plo + lo[1] * lo[2] + lo[2]) * 2
+    f_near, f_factor = 23, 25
+    f_far = 15 + 6 + cheb + 10
+    f_up = 15 + 6 + cheb + 12
+    # coarse -> fine: three mode products (complex x real = 4 flops per MAC)
+    f0, f1, f2 = 3, 3, 3
+    F0, F1, F2 = f0 * lo[0], f1 * lo[1], f2 * lo[2]
+    macs = F0 * hi[0] * hi[1] * hi[2] + F0 * F1 * hi[1] * hi[2] + F0 * F1 * F2 * hi[2]
+    f_c2f = 4 * macs
+    return {
+        "coarse_values": stats["leaf_factor_evals"] * f_factor + stats["upward_node_evals"] * f_up,
+        "coarse_to_fine": stats["coarse_cones_total"] * f_c2f,
+        "target_eval": stats["near_point_pairs"] * f_near + stats["far_target_evals"] * f_far,
+        "permute": 0.0,
+    }
+
+
+def measured_peak_tflops(dtype):
+    """Dense GEMM throughput of this GPU in the given precision (cuBLAS via
+    torch.matmul, 8192^3, best of 5): the measured peak of the FP64 / FP32 pipe."""
+    import torch
+
+    torch.backends.cuda.matmul.allow_tf32 = False
+    n = 8192 if dtype == torch.float64 else 8192
+    a = torch.randn(n, n, dtype=dtype, device="cuda")
+    b = torch.randn(n, n, dtype=dtype, device="cuda")
+    torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 1e30
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a, b
+    return 2 * n ** 3 / (best * 1e-3) / 1e12
+
+
+# ---------------------------------------------------------------------------
+# CPU side: the oracle on a bounded sample (whole level-2 source subtrees)
+# ---------------------------------------------------------------------------
+def cpu_sample_setup(a, pts, w):
+    from oracle import oracle as O
+
+    threads = O.max_threads()
+    op = O.OracleOperator("helmholtz", a.k, a.leaf, a.order)
+    t0 = time.time()
+    op.init(pts, pts)
+    init_s = time.time() - t0
+    # whole subtrees one level below the reference's recursive level (its
+    # parallel unit), one per host thread, evenly spaced over the surface
+    rec = min(op.rec_level() + 1, op.levels() - 1)
+    nb = op.num_boxes(rec)
+    want = a.sample_boxes or threads
+    boxes = np.unique(np.linspace(0, nb - 1, max(1, min(want, nb))).astype(np.int64))
+    ho = op.orders(1)
+    lo = op.orders(0)
+    plo = int(np.prod(lo))
+    cheb = 3 * (plo + lo[1] * lo[2] + lo[2]) * 2
+    wts = np.array([23.0, 25.0, 15 + 6 + cheb + 10, 15 + 6 + cheb + 12])
+    total = float(op.work() @ wts)
+    part = float(op.work(rec, boxes) @ wts)
+    return op, (rec, boxes), total / max(part, 1e-30), threads, init_s, rec, nb
+
+
+def cpu_sample_ms(op, sample, w, threads):
+    """Summed single-thread time of the sampled subtrees spread over all host
+    threads (ideal load balance, which favours the CPU)."""
+    op.mult_sample(w, sample[0], sample[1])
+    return op.last_busy_s * 1e3 / threads
+
+
+# ---------------------------------------------------------------------------
+# arms
+# ---------------------------------------------------------------------------
+def run_reference(a):
+    ws, rank, _ = dist_init()
+    if rank != 0:
+        return
+    pts = W.ellipsoid_points(a.n, seed=0)
+    w = W.densities(a.n, seed=1)
+    op, boxes, scale, threads, init_s, rec, nb = cpu_sample_setup(a, pts, w)
+    for _ in range(a.warmup):
+        cpu_sample_ms(op, boxes, w, threads)
+    samples = [cpu_sample_ms(op, boxes, w, threads) * scale for _ in range(a.steps)]
+    v = float(np.mean(samples))
+    sample = (f"{len(boxes[1])} of {nb} level-{rec} source subtrees per step, scaled to the full "
+              f"matvec by modelled work (x{scale:.1f}); oracle init {init_s:.1f} s untimed")
+    line = {
+        "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": v, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": workload_config(a, "fp64"), "impl": "reference",
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "CPU restatement of the reference mult (oracle/); the reference needs Eigen>=5 "
+                "and oneTBB, absent from this image",
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(a):
+    import torch
+
+    import ifgf_b200 as G
+
+    ws, rank, local = dist_init()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    precision = a.precision or "fp64"
+
+    pts = W.ellipsoid_points(a.n, seed=0)
+    w = W.densities(a.n, seed=1)
+    op = G.HelmholtzIfgfOperator(a.k, a.leaf, a.order)
+    op.set_precision(precision)
+    t0 = time.perf_counter()
+    op.init(pts, pts)
+    torch.cuda.synchronize()
+    init_ms = (time.perf_counter() - t0) * 1e3
+
+    dw = torch.from_numpy(w).to(dev)
+    du = torch.empty_like(dw)
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+
+    for _ in range(a.warmup):
+        op.mult_device(dw.data_ptr(), du.data_ptr(), sp)
+    torch.cuda.synchronize()
+
+    # ---- timed region (device events on the launching stream) ----
+    op.set_profiling(True)
+    clocks = Clocks(local)
+    clocks.start()
+    barrier(ws)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(a.steps):
+        op.mult_device(dw.data_ptr(), du.data_ptr(), sp)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(ws)
+    clk = clocks.stop()
+    ms = max_over_ranks(ws, e0.elapsed_time(e1) / a.steps)
+    stats = op.stats()
+    prof = stats["profile"]
+    op.set_profiling(False)
+
+    # ---- accuracy against the FP64 direct sum (GPU, Kahan) ----
+    u = du.cpu().numpy()
+    idx = W.sample_targets(a.n, 1000, seed=2)
+    d = op.direct_eval(w, idx)
+    err = float(np.linalg.norm(u[idx] - d) / np.linalg.norm(d))
+
+    # ---- end to end through the public API, pinned host buffers ----
+    wp = torch.from_numpy(w).pin_memory()
+    up = torch.empty(a.n, dtype=torch.complex128).pin_memory()
+    wn, un = wp.numpy(), up.numpy()
+    op.mult(wn)
+    torch.cuda.synchronize()
+    ds = torch.cuda.default_stream()
+    barrier(ws)
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(ds)
+    for _ in range(a.steps):
+        un[:] = op.mult(wn)
+    f1.record(ds)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(ws, f0.elapsed_time(f1) / a.steps)
+
+    # ---- roofline of the dominant kernel ----
+    flops = model(stats)
+    kernels = {k: v for k, v in prof.items() if isinstance(v, dict)}
+    dom = max(kernels, key=lambda k: kernels[k]["ms"])
+    per_mult_ms = kernels[dom]["ms"] / max(prof["mults"], 1)
+    peak = measured_peak_tflops(torch.float64 if precision == "fp64" else torch.float32)
+    achieved = flops[dom] / (per_mult_ms * 1e-3) / 1e12
+    roof = {"kernel": dom, "bound": "fp64" if precision == "fp64" else "fp32",
+            "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+            "traffic": None,
+            "peak_source": "measured: cuBLAS GEMM via torch.matmul 8192^3 in this run "
+                           "(MEASURED_PEAKS.json holds only HBM and bf16 figures)",
+            "launches_per_step": kernels[dom]["launches"] / max(prof["mults"], 1),
+            "ms_per_step": per_mult_ms,
+            "model": "survey flop model: transcendental = 1 flop, FMA = 2"}
+    breakdown = {k: v["ms"] / max(prof["mults"], 1) for k, v in kernels.items()}
+
+    line = {
+        "metric": METRIC, "value": ms, "unit": UNIT, "n_gpus": ws, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if precision == "fp64" else "f32+f64",
+        "data": "synthetic", "config": workload_config(a, precision),
+        "rel_err_vs_fp64_direct": err, "tol": TOL, "meets_tol": err <= TOL,
+        "init_ms": init_ms, "kernel_ms_per_step": breakdown,
+        "gpu_launches": int(stats["launches_per_mult"] * a.steps),
+        "e2e": {"value": e2e_ms, "unit": UNIT, "h2d_bytes_per_step": int(w.nbytes),
+                "d2h_bytes_per_step": int(u.nbytes)},
+        "roofline": roof, "clocks": clk,
+        "work": {k: stats[k] for k in ("near_point_pairs", "far_target_evals",
+                                       "leaf_factor_evals", "upward_node_evals",
+                                       "coarse_cones_total", "fine_cones_total")},
+    }
+    if rank == 0 and ws == 1 and not a.no_cpu_baseline:
+        opc, boxes, scale, threads, init_s, rec, nb = cpu_sample_setup(a, pts, w)
+        v = cpu_sample_ms(opc, boxes, w, threads) * scale
+        line["cpu_baseline"] = {
+            "value": v, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{len(boxes[1])} of {nb} level-{rec} source subtrees, scaled by modelled "
+                      f"work (x{scale:.1f})"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)
+
+
+if __name__ == "__main__":
+    main()

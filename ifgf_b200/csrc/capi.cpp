@@ -5,6 +5,7 @@
 #include <cstring>
 #include <exception>
 #include <string>
+#include <vector>
 
 #include "operator.hpp"
 
@@ -125,6 +126,23 @@ extern "C"
         if (!h)
             return null_handle();
         return guarded([&] { h->op.mult_device(d_w, d_u, stream); });
+    }
+
+    int ifgf_direct_eval(ifgf_operator* h, const void* w, const long* tidx, long nt, void* out)
+    {
+        if (!h)
+            return null_handle();
+        return guarded([&] {
+            std::vector<int64_t> t(tidx, tidx + (tidx ? nt : 0));
+            h->op.direct_eval(w, t.data(), nt, out);
+        });
+    }
+
+    int ifgf_set_profiling(ifgf_operator* h, int on)
+    {
+        if (!h)
+            return null_handle();
+        return guarded([&] { h->op.set_profiling(on != 0); });
     }
 
     int ifgf_num_sources(const ifgf_operator* h, long* n)

@@ -103,15 +103,14 @@ struct DeviceState
     DevBuf<double2> w, cvals, fcoef;
     DevBuf<unsigned long long> err;
     DevBuf<double> io_w, io_u; // staging for host-buffer mult
-    cudaEvent_t ev[8] = {};
+    std::vector<cudaEvent_t> prof_ev;
     int n_tleaf = 0;
     size_t c2f_smem = 0;
     int cv_threads = 0;
     ~DeviceState()
     {
-        for (auto& e : ev)
-            if (e)
-                cudaEventDestroy(e);
+        for (auto& e : prof_ev)
+            cudaEventDestroy(e);
     }
 };
 
@@ -1159,36 +1158,119 @@ void Operator::setup_device(const double* normals)
         throw Error(ERR_INVALID, "interpolation order too high for the coarse-to-fine kernel");
     IFGF_CUDA(cudaFuncSetAttribute(coarse_to_fine_kernel,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)D.c2f_smem));
-    for (auto& e : D.ev)
-        if (!e)
-            IFGF_CUDA(cudaEventCreate(&e));
 }
 
+// FP64 direct sum at selected targets: one CTA per target, Kahan-compensated
+// per-thread partial sums, then a pairwise block reduction.
 template <int KIND>
-static void launch_kernels(DeviceState& D, const std::vector<LevelGeom>& lv, const int* lo,
-                           const int* hi, const int* fct, const KParams& kp, bool real,
-                           const void* d_w, void* d_u, cudaStream_t st, bool timed,
-                           StageTimes* times)
+__global__ void __launch_bounds__(256) direct_eval_kernel(SrcArgs S, const double2* __restrict__ w,
+                                                          int ns, const double* __restrict__ tx,
+                                                          const double* __restrict__ ty,
+                                                          const double* __restrict__ tz,
+                                                          const int* __restrict__ tpos,
+                                                          KParams kp, double2* out)
+{
+    using P = Plugin<KIND>;
+    __shared__ double sr[256], si[256];
+    const int j = tpos[blockIdx.x];
+    const double y0 = tx[j], y1 = ty[j], y2 = tz[j];
+    double ar = 0, ai = 0, cr = 0, ci = 0;
+    for (int s = threadIdx.x; s < ns; s += blockDim.x)
+    {
+        const double x[3] = {S.sx[s] - y0, S.sy[s] - y1, S.sz[s] - y2};
+        const double nv[3] = {P::needs_normals ? S.nx[s] : 0.0, P::needs_normals ? S.ny[s] : 0.0,
+                              P::needs_normals ? S.nz[s] : 0.0};
+        const cplx<double> g = P::kernel(x, nv, kp);
+        const double2 wv = w[s];
+        const double vr = wv.x * g.re - wv.y * g.im, vi = wv.x * g.im + wv.y * g.re;
+        double yr = vr - cr, tr = ar + yr;
+        cr = (tr - ar) - yr;
+        ar = tr;
+        double yi = vi - ci, ti = ai + yi;
+        ci = (ti - ai) - yi;
+        ai = ti;
+    }
+    sr[threadIdx.x] = ar;
+    si[threadIdx.x] = ai;
+    __syncthreads();
+    for (int h = blockDim.x / 2; h > 0; h >>= 1)
+    {
+        if (threadIdx.x < h)
+        {
+            sr[threadIdx.x] += sr[threadIdx.x + h];
+            si[threadIdx.x] += si[threadIdx.x + h];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        out[blockIdx.x] = make_double2(sr[0], si[0]);
+}
+
+enum ProfClass
+{
+    PROF_PERMUTE = 0,
+    PROF_COARSE = 1,
+    PROF_C2F = 2,
+    PROF_EVAL = 3
+};
+
+// Records CUDA events around every launch when profiling is on.
+struct LaunchLog
+{
+    DeviceState& D;
+    cudaStream_t st;
+    bool on;
+    std::vector<int> cls;
+    int n = 0;
+    void begin(int c)
+    {
+        if (!on)
+            return;
+        ensure(n + 1);
+        cls.push_back(c);
+        IFGF_CUDA(cudaEventRecord(D.prof_ev[2 * n], st));
+    }
+    void end()
+    {
+        if (!on)
+            return;
+        IFGF_CUDA(cudaEventRecord(D.prof_ev[2 * n + 1], st));
+        n++;
+    }
+    void ensure(int m)
+    {
+        while ((int)D.prof_ev.size() < 2 * m)
+        {
+            cudaEvent_t e;
+            IFGF_CUDA(cudaEventCreate(&e));
+            D.prof_ev.push_back(e);
+        }
+    }
+};
+
+template <int KIND>
+static int launch_kernels(DeviceState& D, const std::vector<LevelGeom>& lv, const int* lo,
+                          const int* hi, const int* fct, const KParams& kp, bool real,
+                          const void* d_w, void* d_u, cudaStream_t st, LaunchLog& log)
 {
     const int L = (int)lv.size();
     const int P_hi = hi[0] * hi[1] * hi[2];
     const int P_lo = lo[0] * lo[1] * lo[2];
     const int64_t ns = (int64_t)D.w.n;
+    int launches = 0;
     TreeArgs TA{D.box_c.p, D.box_H.p, D.box_first.p, D.box_last.p, D.box_child.p, D.box_level.p,
                 D.box_leaf.p};
     SrcArgs SA{D.sx.p, D.sy.p, D.sz.p, D.nx.p, D.ny.p, D.nz.p};
-    if (timed)
-        IFGF_CUDA(cudaEventRecord(D.ev[0], st));
     {
         const int thr = 256;
         const int blocks = (int)std::min<int64_t>((ns + thr - 1) / thr, 148 * 16);
+        log.begin(PROF_PERMUTE);
         permute_weights_kernel<<<blocks, thr, 0, st>>>((const double*)d_w, real ? 1 : 0,
                                                        D.src_perm.p, D.w.p, ns);
         IFGF_CUDA(cudaGetLastError());
+        log.end();
+        launches++;
     }
-    if (timed)
-        IFGF_CUDA(cudaEventRecord(D.ev[1], st));
-    float t_cv = 0, t_c2f = 0;
     for (int l = L - 1; l >= 0; l--)
     {
         const LevelGeom& G = lv[l];
@@ -1214,8 +1296,10 @@ static void launch_kernels(DeviceState& D, const std::vector<LevelGeom>& lv, con
         ca.kp = kp;
         const int thr = D.cv_threads;
         const size_t smem = (size_t)8 * thr * sizeof(double);
+        log.begin(PROF_COARSE);
         coarse_values_kernel<KIND><<<(unsigned)G.n_coarse, thr, smem, st>>>(ca);
         IFGF_CUDA(cudaGetLastError());
+        log.end();
         C2FArgs fa;
         fa.G = G;
         fa.cc_box = D.cc_box[l].p;
@@ -1232,11 +1316,12 @@ static void launch_kernels(DeviceState& D, const std::vector<LevelGeom>& lv, con
         }
         fa.P_hi = P_hi;
         fa.P_lo = P_lo;
+        log.begin(PROF_C2F);
         coarse_to_fine_kernel<<<(unsigned)G.n_coarse, 256, D.c2f_smem, st>>>(fa);
         IFGF_CUDA(cudaGetLastError());
+        log.end();
+        launches += 2;
     }
-    if (timed)
-        IFGF_CUDA(cudaEventRecord(D.ev[2], st));
     EvalArgs ea;
     ea.lv = D.lv.p;
     ea.T = TA;
@@ -1263,26 +1348,35 @@ static void launch_kernels(DeviceState& D, const std::vector<LevelGeom>& lv, con
     ea.kp = kp;
     if (D.n_tleaf > 0)
     {
+        log.begin(PROF_EVAL);
         target_eval_kernel<KIND><<<D.n_tleaf, EVAL_THREADS, 0, st>>>(ea);
         IFGF_CUDA(cudaGetLastError());
+        log.end();
+        launches++;
     }
-    if (timed)
-    {
-        IFGF_CUDA(cudaEventRecord(D.ev[3], st));
-        IFGF_CUDA(cudaEventSynchronize(D.ev[3]));
-        float a = 0, b = 0, c = 0;
-        IFGF_CUDA(cudaEventElapsedTime(&a, D.ev[0], D.ev[1]));
-        IFGF_CUDA(cudaEventElapsedTime(&b, D.ev[1], D.ev[2]));
-        IFGF_CUDA(cudaEventElapsedTime(&c, D.ev[2], D.ev[3]));
-        times->permute = a;
-        times->coarse = b;
-        times->c2f = 0;
-        times->eval = c;
-        times->total = a + b + c;
-    }
-    (void)t_cv;
-    (void)t_c2f;
+    return launches;
 }
+
+template <int KIND>
+static void launch_direct(DeviceState& D, const KParams& kp, const int* d_tpos, int nt,
+                          double2* d_out)
+{
+    SrcArgs SA{D.sx.p, D.sy.p, D.sz.p, D.nx.p, D.ny.p, D.nz.p};
+    direct_eval_kernel<KIND><<<nt, 256>>>(SA, D.w.p, (int)D.w.n, D.tx.p, D.ty.p, D.tz.p, d_tpos,
+                                          kp, d_out);
+    IFGF_CUDA(cudaGetLastError());
+}
+
+#define IFGF_DISPATCH(KINDVAR, CALL)                                                          \
+    switch (KINDVAR)                                                                           \
+    {                                                                                          \
+    case K_LAPLACE: { constexpr int KK = K_LAPLACE; CALL; } break;                            \
+    case K_HELMHOLTZ: { constexpr int KK = K_HELMHOLTZ; CALL; } break;                        \
+    case K_MODHELMHOLTZ: { constexpr int KK = K_MODHELMHOLTZ; CALL; } break;                  \
+    case K_GRADHELMHOLTZ: { constexpr int KK = K_GRADHELMHOLTZ; CALL; } break;                \
+    case K_DOUBLELAYER: { constexpr int KK = K_DOUBLELAYER; CALL; } break;                    \
+    case K_COMBINEDFIELD: { constexpr int KK = K_COMBINEDFIELD; CALL; } break;                \
+    }
 
 void Operator::launch_mult(const void* d_w, void* d_u, void* stream, bool timed)
 {
@@ -1292,27 +1386,48 @@ void Operator::launch_mult(const void* d_w, void* d_u, void* stream, bool timed)
         throw Error(ERR_INVALID, "null density or result buffer");
     const KParams kp{kr_, ki_, dx_};
     cudaStream_t st = (cudaStream_t)stream;
-    switch (kind_)
+    DeviceState& D = *dev_;
+    LaunchLog log{D, st, profiling_ || timed};
+    int launches = 0;
+    IFGF_DISPATCH(kind_, launches = launch_kernels<KK>(D, lv_, lo_, hi_, fct_, kp, is_real(), d_w,
+                                                        d_u, st, log));
+    launches_per_mult_ = launches;
+    if (log.on && log.n > 0)
     {
-    case K_LAPLACE:
-        launch_kernels<K_LAPLACE>(*dev_, lv_, lo_, hi_, fct_, kp, true, d_w, d_u, st, timed, &last_);
-        break;
-    case K_HELMHOLTZ:
-        launch_kernels<K_HELMHOLTZ>(*dev_, lv_, lo_, hi_, fct_, kp, false, d_w, d_u, st, timed, &last_);
-        break;
-    case K_MODHELMHOLTZ:
-        launch_kernels<K_MODHELMHOLTZ>(*dev_, lv_, lo_, hi_, fct_, kp, false, d_w, d_u, st, timed, &last_);
-        break;
-    case K_GRADHELMHOLTZ:
-        launch_kernels<K_GRADHELMHOLTZ>(*dev_, lv_, lo_, hi_, fct_, kp, false, d_w, d_u, st, timed, &last_);
-        break;
-    case K_DOUBLELAYER:
-        launch_kernels<K_DOUBLELAYER>(*dev_, lv_, lo_, hi_, fct_, kp, false, d_w, d_u, st, timed, &last_);
-        break;
-    case K_COMBINEDFIELD:
-        launch_kernels<K_COMBINEDFIELD>(*dev_, lv_, lo_, hi_, fct_, kp, false, d_w, d_u, st, timed, &last_);
-        break;
+        IFGF_CUDA(cudaEventSynchronize(D.prof_ev[2 * log.n - 1]));
+        double cls_ms[NPROF] = {0, 0, 0, 0};
+        for (int i = 0; i < log.n; i++)
+        {
+            float ms = 0;
+            IFGF_CUDA(cudaEventElapsedTime(&ms, D.prof_ev[2 * i], D.prof_ev[2 * i + 1]));
+            cls_ms[log.cls[i]] += ms;
+            if (profiling_)
+            {
+                prof_ms_[log.cls[i]] += ms;
+                prof_launches_[log.cls[i]]++;
+            }
+        }
+        float tot = 0;
+        IFGF_CUDA(cudaEventElapsedTime(&tot, D.prof_ev[0], D.prof_ev[2 * log.n - 1]));
+        if (profiling_)
+            mults_profiled_++;
+        last_.permute = cls_ms[PROF_PERMUTE];
+        last_.coarse = cls_ms[PROF_COARSE];
+        last_.c2f = cls_ms[PROF_C2F];
+        last_.eval = cls_ms[PROF_EVAL];
+        last_.total = tot;
     }
+}
+
+void Operator::set_profiling(bool on)
+{
+    profiling_ = on;
+    for (int i = 0; i < NPROF; i++)
+    {
+        prof_launches_[i] = 0;
+        prof_ms_[i] = 0;
+    }
+    mults_profiled_ = 0;
 }
 
 void Operator::mult_device(const void* d_w, void* d_u, void* stream)
@@ -1345,6 +1460,61 @@ void Operator::mult_host(const void* w, void* u, int64_t batch)
     }
     IFGF_CUDA(cudaMemcpy(&missing_, D.err.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost));
 }
+
+void Operator::direct_eval(const void* w, const int64_t* tidx, int64_t nt, void* out)
+{
+    if (!initialized_)
+        throw Error(ERR_STATE, "direct_eval called before init");
+    if (!w || !out || (nt > 0 && !tidx))
+        throw Error(ERR_INVALID, "null buffer");
+    if (nt <= 0)
+        return;
+    DeviceState& D = *dev_;
+    // sorted position of each requested original target index
+    const auto& perm = plan_.tgt.perm;
+    std::vector<int64_t> inv(perm.size());
+    for (size_t i = 0; i < perm.size(); i++)
+        inv[perm[i]] = (int64_t)i;
+    std::vector<int> pos(nt);
+    for (int64_t q = 0; q < nt; q++)
+    {
+        if (tidx[q] < 0 || tidx[q] >= (int64_t)perm.size())
+            throw Error(ERR_INVALID, "target index out of range");
+        pos[q] = (int)inv[tidx[q]];
+    }
+    const size_t per = is_real() ? 1 : 2;
+    const size_t nw = per * (size_t)n_src();
+    if (D.io_w.n < nw)
+        D.io_w.alloc(nw);
+    IFGF_CUDA(cudaMemcpy(D.io_w.p, w, nw * sizeof(double), cudaMemcpyHostToDevice));
+    {
+        const int64_t ns = (int64_t)D.w.n;
+        const int thr = 256;
+        const int blocks = (int)std::min<int64_t>((ns + thr - 1) / thr, 148 * 16);
+        permute_weights_kernel<<<blocks, thr>>>(D.io_w.p, is_real() ? 1 : 0, D.src_perm.p, D.w.p, ns);
+        IFGF_CUDA(cudaGetLastError());
+    }
+    DevBuf<int> dpos;
+    dpos.upload(pos);
+    DevBuf<double2> dout;
+    dout.alloc(nt);
+    const KParams kp{kr_, ki_, dx_};
+    IFGF_DISPATCH(kind_, launch_direct<KK>(D, kp, dpos.p, (int)nt, dout.p));
+    std::vector<double2> h(nt);
+    IFGF_CUDA(cudaMemcpy(h.data(), dout.p, nt * sizeof(double2), cudaMemcpyDeviceToHost));
+    double* o = (double*)out;
+    for (int64_t q = 0; q < nt; q++)
+    {
+        if (is_real())
+            o[q] = h[q].x;
+        else
+        {
+            o[2 * q] = h[q].x;
+            o[2 * q + 1] = h[q].y;
+        }
+    }
+}
+
 
 void Operator::level_grid(int level, int step, int64_t* n) const
 {
@@ -1403,9 +1573,15 @@ std::string Operator::stats_json() const
       << ",\"leaf_factor_evals\":" << leaf_evals_ << ",\"upward_node_evals\":" << upward_evals_
       << ",\"coarse_cones_total\":" << n_coarse_total_ << ",\"fine_cones_total\":" << n_fine_total_
       << ",\"target_leaves\":" << dev_->n_tleaf << ",\"missing_cone_lookups\":" << missing_
-      << ",\"init_ms\":" << init_ms_ << ",\"last_mult_ms\":{\"permute\":" << last_.permute
-      << ",\"coarse_and_c2f\":" << last_.coarse << ",\"eval\":" << last_.eval
-      << ",\"total\":" << last_.total << "}}";
+      << ",\"init_ms\":" << init_ms_ << ",\"launches_per_mult\":" << launches_per_mult_
+      << ",\"last_mult_ms\":{\"permute\":" << last_.permute << ",\"coarse_values\":" << last_.coarse
+      << ",\"coarse_to_fine\":" << last_.c2f << ",\"target_eval\":" << last_.eval
+      << ",\"total\":" << last_.total << "},\"profile\":{\"mults\":" << mults_profiled_;
+    const char* names[NPROF] = {"permute", "coarse_values", "coarse_to_fine", "target_eval"};
+    for (int i = 0; i < NPROF; i++)
+        o << ",\"" << names[i] << "\":{\"launches\":" << prof_launches_[i] << ",\"ms\":" << prof_ms_[i]
+          << "}";
+    o << "}}";
     return o.str();
 }
 

@@ -39,6 +39,9 @@ class Operator
     void mult_device(const void* d_w, void* d_u, void* stream);
     // host buffers, `batch` right-hand sides
     void mult_host(const void* w, void* u, int64_t batch);
+    // FP64 direct sum at selected targets (original indices), host buffers
+    void direct_eval(const void* w, const int64_t* tidx, int64_t nt, void* out);
+    void set_profiling(bool on);
 
     int kind() const { return kind_; }
     bool is_real() const { return kind_ == K_LAPLACE; }
@@ -81,6 +84,13 @@ class Operator
     int64_t n_coarse_total_ = 0, n_fine_total_ = 0;
     double leaf_evals_ = 0, upward_evals_ = 0;
     unsigned long long missing_ = 0;
+    bool profiling_ = false;
+    // per kernel class: launches and accumulated milliseconds
+    static constexpr int NPROF = 4; // permute, coarse_values, coarse_to_fine, target_eval
+    int64_t prof_launches_[NPROF] = {0, 0, 0, 0};
+    double prof_ms_[NPROF] = {0, 0, 0, 0};
+    int64_t mults_profiled_ = 0;
+    int launches_per_mult_ = 0;
 };
 
 } // namespace ifgf

@@ -130,6 +130,19 @@ class IfgfOperator:
         check(lib.ifgf_mult_device(self._h, C.c_void_p(w_ptr), C.c_void_p(u_ptr),
                                    C.c_void_p(stream_ptr)))
 
+    def direct_eval(self, weights, targets):
+        """FP64 dense direct sum at the given target indices (on the GPU)."""
+        w = np.ascontiguousarray(np.asarray(weights, dtype=self._dtype()))
+        t = np.ascontiguousarray(np.asarray(targets, dtype=np.int64))
+        out = np.empty(len(t), dtype=self._dtype())
+        check(lib.ifgf_direct_eval(self._h, w.ctypes.data, t.ctypes.data_as(C.POINTER(C.c_long)),
+                                   len(t), out.ctypes.data))
+        return out
+
+    def set_profiling(self, on=True):
+        """Per-kernel CUDA-event timing of following mults (see stats()["profile"])."""
+        check(lib.ifgf_set_profiling(self._h, 1 if on else 0))
+
     # -- introspection -------------------------------------------------------
     @property
     def n_src(self):

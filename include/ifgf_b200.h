@@ -100,6 +100,17 @@ int ifgf_mult_batch(ifgf_operator* op, const void* w, void* u, long batch);
  * enqueueing.  No reference counterpart. */
 int ifgf_mult_device(ifgf_operator* op, const void* d_w, void* d_u, void* stream);
 
+/* FP64 dense direct sum u(y_t) = sum_s w_s G(x_s - y_t) on the GPU at the
+ * targets listed in tidx (caller's target indices), for error estimates:
+ * w as in ifgf_mult (host buffer), out receives nt values.  The reference
+ * checks its mult the same way on the host (test/test_ifgf.cpp:143-165). */
+int ifgf_direct_eval(ifgf_operator* op, const void* w, const long* tidx, long nt, void* out);
+
+/* Per-kernel CUDA-event timing of every following mult (on the stream the
+ * kernels run on); on != 0 enables and resets the counters.  Results appear
+ * under "profile" in ifgf_stats_json.  No reference counterpart. */
+int ifgf_set_profiling(ifgf_operator* op, int on);
+
 int ifgf_num_sources(const ifgf_operator* op, long* n);
 int ifgf_num_targets(const ifgf_operator* op, long* n);
 

@@ -1350,6 +1350,73 @@ struct Operator
         return contrib;
     }
 
+    // Modelled work of one source subtree (units of the survey's flop model):
+    // near point pairs, leaf factor evaluations, far target evaluations,
+    // upward node evaluations.
+    void subtree_work(int level, long id, double* wk) const
+    {
+        const Node& nd = src.nodes[level][id];
+        int ho[3];
+        order_of(1, ho);
+        const double P = (double)ho[0] * ho[1] * ho[2];
+        const double ns = (double)(nd.rng.second - nd.rng.first);
+        for (const Range& r : nd.near)
+            wk[0] += ns * (double)(r.second - r.first);
+        for (const Range& r : nd.far)
+            wk[2] += (double)(r.second - r.first);
+        if (nd.leaf)
+            wk[1] += (double)nd.cone[1].active.size() * P * ns;
+        else
+        {
+            int nch = 0;
+            for (int c = 0; c < 8; c++)
+                if (nd.child[c] >= 0)
+                {
+                    nch++;
+                    subtree_work(level + 1, nd.child[c], wk);
+                }
+            wk[3] += (double)nd.cone[1].active.size() * P * nch;
+        }
+    }
+
+    // recursive_mult over a subset of the recursive-level boxes only: a
+    // bounded sample of the matvec for CPU timing (results are partial).
+    // Returns the summed single-thread seconds of the sampled subtrees.
+    double mult_sample(const cd* w_in, int level, const long* boxes, long nb, cd* out) const
+    {
+        double busy = 0;
+        std::vector<cd> w(n_src);
+        for (size_t i = 0; i < n_src; i++)
+            w[i] = w_in[src.perm[i]];
+        int nth = 1;
+#ifdef _OPENMP
+        nth = omp_get_max_threads();
+#endif
+        std::vector<std::vector<cd>> local(nth, std::vector<cd>(n_tgt, cd(0)));
+        // whole subtrees are the parallel unit, as in the reference's TBB loop
+        // (ifgfoperator.hpp:330-340); nested children run serially
+#pragma omp parallel for schedule(dynamic, 1) reduction(+ : busy)
+        for (long q = 0; q < nb; q++)
+        {
+            int t = 0;
+#ifdef _OPENMP
+            t = omp_get_thread_num();
+            const double t0 = omp_get_wtime();
+#endif
+            recursive_mult(boxes[q], level, w.data(), local[t].data());
+#ifdef _OPENMP
+            busy += omp_get_wtime() - t0;
+#endif
+        }
+        std::vector<cd> result(n_tgt, cd(0));
+        for (int t = 0; t < nth; t++)
+            for (size_t j = 0; j < n_tgt; j++)
+                result[j] += local[t][j];
+        for (size_t i = 0; i < n_tgt; i++)
+            out[tgt.perm[i]] = result[i];
+        return busy;
+    }
+
     // IfgfOperator::mult (ifgfoperator.hpp:246-867)
     void mult(const cd* w_in, cd* out) const
     {
@@ -1530,6 +1597,35 @@ extern "C"
         auto* op = (orc::Operator*)h;
         op->mult((const cd*)w, (cd*)out);
         return 0;
+    }
+    // bounded sample: recursive_mult over the listed recursive-level boxes
+    // returns the summed single-thread seconds of the sampled subtrees (< 0 on bad level)
+    double oracle_mult_sample(void* h, const double* w, int level, const long* boxes, long nb,
+                              double* out)
+    {
+        auto* op = (orc::Operator*)h;
+        if (level < op->rec_level || level >= op->src.levels())
+            return -1;
+        return op->mult_sample((const cd*)w, level, boxes, nb, (cd*)out);
+    }
+    // modelled work of the subtrees of the listed boxes of `level` (nb < 0:
+    // every recursive-level box): out[4] = near pairs, leaf evals, far evals,
+    // upward evals
+    void oracle_work(void* h, int level, const long* boxes, long nb, double* out)
+    {
+        auto* op = (orc::Operator*)h;
+        for (int i = 0; i < 4; i++)
+            out[i] = 0;
+        if (op->rec_level >= op->src.levels())
+            return;
+        if (nb < 0)
+        {
+            for (long b = 0; b < (long)op->src.num_boxes(op->rec_level); b++)
+                op->subtree_work(op->rec_level, b, out);
+            return;
+        }
+        for (long q = 0; q < nb; q++)
+            op->subtree_work(level, boxes[q], out);
     }
     int oracle_levels(void* h, int which)
     {

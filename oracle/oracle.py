@@ -45,6 +45,10 @@ def lib():
         L.oracle_set_threads.argtypes = [C.c_int]
         L.oracle_init.argtypes = [C.c_void_p, _dp, C.c_long, _dp, C.c_long, _dp]
         L.oracle_mult.argtypes = [C.c_void_p, _dp, _dp]
+        L.oracle_mult_sample.argtypes = [C.c_void_p, _dp, C.c_int, _lp, C.c_long, _dp]
+        L.oracle_mult_sample.restype = C.c_double
+        L.oracle_work.argtypes = [C.c_void_p, C.c_int, _lp, C.c_long, _dp]
+        L.oracle_max_threads.restype = C.c_int
         L.oracle_levels.argtypes = [C.c_void_p, C.c_int]
         L.oracle_num_boxes.restype = C.c_long
         L.oracle_num_boxes.argtypes = [C.c_void_p, C.c_int, C.c_int]
@@ -118,6 +122,31 @@ class OracleOperator:
         out = np.zeros(self.n_tgt, dtype=np.complex128)
         lib().oracle_mult(self.h, _p(w.view(np.float64)), _p(out.view(np.float64)))
         return out.real.copy() if self.kind == 0 else out
+
+    def mult_sample(self, w, level, boxes):
+        """recursive_mult over the subtrees of the given source boxes of
+        `level` (>= the recursive level) only: a bounded sample of the
+        matvec, one subtree per thread; the result is partial."""
+        w = np.ascontiguousarray(np.asarray(w, dtype=np.complex128))
+        b = np.ascontiguousarray(np.asarray(boxes, dtype=np.int64))
+        out = np.zeros(self.n_tgt, dtype=np.complex128)
+        busy = lib().oracle_mult_sample(self.h, _p(w.view(np.float64)), int(level), _p(b, _lp),
+                                        len(b), _p(out.view(np.float64)))
+        if busy < 0:
+            raise ValueError("sample level must be >= the recursive level")
+        self.last_busy_s = busy  # summed single-thread seconds of the sampled subtrees
+        return out
+
+    def work(self, level=None, boxes=None):
+        """Modelled work [near pairs, leaf evals, far evals, upward evals] of
+        the subtrees of the given boxes of `level` (None: the whole tree)."""
+        out = np.zeros(4)
+        if boxes is None:
+            lib().oracle_work(self.h, 0, None, -1, _p(out))
+        else:
+            b = np.ascontiguousarray(np.asarray(boxes, dtype=np.int64))
+            lib().oracle_work(self.h, int(level), _p(b, _lp), len(b), _p(out))
+        return out
 
     # ---- table dumps -------------------------------------------------
     def levels(self, which=0):
