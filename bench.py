@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--sample-boxes", type=int, default=0,
                     help="source subtrees in the CPU sample (0: one per host thread)")
+    ap.add_argument("--sample-depth", type=int, default=2,
+                    help="levels below the recursive level of the sampled subtrees")
     return ap.parse_args()
 
 
@@ -209,9 +211,9 @@ def cpu_sample_setup(a, pts, w):
     t0 = time.time()
     op.init(pts, pts)
     init_s = time.time() - t0
-    # whole subtrees one level below the reference's recursive level (its
+    # whole subtrees two levels below the reference's recursive level (its
     # parallel unit), one per host thread, evenly spaced over the surface
-    rec = min(op.rec_level() + 1, op.levels() - 1)
+    rec = min(op.rec_level() + a.sample_depth, op.levels() - 1)
     nb = op.num_boxes(rec)
     want = a.sample_boxes or threads
     boxes = np.unique(np.linspace(0, nb - 1, max(1, min(want, nb))).astype(np.int64))
