@@ -18,7 +18,7 @@ NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I", CSRC, "-I", INCLUDE]
 
-SOURCES = ["operator.cu", "plan.cpp", "capi.cpp"]
+SOURCES = ["operator.cu", "plan.cpp", "capi.cpp", "noalloc.cu"]
 HEADERS = ["common.hpp", "plan.hpp", "operator.hpp", "device_math.cuh"]
 
 

@@ -9,6 +9,11 @@
 
 #include "operator.hpp"
 
+namespace ifgf
+{
+void* noalloc_scratch(size_t* bytes); // noalloc.cu
+}
+
 struct ifgf_operator
 {
     ifgf::Operator op;
@@ -143,6 +148,17 @@ extern "C"
         if (!h)
             return null_handle();
         return guarded([&] { h->op.set_profiling(on != 0); });
+    }
+
+    int ifgf_mult_device_noalloc(ifgf_operator* h, const void* d_w, void* d_u, void* stream)
+    {
+        if (!h)
+            return null_handle();
+        return guarded([&] {
+            size_t bytes = 0;
+            void* scratch = ifgf::noalloc_scratch(&bytes);
+            h->op.mult_device_external_scratch(d_w, d_u, stream, scratch, bytes);
+        });
     }
 
     int ifgf_num_sources(const ifgf_operator* h, long* n)

@@ -1461,6 +1461,52 @@ void Operator::mult_host(const void* w, void* u, int64_t batch)
     IFGF_CUDA(cudaMemcpy(&missing_, D.err.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost));
 }
 
+void Operator::mult_device_external_scratch(const void* d_w, void* d_u, void* stream,
+                                            void* scratch, size_t scratch_bytes)
+{
+    if (!initialized_)
+        throw Error(ERR_STATE, "mult called before init");
+    if (!d_w || !d_u || !scratch)
+        throw Error(ERR_INVALID, "null density, result or scratch buffer");
+    DeviceState& D = *dev_;
+    auto up = [](size_t b) { return (b + 255) / 256 * 256; };
+    const size_t bw = up(D.w.n * sizeof(double2)), bc = up(D.cvals.n * sizeof(double2)),
+                 bf = up(D.fcoef.n * sizeof(double2));
+    const size_t need = bw + bc + bf;
+    if (need > scratch_bytes)
+        throw Error(ERR_INVALID, "this operator needs " + std::to_string(need) +
+                                     " bytes of matvec scratch; the fixed no-allocation scratch "
+                                     "holds " + std::to_string(scratch_bytes) +
+                                     " bytes (use ifgf_mult_device for larger problems)");
+    unsigned char* base = static_cast<unsigned char*>(scratch);
+    double2* w = reinterpret_cast<double2*>(base);
+    double2* cv = reinterpret_cast<double2*>(base + bw);
+    double2* fc = reinterpret_cast<double2*>(base + bw + bc);
+    cudaStream_t st = (cudaStream_t)stream;
+    // fine cones without an active coarse parent must read as zero; the
+    // shared scratch still holds the previous call's coefficients
+    IFGF_CUDA(cudaMemsetAsync(fc, 0, D.fcoef.n * sizeof(double2), st));
+    // point the operator's scratch buffers at the caller's region for this
+    // call only (sizes unchanged), restoring them on every exit path
+    struct Redirect
+    {
+        DeviceState& D;
+        double2 *w, *cv, *fc;
+        ~Redirect()
+        {
+            D.w.p = w;
+            D.cvals.p = cv;
+            D.fcoef.p = fc;
+        }
+    } restore{D, D.w.p, D.cvals.p, D.fcoef.p};
+    D.w.p = w;
+    D.cvals.p = cv;
+    D.fcoef.p = fc;
+    const KParams kp{kr_, ki_, dx_};
+    LaunchLog log{D, st, false}; // no events: this path creates no resources
+    IFGF_DISPATCH(kind_, launch_kernels<KK>(D, lv_, lo_, hi_, fct_, kp, is_real(), d_w, d_u, st, log));
+}
+
 void Operator::direct_eval(const void* w, const int64_t* tidx, int64_t nt, void* out)
 {
     if (!initialized_)

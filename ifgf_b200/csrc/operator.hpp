@@ -39,6 +39,10 @@ class Operator
     void mult_device(const void* d_w, void* d_u, void* stream);
     // host buffers, `batch` right-hand sides
     void mult_host(const void* w, void* u, int64_t batch);
+    // mult_device with its scratch in a caller-provided device region instead
+    // of the buffers allocated at init; allocates nothing
+    void mult_device_external_scratch(const void* d_w, void* d_u, void* stream, void* scratch,
+                                      size_t scratch_bytes);
     // FP64 direct sum at selected targets (original indices), host buffers
     void direct_eval(const void* w, const int64_t* tidx, int64_t nt, void* out);
     void set_profiling(bool on);

@@ -100,6 +100,18 @@ int ifgf_mult_batch(ifgf_operator* op, const void* w, void* u, long batch);
  * enqueueing.  No reference counterpart. */
 int ifgf_mult_device(ifgf_operator* op, const void* d_w, void* d_u, void* stream);
 
+/* ifgf_mult_device for callers that cannot allocate device memory while they
+ * apply the operator -- e.g. code inside a stream capture, or an application
+ * whose memory pool owns the whole GPU.  This call allocates and frees
+ * nothing: its per-call scratch lives in a fixed 64 MiB device array that the
+ * library holds on every GPU that loads it, instead of the buffers init
+ * allocated.  Operators whose matvec scratch exceeds 64 MiB are rejected with
+ * IFGF_ERR_INVALID_ARG (use ifgf_mult_device for them).  The first call on a
+ * device looks up the array's device address; make that first call before
+ * any stream capture.  All calls share the one array, so calls whose GPU work
+ * overlaps race and must be serialised.  No reference counterpart. */
+int ifgf_mult_device_noalloc(ifgf_operator* op, const void* d_w, void* d_u, void* stream);
+
 /* FP64 dense direct sum u(y_t) = sum_s w_s G(x_s - y_t) on the GPU at the
  * targets listed in tidx (caller's target indices), for error estimates:
  * w as in ifgf_mult (host buffer), out receives nt values.  The reference
