@@ -18,8 +18,10 @@ NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I", CSRC, "-I", INCLUDE]
 
-SOURCES = ["operator.cu", "plan.cpp", "capi.cpp", "noalloc.cu"]
-HEADERS = ["common.hpp", "plan.hpp", "operator.hpp", "device_math.cuh"]
+SOURCES = ["operator.cu", "plan.cpp", "capi.cpp", "noalloc.cu"] + [
+    f"kernels_k{k}.cu" for k in range(6)]
+HEADERS = ["common.hpp", "plan.hpp", "operator.hpp", "device_math.cuh", "mult.hpp",
+           "mult_kernels.cuh"]
 
 
 def _newer(target, deps):
@@ -32,20 +34,30 @@ def _newer(target, deps):
 def build(force: bool = False, verbose: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
     headers = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(INCLUDE, "ifgf_b200.h")]
-    objs = []
+    objs, cmds = [], []
     for src in SOURCES:
         path = os.path.join(CSRC, src)
         obj = os.path.join(BUILD, src + ".o")
         objs.append(obj)
         if force or _newer(obj, [path, *headers]):
             cmd = [NVCC, *ARCH, *COMMON, "-c", path, "-o", obj]
-            if src.endswith(".cu"):
-                cmd += ["-Xptxas", "-v"] if verbose else []
-            else:
-                cmd += ["-x", "cu"] if False else []
-            if verbose:
-                print(" ".join(cmd), flush=True)
-            subprocess.run(cmd, check=True)
+            if verbose and src.endswith(".cu"):
+                cmd += ["-Xptxas", "-v"]
+            cmds.append(cmd)
+    # translation units compile in parallel (one per kernel plug-in)
+    from concurrent.futures import ThreadPoolExecutor
+
+    def run(cmd):
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        return subprocess.run(cmd, capture_output=not verbose)
+
+    with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as ex:
+        for cmd, r in zip(cmds, ex.map(run, cmds)):
+            if r.returncode != 0:
+                if not verbose:
+                    sys.stderr.write(r.stdout.decode() + r.stderr.decode())
+                raise subprocess.CalledProcessError(r.returncode, cmd)
     if force or _newer(LIB, objs):
         cmd = [NVCC, *ARCH, "-shared", "-cudart", "static", "-o", LIB, *objs]
         if verbose:

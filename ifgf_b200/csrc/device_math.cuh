@@ -42,7 +42,22 @@ struct KParams
 {
     double kr, ki; // k = kr + i ki (real kernels use kr)
     int dx;        // GradHelmholtz derivative direction, -1 = plain single layer
+    // kr and ki split into two floats each (hi + lo), for the mixed pipeline
+    float krh, krl, kih, kil;
 };
+
+inline KParams make_kparams(double kr, double ki, int dx)
+{
+    KParams p;
+    p.kr = kr;
+    p.ki = ki;
+    p.dx = dx;
+    p.krh = (float)kr;
+    p.krl = (float)(kr - (double)p.krh);
+    p.kih = (float)ki;
+    p.kil = (float)(ki - (double)p.kih);
+    return p;
+}
 
 // e^{-k d} for complex k: e^{-kr d} (cos(ki d), -sin(ki d))
 __device__ __forceinline__ cplx<double> exp_mk(const KParams& p, double d)
@@ -427,5 +442,303 @@ template <> struct Plugin<K_COMBINEDFIELD>
         return {f * (A * nxy + B * kap * (d * nxy + d2)), f * (-A * kap * (d * nxy + d2) + B * nxy)};
     }
 };
+
+// ===========================================================================
+// Mixed precision: FP32 arithmetic on coordinates relative to a nearby box
+// centre, with the phase k*r formed and reduced modulo 2 pi in FP64 and the
+// reduced angle (|r| <= pi) fed to the FP32 sine/cosine unit.
+// ===========================================================================
+constexpr float INV4PIF = (float)INV4PI;
+
+// (cos(k r), sin(k r)) with k r and its reduction in FP64
+__device__ __forceinline__ cplx<float> phase_sc(double k, double r)
+{
+    const double th = k * r;
+    const double n = rint(th * (1.0 / (2.0 * DPI)));
+    const float red = (float)fma(-n, 2.0 * DPI, th);
+    float s, c;
+    __sincosf(red, &s, &c);
+    return {c, s};
+}
+
+// (cos(k r), sin(k r)) for an FP32 distance r, with k r formed and reduced
+// modulo 2 pi in double-float arithmetic: k = kh + kl (two floats, made on the
+// host), the product k r as an unevaluated float pair (exact through FMA) and
+// 2 pi as a three-float sum (Cody-Waite), so the reduced angle carries the
+// accuracy of an FP64 reduction without leaving the FP32 pipes.
+__device__ __forceinline__ cplx<float> phase_sc_ff(float kh, float kl, float r)
+{
+    const float th = kh * r;
+    const float tl = fmaf(kh, r, -th) + kl * r;
+    constexpr float C1 = 6.2831854820251465f;      // float(2 pi)
+    constexpr float C2 = -1.7484555314695172e-07f; // float(2 pi - C1)
+    constexpr float C3 = -6.8604980400235275e-15f; // float(2 pi - C1 - C2)
+    const float n = rintf(th * 0.15915493667125702f);
+    float red = fmaf(-n, C1, th);
+    red = fmaf(-n, C2, red);
+    red = fmaf(-n, C3, red) + tl;
+    float s, c;
+    __sincosf(red, &s, &c);
+    return {c, s};
+}
+
+// e^{-k r} for complex k (FP64 distance): e^{-kr r} (cos(ki r), -sin(ki r))
+__device__ __forceinline__ cplx<float> exp_mk_f(const KParams& p, double r)
+{
+    const cplx<float> e = phase_sc(-p.ki, r);
+    const float m = __expf((float)(-p.kr * r));
+    return {m * e.re, m * e.im};
+}
+__device__ __forceinline__ cplx<float> exp_ik_f(double k, double r) { return phase_sc(k, r); }
+
+// the same for an FP32 distance (double-float phase)
+__device__ __forceinline__ cplx<float> exp_ik_ff(const KParams& p, float r)
+{
+    return phase_sc_ff(p.krh, p.krl, r);
+}
+__device__ __forceinline__ cplx<float> exp_mk_ff(const KParams& p, float r)
+{
+    const cplx<float> e = phase_sc_ff(-p.kih, -p.kil, r);
+    const float m = __expf(-p.krh * r);
+    return {m * e.re, m * e.im};
+}
+
+template <typename R> __device__ __forceinline__ void cfmaf(cplx<R>& acc, cplx<R> a, cplx<R> b)
+{
+    acc.re = fmaf(a.re, b.re, fmaf(-a.im, b.im, acc.re));
+    acc.im = fmaf(a.re, b.im, fmaf(a.im, b.re, acc.im));
+}
+
+template <int KIND> struct PluginF;
+
+// Near field: kernel(x, n) with x = x_src - y_tgt in FP32.  Kernels with
+// normals take x and n in FP64 (kernel_d): for neighbouring points of a
+// surface x.n is O(|x|^2) and would cancel in FP32, so x.n and |x|^2 are
+// formed in FP64 and only the rest in FP32.
+//
+// Leaf sampling: factored(a, aa, b, n, w, dc) = w G(y, x)/G(y, xc) with
+// a = x - xc, aa = |a|^2, b = y - xc (FP32) and dc = |b|; the difference
+// d - dc is formed as (aa - 2 a.b) / (d + dc), free of cancellation.
+__device__ __forceinline__ void factored_geom(const float* a, float aa, const float* b, float dc,
+                                              float& inv, float& d, float& dd, float& d2)
+{
+    const float v0 = a[0] - b[0], v1 = a[1] - b[1], v2 = a[2] - b[2];
+    d2 = v0 * v0 + v1 * v1 + v2 * v2;
+    inv = rsqrtf(d2);
+    d = d2 * inv;
+    const float ab = a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
+    dd = __fdividef(fmaf(-2.f, ab, aa), d + dc);
+}
+
+template <> struct PluginF<K_LAPLACE>
+{
+    static constexpr bool needs_normals = false;
+    __device__ static cplx<float> kernel(const float* x, const float*, const KParams&)
+    {
+        const float d2 = x[0] * x[0] + x[1] * x[1] + x[2] * x[2];
+        return {d2 == 0.f ? 0.f : INV4PIF * rsqrtf(d2), 0.f};
+    }
+    __device__ static cplx<float> factored(const float* a, float, const float* b, const float*,
+                                           cplx<float> w, float dc, const KParams&)
+    {
+        const float v0 = a[0] - b[0], v1 = a[1] - b[1], v2 = a[2] - b[2];
+        const float d2 = v0 * v0 + v1 * v1 + v2 * v2;
+        return {d2 == 0.f ? 0.f : w.re * dc * rsqrtf(d2), 0.f};
+    }
+};
+
+template <> struct PluginF<K_HELMHOLTZ>
+{
+    static constexpr bool needs_normals = false;
+    __device__ static cplx<float> kernel(const float* x, const float*, const KParams& p)
+    {
+        const float d2 = x[0] * x[0] + x[1] * x[1] + x[2] * x[2];
+        if (d2 == 0.f)
+            return {0.f, 0.f};
+        const float inv = rsqrtf(d2);
+        const cplx<float> e = exp_ik_ff(p, d2 * inv);
+        const float f = inv * INV4PIF;
+        return {e.re * f, e.im * f};
+    }
+    __device__ static cplx<float> factored(const float* a, float aa, const float* b, const float*,
+                                           cplx<float> w, float dc, const KParams& p)
+    {
+        float inv, d, dd, d2;
+        factored_geom(a, aa, b, dc, inv, d, dd, d2);
+        const cplx<float> e = exp_ik_ff(p, dd);
+        const float f = dc * inv;
+        return {f * (w.re * e.re - w.im * e.im), f * (w.re * e.im + w.im * e.re)};
+    }
+};
+
+template <> struct PluginF<K_MODHELMHOLTZ>
+{
+    static constexpr bool needs_normals = false;
+    __device__ static cplx<float> kernel(const float* x, const float*, const KParams& p)
+    {
+        const float d2 = x[0] * x[0] + x[1] * x[1] + x[2] * x[2];
+        if (d2 == 0.f)
+            return {0.f, 0.f};
+        const float inv = rsqrtf(d2);
+        const cplx<float> e = exp_mk_ff(p, d2 * inv);
+        const float f = inv * INV4PIF;
+        return {e.re * f, e.im * f};
+    }
+    __device__ static cplx<float> factored(const float* a, float aa, const float* b, const float*,
+                                           cplx<float> w, float dc, const KParams& p)
+    {
+        float inv, d, dd, d2;
+        factored_geom(a, aa, b, dc, inv, d, dd, d2);
+        if (d2 == 0.f)
+            return {0.f, 0.f};
+        const cplx<float> e = exp_mk_ff(p, dd);
+        const float f = dc * inv;
+        return {f * (w.re * e.re - w.im * e.im), f * (w.re * e.im + w.im * e.re)};
+    }
+};
+
+template <> struct PluginF<K_GRADHELMHOLTZ>
+{
+    static constexpr bool needs_normals = false;
+    __device__ static cplx<float> kernel(const float* x, const float*, const KParams& p)
+    {
+        const float d2 = x[0] * x[0] + x[1] * x[1] + x[2] * x[2];
+        if (!(d2 >= 1e-24f))
+            return {0.f, 0.f};
+        const float inv = rsqrtf(d2), d = d2 * inv;
+        const cplx<float> e = exp_mk_ff(p, d);
+        if (p.dx < 0)
+            return {e.re * inv * INV4PIF, e.im * inv * INV4PIF};
+        // -(1/4pi) (1/d^2) e^{-kd} (-k - 1/d) x[dx]
+        const float mr = -p.krh - inv, mi = -p.kih;
+        const float s = -INV4PIF * inv * inv * x[p.dx];
+        return {s * (e.re * mr - e.im * mi), s * (e.re * mi + e.im * mr)};
+    }
+    __device__ static cplx<float> factored(const float* a, float aa, const float* b, const float*,
+                                           cplx<float> w, float dc, const KParams& p)
+    {
+        float inv, d, dd, d2;
+        factored_geom(a, aa, b, dc, inv, d, dd, d2);
+        if (!(d2 > 1e-12f))
+            inv = 0.f;
+        const cplx<float> e = exp_mk_ff(p, dd);
+        const cplx<float> we = {w.re * e.re - w.im * e.im, w.re * e.im + w.im * e.re};
+        if (p.dx < 0)
+            return {we.re * dc * inv, we.im * dc * inv};
+        const float ww = -(inv * inv) * dc * (a[p.dx] - b[p.dx]);
+        const float mr = -p.krh - inv, mi = -p.kih;
+        return {ww * (we.re * mr - we.im * mi), ww * (we.re * mi + we.im * mr)};
+    }
+};
+
+template <> struct PluginF<K_DOUBLELAYER>
+{
+    static constexpr bool needs_normals = true;
+    __device__ static cplx<float> kernel_d(const double* x, const double* n, const KParams& p)
+    {
+        const double d2d = x[0] * x[0] + x[1] * x[1] + x[2] * x[2];
+        if (!(d2d >= 1e-24))
+            return {0.f, 0.f};
+        const float xn = (float)(x[0] * n[0] + x[1] * n[1] + x[2] * n[2]);
+        const float d2 = (float)d2d;
+        const float inv = rsqrtf(d2), d = d2 * inv;
+        const cplx<float> e = exp_mk_ff(p, d);
+        const float mr = -p.krh - inv, mi = -p.kih;
+        const float s = -INV4PIF * inv * inv * xn;
+        return {s * (e.re * mr - e.im * mi), s * (e.re * mi + e.im * mr)};
+    }
+    __device__ static cplx<float> factored(const float* a, float aa, const float* b, const float* n,
+                                           cplx<float> w, float dc, const KParams& p)
+    {
+        float inv, d, dd, d2;
+        factored_geom(a, aa, b, dc, inv, d, dd, d2);
+        if (!(d2 > 1e-12f))
+            inv = 0.f;
+        const float an = (a[0] - b[0]) * n[0] + (a[1] - b[1]) * n[1] + (a[2] - b[2]) * n[2];
+        const float ww = -(inv * inv) * dc * an;
+        const cplx<float> e = exp_mk_ff(p, dd);
+        const cplx<float> we = {w.re * e.re - w.im * e.im, w.re * e.im + w.im * e.re};
+        const float mr = -p.krh - inv, mi = -p.kih;
+        return {ww * (we.re * mr - we.im * mi), ww * (we.re * mi + we.im * mr)};
+    }
+};
+
+template <> struct PluginF<K_COMBINEDFIELD>
+{
+    static constexpr bool needs_normals = true;
+    __device__ static cplx<float> kernel_d(const double* x, const double* n, const KParams& p)
+    {
+        const double d2d = x[0] * x[0] + x[1] * x[1] + x[2] * x[2];
+        if (!(d2d >= 1e-14))
+            return {0.f, 0.f};
+        const float kap = p.krh;
+        const float nxy = (float)-(n[0] * x[0] + n[1] * x[1] + n[2] * x[2]);
+        const float d2 = (float)d2d;
+        const float inv = rsqrtf(d2), d = d2 * inv;
+        const cplx<float> e = exp_ik_ff(p, d);
+        const float f = INV4PIF * inv * inv * inv;
+        return {f * (e.re * nxy + e.im * kap * (d * nxy + d2)),
+                f * (-e.re * kap * (d * nxy + d2) + e.im * nxy)};
+    }
+    __device__ static cplx<float> factored(const float* a, float aa, const float* b, const float* n,
+                                           cplx<float> w, float dc, const KParams& p)
+    {
+        float inv, d, dd, d2;
+        factored_geom(a, aa, b, dc, inv, d, dd, d2);
+        if (!(d2 > 1e-14f))
+            return {0.f, 0.f};
+        const float kap = p.krh;
+        // z = y - x = b - a
+        const float nxy = (b[0] - a[0]) * n[0] + (b[1] - a[1]) * n[1] + (b[2] - a[2]) * n[2];
+        const cplx<float> e = exp_ik_ff(p, dd);
+        const float f = dc * inv * inv * inv;
+        const float A = w.re * e.re - w.im * e.im, B = w.re * e.im + w.im * e.re;
+        return {f * (A * nxy + B * kap * (d * nxy + d2)), f * (-A * kap * (d * nxy + d2) + B * nxy)};
+    }
+};
+
+
+// Centred factor CF(y - xc) and centre-shift factor G(y, xc)/G(y, pxc) in
+// mixed precision: distances in FP64 (d2 given), phases reduced in FP64.
+template <int KIND>
+__device__ __forceinline__ cplx<float> cf_mixed(double d2, const KParams& p)
+{
+    const double d = sqrt(d2);
+    const float id = (float)(1.0 / d) * INV4PIF;
+    if (KIND == K_LAPLACE)
+        return {id, 0.f};
+    if (KIND == K_HELMHOLTZ || KIND == K_COMBINEDFIELD)
+    {
+        const cplx<float> e = exp_ik_f(p.kr, d);
+        return {e.re * id, e.im * id};
+    }
+    const cplx<float> e = exp_mk_f(p, d);
+    return {e.re * id, e.im * id};
+}
+
+template <int KIND>
+__device__ __forceinline__ cplx<float> transfer_mixed(double d2, double dp2, const KParams& p)
+{
+    const double d = sqrt(d2), dp = sqrt(dp2);
+    const float ratio = (float)(dp / d);
+    if (KIND == K_LAPLACE)
+        return {ratio, 0.f};
+    if (KIND == K_HELMHOLTZ || KIND == K_COMBINEDFIELD)
+    {
+        const cplx<float> e = exp_ik_f(p.kr, d - dp);
+        return {e.re * ratio, e.im * ratio};
+    }
+    const cplx<float> e = exp_mk_f(p, d - dp);
+    return {e.re * ratio, e.im * ratio};
+}
+
+// FP32 coordinates: (s, theta, phi) from an FP32 difference vector
+__device__ __forceinline__ void cart_to_interp_f(float p0, float p1, float p2, float H, float* s)
+{
+    const float a = p0 * p0 + p1 * p1;
+    s[2] = fminf(fmaxf(atan2f(p1, p0), -(float)DPI), (float)DPI);
+    s[1] = fminf(fmaxf(atan2f(sqrtf(a), p2), 0.f), (float)DPI);
+    s[0] = H * rsqrtf(a + p2 * p2);
+}
 
 } // namespace ifgf

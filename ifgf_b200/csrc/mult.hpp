@@ -1,0 +1,146 @@
+// Launch interface of the matvec kernels (implemented in mult_kernels.cuh,
+// instantiated once per kernel plug-in in kernels_k<KIND>.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "common.hpp"
+#include "device_math.cuh"
+
+namespace ifgf
+{
+
+struct TreeArgs
+{
+    const double* __restrict__ box_c;
+    const double* __restrict__ box_H;
+    const int* __restrict__ box_first;
+    const int* __restrict__ box_last;
+    const int* __restrict__ box_child;
+    const int* __restrict__ box_level;
+    const unsigned char* __restrict__ box_leaf;
+};
+
+struct SrcArgs
+{
+    const double* __restrict__ sx;
+    const double* __restrict__ sy;
+    const double* __restrict__ sz;
+    const double* __restrict__ nx;
+    const double* __restrict__ ny;
+    const double* __restrict__ nz;
+};
+
+// Box-independent geometry of the upward transfer at one level: for parent
+// cone element slot s, octant o and Chebyshev node n of the parent cone, the
+// child's fine element (or -1 when the node lies outside the child's
+// interpolation domain), the node's local coordinates in that element and
+// the centre-shift factor G(y, x_child)/G(y, x_parent).
+// Each (slot, octant) row is sorted by child element, so that the threads of
+// a warp gather the same cone's coefficients; `node` is the parent node the
+// entry belongs to.
+struct UpGeo64
+{
+    double loc[3];
+    double tr, ti;
+    int fe;
+    int node;
+};
+struct UpGeo32
+{
+    float loc[3];
+    float tr, ti;
+    int fe;
+    int node;
+    int pad;
+};
+
+// Per-level device lists of one operator.
+struct LevelLists
+{
+    const int* cc_box;   // coarse cone -> global box id
+    const int* cc_el;    // coarse cone -> element id
+    const int* leaf_idx; // coarse cones of leaf boxes (indices into cc_*)
+    const int* up_idx;   // coarse cones of boxes with children, ordered by element
+    const int* up_slot;  // element slot of each up_idx entry (geometry table row)
+    const UpGeo64* geo64; // [slot][octant][node]
+    const UpGeo32* geo32;
+    int n_leaf, n_up;
+};
+
+// Builds the upward geometry tables of one level (device, FP64).
+// slot_el: element id of each slot; off: 8 child-centre offsets (24 doubles).
+template <int KIND>
+void launch_build_upgeo(const LevelGeom& PG, const LevelGeom& CG, double pH, double cH,
+                        const double* off_dev, const int* slot_el, int n_slots,
+                        const double* hi_nodes, int P_hi, KParams kp, UpGeo64* g64, UpGeo32* g32);
+
+// Everything one matvec launch needs (device pointers, sizes, orders).
+struct MultPtrs
+{
+    int L;
+    const LevelGeom* lv_host; // host copy (grid sizes)
+    const LevelGeom* lv_dev;  // device copy (read by target_eval)
+    const LevelLists* lists;  // host array of L entries
+    TreeArgs T;
+    SrcArgs S;
+    const double* tx;
+    const double* ty;
+    const double* tz;
+    const long long* src_perm;
+    const long long* tgt_perm;
+    const double* hi_nodes;
+    const double* A;
+    const int* fmap;
+    const int* tl_first;
+    const int* tl_last;
+    const long long* tl_far_off;
+    const int* tl_far_src;
+    const long long* tl_near_off;
+    const int* tl_near_src;
+    int n_tleaf;
+    long long n_src;
+    double2* w;
+    double2* cvals;
+    double2* fcoef;
+    unsigned long long* err;
+    int lo[3], hi[3], fct[3];
+    int P_lo, P_hi;
+    size_t c2f_smem; // for FP64 buffers (half of it in mixed precision)
+    KParams kp;
+    bool mixed; // mixed-precision pipeline (buffers hold float2)
+};
+
+// Stage classes for per-kernel timing.
+enum ProfClass
+{
+    PROF_PERMUTE = 0,
+    PROF_COARSE = 1, // leaf sampling
+    PROF_C2F = 2,
+    PROF_EVAL = 3,
+    PROF_UPWARD = 4
+};
+
+struct LaunchHooks
+{
+    virtual void begin(int cls) = 0;
+    virtual void end() = 0;
+    virtual ~LaunchHooks() = default;
+};
+
+// Enqueues one matvec on `st`; returns the number of kernels launched.
+template <int KIND>
+int launch_mult_kernels(const MultPtrs& m, const void* d_w, void* d_u, bool real, cudaStream_t st,
+                        LaunchHooks* hooks);
+
+// Only the density permutation into m.w (for direct sums).
+template <int KIND>
+void permute_only(const MultPtrs& m, const void* d_w, bool real, cudaStream_t st);
+
+// FP64 direct sums at the sorted target positions tpos[0..nt) (weights must
+// already be permuted into m.w).
+template <int KIND>
+void launch_direct_kernel(const MultPtrs& m, const int* tpos, int nt, double2* out,
+                          cudaStream_t st);
+
+} // namespace ifgf

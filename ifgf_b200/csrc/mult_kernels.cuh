@@ -1,0 +1,1595 @@
+// Matvec kernels of the IFGF pipeline (IfgfOperator::mult,
+// ifgfoperator.hpp:246-867), restructured level-synchronously for sm_100a:
+//
+//   permute_weights     w -> Morton order (ifgfoperator.hpp:252-254)
+//   per level, deepest first:
+//     leaf_sample       nodal values of leaf boxes' coarse cones
+//                       (evaluateFactoredKernel at the cone's Chebyshev nodes,
+//                       ifgfoperator.hpp:1057-1073, 423-462)
+//     upward            nodal values of other boxes' coarse cones: children's
+//                       fine interpolants at the nodes x transfer_factor
+//                       (transferInterp, ifgfoperator.hpp:1639-1705, 633-688)
+//     coarse_to_fine    chebtransform, coarseToFine and the fine chebtransform
+//                       (ifgfoperator.hpp:1087-1124, 1539-1637) as three
+//                       per-dimension matrix products
+//   target_eval         per target leaf: near field + far field of every
+//                       admissible source box, written in caller order
+//                       (ifgfoperator.hpp:900-1012, 1707-1891, 862-866)
+//
+// Included by one translation unit per kernel plug-in (kernels_k<KIND>.cu).
+#pragma once
+
+#include <type_traits>
+
+#include "mult.hpp"
+
+namespace ifgf
+{
+
+// ---------------------------------------------------------------------------
+// Tensor-product Chebyshev sums with compile-time orders (registers only);
+// N0 = 0 selects the runtime-order fallback.
+// ---------------------------------------------------------------------------
+template <int N> __device__ __forceinline__ void cheb_T(double x, double* t)
+{
+    t[0] = 1.0;
+    if (N > 1)
+        t[1] = x;
+    const double x2 = 2.0 * x;
+#pragma unroll
+    for (int i = 2; i < N; i++)
+        t[i] = fma(x2, t[i - 1], -t[i - 2]);
+}
+
+template <int N0, int N1, int N2> struct Cheb
+{
+    __device__ static __forceinline__ cplx<double> eval(const double2* __restrict__ c,
+                                                        const double* x, const int*)
+    {
+        double t0[N0], t1[N1], t2[N2];
+        cheb_T<N0>(x[0], t0);
+        cheb_T<N1>(x[1], t1);
+        cheb_T<N2>(x[2], t2);
+        double ar = 0, ai = 0;
+#pragma unroll
+        for (int k = 0; k < N2; k++)
+        {
+            double br = 0, bi = 0;
+#pragma unroll
+            for (int j = 0; j < N1; j++)
+            {
+                double cr = 0, ci = 0;
+#pragma unroll
+                for (int i = 0; i < N0; i++)
+                {
+                    const double2 v = __ldg(c + i + N0 * (j + N1 * k));
+                    cr = fma(v.x, t0[i], cr);
+                    ci = fma(v.y, t0[i], ci);
+                }
+                br = fma(cr, t1[j], br);
+                bi = fma(ci, t1[j], bi);
+            }
+            ar = fma(br, t2[k], ar);
+            ai = fma(bi, t2[k], ai);
+        }
+        return {ar, ai};
+    }
+};
+
+template <> struct Cheb<0, 0, 0>
+{
+    __device__ static __forceinline__ cplx<double> eval(const double2* __restrict__ c,
+                                                        const double* x, const int* n)
+    {
+        return cheb_eval3<16>(c, x, n);
+    }
+};
+
+// ---------------------------------------------------------------------------
+static __global__ void permute_weights_kernel(const double* __restrict__ in, int real_in,
+                                              const long long* __restrict__ perm, double2* w,
+                                              long long n)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+    {
+        const long long j = perm[i];
+        w[i] = real_in ? make_double2(in[j], 0.0) : reinterpret_cast<const double2*>(in)[j];
+    }
+}
+
+constexpr int NPT = 2;           // coarse-cone nodes per thread
+constexpr int NODE_THREADS = 256; // threads of the leaf / upward CTAs (max)
+
+struct LeafArgs
+{
+    LevelGeom G;
+    TreeArgs T;
+    SrcArgs S;
+    const int* __restrict__ cc_box;
+    const int* __restrict__ cc_el;
+    const int* __restrict__ idx;
+    const double* __restrict__ hi_nodes;
+    const double2* __restrict__ w;
+    double2* cvals;
+    int P_hi;
+    KParams kp;
+};
+
+// Cartesian position of Chebyshev node n of coarse cone `el` of a box.
+__device__ __forceinline__ void node_position(const LevelGeom& G, int el, int n,
+                                              const double* __restrict__ hi_nodes,
+                                              const double* xc, double H, double* y)
+{
+    const double loc[3] = {hi_nodes[3 * n], hi_nodes[3 * n + 1], hi_nodes[3 * n + 2]};
+    double s[3];
+    from_local(el, loc, G.dmin, G.hc, G.nc, s);
+    interp_to_cart(s, xc, H, y);
+}
+
+// One CTA per coarse cone of a leaf box: sum over the leaf's sources
+// (staged in shared memory) at NPT nodes per thread.
+template <int KIND>
+__global__ void __launch_bounds__(NODE_THREADS) leaf_sample_kernel(LeafArgs a)
+{
+    using P = Plugin<KIND>;
+    extern __shared__ double sm[];
+    const int c = a.idx[blockIdx.x];
+    const int node0 = blockIdx.y * NPT * blockDim.x; // node chunk of this CTA
+    const int box = a.cc_box[c], el = a.cc_el[c];
+    const double xc[3] = {a.T.box_c[3 * box], a.T.box_c[3 * box + 1], a.T.box_c[3 * box + 2]};
+    const double H = a.T.box_H[box];
+    double y[NPT][3], dc[NPT];
+    cplx<double> acc[NPT];
+#pragma unroll
+    for (int q = 0; q < NPT; q++)
+    {
+        const int n = node0 + threadIdx.x + q * blockDim.x;
+        acc[q] = {0.0, 0.0};
+        y[q][0] = y[q][1] = y[q][2] = 0;
+        dc[q] = 0;
+        if (n < a.P_hi)
+        {
+            node_position(a.G, el, n, a.hi_nodes, xc, H, y[q]);
+            const double e0 = y[q][0] - xc[0], e1 = y[q][1] - xc[1], e2 = y[q][2] - xc[2];
+            dc[q] = sqrt(e0 * e0 + e1 * e1 + e2 * e2);
+        }
+    }
+    const int nt = blockDim.x;
+    double* xs = sm;
+    double* ys = xs + nt;
+    double* zs = ys + nt;
+    double* wr = zs + nt;
+    double* wi = wr + nt;
+    double* n0 = wi + nt;
+    double* n1 = n0 + nt;
+    double* n2 = n1 + nt;
+    const int f = a.T.box_first[box], l = a.T.box_last[box];
+    for (int cs = f; cs < l; cs += nt)
+    {
+        const int cnt = min(nt, l - cs);
+        __syncthreads();
+        if (threadIdx.x < cnt)
+        {
+            const int i = cs + threadIdx.x;
+            xs[threadIdx.x] = a.S.sx[i];
+            ys[threadIdx.x] = a.S.sy[i];
+            zs[threadIdx.x] = a.S.sz[i];
+            const double2 wv = a.w[i];
+            wr[threadIdx.x] = wv.x;
+            wi[threadIdx.x] = wv.y;
+            if (P::needs_normals)
+            {
+                n0[threadIdx.x] = a.S.nx[i];
+                n1[threadIdx.x] = a.S.ny[i];
+                n2[threadIdx.x] = a.S.nz[i];
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < NPT; q++)
+        {
+            if (node0 + threadIdx.x + q * blockDim.x >= a.P_hi)
+                continue;
+            for (int i = 0; i < cnt; i++)
+            {
+                const double av[3] = {xs[i] - y[q][0], ys[i] - y[q][1], zs[i] - y[q][2]};
+                const double nv[3] = {P::needs_normals ? n0[i] : 0.0, P::needs_normals ? n1[i] : 0.0,
+                                      P::needs_normals ? n2[i] : 0.0};
+                acc[q] = cadd(acc[q], P::factored(av, nv, {wr[i], wi[i]}, y[q], dc[q], a.kp));
+            }
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < NPT; q++)
+    {
+        const int n = node0 + threadIdx.x + q * blockDim.x;
+        if (n < a.P_hi)
+            a.cvals[(size_t)c * a.P_hi + n] = make_double2(acc[q].re, acc[q].im);
+    }
+}
+
+struct UpArgs
+{
+    LevelGeom G;  // this (parent) level
+    LevelGeom GC; // child level
+    TreeArgs T;
+    const int* __restrict__ cc_box;
+    const int* __restrict__ cc_el;
+    const int* __restrict__ idx;
+    const int* __restrict__ slot;
+    const UpGeo64* __restrict__ geo64;
+    const UpGeo32* __restrict__ geo32;
+    const double* __restrict__ hi_nodes;
+    const int* __restrict__ fmap;
+    const double2* __restrict__ fcoef;
+    double2* cvals;
+    unsigned long long* err;
+    int P_hi, P_lo;
+    int lo[3];
+    KParams kp;
+};
+
+// One CTA per coarse cone of a box with children (CTAs ordered by cone
+// element, so consecutive CTAs share their geometry-table rows in L2): every
+// child's fine interpolant at the cone's nodes, times the centre-shift
+// factor, with the box-independent geometry read from the level's table.
+// Should a tabulated element be inactive in this child (the table works in
+// coordinates relative to the parent, the activation in absolute ones), the
+// node is recomputed from absolute coordinates as the reference does.
+template <int KIND, int N0, int N1, int N2>
+__device__ __forceinline__ bool upward_fallback64(const UpArgs& a, int box, int el, int n, int cb,
+                                                  const int* fm, cplx<double>& v_out)
+{
+    using P = Plugin<KIND>;
+    const LevelGeom& C = a.GC;
+    const double xc[3] = {a.T.box_c[3 * box], a.T.box_c[3 * box + 1], a.T.box_c[3 * box + 2]};
+    double y[3];
+    node_position(a.G, el, n, a.hi_nodes, xc, a.T.box_H[box], y);
+    const double p0 = y[0] - a.T.box_c[3 * cb], p1 = y[1] - a.T.box_c[3 * cb + 1],
+                 p2 = y[2] - a.T.box_c[3 * cb + 2];
+    double s[3], loc[3];
+    cart_to_interp(p0, p1, p2, a.T.box_H[cb], s);
+    const int fe = element_for_point(s, C.dmin, C.dmax, C.hf, C.nf);
+    if (fe < 0)
+        return false;
+    const int gf = fm[fe];
+    if (gf < 0)
+    {
+        atomicAdd(a.err, 1ull);
+        return false;
+    }
+    to_local(fe, s, C.dmin, C.hf, C.nf, loc);
+    const cplx<double> v = Cheb<N0, N1, N2>::eval(a.fcoef + (size_t)gf * a.P_lo, loc, a.lo);
+    const double e0 = y[0] - xc[0], e1 = y[1] - xc[1], e2 = y[2] - xc[2];
+    v_out = cmul(v, P::transfer(p0 * p0 + p1 * p1 + p2 * p2, e0 * e0 + e1 * e1 + e2 * e2, a.kp));
+    return true;
+}
+
+template <int KIND, int N0, int N1, int N2>
+__global__ void __launch_bounds__(NODE_THREADS) upward_kernel(UpArgs a)
+{
+    extern __shared__ double2 acc64[]; // one accumulator per node of the cone
+    const int c = a.idx[blockIdx.x];
+    const int slot = a.slot[blockIdx.x];
+    const int box = a.cc_box[c], el = a.cc_el[c];
+    for (int n = threadIdx.x; n < a.P_hi; n += blockDim.x)
+        acc64[n] = make_double2(0.0, 0.0);
+    const LevelGeom& C = a.GC;
+    const long long nf = (long long)C.nf[0] * C.nf[1] * C.nf[2];
+    for (int o = 0; o < 8; o++)
+    {
+        const int cb = a.T.box_child[8 * box + o];
+        if (cb < 0)
+            continue;
+        __syncthreads(); // every node is updated once per octant
+        const int* fm = a.fmap + C.fmap_off + (long long)(cb - C.box_off) * nf;
+        const UpGeo64* row = a.geo64 + ((size_t)slot * 8 + o) * a.P_hi;
+        for (int i = threadIdx.x; i < a.P_hi; i += blockDim.x)
+        {
+            const UpGeo64& g = row[i];
+            if (g.fe < 0)
+                continue;
+            const int gf = fm[g.fe];
+            cplx<double> v;
+            if (gf < 0)
+            {
+                if (!upward_fallback64<KIND, N0, N1, N2>(a, box, el, g.node, cb, fm, v))
+                    continue;
+            }
+            else
+                v = cmul(Cheb<N0, N1, N2>::eval(a.fcoef + (size_t)gf * a.P_lo, g.loc, a.lo),
+                         cplx<double>{g.tr, g.ti});
+            double2 s = acc64[g.node];
+            s.x += v.re;
+            s.y += v.im;
+            acc64[g.node] = s;
+        }
+    }
+    __syncthreads();
+    for (int n = threadIdx.x; n < a.P_hi; n += blockDim.x)
+        a.cvals[(size_t)c * a.P_hi + n] = acc64[n];
+}
+
+// Builds one level's upward geometry (FP64 values and their FP32 copies):
+// the parent box is centred at the origin, child o at off[o].  One CTA per
+// (slot, octant) row; the row is sorted by child element (then node).
+template <int KIND>
+__global__ void __launch_bounds__(256) build_upgeo_kernel(LevelGeom PG, LevelGeom CG, double pH,
+                                                          double cH, const double* __restrict__ off,
+                                                          const int* __restrict__ slot_el,
+                                                          const double* __restrict__ hi_nodes,
+                                                          int P_hi, KParams kp, UpGeo64* g64,
+                                                          UpGeo32* g32)
+{
+    using P = Plugin<KIND>;
+    extern __shared__ int key[]; // sort key per node: element (outside -> last), then node
+    const int slot = blockIdx.x >> 3, o = blockIdx.x & 7;
+    const int el = slot_el[slot];
+    const double zero[3] = {0.0, 0.0, 0.0};
+    const size_t base = ((size_t)slot * 8 + o) * P_hi;
+    for (int n = threadIdx.x; n < P_hi; n += blockDim.x)
+    {
+        double y[3], s[3];
+        node_position(PG, el, n, hi_nodes, zero, pH, y);
+        const double p0 = y[0] - off[3 * o], p1 = y[1] - off[3 * o + 1], p2 = y[2] - off[3 * o + 2];
+        cart_to_interp(p0, p1, p2, cH, s);
+        const int fe = element_for_point(s, CG.dmin, CG.dmax, CG.hf, CG.nf);
+        key[n] = fe < 0 ? 0x7fffffff : fe;
+    }
+    __syncthreads();
+    for (int n = threadIdx.x; n < P_hi; n += blockDim.x)
+    {
+        // rank of (key, n) among the row
+        const int kn = key[n];
+        int rank = 0;
+        for (int m = 0; m < P_hi; m++)
+        {
+            const int km = key[m];
+            rank += (km < kn) || (km == kn && m < n);
+        }
+        double y[3], s[3];
+        node_position(PG, el, n, hi_nodes, zero, pH, y);
+        const double dp2 = y[0] * y[0] + y[1] * y[1] + y[2] * y[2];
+        const double p0 = y[0] - off[3 * o], p1 = y[1] - off[3 * o + 1], p2 = y[2] - off[3 * o + 2];
+        cart_to_interp(p0, p1, p2, cH, s);
+        UpGeo64 g;
+        g.fe = element_for_point(s, CG.dmin, CG.dmax, CG.hf, CG.nf);
+        g.node = n;
+        g.loc[0] = g.loc[1] = g.loc[2] = 0.0;
+        g.tr = g.ti = 0.0;
+        if (g.fe >= 0)
+        {
+            to_local(g.fe, s, CG.dmin, CG.hf, CG.nf, g.loc);
+            const cplx<double> tf = P::transfer(p0 * p0 + p1 * p1 + p2 * p2, dp2, kp);
+            g.tr = tf.re;
+            g.ti = tf.im;
+        }
+        g64[base + rank] = g;
+        UpGeo32 h;
+        h.fe = g.fe;
+        h.node = n;
+        h.pad = 0;
+        h.loc[0] = (float)g.loc[0];
+        h.loc[1] = (float)g.loc[1];
+        h.loc[2] = (float)g.loc[2];
+        h.tr = (float)g.tr;
+        h.ti = (float)g.ti;
+        g32[base + rank] = h;
+    }
+}
+
+template <int KIND>
+void launch_build_upgeo(const LevelGeom& PG, const LevelGeom& CG, double pH, double cH,
+                        const double* off_dev, const int* slot_el, int n_slots,
+                        const double* hi_nodes, int P_hi, KParams kp, UpGeo64* g64, UpGeo32* g32)
+{
+    if (n_slots <= 0)
+        return;
+    build_upgeo_kernel<KIND><<<n_slots * 8, 256, P_hi * sizeof(int)>>>(
+        PG, CG, pH, cH, off_dev, slot_el, hi_nodes, P_hi, kp, g64, g32);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess)
+        throw Error(2, std::string("build_upgeo_kernel: ") + cudaGetErrorString(e));
+}
+
+
+struct C2FArgs
+{
+    LevelGeom G;
+    const int* __restrict__ cc_box;
+    const int* __restrict__ cc_el;
+    const double2* __restrict__ cvals;
+    const double* __restrict__ A; // A0 | A1 | A2, row-major (f_d lo_d) x ho_d
+    const int* __restrict__ fmap;
+    double2* fcoef;
+    int hi[3], lo[3], f[3];
+    int P_hi, P_lo;
+};
+
+// Coarse nodal values -> fine Chebyshev coefficients of the active sub-cones.
+static __global__ void __launch_bounds__(256) coarse_to_fine_kernel(C2FArgs a)
+{
+    extern __shared__ double2 s2[];
+    const int c = blockIdx.x;
+    const int box = a.cc_box[c], el = a.cc_el[c];
+    const int h0 = a.hi[0], h1 = a.hi[1], h2 = a.hi[2];
+    const int F0 = a.f[0] * a.lo[0], F1 = a.f[1] * a.lo[1];
+    const int sz0 = a.P_hi;
+    const int sz2 = max(F0 * h1 * h2, F0 * F1 * a.lo[2]);
+    double2* B0 = s2;
+    double2* B2 = B0 + sz0;
+    double2* B1 = B2 + sz2;
+    const double* A0 = a.A;
+    const double* A1 = A0 + F0 * h0;
+    const double* A2 = A1 + F1 * h1;
+
+    for (int i = threadIdx.x; i < sz0; i += blockDim.x)
+        B0[i] = a.cvals[(size_t)c * a.P_hi + i];
+    __syncthreads();
+    for (int o = threadIdx.x; o < F0 * h1 * h2; o += blockDim.x)
+    {
+        const int i0 = o % F0, r = o / F0;
+        double re = 0, im = 0;
+        for (int m = 0; m < h0; m++)
+        {
+            const double av = A0[i0 * h0 + m];
+            const double2 v = B0[m + h0 * r];
+            re = fma(av, v.x, re);
+            im = fma(av, v.y, im);
+        }
+        B2[o] = make_double2(re, im);
+    }
+    __syncthreads();
+    for (int o = threadIdx.x; o < F0 * F1 * h2; o += blockDim.x)
+    {
+        const int i0 = o % F0, r = o / F0;
+        const int i1 = r % F1, m2 = r / F1;
+        double re = 0, im = 0;
+        for (int m = 0; m < h1; m++)
+        {
+            const double av = A1[i1 * h1 + m];
+            const double2 v = B2[i0 + F0 * (m + h1 * m2)];
+            re = fma(av, v.x, re);
+            im = fma(av, v.y, im);
+        }
+        B1[o] = make_double2(re, im);
+    }
+    const int nc0 = a.G.nc[0], nc1 = a.G.nc[1];
+    const int hid0 = el % nc0, hid1 = (el / nc0) % nc1, hid2 = el / (nc0 * nc1);
+    const int nf0 = a.G.nf[0], nf1 = a.G.nf[1];
+    const long long nft = (long long)nf0 * nf1 * a.G.nf[2];
+    const int* fm = a.fmap + a.G.fmap_off + (long long)(box - a.G.box_off) * nft;
+    const int lo0 = a.lo[0], lo1 = a.lo[1], lo2 = a.lo[2];
+    for (int j2 = 0; j2 < a.f[2]; j2++)
+    {
+        __syncthreads();
+        for (int o = threadIdx.x; o < F0 * F1 * lo2; o += blockDim.x)
+        {
+            const int i01 = o % (F0 * F1), i2 = o / (F0 * F1);
+            const int row = j2 * lo2 + i2;
+            double re = 0, im = 0;
+            for (int m = 0; m < h2; m++)
+            {
+                const double av = A2[row * h2 + m];
+                const double2 v = B1[i01 + F0 * F1 * m];
+                re = fma(av, v.x, re);
+                im = fma(av, v.y, im);
+            }
+            B2[o] = make_double2(re, im);
+        }
+        __syncthreads();
+        const int nsub = a.f[0] * a.f[1];
+        for (int o = threadIdx.x; o < nsub * a.P_lo; o += blockDim.x)
+        {
+            const int sub = o / a.P_lo, q = o % a.P_lo;
+            const int j0 = sub % a.f[0], j1 = sub / a.f[0];
+            const int fel = ((hid2 * a.f[2] + j2) * nf1 + (hid1 * a.f[1] + j1)) * nf0 +
+                            (hid0 * a.f[0] + j0);
+            const int gf = fm[fel];
+            if (gf < 0)
+                continue;
+            const int i0 = q % lo0, i1 = (q / lo0) % lo1, i2 = q / (lo0 * lo1);
+            a.fcoef[(size_t)gf * a.P_lo + q] = B2[(j0 * lo0 + i0) + F0 * ((j1 * lo1 + i1) + F1 * i2)];
+        }
+    }
+}
+
+struct EvalArgs
+{
+    const LevelGeom* __restrict__ lv;
+    TreeArgs T;
+    SrcArgs S;
+    const double* __restrict__ tx;
+    const double* __restrict__ ty;
+    const double* __restrict__ tz;
+    const long long* __restrict__ tgt_perm;
+    const int* __restrict__ tl_first;
+    const int* __restrict__ tl_last;
+    const long long* __restrict__ far_off;
+    const int* __restrict__ far_src;
+    const long long* __restrict__ near_off;
+    const int* __restrict__ near_src;
+    const double2* __restrict__ w;
+    const int* __restrict__ fmap;
+    const double2* __restrict__ fcoef;
+    double* out; // complex (interleaved) or real for Laplace
+    int real_out;
+    unsigned long long* err;
+    int P_lo;
+    int lo[3];
+    KParams kp;
+};
+
+constexpr int EVAL_THREADS = 128;
+
+// One CTA per target leaf.  A leaf holds fewer targets than threads, so
+// thread (ti, si) takes target ti and every S-th near source / far box
+// (S = threads / targets); the S partial sums are added in a fixed order.
+template <int KIND, int N0, int N1, int N2>
+__global__ void __launch_bounds__(EVAL_THREADS) target_eval_kernel(EvalArgs a)
+{
+    using P = Plugin<KIND>;
+    __shared__ double xs[EVAL_THREADS], ys[EVAL_THREADS], zs[EVAL_THREADS];
+    __shared__ double wr[EVAL_THREADS], wi[EVAL_THREADS];
+    __shared__ double n0[P::needs_normals ? EVAL_THREADS : 1], n1[P::needs_normals ? EVAL_THREADS : 1],
+        n2[P::needs_normals ? EVAL_THREADS : 1];
+    __shared__ double rr[EVAL_THREADS], ri[EVAL_THREADS];
+    const int tl = blockIdx.x;
+    const int tf = a.tl_first[tl], tlast = a.tl_last[tl];
+    const long long nb0 = a.near_off[tl], nb1 = a.near_off[tl + 1];
+    const long long fb0 = a.far_off[tl], fb1 = a.far_off[tl + 1];
+    for (int base = tf; base < tlast; base += EVAL_THREADS)
+    {
+        const int cnt = min(EVAL_THREADS, tlast - base);
+        const int S = EVAL_THREADS / cnt;
+        const int ti = threadIdx.x % cnt, si = threadIdx.x / cnt;
+        const bool active = si < S;
+        const int t = base + ti;
+        const double y0 = a.tx[t], y1 = a.ty[t], y2 = a.tz[t];
+        cplx<double> acc = {0.0, 0.0};
+        for (long long e = nb0; e < nb1; e++)
+        {
+            const int sb = a.near_src[e];
+            const int sf = a.T.box_first[sb], sl = a.T.box_last[sb];
+            for (int cs = sf; cs < sl; cs += EVAL_THREADS)
+            {
+                const int ccnt = min(EVAL_THREADS, sl - cs);
+                __syncthreads();
+                if (threadIdx.x < ccnt)
+                {
+                    const int i = cs + threadIdx.x;
+                    xs[threadIdx.x] = a.S.sx[i];
+                    ys[threadIdx.x] = a.S.sy[i];
+                    zs[threadIdx.x] = a.S.sz[i];
+                    const double2 wv = a.w[i];
+                    wr[threadIdx.x] = wv.x;
+                    wi[threadIdx.x] = wv.y;
+                    if (P::needs_normals)
+                    {
+                        n0[threadIdx.x] = a.S.nx[i];
+                        n1[threadIdx.x] = a.S.ny[i];
+                        n2[threadIdx.x] = a.S.nz[i];
+                    }
+                }
+                __syncthreads();
+                if (active)
+                    for (int i = si; i < ccnt; i += S)
+                    {
+                        const double x[3] = {xs[i] - y0, ys[i] - y1, zs[i] - y2};
+                        const double nv[3] = {P::needs_normals ? n0[i] : 0.0,
+                                              P::needs_normals ? n1[i] : 0.0,
+                                              P::needs_normals ? n2[i] : 0.0};
+                        cfma(acc, cplx<double>{wr[i], wi[i]}, P::kernel(x, nv, a.kp));
+                    }
+            }
+        }
+        if (active)
+            for (long long e = fb0 + si; e < fb1; e += S)
+            {
+                const int sb = a.far_src[e];
+                const LevelGeom& G = a.lv[a.T.box_level[sb]];
+                const double p[3] = {y0 - a.T.box_c[3 * sb], y1 - a.T.box_c[3 * sb + 1],
+                                     y2 - a.T.box_c[3 * sb + 2]};
+                double s[3], loc[3];
+                cart_to_interp(p[0], p[1], p[2], a.T.box_H[sb], s);
+                const int fe = element_for_point(s, G.dmin, G.dmax, G.hf, G.nf);
+                if (fe < 0)
+                    continue;
+                const long long nft = (long long)G.nf[0] * G.nf[1] * G.nf[2];
+                const int gf = a.fmap[G.fmap_off + (long long)(sb - G.box_off) * nft + fe];
+                if (gf < 0)
+                {
+                    atomicAdd(a.err, 1ull);
+                    continue;
+                }
+                to_local(fe, s, G.dmin, G.hf, G.nf, loc);
+                const cplx<double> v = Cheb<N0, N1, N2>::eval(a.fcoef + (size_t)gf * a.P_lo, loc, a.lo);
+                cfma(acc, v, P::cf(p, a.kp));
+            }
+        __syncthreads();
+        rr[threadIdx.x] = acc.re;
+        ri[threadIdx.x] = acc.im;
+        __syncthreads();
+        if (active && si == 0)
+        {
+            double sr = 0, sim = 0;
+            for (int s = 0; s < S; s++)
+            {
+                sr += rr[ti + s * cnt];
+                sim += ri[ti + s * cnt];
+            }
+            const long long o = a.tgt_perm[t];
+            if (a.real_out)
+                a.out[o] = sr;
+            else
+            {
+                a.out[2 * o] = sr;
+                a.out[2 * o + 1] = sim;
+            }
+        }
+    }
+}
+
+// FP64 direct sum at selected targets: one CTA per target, Kahan-compensated
+// per-thread partial sums, then a pairwise block reduction.
+template <int KIND>
+__global__ void __launch_bounds__(256) direct_eval_kernel(SrcArgs S, const double2* __restrict__ w,
+                                                          long long ns, const double* __restrict__ tx,
+                                                          const double* __restrict__ ty,
+                                                          const double* __restrict__ tz,
+                                                          const int* __restrict__ tpos, KParams kp,
+                                                          double2* out)
+{
+    using P = Plugin<KIND>;
+    __shared__ double sr[256], si[256];
+    const int j = tpos[blockIdx.x];
+    const double y0 = tx[j], y1 = ty[j], y2 = tz[j];
+    double ar = 0, ai = 0, cr = 0, ci = 0;
+    for (long long s = threadIdx.x; s < ns; s += blockDim.x)
+    {
+        const double x[3] = {S.sx[s] - y0, S.sy[s] - y1, S.sz[s] - y2};
+        const double nv[3] = {P::needs_normals ? S.nx[s] : 0.0, P::needs_normals ? S.ny[s] : 0.0,
+                              P::needs_normals ? S.nz[s] : 0.0};
+        const cplx<double> g = P::kernel(x, nv, kp);
+        const double2 wv = w[s];
+        const double vr = wv.x * g.re - wv.y * g.im, vi = wv.x * g.im + wv.y * g.re;
+        double yr = vr - cr, tr = ar + yr;
+        cr = (tr - ar) - yr;
+        ar = tr;
+        double yi = vi - ci, ti = ai + yi;
+        ci = (ti - ai) - yi;
+        ai = ti;
+    }
+    sr[threadIdx.x] = ar;
+    si[threadIdx.x] = ai;
+    __syncthreads();
+    for (int h = blockDim.x / 2; h > 0; h >>= 1)
+    {
+        if (threadIdx.x < h)
+        {
+            sr[threadIdx.x] += sr[threadIdx.x + h];
+            si[threadIdx.x] += si[threadIdx.x + h];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        out[blockIdx.x] = make_double2(sr[0], si[0]);
+}
+
+// ===========================================================================
+// Mixed-precision variants.  Buffers are reused as float2: permuted
+// densities, coarse nodal values and fine coefficients in FP32.
+// ===========================================================================
+template <int N0, int N1, int N2> struct ChebF
+{
+    __device__ static __forceinline__ cplx<float> eval(const float2* __restrict__ c, const float* x,
+                                                       const int*)
+    {
+        float t0[N0], t1[N1], t2[N2];
+        t0[0] = t1[0] = t2[0] = 1.f;
+        if (N0 > 1)
+            t0[1] = x[0];
+        if (N1 > 1)
+            t1[1] = x[1];
+        if (N2 > 1)
+            t2[1] = x[2];
+#pragma unroll
+        for (int i = 2; i < N0; i++)
+            t0[i] = fmaf(2.f * x[0], t0[i - 1], -t0[i - 2]);
+#pragma unroll
+        for (int i = 2; i < N1; i++)
+            t1[i] = fmaf(2.f * x[1], t1[i - 1], -t1[i - 2]);
+#pragma unroll
+        for (int i = 2; i < N2; i++)
+            t2[i] = fmaf(2.f * x[2], t2[i - 1], -t2[i - 2]);
+        float ar = 0, ai = 0;
+#pragma unroll
+        for (int k = 0; k < N2; k++)
+        {
+            float br = 0, bi = 0;
+#pragma unroll
+            for (int j = 0; j < N1; j++)
+            {
+                float cr = 0, ci = 0;
+#pragma unroll
+                for (int i = 0; i < N0; i++)
+                {
+                    const float2 v = __ldg(c + i + N0 * (j + N1 * k));
+                    cr = fmaf(v.x, t0[i], cr);
+                    ci = fmaf(v.y, t0[i], ci);
+                }
+                br = fmaf(cr, t1[j], br);
+                bi = fmaf(ci, t1[j], bi);
+            }
+            ar = fmaf(br, t2[k], ar);
+            ai = fmaf(bi, t2[k], ai);
+        }
+        return {ar, ai};
+    }
+};
+
+template <> struct ChebF<0, 0, 0>
+{
+    __device__ static __forceinline__ cplx<float> eval(const float2* __restrict__ c, const float* x,
+                                                       const int* n)
+    {
+        float t0[16], t1[16], t2[16];
+        float* ts[3] = {t0, t1, t2};
+        for (int d = 0; d < 3; d++)
+        {
+            ts[d][0] = 1.f;
+            if (n[d] > 1)
+                ts[d][1] = x[d];
+            for (int i = 2; i < n[d]; i++)
+                ts[d][i] = fmaf(2.f * x[d], ts[d][i - 1], -ts[d][i - 2]);
+        }
+        float ar = 0, ai = 0;
+        int q = 0;
+        for (int k = 0; k < n[2]; k++)
+        {
+            float br = 0, bi = 0;
+            for (int j = 0; j < n[1]; j++)
+            {
+                float cr = 0, ci = 0;
+                for (int i = 0; i < n[0]; i++, q++)
+                {
+                    const float2 v = __ldg(c + q);
+                    cr = fmaf(v.x, t0[i], cr);
+                    ci = fmaf(v.y, t0[i], ci);
+                }
+                br = fmaf(cr, t1[j], br);
+                bi = fmaf(ci, t1[j], bi);
+            }
+            ar = fmaf(br, t2[k], ar);
+            ai = fmaf(bi, t2[k], ai);
+        }
+        return {ar, ai};
+    }
+};
+
+// Fine cone of the point p (difference to the box centre, FP64) in a box of
+// side H: FP32 angles first; when they land outside the domain or in an
+// inactive cone, the lookup is redone in FP64, the arithmetic the active-cone
+// tables were built with.  Returns the global fine cone (or -1 when the point
+// is outside the domain) and the local coordinates.
+__device__ __forceinline__ int fine_lookup_mixed(const LevelGeom& G, const int* __restrict__ fm,
+                                                 const double* p, double H, float* loc,
+                                                 unsigned long long* err)
+{
+    float sf[3];
+    cart_to_interp_f((float)p[0], (float)p[1], (float)p[2], (float)H, sf);
+    int fe = -1;
+    {
+        bool inside = true;
+        int id = 0, stride = 1;
+#pragma unroll
+        for (int j = 0; j < 3; j++)
+        {
+            const float lo = (float)G.dmin[j], hi = (float)G.dmax[j];
+            inside = inside && sf[j] >= lo && sf[j] <= hi;
+            int q = (int)floorf((sf[j] - lo) / (float)G.hf[j]);
+            q = min(max(q, 0), G.nf[j] - 1);
+            id += q * stride;
+            stride *= G.nf[j];
+        }
+        if (inside)
+            fe = id;
+    }
+    int gf = fe >= 0 ? fm[fe] : -1;
+    if (gf >= 0)
+    {
+        int r = fe;
+        const int i0 = r % G.nf[0];
+        r /= G.nf[0];
+        const int i1 = r % G.nf[1], i2 = r / G.nf[1];
+        const int idx[3] = {i0, i1, i2};
+#pragma unroll
+        for (int d = 0; d < 3; d++)
+        {
+            const float a = 0.5f * (float)G.hf[d];
+            const float b = (float)(G.dmin[d] + ((double)idx[d] + 0.5) * G.hf[d]);
+            loc[d] = (sf[d] - b) / a;
+        }
+        return gf;
+    }
+    double s[3], ld[3];
+    cart_to_interp(p[0], p[1], p[2], H, s);
+    fe = element_for_point(s, G.dmin, G.dmax, G.hf, G.nf);
+    if (fe < 0)
+        return -1;
+    gf = fm[fe];
+    if (gf < 0)
+    {
+        atomicAdd(err, 1ull);
+        return -1;
+    }
+    to_local(fe, s, G.dmin, G.hf, G.nf, ld);
+    loc[0] = (float)ld[0];
+    loc[1] = (float)ld[1];
+    loc[2] = (float)ld[2];
+    return gf;
+}
+
+static __global__ void permute_weights_mixed_kernel(const double* __restrict__ in, int real_in,
+                                                    const long long* __restrict__ perm, float2* w,
+                                                    long long n)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+    {
+        const long long j = perm[i];
+        if (real_in)
+            w[i] = make_float2((float)in[j], 0.f);
+        else
+        {
+            const double2 v = reinterpret_cast<const double2*>(in)[j];
+            w[i] = make_float2((float)v.x, (float)v.y);
+        }
+    }
+}
+
+template <int KIND>
+__global__ void __launch_bounds__(NODE_THREADS) leaf_sample_mixed_kernel(LeafArgs a)
+{
+    using P = PluginF<KIND>;
+    extern __shared__ float smf[];
+    const int c = a.idx[blockIdx.x];
+    const int node0 = blockIdx.y * NPT * blockDim.x;
+    const int box = a.cc_box[c], el = a.cc_el[c];
+    const double xc[3] = {a.T.box_c[3 * box], a.T.box_c[3 * box + 1], a.T.box_c[3 * box + 2]};
+    const double H = a.T.box_H[box];
+    const float2* wf = reinterpret_cast<const float2*>(a.w);
+    float b[NPT][3], dc[NPT];
+    cplx<float> acc[NPT];
+#pragma unroll
+    for (int q = 0; q < NPT; q++)
+    {
+        const int n = node0 + threadIdx.x + q * blockDim.x;
+        acc[q] = {0.f, 0.f};
+        b[q][0] = b[q][1] = b[q][2] = 0.f;
+        dc[q] = 1.f;
+        if (n < a.P_hi)
+        {
+            double y[3];
+            node_position(a.G, el, n, a.hi_nodes, xc, H, y);
+            const double e0 = y[0] - xc[0], e1 = y[1] - xc[1], e2 = y[2] - xc[2];
+            b[q][0] = (float)e0;
+            b[q][1] = (float)e1;
+            b[q][2] = (float)e2;
+            dc[q] = (float)sqrt(e0 * e0 + e1 * e1 + e2 * e2);
+        }
+    }
+    const int nt = blockDim.x;
+    float* ax = smf;
+    float* ay = ax + nt;
+    float* az = ay + nt;
+    float* wr = az + nt;
+    float* wi = wr + nt;
+    float* n0 = wi + nt;
+    float* n1 = n0 + nt;
+    float* n2 = n1 + nt;
+    float* aa = n2 + nt;
+    const int f = a.T.box_first[box], l = a.T.box_last[box];
+    for (int cs = f; cs < l; cs += nt)
+    {
+        const int cnt = min(nt, l - cs);
+        __syncthreads();
+        if (threadIdx.x < cnt)
+        {
+            const int i = cs + threadIdx.x;
+            const double a0 = a.S.sx[i] - xc[0], a1 = a.S.sy[i] - xc[1], a2 = a.S.sz[i] - xc[2];
+            ax[threadIdx.x] = (float)a0;
+            ay[threadIdx.x] = (float)a1;
+            az[threadIdx.x] = (float)a2;
+            aa[threadIdx.x] = (float)(a0 * a0 + a1 * a1 + a2 * a2);
+            const float2 wv = wf[i];
+            wr[threadIdx.x] = wv.x;
+            wi[threadIdx.x] = wv.y;
+            if (P::needs_normals)
+            {
+                n0[threadIdx.x] = (float)a.S.nx[i];
+                n1[threadIdx.x] = (float)a.S.ny[i];
+                n2[threadIdx.x] = (float)a.S.nz[i];
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < NPT; q++)
+        {
+            if (node0 + threadIdx.x + q * blockDim.x >= a.P_hi)
+                continue;
+            for (int i = 0; i < cnt; i++)
+            {
+                const float av[3] = {ax[i], ay[i], az[i]};
+                const float nv[3] = {P::needs_normals ? n0[i] : 0.f, P::needs_normals ? n1[i] : 0.f,
+                                     P::needs_normals ? n2[i] : 0.f};
+                const cplx<float> v = P::factored(av, aa[i], b[q], nv, {wr[i], wi[i]}, dc[q], a.kp);
+                acc[q].re += v.re;
+                acc[q].im += v.im;
+            }
+        }
+    }
+    float2* cv = reinterpret_cast<float2*>(a.cvals);
+#pragma unroll
+    for (int q = 0; q < NPT; q++)
+    {
+        const int n = node0 + threadIdx.x + q * blockDim.x;
+        if (n < a.P_hi)
+            cv[(size_t)c * a.P_hi + n] = make_float2(acc[q].re, acc[q].im);
+    }
+}
+
+template <int KIND, int N0, int N1, int N2>
+__global__ void __launch_bounds__(NODE_THREADS) upward_mixed_kernel(UpArgs a)
+{
+    extern __shared__ float2 acc32[]; // one accumulator per node of the cone
+    const int c = a.idx[blockIdx.x];
+    const int slot = a.slot[blockIdx.x];
+    const int box = a.cc_box[c], el = a.cc_el[c];
+    const float2* fcf = reinterpret_cast<const float2*>(a.fcoef);
+    for (int n = threadIdx.x; n < a.P_hi; n += blockDim.x)
+        acc32[n] = make_float2(0.f, 0.f);
+    const LevelGeom& C = a.GC;
+    const long long nf = (long long)C.nf[0] * C.nf[1] * C.nf[2];
+    for (int o = 0; o < 8; o++)
+    {
+        const int cb = a.T.box_child[8 * box + o];
+        if (cb < 0)
+            continue;
+        __syncthreads(); // every node is updated once per octant
+        const int* fm = a.fmap + C.fmap_off + (long long)(cb - C.box_off) * nf;
+        const UpGeo32* row = a.geo32 + ((size_t)slot * 8 + o) * a.P_hi;
+        for (int i = threadIdx.x; i < a.P_hi; i += blockDim.x)
+        {
+            const UpGeo32 g = row[i];
+            if (g.fe < 0)
+                continue;
+            const int gf = fm[g.fe];
+            cplx<float> v = {0.f, 0.f};
+            if (gf < 0)
+            {
+                // tabulated element inactive in this child: absolute coordinates
+                const double xc[3] = {a.T.box_c[3 * box], a.T.box_c[3 * box + 1],
+                                      a.T.box_c[3 * box + 2]};
+                double y[3];
+                node_position(a.G, el, g.node, a.hi_nodes, xc, a.T.box_H[box], y);
+                const double p[3] = {y[0] - a.T.box_c[3 * cb], y[1] - a.T.box_c[3 * cb + 1],
+                                     y[2] - a.T.box_c[3 * cb + 2]};
+                float loc[3];
+                const int gf2 = fine_lookup_mixed(C, fm, p, a.T.box_H[cb], loc, a.err);
+                if (gf2 < 0)
+                    continue;
+                const double e0 = y[0] - xc[0], e1 = y[1] - xc[1], e2 = y[2] - xc[2];
+                cfmaf(v, ChebF<N0, N1, N2>::eval(fcf + (size_t)gf2 * a.P_lo, loc, a.lo),
+                      transfer_mixed<KIND>(p[0] * p[0] + p[1] * p[1] + p[2] * p[2],
+                                           e0 * e0 + e1 * e1 + e2 * e2, a.kp));
+            }
+            else
+                cfmaf(v, ChebF<N0, N1, N2>::eval(fcf + (size_t)gf * a.P_lo, g.loc, a.lo),
+                      cplx<float>{g.tr, g.ti});
+            float2 s = acc32[g.node];
+            s.x += v.re;
+            s.y += v.im;
+            acc32[g.node] = s;
+        }
+    }
+    __syncthreads();
+    float2* cv = reinterpret_cast<float2*>(a.cvals);
+    for (int n = threadIdx.x; n < a.P_hi; n += blockDim.x)
+        cv[(size_t)c * a.P_hi + n] = acc32[n];
+}
+
+static __global__ void __launch_bounds__(256) coarse_to_fine_mixed_kernel(C2FArgs a)
+{
+    extern __shared__ float2 s2f[];
+    const int c = blockIdx.x;
+    const int box = a.cc_box[c], el = a.cc_el[c];
+    const int h0 = a.hi[0], h1 = a.hi[1], h2 = a.hi[2];
+    const int F0 = a.f[0] * a.lo[0], F1 = a.f[1] * a.lo[1];
+    const int sz0 = a.P_hi;
+    const int sz2 = max(F0 * h1 * h2, F0 * F1 * a.lo[2]);
+    float2* B0 = s2f;
+    float2* B2 = B0 + sz0;
+    float2* B1 = B2 + sz2;
+    const double* A0 = a.A;
+    const double* A1 = A0 + F0 * h0;
+    const double* A2 = A1 + F1 * h1;
+    const float2* cv = reinterpret_cast<const float2*>(a.cvals);
+    float2* fco = reinterpret_cast<float2*>(a.fcoef);
+
+    for (int i = threadIdx.x; i < sz0; i += blockDim.x)
+        B0[i] = cv[(size_t)c * a.P_hi + i];
+    __syncthreads();
+    for (int o = threadIdx.x; o < F0 * h1 * h2; o += blockDim.x)
+    {
+        const int i0 = o % F0, r = o / F0;
+        float re = 0, im = 0;
+        for (int m = 0; m < h0; m++)
+        {
+            const float av = (float)A0[i0 * h0 + m];
+            const float2 v = B0[m + h0 * r];
+            re = fmaf(av, v.x, re);
+            im = fmaf(av, v.y, im);
+        }
+        B2[o] = make_float2(re, im);
+    }
+    __syncthreads();
+    for (int o = threadIdx.x; o < F0 * F1 * h2; o += blockDim.x)
+    {
+        const int i0 = o % F0, r = o / F0;
+        const int i1 = r % F1, m2 = r / F1;
+        float re = 0, im = 0;
+        for (int m = 0; m < h1; m++)
+        {
+            const float av = (float)A1[i1 * h1 + m];
+            const float2 v = B2[i0 + F0 * (m + h1 * m2)];
+            re = fmaf(av, v.x, re);
+            im = fmaf(av, v.y, im);
+        }
+        B1[o] = make_float2(re, im);
+    }
+    const int nc0 = a.G.nc[0], nc1 = a.G.nc[1];
+    const int hid0 = el % nc0, hid1 = (el / nc0) % nc1, hid2 = el / (nc0 * nc1);
+    const int nf0 = a.G.nf[0], nf1 = a.G.nf[1];
+    const long long nft = (long long)nf0 * nf1 * a.G.nf[2];
+    const int* fm = a.fmap + a.G.fmap_off + (long long)(box - a.G.box_off) * nft;
+    const int lo0 = a.lo[0], lo1 = a.lo[1], lo2 = a.lo[2];
+    for (int j2 = 0; j2 < a.f[2]; j2++)
+    {
+        __syncthreads();
+        for (int o = threadIdx.x; o < F0 * F1 * lo2; o += blockDim.x)
+        {
+            const int i01 = o % (F0 * F1), i2 = o / (F0 * F1);
+            const int row = j2 * lo2 + i2;
+            float re = 0, im = 0;
+            for (int m = 0; m < h2; m++)
+            {
+                const float av = (float)A2[row * h2 + m];
+                const float2 v = B1[i01 + F0 * F1 * m];
+                re = fmaf(av, v.x, re);
+                im = fmaf(av, v.y, im);
+            }
+            B2[o] = make_float2(re, im);
+        }
+        __syncthreads();
+        const int nsub = a.f[0] * a.f[1];
+        for (int o = threadIdx.x; o < nsub * a.P_lo; o += blockDim.x)
+        {
+            const int sub = o / a.P_lo, q = o % a.P_lo;
+            const int j0 = sub % a.f[0], j1 = sub / a.f[0];
+            const int fel = ((hid2 * a.f[2] + j2) * nf1 + (hid1 * a.f[1] + j1)) * nf0 +
+                            (hid0 * a.f[0] + j0);
+            const int gf = fm[fel];
+            if (gf < 0)
+                continue;
+            const int i0 = q % lo0, i1 = (q / lo0) % lo1, i2 = q / (lo0 * lo1);
+            fco[(size_t)gf * a.P_lo + q] = B2[(j0 * lo0 + i0) + F0 * ((j1 * lo1 + i1) + F1 * i2)];
+        }
+    }
+}
+
+// Coarse-to-fine with compile-time orders and refinement factor F (the same
+// in every dimension), for the common order triples.  T is the working
+// precision (double, or float in the mixed pipeline); the three matrices are
+// staged in shared memory in T.
+template <typename T> struct Vec2;
+template <> struct Vec2<double>
+{
+    using type = double2;
+};
+template <> struct Vec2<float>
+{
+    using type = float2;
+};
+
+template <int H0, int H1, int H2, int L0, int L1, int L2, int F, typename T>
+__global__ void __launch_bounds__(256) coarse_to_fine_fixed_kernel(C2FArgs a)
+{
+    using V = typename Vec2<T>::type;
+    constexpr int F0 = F * L0, F1 = F * L1, F2 = F * L2;
+    constexpr int P_HI = H0 * H1 * H2, P_LO = L0 * L1 * L2;
+    constexpr int SZ2 = (F0 * H1 * H2 > F0 * F1 * L2) ? F0 * H1 * H2 : F0 * F1 * L2;
+    constexpr int SZ1 = F0 * F1 * H2;
+    constexpr int NA0 = F0 * H0, NA1 = F1 * H1, NA2 = F2 * H2;
+    extern __shared__ __align__(16) unsigned char c2f_raw[];
+    V* B0 = reinterpret_cast<V*>(c2f_raw);
+    V* B2 = B0 + P_HI;
+    V* B1 = B2 + SZ2;
+    T* A0 = reinterpret_cast<T*>(B1 + SZ1);
+    T* A1 = A0 + NA0;
+    T* A2 = A1 + NA1;
+    __shared__ int gsub[F * F];
+    const int c = blockIdx.x;
+    const int box = a.cc_box[c], el = a.cc_el[c];
+    const V* cv = reinterpret_cast<const V*>(a.cvals) + (size_t)c * P_HI;
+    V* fco = reinterpret_cast<V*>(a.fcoef);
+    for (int i = threadIdx.x; i < NA0 + NA1 + NA2; i += blockDim.x)
+        A0[i] = (T)a.A[i];
+    for (int i = threadIdx.x; i < P_HI; i += blockDim.x)
+        B0[i] = cv[i];
+    __syncthreads();
+    for (int o = threadIdx.x; o < F0 * H1 * H2; o += blockDim.x)
+    {
+        const int i0 = o % F0, r = o / F0;
+        T re = 0, im = 0;
+#pragma unroll
+        for (int m = 0; m < H0; m++)
+        {
+            const T av = A0[i0 * H0 + m];
+            const V v = B0[m + H0 * r];
+            re = fma(av, v.x, re);
+            im = fma(av, v.y, im);
+        }
+        B2[o] = V{re, im};
+    }
+    __syncthreads();
+    for (int o = threadIdx.x; o < SZ1; o += blockDim.x)
+    {
+        const int i0 = o % F0, r = o / F0;
+        const int i1 = r % F1, m2 = r / F1;
+        T re = 0, im = 0;
+#pragma unroll
+        for (int m = 0; m < H1; m++)
+        {
+            const T av = A1[i1 * H1 + m];
+            const V v = B2[i0 + F0 * (m + H1 * m2)];
+            re = fma(av, v.x, re);
+            im = fma(av, v.y, im);
+        }
+        B1[o] = V{re, im};
+    }
+    const int nc0 = a.G.nc[0], nc1 = a.G.nc[1];
+    const int hid0 = el % nc0, hid1 = (el / nc0) % nc1, hid2 = el / (nc0 * nc1);
+    const int nf0 = a.G.nf[0], nf1 = a.G.nf[1];
+    const long long nft = (long long)nf0 * nf1 * a.G.nf[2];
+    const int* fm = a.fmap + a.G.fmap_off + (long long)(box - a.G.box_off) * nft;
+    for (int j2 = 0; j2 < F; j2++)
+    {
+        __syncthreads();
+        if (threadIdx.x < F * F)
+        {
+            const int j0 = threadIdx.x % F, j1 = threadIdx.x / F;
+            gsub[threadIdx.x] =
+                fm[((hid2 * F + j2) * nf1 + (hid1 * F + j1)) * nf0 + (hid0 * F + j0)];
+        }
+        for (int o = threadIdx.x; o < F0 * F1 * L2; o += blockDim.x)
+        {
+            const int i01 = o % (F0 * F1), i2 = o / (F0 * F1);
+            const int row = j2 * L2 + i2;
+            T re = 0, im = 0;
+#pragma unroll
+            for (int m = 0; m < H2; m++)
+            {
+                const T av = A2[row * H2 + m];
+                const V v = B1[i01 + F0 * F1 * m];
+                re = fma(av, v.x, re);
+                im = fma(av, v.y, im);
+            }
+            B2[o] = V{re, im};
+        }
+        __syncthreads();
+        for (int o = threadIdx.x; o < F * F * P_LO; o += blockDim.x)
+        {
+            const int sub = o / P_LO, q = o % P_LO;
+            const int gf = gsub[sub];
+            if (gf < 0)
+                continue;
+            const int j0 = sub % F, j1 = sub / F;
+            const int i0 = q % L0, i1 = (q / L0) % L1, i2 = q / (L0 * L1);
+            fco[(size_t)gf * P_LO + q] = B2[(j0 * L0 + i0) + F0 * ((j1 * L1 + i1) + F1 * i2)];
+        }
+    }
+}
+
+template <int H0, int H1, int H2, int L0, int L1, int L2, int F, typename T>
+constexpr size_t c2f_fixed_smem()
+{
+    constexpr int F0 = F * L0, F1 = F * L1, F2 = F * L2;
+    constexpr int SZ2 = (F0 * H1 * H2 > F0 * F1 * L2) ? F0 * H1 * H2 : F0 * F1 * L2;
+    return (size_t)(H0 * H1 * H2 + SZ2 + F0 * F1 * H2) * 2 * sizeof(T) +
+           (size_t)(F0 * H0 + F1 * H1 + F2 * H2) * sizeof(T);
+}
+
+// Launches the fixed-size coarse-to-fine kernel when (hi, lo, f) is one of the
+// instantiated shapes; returns false otherwise.
+template <typename T>
+static bool launch_c2f_fixed(const C2FArgs& fa, unsigned grid, cudaStream_t st)
+{
+    const int* h = fa.hi;
+    const int* l = fa.lo;
+    const int f = fa.f[0];
+    if (fa.f[1] != f || fa.f[2] != f || f != 3)
+        return false;
+#define IFGF_C2F_CASE(A, B, C, D, E, G)                                                       \
+    if (h[0] == A && h[1] == B && h[2] == C && l[0] == D && l[1] == E && l[2] == G)            \
+    {                                                                                          \
+        constexpr size_t sm = c2f_fixed_smem<A, B, C, D, E, G, 3, T>();                        \
+        auto kern = coarse_to_fine_fixed_kernel<A, B, C, D, E, G, 3, T>;                       \
+        if (sm > 48 * 1024)                                                                    \
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);  \
+        kern<<<grid, 256, sm, st>>>(fa);                                                       \
+        return true;                                                                           \
+    }
+    IFGF_C2F_CASE(5, 8, 8, 2, 5, 5)
+    IFGF_C2F_CASE(6, 9, 9, 3, 6, 6)
+    IFGF_C2F_CASE(7, 10, 10, 4, 7, 7)
+#undef IFGF_C2F_CASE
+    return false;
+}
+
+// Mixed-precision target leaf evaluation: near-field terms in FP32 on
+// coordinates relative to the leaf's first target, far-field Chebyshev sums
+// in FP32, every contribution accumulated in FP64.
+template <int KIND, int N0, int N1, int N2>
+__global__ void __launch_bounds__(EVAL_THREADS) target_eval_mixed_kernel(EvalArgs a)
+{
+    using P = PluginF<KIND>;
+    // kernels with normals stage FP64 coordinates (see PluginF::kernel_d)
+    using CT = typename std::conditional<P::needs_normals, double, float>::type;
+    __shared__ CT xs[EVAL_THREADS], ys[EVAL_THREADS], zs[EVAL_THREADS];
+    __shared__ float wr[EVAL_THREADS], wi[EVAL_THREADS];
+    __shared__ double n0[P::needs_normals ? EVAL_THREADS : 1], n1[P::needs_normals ? EVAL_THREADS : 1],
+        n2[P::needs_normals ? EVAL_THREADS : 1];
+    __shared__ double rr[EVAL_THREADS], ri[EVAL_THREADS];
+    const float2* wf = reinterpret_cast<const float2*>(a.w);
+    const float2* fcf = reinterpret_cast<const float2*>(a.fcoef);
+    const int tl = blockIdx.x;
+    const int tf = a.tl_first[tl], tlast = a.tl_last[tl];
+    const double r0 = a.tx[tf], r1 = a.ty[tf], r2 = a.tz[tf]; // local origin
+    const long long nb0 = a.near_off[tl], nb1 = a.near_off[tl + 1];
+    const long long fb0 = a.far_off[tl], fb1 = a.far_off[tl + 1];
+    for (int base = tf; base < tlast; base += EVAL_THREADS)
+    {
+        const int cnt = min(EVAL_THREADS, tlast - base);
+        const int S = EVAL_THREADS / cnt;
+        const int ti = threadIdx.x % cnt, si = threadIdx.x / cnt;
+        const bool active = si < S;
+        const int t = base + ti;
+        const double y0 = a.tx[t], y1 = a.ty[t], y2 = a.tz[t];
+        const float yl0 = (float)(y0 - r0), yl1 = (float)(y1 - r1), yl2 = (float)(y2 - r2);
+        double accr = 0, acci = 0;
+        for (long long e = nb0; e < nb1; e++)
+        {
+            const int sb = a.near_src[e];
+            const int sf = a.T.box_first[sb], sl = a.T.box_last[sb];
+            for (int cs = sf; cs < sl; cs += EVAL_THREADS)
+            {
+                const int ccnt = min(EVAL_THREADS, sl - cs);
+                __syncthreads();
+                if (threadIdx.x < ccnt)
+                {
+                    const int i = cs + threadIdx.x;
+                    xs[threadIdx.x] = (CT)(a.S.sx[i] - r0);
+                    ys[threadIdx.x] = (CT)(a.S.sy[i] - r1);
+                    zs[threadIdx.x] = (CT)(a.S.sz[i] - r2);
+                    const float2 wv = wf[i];
+                    wr[threadIdx.x] = wv.x;
+                    wi[threadIdx.x] = wv.y;
+                    if (P::needs_normals)
+                    {
+                        n0[threadIdx.x] = a.S.nx[i];
+                        n1[threadIdx.x] = a.S.ny[i];
+                        n2[threadIdx.x] = a.S.nz[i];
+                    }
+                }
+                __syncthreads();
+                if (active)
+                {
+                    cplx<float> acc = {0.f, 0.f};
+                    if constexpr (P::needs_normals)
+                    {
+                        const double yd0 = y0 - r0, yd1 = y1 - r1, yd2 = y2 - r2;
+                        for (int i = si; i < ccnt; i += S)
+                        {
+                            const double x[3] = {xs[i] - yd0, ys[i] - yd1, zs[i] - yd2};
+                            const double nv[3] = {n0[i], n1[i], n2[i]};
+                            cfmaf(acc, cplx<float>{wr[i], wi[i]}, P::kernel_d(x, nv, a.kp));
+                        }
+                    }
+                    else
+                    {
+                        for (int i = si; i < ccnt; i += S)
+                        {
+                            const float x[3] = {xs[i] - yl0, ys[i] - yl1, zs[i] - yl2};
+                            cfmaf(acc, cplx<float>{wr[i], wi[i]}, P::kernel(x, nullptr, a.kp));
+                        }
+                    }
+                    accr += acc.re;
+                    acci += acc.im;
+                }
+            }
+        }
+        if (active)
+            for (long long e = fb0 + si; e < fb1; e += S)
+            {
+                const int sb = a.far_src[e];
+                const LevelGeom& G = a.lv[a.T.box_level[sb]];
+                const double p[3] = {y0 - a.T.box_c[3 * sb], y1 - a.T.box_c[3 * sb + 1],
+                                     y2 - a.T.box_c[3 * sb + 2]};
+                const long long nft = (long long)G.nf[0] * G.nf[1] * G.nf[2];
+                const int* fm = a.fmap + G.fmap_off + (long long)(sb - G.box_off) * nft;
+                float loc[3];
+                const int gf = fine_lookup_mixed(G, fm, p, a.T.box_H[sb], loc, a.err);
+                if (gf < 0)
+                    continue;
+                const cplx<float> v = ChebF<N0, N1, N2>::eval(fcf + (size_t)gf * a.P_lo, loc, a.lo);
+                const cplx<float> cf = cf_mixed<KIND>(p[0] * p[0] + p[1] * p[1] + p[2] * p[2], a.kp);
+                accr += (double)(v.re * cf.re - v.im * cf.im);
+                acci += (double)(v.re * cf.im + v.im * cf.re);
+            }
+        __syncthreads();
+        rr[threadIdx.x] = accr;
+        ri[threadIdx.x] = acci;
+        __syncthreads();
+        if (active && si == 0)
+        {
+            double sr = 0, sim = 0;
+            for (int s = 0; s < S; s++)
+            {
+                sr += rr[ti + s * cnt];
+                sim += ri[ti + s * cnt];
+            }
+            const long long o = a.tgt_perm[t];
+            if (a.real_out)
+                a.out[o] = sr;
+            else
+            {
+                a.out[2 * o] = sr;
+                a.out[2 * o + 1] = sim;
+            }
+        }
+    }
+}
+
+#define IFGF_CHECK_LAUNCH()                                                                   \
+    do                                                                                         \
+    {                                                                                          \
+        cudaError_t e_ = cudaGetLastError();                                                   \
+        if (e_ != cudaSuccess)                                                                 \
+            throw Error(2, std::string("kernel launch: ") + cudaGetErrorString(e_));          \
+    } while (0)
+
+// threads of a node CTA (NPT nodes per thread, a multiple of 32, at most
+// NODE_THREADS) and the number of node chunks (grid.y) covering P_hi nodes
+inline int node_threads(int P_hi)
+{
+    int t = (P_hi + NPT - 1) / NPT;
+    t = (t + 31) / 32 * 32;
+    return t < 32 ? 32 : (t > NODE_THREADS ? NODE_THREADS : t);
+}
+inline int node_chunks(int P_hi)
+{
+    const int per = NPT * node_threads(P_hi);
+    return (P_hi + per - 1) / per;
+}
+
+template <int KIND, int N0, int N1, int N2, bool MIXED>
+static int run_mult(const MultPtrs& m, const void* d_w, void* d_u, bool real, cudaStream_t st,
+                    LaunchHooks* hk)
+{
+    int launches = 0;
+    const size_t c2f_smem = MIXED ? m.c2f_smem / 2 : m.c2f_smem;
+    if (c2f_smem > 48 * 1024)
+    {
+        const cudaError_t e = MIXED ? cudaFuncSetAttribute(coarse_to_fine_mixed_kernel,
+                                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                           (int)c2f_smem)
+                                    : cudaFuncSetAttribute(coarse_to_fine_kernel,
+                                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                           (int)c2f_smem);
+        if (e != cudaSuccess)
+            throw Error(2, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
+    }
+    {
+        const int thr = 256;
+        const int blocks = (int)std::min<long long>((m.n_src + thr - 1) / thr, 148 * 16);
+        if (hk)
+            hk->begin(PROF_PERMUTE);
+        if (MIXED)
+            permute_weights_mixed_kernel<<<blocks, thr, 0, st>>>(
+                (const double*)d_w, real ? 1 : 0, m.src_perm, reinterpret_cast<float2*>(m.w), m.n_src);
+        else
+            permute_weights_kernel<<<blocks, thr, 0, st>>>((const double*)d_w, real ? 1 : 0,
+                                                           m.src_perm, m.w, m.n_src);
+        IFGF_CHECK_LAUNCH();
+        if (hk)
+            hk->end();
+        launches++;
+    }
+    const int nthr = node_threads(m.P_hi);
+    const int nchk = node_chunks(m.P_hi);
+    for (int l = m.L - 1; l >= 0; l--)
+    {
+        const LevelGeom& G = m.lv_host[l];
+        if (G.n_coarse == 0)
+            continue;
+        const LevelLists& LL = m.lists[l];
+        if (LL.n_leaf > 0)
+        {
+            LeafArgs la{G, m.T, m.S, LL.cc_box, LL.cc_el, LL.leaf_idx, m.hi_nodes, m.w, m.cvals,
+                        m.P_hi, m.kp};
+            if (hk)
+                hk->begin(PROF_COARSE);
+            if (MIXED)
+                leaf_sample_mixed_kernel<KIND>
+                    <<<dim3(LL.n_leaf, nchk), nthr, 9 * nthr * sizeof(float), st>>>(la);
+            else
+                leaf_sample_kernel<KIND>
+                    <<<dim3(LL.n_leaf, nchk), nthr, 8 * nthr * sizeof(double), st>>>(la);
+            IFGF_CHECK_LAUNCH();
+            if (hk)
+                hk->end();
+            launches++;
+        }
+        if (LL.n_up > 0)
+        {
+            UpArgs ua;
+            ua.G = G;
+            ua.GC = l + 1 < m.L ? m.lv_host[l + 1] : G;
+            ua.T = m.T;
+            ua.cc_box = LL.cc_box;
+            ua.cc_el = LL.cc_el;
+            ua.idx = LL.up_idx;
+            ua.slot = LL.up_slot;
+            ua.geo64 = LL.geo64;
+            ua.geo32 = LL.geo32;
+            ua.hi_nodes = m.hi_nodes;
+            ua.fmap = m.fmap;
+            ua.fcoef = m.fcoef;
+            ua.cvals = m.cvals;
+            ua.err = m.err;
+            ua.P_hi = m.P_hi;
+            ua.P_lo = m.P_lo;
+            for (int d = 0; d < 3; d++)
+                ua.lo[d] = m.lo[d];
+            ua.kp = m.kp;
+            if (hk)
+                hk->begin(PROF_UPWARD);
+            if (MIXED)
+                upward_mixed_kernel<KIND, N0, N1, N2>
+                    <<<LL.n_up, NODE_THREADS, m.P_hi * sizeof(float2), st>>>(ua);
+            else
+                upward_kernel<KIND, N0, N1, N2>
+                    <<<LL.n_up, NODE_THREADS, m.P_hi * sizeof(double2), st>>>(ua);
+            IFGF_CHECK_LAUNCH();
+            if (hk)
+                hk->end();
+            launches++;
+        }
+        C2FArgs fa;
+        fa.G = G;
+        fa.cc_box = LL.cc_box;
+        fa.cc_el = LL.cc_el;
+        fa.cvals = m.cvals;
+        fa.A = m.A;
+        fa.fmap = m.fmap;
+        fa.fcoef = m.fcoef;
+        for (int d = 0; d < 3; d++)
+        {
+            fa.hi[d] = m.hi[d];
+            fa.lo[d] = m.lo[d];
+            fa.f[d] = m.fct[d];
+        }
+        fa.P_hi = m.P_hi;
+        fa.P_lo = m.P_lo;
+        if (hk)
+            hk->begin(PROF_C2F);
+        if (launch_c2f_fixed<typename std::conditional<MIXED, float, double>::type>(
+                fa, (unsigned)G.n_coarse, st))
+        {
+        }
+        else if (MIXED)
+            coarse_to_fine_mixed_kernel<<<(unsigned)G.n_coarse, 256, c2f_smem, st>>>(fa);
+        else
+            coarse_to_fine_kernel<<<(unsigned)G.n_coarse, 256, c2f_smem, st>>>(fa);
+        IFGF_CHECK_LAUNCH();
+        if (hk)
+            hk->end();
+        launches++;
+    }
+    if (m.n_tleaf > 0)
+    {
+        EvalArgs ea;
+        ea.lv = m.lv_dev;
+        ea.T = m.T;
+        ea.S = m.S;
+        ea.tx = m.tx;
+        ea.ty = m.ty;
+        ea.tz = m.tz;
+        ea.tgt_perm = m.tgt_perm;
+        ea.tl_first = m.tl_first;
+        ea.tl_last = m.tl_last;
+        ea.far_off = m.tl_far_off;
+        ea.far_src = m.tl_far_src;
+        ea.near_off = m.tl_near_off;
+        ea.near_src = m.tl_near_src;
+        ea.w = m.w;
+        ea.fmap = m.fmap;
+        ea.fcoef = m.fcoef;
+        ea.out = (double*)d_u;
+        ea.real_out = real ? 1 : 0;
+        ea.err = m.err;
+        ea.P_lo = m.P_lo;
+        for (int d = 0; d < 3; d++)
+            ea.lo[d] = m.lo[d];
+        ea.kp = m.kp;
+        if (hk)
+            hk->begin(PROF_EVAL);
+        if (MIXED)
+            target_eval_mixed_kernel<KIND, N0, N1, N2><<<m.n_tleaf, EVAL_THREADS, 0, st>>>(ea);
+        else
+            target_eval_kernel<KIND, N0, N1, N2><<<m.n_tleaf, EVAL_THREADS, 0, st>>>(ea);
+        IFGF_CHECK_LAUNCH();
+        if (hk)
+            hk->end();
+        launches++;
+    }
+    return launches;
+}
+
+template <int KIND>
+int launch_mult_kernels(const MultPtrs& m, const void* d_w, void* d_u, bool real, cudaStream_t st,
+                        LaunchHooks* hk)
+{
+    const int* lo = m.lo;
+#define IFGF_RUN(A, B, C)                                                                     \
+    return m.mixed ? run_mult<KIND, A, B, C, true>(m, d_w, d_u, real, st, hk)                  \
+                   : run_mult<KIND, A, B, C, false>(m, d_w, d_u, real, st, hk)
+    if (lo[0] == 2 && lo[1] == 5 && lo[2] == 5)
+        IFGF_RUN(2, 5, 5);
+    if (lo[0] == 3 && lo[1] == 6 && lo[2] == 6)
+        IFGF_RUN(3, 6, 6);
+    if (lo[0] == 4 && lo[1] == 7 && lo[2] == 7)
+        IFGF_RUN(4, 7, 7);
+    IFGF_RUN(0, 0, 0);
+#undef IFGF_RUN
+}
+
+template <int KIND>
+void permute_only(const MultPtrs& m, const void* d_w, bool real, cudaStream_t st)
+{
+    const int thr = 256;
+    const int blocks = (int)std::min<long long>((m.n_src + thr - 1) / thr, 148 * 16);
+    permute_weights_kernel<<<blocks, thr, 0, st>>>((const double*)d_w, real ? 1 : 0, m.src_perm,
+                                                   m.w, m.n_src);
+    IFGF_CHECK_LAUNCH();
+}
+
+template <int KIND>
+void launch_direct_kernel(const MultPtrs& m, const int* tpos, int nt, double2* out, cudaStream_t st)
+{
+    direct_eval_kernel<KIND><<<nt, 256, 0, st>>>(m.S, m.w, m.n_src, m.tx, m.ty, m.tz, tpos, m.kp, out);
+    IFGF_CHECK_LAUNCH();
+}
+
+#define IFGF_INSTANTIATE_KIND(K)                                                              \
+    template int launch_mult_kernels<K>(const MultPtrs&, const void*, void*, bool, cudaStream_t, \
+                                        LaunchHooks*);                                         \
+    template void launch_direct_kernel<K>(const MultPtrs&, const int*, int, double2*, cudaStream_t); \
+    template void permute_only<K>(const MultPtrs&, const void*, bool, cudaStream_t);         \
+    template void launch_build_upgeo<K>(const LevelGeom&, const LevelGeom&, double, double,   \
+                                        const double*, const int*, int, const double*, int,     \
+                                        KParams, UpGeo64*, UpGeo32*);
+
+} // namespace ifgf

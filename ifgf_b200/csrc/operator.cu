@@ -1,19 +1,5 @@
-// IFGF operator: device tables and the per-level CUDA pipeline for sm_100a.
-//
-// mult (IfgfOperator::mult, ifgfoperator.hpp:246-867) runs level-synchronously
-// from the deepest source level to the root.  Per level:
-//   coarse_values  -- nodal values of every active coarse cone: leaves sample
-//                     the factored kernel (evaluateFactoredKernel), other
-//                     boxes sum their children's fine interpolants at the
-//                     cone's Chebyshev nodes times the centre-shift factor
-//                     (transferInterp + transfer_factor);
-//   coarse_to_fine -- coarse nodal values -> fine Chebyshev coefficients of the
-//                     active sub-cones (chebtransform, coarseToFine and the
-//                     second chebtransform folded into three small matrices).
-// Then one target_eval launch per target leaf adds the near field (direct
-// sums over neighbouring source leaves) and the far field (fine interpolants
-// of every admissible source box times the centred factor CF) and writes the
-// result in the caller's order.
+// IFGF operator: init (host planner + GPU active-cone tables) and the host side
+// of mult.  The matvec kernels themselves are in mult_kernels.cuh.
 #include <cub/device/device_scan.cuh>
 
 #include <algorithm>
@@ -23,12 +9,25 @@
 #include <sstream>
 
 #include "device_math.cuh"
+#include "mult.hpp"
 #include "operator.hpp"
 
 namespace ifgf
 {
 
 static constexpr int ERR_INVALID = 1, ERR_CUDA = 2, ERR_STATE = 3, ERR_OOM = 4;
+
+// Calls CALL with the compile-time kernel kind KK matching KINDVAR.
+#define IFGF_DISPATCH(KINDVAR, CALL)                                                          \
+    switch (KINDVAR)                                                                           \
+    {                                                                                          \
+    case K_LAPLACE: { constexpr int KK = K_LAPLACE; CALL; } break;                            \
+    case K_HELMHOLTZ: { constexpr int KK = K_HELMHOLTZ; CALL; } break;                        \
+    case K_MODHELMHOLTZ: { constexpr int KK = K_MODHELMHOLTZ; CALL; } break;                  \
+    case K_GRADHELMHOLTZ: { constexpr int KK = K_GRADHELMHOLTZ; CALL; } break;                \
+    case K_DOUBLELAYER: { constexpr int KK = K_DOUBLELAYER; CALL; } break;                    \
+    case K_COMBINEDFIELD: { constexpr int KK = K_COMBINEDFIELD; CALL; } break;                \
+    }
 
 #define IFGF_CUDA(x)                                                                          \
     do                                                                                         \
@@ -96,6 +95,10 @@ struct DeviceState
     DevBuf<double> sx, sy, sz, nx, ny, nz, tx, ty, tz;
     DevBuf<long long> src_perm, tgt_perm;
     std::vector<DevBuf<int>> cc_box, cc_el, fc_box, fc_el; // per level
+    std::vector<DevBuf<int>> leaf_idx, up_idx, up_slot;    // per level coarse-cone partition
+    std::vector<DevBuf<UpGeo64>> geo64;                    // per level upward geometry
+    std::vector<DevBuf<UpGeo32>> geo32;
+    std::vector<LevelLists> lists;                         // per level views of the above
     DevBuf<int> fmap;
     DevBuf<double> hi_nodes, A;
     DevBuf<int> tl_first, tl_last, tl_far_src, tl_near_src;
@@ -106,36 +109,11 @@ struct DeviceState
     std::vector<cudaEvent_t> prof_ev;
     int n_tleaf = 0;
     size_t c2f_smem = 0;
-    int cv_threads = 0;
     ~DeviceState()
     {
         for (auto& e : prof_ev)
             cudaEventDestroy(e);
     }
-};
-
-// ---------------------------------------------------------------------------
-// Kernel arguments
-// ---------------------------------------------------------------------------
-struct TreeArgs
-{
-    const double* __restrict__ box_c;
-    const double* __restrict__ box_H;
-    const int* __restrict__ box_first;
-    const int* __restrict__ box_last;
-    const int* __restrict__ box_child;
-    const int* __restrict__ box_level;
-    const unsigned char* __restrict__ box_leaf;
-};
-
-struct SrcArgs
-{
-    const double* __restrict__ sx;
-    const double* __restrict__ sy;
-    const double* __restrict__ sz;
-    const double* __restrict__ nx;
-    const double* __restrict__ ny;
-    const double* __restrict__ nz;
 };
 
 // ---------------------------------------------------------------------------
@@ -227,410 +205,6 @@ __global__ void finalize_map_kernel(int* map, const int* __restrict__ idx, long 
         else
         {
             map[i] = -1;
-        }
-    }
-}
-
-// ---------------------------------------------------------------------------
-// mult kernels
-// ---------------------------------------------------------------------------
-__global__ void permute_weights_kernel(const double* __restrict__ in, int real_in,
-                                       const long long* __restrict__ perm, double2* w,
-                                       long long n)
-{
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-         i += (long long)gridDim.x * blockDim.x)
-    {
-        const long long j = perm[i];
-        w[i] = real_in ? make_double2(in[j], 0.0) : reinterpret_cast<const double2*>(in)[j];
-    }
-}
-
-struct CoarseArgs
-{
-    LevelGeom G;  // this level
-    LevelGeom GC; // child level (valid when the level has children)
-    TreeArgs T;
-    SrcArgs S;
-    const int* __restrict__ cc_box;
-    const int* __restrict__ cc_el;
-    const double* __restrict__ hi_nodes;
-    const double2* __restrict__ w;
-    const int* __restrict__ fmap;
-    const double2* __restrict__ fcoef;
-    double2* cvals;
-    unsigned long long* err;
-    int P_hi, P_lo;
-    int lo[3];
-    KParams kp;
-};
-
-constexpr int CV_MAXNPT = 4; // nodes per thread
-
-// Nodal values of one active coarse cone per CTA.
-template <int KIND>
-__global__ void __launch_bounds__(512) coarse_values_kernel(CoarseArgs a)
-{
-    using P = Plugin<KIND>;
-    extern __shared__ double sm[];
-    const int c = blockIdx.x;
-    const int box = a.cc_box[c], el = a.cc_el[c];
-    const double xc[3] = {a.T.box_c[3 * box], a.T.box_c[3 * box + 1], a.T.box_c[3 * box + 2]};
-    const double H = a.T.box_H[box];
-    const bool leaf = a.T.box_leaf[box];
-
-    double y[CV_MAXNPT][3];
-    double dc[CV_MAXNPT];
-    cplx<double> acc[CV_MAXNPT];
-#pragma unroll
-    for (int q = 0; q < CV_MAXNPT; q++)
-    {
-        const int n = threadIdx.x + q * blockDim.x;
-        acc[q] = {0.0, 0.0};
-        dc[q] = 0;
-        y[q][0] = y[q][1] = y[q][2] = 0;
-        if (n < a.P_hi)
-        {
-            const double loc[3] = {a.hi_nodes[3 * n], a.hi_nodes[3 * n + 1], a.hi_nodes[3 * n + 2]};
-            double s[3];
-            from_local(el, loc, a.G.dmin, a.G.hc, a.G.nc, s);
-            interp_to_cart(s, xc, H, y[q]);
-            const double e0 = y[q][0] - xc[0], e1 = y[q][1] - xc[1], e2 = y[q][2] - xc[2];
-            dc[q] = sqrt(e0 * e0 + e1 * e1 + e2 * e2);
-        }
-    }
-
-    if (leaf)
-    {
-        // evaluateFactoredKernel over the leaf's sources, staged in shared memory
-        const int nt = blockDim.x;
-        double* xs = sm;
-        double* ys = xs + nt;
-        double* zs = ys + nt;
-        double* wr = zs + nt;
-        double* wi = wr + nt;
-        double* n0 = wi + nt;
-        double* n1 = n0 + nt;
-        double* n2 = n1 + nt;
-        const int f = a.T.box_first[box], l = a.T.box_last[box];
-        for (int cs = f; cs < l; cs += nt)
-        {
-            const int cnt = min(nt, l - cs);
-            __syncthreads();
-            if (threadIdx.x < cnt)
-            {
-                const int i = cs + threadIdx.x;
-                xs[threadIdx.x] = a.S.sx[i];
-                ys[threadIdx.x] = a.S.sy[i];
-                zs[threadIdx.x] = a.S.sz[i];
-                const double2 wv = a.w[i];
-                wr[threadIdx.x] = wv.x;
-                wi[threadIdx.x] = wv.y;
-                if (P::needs_normals)
-                {
-                    n0[threadIdx.x] = a.S.nx[i];
-                    n1[threadIdx.x] = a.S.ny[i];
-                    n2[threadIdx.x] = a.S.nz[i];
-                }
-            }
-            __syncthreads();
-#pragma unroll
-            for (int q = 0; q < CV_MAXNPT; q++)
-            {
-                const int n = threadIdx.x + q * blockDim.x;
-                if (n >= a.P_hi)
-                    continue;
-                for (int i = 0; i < cnt; i++)
-                {
-                    const double av[3] = {xs[i] - y[q][0], ys[i] - y[q][1], zs[i] - y[q][2]};
-                    const double nv[3] = {P::needs_normals ? n0[i] : 0.0,
-                                          P::needs_normals ? n1[i] : 0.0,
-                                          P::needs_normals ? n2[i] : 0.0};
-                    const cplx<double> v = P::factored(av, nv, {wr[i], wi[i]}, y[q], dc[q], a.kp);
-                    acc[q] = cadd(acc[q], v);
-                }
-            }
-        }
-    }
-    else
-    {
-        // transferInterp from every child's fine interpolant
-        const LevelGeom& C = a.GC;
-        const long long nf = (long long)C.nf[0] * C.nf[1] * C.nf[2];
-        for (int o = 0; o < 8; o++)
-        {
-            const int cb = a.T.box_child[8 * box + o];
-            if (cb < 0)
-                continue;
-            const double cxc[3] = {a.T.box_c[3 * cb], a.T.box_c[3 * cb + 1], a.T.box_c[3 * cb + 2]};
-            const double cH = a.T.box_H[cb];
-            const int* fm = a.fmap + C.fmap_off + (long long)(cb - C.box_off) * nf;
-#pragma unroll
-            for (int q = 0; q < CV_MAXNPT; q++)
-            {
-                const int n = threadIdx.x + q * blockDim.x;
-                if (n >= a.P_hi)
-                    continue;
-                const double p0 = y[q][0] - cxc[0], p1 = y[q][1] - cxc[1], p2 = y[q][2] - cxc[2];
-                double s[3], loc[3];
-                cart_to_interp(p0, p1, p2, cH, s);
-                const int fe = element_for_point(s, C.dmin, C.dmax, C.hf, C.nf);
-                if (fe < 0)
-                    continue;
-                const int gf = fm[fe];
-                if (gf < 0)
-                {
-                    atomicAdd(a.err, 1ull);
-                    continue;
-                }
-                to_local(fe, s, C.dmin, C.hf, C.nf, loc);
-                const cplx<double> v =
-                    cheb_eval3<16>(a.fcoef + (size_t)gf * a.P_lo, loc, a.lo);
-                const double e0 = y[q][0] - xc[0], e1 = y[q][1] - xc[1], e2 = y[q][2] - xc[2];
-                const cplx<double> tf =
-                    P::transfer(p0 * p0 + p1 * p1 + p2 * p2, e0 * e0 + e1 * e1 + e2 * e2, a.kp);
-                acc[q] = cadd(acc[q], cmul(v, tf));
-            }
-        }
-    }
-#pragma unroll
-    for (int q = 0; q < CV_MAXNPT; q++)
-    {
-        const int n = threadIdx.x + q * blockDim.x;
-        if (n < a.P_hi)
-            a.cvals[(size_t)c * a.P_hi + n] = make_double2(acc[q].re, acc[q].im);
-    }
-}
-
-struct C2FArgs
-{
-    LevelGeom G;
-    const int* __restrict__ cc_box;
-    const int* __restrict__ cc_el;
-    const double2* __restrict__ cvals;
-    const double* __restrict__ A; // A0 | A1 | A2, row-major (f_d lo_d) x ho_d
-    const int* __restrict__ fmap;
-    double2* fcoef;
-    int hi[3], lo[3], f[3];
-    int P_hi, P_lo;
-};
-
-// Coarse nodal values -> fine Chebyshev coefficients of the active sub-cones
-// (chebtransform chebinterp.hpp:176-250, coarseToFine ifgfoperator.hpp:1539-1637
-// and the fine chebtransform :1115-1124, composed per dimension).
-__global__ void __launch_bounds__(256) coarse_to_fine_kernel(C2FArgs a)
-{
-    extern __shared__ double2 s2[];
-    const int c = blockIdx.x;
-    const int box = a.cc_box[c], el = a.cc_el[c];
-    const int h0 = a.hi[0], h1 = a.hi[1], h2 = a.hi[2];
-    const int F0 = a.f[0] * a.lo[0], F1 = a.f[1] * a.lo[1];
-    const int sz0 = a.P_hi;
-    const int sz2 = max(F0 * h1 * h2, F0 * F1 * a.lo[2]);
-    double2* B0 = s2;
-    double2* B2 = B0 + sz0;
-    double2* B1 = B2 + sz2;
-    const double* A0 = a.A;
-    const double* A1 = A0 + F0 * h0;
-    const double* A2 = A1 + F1 * h1;
-
-    for (int i = threadIdx.x; i < sz0; i += blockDim.x)
-        B0[i] = a.cvals[(size_t)c * a.P_hi + i];
-    __syncthreads();
-    // mode 0
-    for (int o = threadIdx.x; o < F0 * h1 * h2; o += blockDim.x)
-    {
-        const int i0 = o % F0, r = o / F0; // r = m1 + h1 m2
-        double re = 0, im = 0;
-        for (int m = 0; m < h0; m++)
-        {
-            const double av = A0[i0 * h0 + m];
-            const double2 v = B0[m + h0 * r];
-            re = fma(av, v.x, re);
-            im = fma(av, v.y, im);
-        }
-        B2[o] = make_double2(re, im);
-    }
-    __syncthreads();
-    // mode 1
-    for (int o = threadIdx.x; o < F0 * F1 * h2; o += blockDim.x)
-    {
-        const int i0 = o % F0, r = o / F0;
-        const int i1 = r % F1, m2 = r / F1;
-        double re = 0, im = 0;
-        for (int m = 0; m < h1; m++)
-        {
-            const double av = A1[i1 * h1 + m];
-            const double2 v = B2[i0 + F0 * (m + h1 * m2)];
-            re = fma(av, v.x, re);
-            im = fma(av, v.y, im);
-        }
-        B1[o] = make_double2(re, im);
-    }
-    const int nc0 = a.G.nc[0], nc1 = a.G.nc[1];
-    const int hid0 = el % nc0, hid1 = (el / nc0) % nc1, hid2 = el / (nc0 * nc1);
-    const int nf0 = a.G.nf[0], nf1 = a.G.nf[1];
-    const long long nft = (long long)nf0 * nf1 * a.G.nf[2];
-    const int* fm = a.fmap + a.G.fmap_off + (long long)(box - a.G.box_off) * nft;
-    const int lo0 = a.lo[0], lo1 = a.lo[1], lo2 = a.lo[2];
-    for (int j2 = 0; j2 < a.f[2]; j2++)
-    {
-        __syncthreads();
-        // mode 2, rows j2*lo2 .. j2*lo2+lo2-1
-        for (int o = threadIdx.x; o < F0 * F1 * lo2; o += blockDim.x)
-        {
-            const int i01 = o % (F0 * F1), i2 = o / (F0 * F1);
-            const int row = j2 * lo2 + i2;
-            double re = 0, im = 0;
-            for (int m = 0; m < h2; m++)
-            {
-                const double av = A2[row * h2 + m];
-                const double2 v = B1[i01 + F0 * F1 * m];
-                re = fma(av, v.x, re);
-                im = fma(av, v.y, im);
-            }
-            B2[o] = make_double2(re, im);
-        }
-        __syncthreads();
-        // scatter the f0 x f1 sub-cones of this slice
-        const int nsub = a.f[0] * a.f[1];
-        for (int o = threadIdx.x; o < nsub * a.P_lo; o += blockDim.x)
-        {
-            const int sub = o / a.P_lo, q = o % a.P_lo;
-            const int j0 = sub % a.f[0], j1 = sub / a.f[0];
-            const int fel = ((hid2 * a.f[2] + j2) * nf1 + (hid1 * a.f[1] + j1)) * nf0 +
-                            (hid0 * a.f[0] + j0);
-            const int gf = fm[fel];
-            if (gf < 0)
-                continue;
-            const int i0 = q % lo0, i1 = (q / lo0) % lo1, i2 = q / (lo0 * lo1);
-            a.fcoef[(size_t)gf * a.P_lo + q] =
-                B2[(j0 * lo0 + i0) + F0 * ((j1 * lo1 + i1) + F1 * i2)];
-        }
-    }
-}
-
-struct EvalArgs
-{
-    const LevelGeom* __restrict__ lv;
-    TreeArgs T;
-    SrcArgs S;
-    const double* __restrict__ tx;
-    const double* __restrict__ ty;
-    const double* __restrict__ tz;
-    const long long* __restrict__ tgt_perm;
-    const int* __restrict__ tl_first;
-    const int* __restrict__ tl_last;
-    const long long* __restrict__ far_off;
-    const int* __restrict__ far_src;
-    const long long* __restrict__ near_off;
-    const int* __restrict__ near_src;
-    const double2* __restrict__ w;
-    const int* __restrict__ fmap;
-    const double2* __restrict__ fcoef;
-    double* out; // complex (interleaved) or real for Laplace
-    int real_out;
-    unsigned long long* err;
-    int P_lo;
-    int lo[3];
-    KParams kp;
-};
-
-constexpr int EVAL_THREADS = 128;
-
-// One CTA per target leaf: near field + far field, written in caller order.
-template <int KIND>
-__global__ void __launch_bounds__(EVAL_THREADS) target_eval_kernel(EvalArgs a)
-{
-    using P = Plugin<KIND>;
-    __shared__ double xs[EVAL_THREADS], ys[EVAL_THREADS], zs[EVAL_THREADS];
-    __shared__ double wr[EVAL_THREADS], wi[EVAL_THREADS];
-    __shared__ double n0[P::needs_normals ? EVAL_THREADS : 1], n1[P::needs_normals ? EVAL_THREADS : 1],
-        n2[P::needs_normals ? EVAL_THREADS : 1];
-    const int tl = blockIdx.x;
-    const int tf = a.tl_first[tl], tlast = a.tl_last[tl];
-    const long long nb0 = a.near_off[tl], nb1 = a.near_off[tl + 1];
-    const long long fb0 = a.far_off[tl], fb1 = a.far_off[tl + 1];
-    for (int base = tf; base < tlast; base += EVAL_THREADS)
-    {
-        const int t = base + threadIdx.x;
-        const bool valid = t < tlast;
-        const double y0 = valid ? a.tx[t] : 0.0, y1 = valid ? a.ty[t] : 0.0,
-                     y2 = valid ? a.tz[t] : 0.0;
-        cplx<double> acc = {0.0, 0.0};
-        // near field (evaluateNearField, ifgfoperator.hpp:900-960)
-        for (long long e = nb0; e < nb1; e++)
-        {
-            const int sb = a.near_src[e];
-            const int sf = a.T.box_first[sb], sl = a.T.box_last[sb];
-            for (int cs = sf; cs < sl; cs += EVAL_THREADS)
-            {
-                const int cnt = min(EVAL_THREADS, sl - cs);
-                __syncthreads();
-                if (threadIdx.x < cnt)
-                {
-                    const int i = cs + threadIdx.x;
-                    xs[threadIdx.x] = a.S.sx[i];
-                    ys[threadIdx.x] = a.S.sy[i];
-                    zs[threadIdx.x] = a.S.sz[i];
-                    const double2 wv = a.w[i];
-                    wr[threadIdx.x] = wv.x;
-                    wi[threadIdx.x] = wv.y;
-                    if (P::needs_normals)
-                    {
-                        n0[threadIdx.x] = a.S.nx[i];
-                        n1[threadIdx.x] = a.S.ny[i];
-                        n2[threadIdx.x] = a.S.nz[i];
-                    }
-                }
-                __syncthreads();
-                if (valid)
-                {
-                    for (int i = 0; i < cnt; i++)
-                    {
-                        const double x[3] = {xs[i] - y0, ys[i] - y1, zs[i] - y2};
-                        const double nv[3] = {P::needs_normals ? n0[i] : 0.0,
-                                              P::needs_normals ? n1[i] : 0.0,
-                                              P::needs_normals ? n2[i] : 0.0};
-                        const cplx<double> g = P::kernel(x, nv, a.kp);
-                        cfma(acc, cplx<double>{wr[i], wi[i]}, g);
-                    }
-                }
-            }
-        }
-        // far field (evaluateFarField / evaluateFromInterp, ifgfoperator.hpp:963-1012, 1736-1891)
-        if (valid)
-        {
-            for (long long e = fb0; e < fb1; e++)
-            {
-                const int sb = a.far_src[e];
-                const LevelGeom& G = a.lv[a.T.box_level[sb]];
-                const double p[3] = {y0 - a.T.box_c[3 * sb], y1 - a.T.box_c[3 * sb + 1],
-                                     y2 - a.T.box_c[3 * sb + 2]};
-                double s[3], loc[3];
-                cart_to_interp(p[0], p[1], p[2], a.T.box_H[sb], s);
-                const int fe = element_for_point(s, G.dmin, G.dmax, G.hf, G.nf);
-                if (fe < 0)
-                    continue;
-                const long long nft = (long long)G.nf[0] * G.nf[1] * G.nf[2];
-                const int gf = a.fmap[G.fmap_off + (long long)(sb - G.box_off) * nft + fe];
-                if (gf < 0)
-                {
-                    atomicAdd(a.err, 1ull);
-                    continue;
-                }
-                to_local(fe, s, G.dmin, G.hf, G.nf, loc);
-                const cplx<double> v = cheb_eval3<16>(a.fcoef + (size_t)gf * a.P_lo, loc, a.lo);
-                cfma(acc, v, P::cf(p, a.kp));
-            }
-            const long long o = a.tgt_perm[t];
-            if (a.real_out)
-                a.out[o] = acc.re;
-            else
-            {
-                a.out[2 * o] = acc.re;
-                a.out[2 * o + 1] = acc.im;
-            }
         }
     }
 }
@@ -733,6 +307,10 @@ void Operator::set_precision(int mode)
 {
     if (mode != PREC_FP64 && mode != PREC_MIXED)
         throw Error(ERR_INVALID, "precision must be FP64 (0) or MIXED (1)");
+    // the fine-coefficient buffer changes element type: cones that are never
+    // written (no active coarse parent) must read zero in the new layout
+    if (mode != precision_ && initialized_)
+        dev_->fcoef.zero();
     precision_ = mode;
 }
 
@@ -1042,6 +620,17 @@ void Operator::setup_device(const double* normals)
     D.cc_el.resize(L);
     D.fc_box.resize(L);
     D.fc_el.resize(L);
+    D.leaf_idx.clear();
+    D.up_idx.clear();
+    D.up_slot.clear();
+    D.geo64.clear();
+    D.geo32.clear();
+    D.leaf_idx.resize(L);
+    D.up_idx.resize(L);
+    D.up_slot.resize(L);
+    D.geo64.resize(L);
+    D.geo32.resize(L);
+    std::vector<std::vector<int>> up_host(L);
     int64_t coarse_tot = 0, fine_tot = 0;
     leaf_evals_ = upward_evals_ = 0;
     for (int l = 0; l < L; l++)
@@ -1114,18 +703,25 @@ void Operator::setup_device(const double* normals)
         fine_tot += G.n_fine;
         if (fine_tot > (1ll << 31) - 1)
             throw Error(ERR_OOM, "too many active fine cones");
-        // work counts of the flop model
+        // leaf / non-leaf partition of the coarse cones and the work counts
+        // of the flop model
+        std::vector<int> lidx, uidx;
         if (G.n_coarse > 0)
         {
             std::vector<int> cb(G.n_coarse);
             IFGF_CUDA(cudaMemcpy(cb.data(), D.cc_box[l].p, cb.size() * sizeof(int),
                                  cudaMemcpyDeviceToHost));
-            for (int g : cb)
+            for (int64_t i = 0; i < G.n_coarse; i++)
             {
+                const int g = cb[i];
                 if (bleaf[g])
+                {
+                    lidx.push_back((int)i);
                     leaf_evals_ += (double)P_hi * (bl[g] - bf[g]);
+                }
                 else
                 {
+                    uidx.push_back((int)i);
                     int nch = 0;
                     for (int j = 0; j < 8; j++)
                         nch += bch[8 * g + j] >= 0;
@@ -1133,7 +729,62 @@ void Operator::setup_device(const double* normals)
                 }
             }
         }
+        D.leaf_idx[l].upload(lidx);
+        up_host[l] = std::move(uidx);
     }
+    // Upward transfer: order each level's cones of non-leaf boxes by element
+    // (stable, so boxes stay ordered within an element), give every distinct
+    // element a slot and tabulate the box-independent geometry per slot.
+    for (int l = 0; l + 1 < L; l++)
+    {
+        std::vector<int>& uidx = up_host[l];
+        std::vector<int> slot_of(uidx.size()), slot_el;
+        if (!uidx.empty())
+        {
+            std::vector<int> el(lv_[l].n_coarse);
+            IFGF_CUDA(cudaMemcpy(el.data(), D.cc_el[l].p, el.size() * sizeof(int),
+                                 cudaMemcpyDeviceToHost));
+            std::stable_sort(uidx.begin(), uidx.end(), [&](int a, int b) { return el[a] < el[b]; });
+            for (size_t i = 0; i < uidx.size(); i++)
+            {
+                if (i == 0 || el[uidx[i]] != el[uidx[i - 1]])
+                    slot_el.push_back(el[uidx[i]]);
+                slot_of[i] = (int)slot_el.size() - 1;
+            }
+            // child-centre offsets of a box of this level, as the tree builds them
+            const TreeLevel& TL = S.levels[l];
+            double off[24];
+            for (int o = 0; o < 8; o++)
+                for (int d = 0; d < 3; d++)
+                {
+                    const double mn = TL.bbmin[d], mx = TL.bbmax[d];
+                    const double size = 0.5 * (mx - mn);
+                    const double cmn = mn + size * (double)((o >> d) & 1), cmx = cmn + size;
+                    off[3 * o + d] = (cmx + cmn) / 2.0 - (mx + mn) / 2.0;
+                }
+            DevBuf<double> doff;
+            doff.upload(off, 24);
+            DevBuf<int> dslot_el;
+            dslot_el.upload(slot_el);
+            const size_t n_ent = slot_el.size() * 8 * (size_t)P_hi;
+            D.geo64[l].alloc(n_ent);
+            D.geo32[l].alloc(n_ent);
+            const KParams kp = make_kparams(kr_, ki_, dx_);
+            const double pH = S.levels[l].side, cH = S.levels[l + 1].side;
+            IFGF_DISPATCH(kind_, launch_build_upgeo<KK>(lv_[l], lv_[l + 1], pH, cH, doff.p,
+                                                         dslot_el.p, (int)slot_el.size(),
+                                                         D.hi_nodes.p, P_hi, kp, D.geo64[l].p,
+                                                         D.geo32[l].p));
+            IFGF_CUDA(cudaDeviceSynchronize());
+        }
+        D.up_idx[l].upload(uidx);
+        D.up_slot[l].upload(slot_of);
+    }
+    D.lists.assign(L, LevelLists{});
+    for (int l = 0; l < L; l++)
+        D.lists[l] = LevelLists{D.cc_box[l].p, D.cc_el[l].p, D.leaf_idx[l].p, D.up_idx[l].p,
+                                D.up_slot[l].p, D.geo64[l].p, D.geo32[l].p,
+                                (int)D.leaf_idx[l].n, (int)D.up_idx[l].n};
     n_coarse_total_ = coarse_tot;
     n_fine_total_ = fine_tot;
     D.lv.upload(lv_);
@@ -1146,237 +797,82 @@ void Operator::setup_device(const double* normals)
     D.w.alloc(S.n);
     D.err.alloc(1);
     D.err.zero();
-    // launch shapes
-    const int npt = (P_hi + 511) / 512;
-    D.cv_threads = ((P_hi + npt - 1) / npt + 31) / 32 * 32;
-    if (npt > CV_MAXNPT)
-        throw Error(ERR_INVALID, "interpolation order too high");
     const int F0 = fct_[0] * lo_[0], F1 = fct_[1] * lo_[1];
     const size_t sz2 = std::max<size_t>((size_t)F0 * hi_[1] * hi_[2], (size_t)F0 * F1 * lo_[2]);
     D.c2f_smem = (P_hi + sz2 + (size_t)F0 * F1 * hi_[2]) * sizeof(double2);
     if (D.c2f_smem > 220 * 1024)
         throw Error(ERR_INVALID, "interpolation order too high for the coarse-to-fine kernel");
-    IFGF_CUDA(cudaFuncSetAttribute(coarse_to_fine_kernel,
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)D.c2f_smem));
 }
 
-// FP64 direct sum at selected targets: one CTA per target, Kahan-compensated
-// per-thread partial sums, then a pairwise block reduction.
-template <int KIND>
-__global__ void __launch_bounds__(256) direct_eval_kernel(SrcArgs S, const double2* __restrict__ w,
-                                                          int ns, const double* __restrict__ tx,
-                                                          const double* __restrict__ ty,
-                                                          const double* __restrict__ tz,
-                                                          const int* __restrict__ tpos,
-                                                          KParams kp, double2* out)
-{
-    using P = Plugin<KIND>;
-    __shared__ double sr[256], si[256];
-    const int j = tpos[blockIdx.x];
-    const double y0 = tx[j], y1 = ty[j], y2 = tz[j];
-    double ar = 0, ai = 0, cr = 0, ci = 0;
-    for (int s = threadIdx.x; s < ns; s += blockDim.x)
-    {
-        const double x[3] = {S.sx[s] - y0, S.sy[s] - y1, S.sz[s] - y2};
-        const double nv[3] = {P::needs_normals ? S.nx[s] : 0.0, P::needs_normals ? S.ny[s] : 0.0,
-                              P::needs_normals ? S.nz[s] : 0.0};
-        const cplx<double> g = P::kernel(x, nv, kp);
-        const double2 wv = w[s];
-        const double vr = wv.x * g.re - wv.y * g.im, vi = wv.x * g.im + wv.y * g.re;
-        double yr = vr - cr, tr = ar + yr;
-        cr = (tr - ar) - yr;
-        ar = tr;
-        double yi = vi - ci, ti = ai + yi;
-        ci = (ti - ai) - yi;
-        ai = ti;
-    }
-    sr[threadIdx.x] = ar;
-    si[threadIdx.x] = ai;
-    __syncthreads();
-    for (int h = blockDim.x / 2; h > 0; h >>= 1)
-    {
-        if (threadIdx.x < h)
-        {
-            sr[threadIdx.x] += sr[threadIdx.x + h];
-            si[threadIdx.x] += si[threadIdx.x + h];
-        }
-        __syncthreads();
-    }
-    if (threadIdx.x == 0)
-        out[blockIdx.x] = make_double2(sr[0], si[0]);
-}
-
-enum ProfClass
-{
-    PROF_PERMUTE = 0,
-    PROF_COARSE = 1,
-    PROF_C2F = 2,
-    PROF_EVAL = 3
-};
-
-// Records CUDA events around every launch when profiling is on.
-struct LaunchLog
+// CUDA-event timing of every launch, used when profiling is on.
+struct EventHooks : LaunchHooks
 {
     DeviceState& D;
     cudaStream_t st;
-    bool on;
     std::vector<int> cls;
     int n = 0;
-    void begin(int c)
+    EventHooks(DeviceState& d, cudaStream_t s) : D(d), st(s) {}
+    void begin(int c) override
     {
-        if (!on)
-            return;
-        ensure(n + 1);
-        cls.push_back(c);
-        IFGF_CUDA(cudaEventRecord(D.prof_ev[2 * n], st));
-    }
-    void end()
-    {
-        if (!on)
-            return;
-        IFGF_CUDA(cudaEventRecord(D.prof_ev[2 * n + 1], st));
-        n++;
-    }
-    void ensure(int m)
-    {
-        while ((int)D.prof_ev.size() < 2 * m)
+        while ((int)D.prof_ev.size() < 2 * (n + 1))
         {
             cudaEvent_t e;
             IFGF_CUDA(cudaEventCreate(&e));
             D.prof_ev.push_back(e);
         }
+        cls.push_back(c);
+        IFGF_CUDA(cudaEventRecord(D.prof_ev[2 * n], st));
+    }
+    void end() override
+    {
+        IFGF_CUDA(cudaEventRecord(D.prof_ev[2 * n + 1], st));
+        n++;
     }
 };
 
-template <int KIND>
-static int launch_kernels(DeviceState& D, const std::vector<LevelGeom>& lv, const int* lo,
-                          const int* hi, const int* fct, const KParams& kp, bool real,
-                          const void* d_w, void* d_u, cudaStream_t st, LaunchLog& log)
+void Operator::fill_mult_ptrs(MultPtrs& m) const
 {
-    const int L = (int)lv.size();
-    const int P_hi = hi[0] * hi[1] * hi[2];
-    const int P_lo = lo[0] * lo[1] * lo[2];
-    const int64_t ns = (int64_t)D.w.n;
-    int launches = 0;
-    TreeArgs TA{D.box_c.p, D.box_H.p, D.box_first.p, D.box_last.p, D.box_child.p, D.box_level.p,
-                D.box_leaf.p};
-    SrcArgs SA{D.sx.p, D.sy.p, D.sz.p, D.nx.p, D.ny.p, D.nz.p};
-    {
-        const int thr = 256;
-        const int blocks = (int)std::min<int64_t>((ns + thr - 1) / thr, 148 * 16);
-        log.begin(PROF_PERMUTE);
-        permute_weights_kernel<<<blocks, thr, 0, st>>>((const double*)d_w, real ? 1 : 0,
-                                                       D.src_perm.p, D.w.p, ns);
-        IFGF_CUDA(cudaGetLastError());
-        log.end();
-        launches++;
-    }
-    for (int l = L - 1; l >= 0; l--)
-    {
-        const LevelGeom& G = lv[l];
-        if (G.n_coarse == 0)
-            continue;
-        CoarseArgs ca;
-        ca.G = G;
-        ca.GC = l + 1 < L ? lv[l + 1] : G;
-        ca.T = TA;
-        ca.S = SA;
-        ca.cc_box = D.cc_box[l].p;
-        ca.cc_el = D.cc_el[l].p;
-        ca.hi_nodes = D.hi_nodes.p;
-        ca.w = D.w.p;
-        ca.fmap = D.fmap.p;
-        ca.fcoef = D.fcoef.p;
-        ca.cvals = D.cvals.p;
-        ca.err = D.err.p;
-        ca.P_hi = P_hi;
-        ca.P_lo = P_lo;
-        for (int d = 0; d < 3; d++)
-            ca.lo[d] = lo[d];
-        ca.kp = kp;
-        const int thr = D.cv_threads;
-        const size_t smem = (size_t)8 * thr * sizeof(double);
-        log.begin(PROF_COARSE);
-        coarse_values_kernel<KIND><<<(unsigned)G.n_coarse, thr, smem, st>>>(ca);
-        IFGF_CUDA(cudaGetLastError());
-        log.end();
-        C2FArgs fa;
-        fa.G = G;
-        fa.cc_box = D.cc_box[l].p;
-        fa.cc_el = D.cc_el[l].p;
-        fa.cvals = D.cvals.p;
-        fa.A = D.A.p;
-        fa.fmap = D.fmap.p;
-        fa.fcoef = D.fcoef.p;
-        for (int d = 0; d < 3; d++)
-        {
-            fa.hi[d] = hi[d];
-            fa.lo[d] = lo[d];
-            fa.f[d] = fct[d];
-        }
-        fa.P_hi = P_hi;
-        fa.P_lo = P_lo;
-        log.begin(PROF_C2F);
-        coarse_to_fine_kernel<<<(unsigned)G.n_coarse, 256, D.c2f_smem, st>>>(fa);
-        IFGF_CUDA(cudaGetLastError());
-        log.end();
-        launches += 2;
-    }
-    EvalArgs ea;
-    ea.lv = D.lv.p;
-    ea.T = TA;
-    ea.S = SA;
-    ea.tx = D.tx.p;
-    ea.ty = D.ty.p;
-    ea.tz = D.tz.p;
-    ea.tgt_perm = D.tgt_perm.p;
-    ea.tl_first = D.tl_first.p;
-    ea.tl_last = D.tl_last.p;
-    ea.far_off = D.tl_far_off.p;
-    ea.far_src = D.tl_far_src.p;
-    ea.near_off = D.tl_near_off.p;
-    ea.near_src = D.tl_near_src.p;
-    ea.w = D.w.p;
-    ea.fmap = D.fmap.p;
-    ea.fcoef = D.fcoef.p;
-    ea.out = (double*)d_u;
-    ea.real_out = real ? 1 : 0;
-    ea.err = D.err.p;
-    ea.P_lo = P_lo;
+    const DeviceState& D = *dev_;
+    m.L = (int)lv_.size();
+    m.lv_host = lv_.data();
+    m.lv_dev = D.lv.p;
+    m.lists = D.lists.data();
+    m.T = TreeArgs{D.box_c.p, D.box_H.p, D.box_first.p, D.box_last.p, D.box_child.p,
+                   D.box_level.p, D.box_leaf.p};
+    m.S = SrcArgs{D.sx.p, D.sy.p, D.sz.p, D.nx.p, D.ny.p, D.nz.p};
+    m.tx = D.tx.p;
+    m.ty = D.ty.p;
+    m.tz = D.tz.p;
+    m.src_perm = D.src_perm.p;
+    m.tgt_perm = D.tgt_perm.p;
+    m.hi_nodes = D.hi_nodes.p;
+    m.A = D.A.p;
+    m.fmap = D.fmap.p;
+    m.tl_first = D.tl_first.p;
+    m.tl_last = D.tl_last.p;
+    m.tl_far_off = D.tl_far_off.p;
+    m.tl_far_src = D.tl_far_src.p;
+    m.tl_near_off = D.tl_near_off.p;
+    m.tl_near_src = D.tl_near_src.p;
+    m.n_tleaf = D.n_tleaf;
+    m.n_src = (long long)D.w.n;
+    m.w = D.w.p;
+    m.cvals = D.cvals.p;
+    m.fcoef = D.fcoef.p;
+    m.err = D.err.p;
     for (int d = 0; d < 3; d++)
-        ea.lo[d] = lo[d];
-    ea.kp = kp;
-    if (D.n_tleaf > 0)
     {
-        log.begin(PROF_EVAL);
-        target_eval_kernel<KIND><<<D.n_tleaf, EVAL_THREADS, 0, st>>>(ea);
-        IFGF_CUDA(cudaGetLastError());
-        log.end();
-        launches++;
+        m.lo[d] = lo_[d];
+        m.hi[d] = hi_[d];
+        m.fct[d] = fct_[d];
     }
-    return launches;
+    m.P_lo = lo_[0] * lo_[1] * lo_[2];
+    m.P_hi = hi_[0] * hi_[1] * hi_[2];
+    m.c2f_smem = D.c2f_smem;
+    m.kp = make_kparams(kr_, ki_, dx_);
+    m.mixed = precision_ == PREC_MIXED;
 }
 
-template <int KIND>
-static void launch_direct(DeviceState& D, const KParams& kp, const int* d_tpos, int nt,
-                          double2* d_out)
-{
-    SrcArgs SA{D.sx.p, D.sy.p, D.sz.p, D.nx.p, D.ny.p, D.nz.p};
-    direct_eval_kernel<KIND><<<nt, 256>>>(SA, D.w.p, (int)D.w.n, D.tx.p, D.ty.p, D.tz.p, d_tpos,
-                                          kp, d_out);
-    IFGF_CUDA(cudaGetLastError());
-}
-
-#define IFGF_DISPATCH(KINDVAR, CALL)                                                          \
-    switch (KINDVAR)                                                                           \
-    {                                                                                          \
-    case K_LAPLACE: { constexpr int KK = K_LAPLACE; CALL; } break;                            \
-    case K_HELMHOLTZ: { constexpr int KK = K_HELMHOLTZ; CALL; } break;                        \
-    case K_MODHELMHOLTZ: { constexpr int KK = K_MODHELMHOLTZ; CALL; } break;                  \
-    case K_GRADHELMHOLTZ: { constexpr int KK = K_GRADHELMHOLTZ; CALL; } break;                \
-    case K_DOUBLELAYER: { constexpr int KK = K_DOUBLELAYER; CALL; } break;                    \
-    case K_COMBINEDFIELD: { constexpr int KK = K_COMBINEDFIELD; CALL; } break;                \
-    }
 
 void Operator::launch_mult(const void* d_w, void* d_u, void* stream, bool timed)
 {
@@ -1384,18 +880,20 @@ void Operator::launch_mult(const void* d_w, void* d_u, void* stream, bool timed)
         throw Error(ERR_STATE, "mult called before init");
     if (!d_w || !d_u)
         throw Error(ERR_INVALID, "null density or result buffer");
-    const KParams kp{kr_, ki_, dx_};
     cudaStream_t st = (cudaStream_t)stream;
     DeviceState& D = *dev_;
-    LaunchLog log{D, st, profiling_ || timed};
+    MultPtrs m;
+    fill_mult_ptrs(m);
+    EventHooks log(D, st);
+    const bool on = profiling_ || timed;
     int launches = 0;
-    IFGF_DISPATCH(kind_, launches = launch_kernels<KK>(D, lv_, lo_, hi_, fct_, kp, is_real(), d_w,
-                                                        d_u, st, log));
+    IFGF_DISPATCH(kind_, launches = launch_mult_kernels<KK>(m, d_w, d_u, is_real(), st,
+                                                             on ? &log : nullptr));
     launches_per_mult_ = launches;
-    if (log.on && log.n > 0)
+    if (on && log.n > 0)
     {
         IFGF_CUDA(cudaEventSynchronize(D.prof_ev[2 * log.n - 1]));
-        double cls_ms[NPROF] = {0, 0, 0, 0};
+        double cls_ms[NPROF] = {0, 0, 0, 0, 0};
         for (int i = 0; i < log.n; i++)
         {
             float ms = 0;
@@ -1415,6 +913,7 @@ void Operator::launch_mult(const void* d_w, void* d_u, void* stream, bool timed)
         last_.coarse = cls_ms[PROF_COARSE];
         last_.c2f = cls_ms[PROF_C2F];
         last_.eval = cls_ms[PROF_EVAL];
+        last_.upward = cls_ms[PROF_UPWARD];
         last_.total = tot;
     }
 }
@@ -1502,9 +1001,9 @@ void Operator::mult_device_external_scratch(const void* d_w, void* d_u, void* st
     D.w.p = w;
     D.cvals.p = cv;
     D.fcoef.p = fc;
-    const KParams kp{kr_, ki_, dx_};
-    LaunchLog log{D, st, false}; // no events: this path creates no resources
-    IFGF_DISPATCH(kind_, launch_kernels<KK>(D, lv_, lo_, hi_, fct_, kp, is_real(), d_w, d_u, st, log));
+    MultPtrs m;
+    fill_mult_ptrs(m); // no hooks: this path creates no events
+    IFGF_DISPATCH(kind_, launch_mult_kernels<KK>(m, d_w, d_u, is_real(), st, nullptr));
 }
 
 void Operator::direct_eval(const void* w, const int64_t* tidx, int64_t nt, void* out)
@@ -1533,19 +1032,14 @@ void Operator::direct_eval(const void* w, const int64_t* tidx, int64_t nt, void*
     if (D.io_w.n < nw)
         D.io_w.alloc(nw);
     IFGF_CUDA(cudaMemcpy(D.io_w.p, w, nw * sizeof(double), cudaMemcpyHostToDevice));
-    {
-        const int64_t ns = (int64_t)D.w.n;
-        const int thr = 256;
-        const int blocks = (int)std::min<int64_t>((ns + thr - 1) / thr, 148 * 16);
-        permute_weights_kernel<<<blocks, thr>>>(D.io_w.p, is_real() ? 1 : 0, D.src_perm.p, D.w.p, ns);
-        IFGF_CUDA(cudaGetLastError());
-    }
     DevBuf<int> dpos;
     dpos.upload(pos);
     DevBuf<double2> dout;
     dout.alloc(nt);
-    const KParams kp{kr_, ki_, dx_};
-    IFGF_DISPATCH(kind_, launch_direct<KK>(D, kp, dpos.p, (int)nt, dout.p));
+    MultPtrs m;
+    fill_mult_ptrs(m);
+    IFGF_DISPATCH(kind_, permute_only<KK>(m, D.io_w.p, is_real(), nullptr);
+                  launch_direct_kernel<KK>(m, dpos.p, (int)nt, dout.p, nullptr));
     std::vector<double2> h(nt);
     IFGF_CUDA(cudaMemcpy(h.data(), dout.p, nt * sizeof(double2), cudaMemcpyDeviceToHost));
     double* o = (double*)out;
@@ -1620,10 +1114,11 @@ std::string Operator::stats_json() const
       << ",\"coarse_cones_total\":" << n_coarse_total_ << ",\"fine_cones_total\":" << n_fine_total_
       << ",\"target_leaves\":" << dev_->n_tleaf << ",\"missing_cone_lookups\":" << missing_
       << ",\"init_ms\":" << init_ms_ << ",\"launches_per_mult\":" << launches_per_mult_
-      << ",\"last_mult_ms\":{\"permute\":" << last_.permute << ",\"coarse_values\":" << last_.coarse
-      << ",\"coarse_to_fine\":" << last_.c2f << ",\"target_eval\":" << last_.eval
-      << ",\"total\":" << last_.total << "},\"profile\":{\"mults\":" << mults_profiled_;
-    const char* names[NPROF] = {"permute", "coarse_values", "coarse_to_fine", "target_eval"};
+      << ",\"last_mult_ms\":{\"permute\":" << last_.permute << ",\"leaf_sample\":" << last_.coarse
+      << ",\"upward\":" << last_.upward << ",\"coarse_to_fine\":" << last_.c2f
+      << ",\"target_eval\":" << last_.eval << ",\"total\":" << last_.total
+      << "},\"profile\":{\"mults\":" << mults_profiled_;
+    const char* names[NPROF] = {"permute", "leaf_sample", "coarse_to_fine", "target_eval", "upward"};
     for (int i = 0; i < NPROF; i++)
         o << ",\"" << names[i] << "\":{\"launches\":" << prof_launches_[i] << ",\"ms\":" << prof_ms_[i]
           << "}";

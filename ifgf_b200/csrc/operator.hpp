@@ -15,10 +15,11 @@ namespace ifgf
 {
 
 struct DeviceState; // device buffers, defined in operator.cu
+struct MultPtrs;    // kernel launch view, defined in mult.hpp
 
 struct StageTimes
 {
-    double permute = 0, coarse = 0, c2f = 0, eval = 0, total = 0;
+    double permute = 0, coarse = 0, c2f = 0, eval = 0, upward = 0, total = 0;
 };
 
 class Operator
@@ -65,6 +66,7 @@ class Operator
     double cutoff_limit(double H) const;
     void setup_device(const double* normals);
     void launch_mult(const void* d_w, void* d_u, void* stream, bool timed);
+    void fill_mult_ptrs(MultPtrs& m) const;
 
     int kind_;
     double kr_, ki_;
@@ -90,9 +92,10 @@ class Operator
     unsigned long long missing_ = 0;
     bool profiling_ = false;
     // per kernel class: launches and accumulated milliseconds
-    static constexpr int NPROF = 4; // permute, coarse_values, coarse_to_fine, target_eval
-    int64_t prof_launches_[NPROF] = {0, 0, 0, 0};
-    double prof_ms_[NPROF] = {0, 0, 0, 0};
+    // permute, leaf_sample, coarse_to_fine, target_eval, upward
+    static constexpr int NPROF = 5;
+    int64_t prof_launches_[NPROF] = {0, 0, 0, 0, 0};
+    double prof_ms_[NPROF] = {0, 0, 0, 0, 0};
     int64_t mults_profiled_ = 0;
     int launches_per_mult_ = 0;
 };

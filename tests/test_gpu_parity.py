@@ -34,6 +34,45 @@ def test_matvec_parity_all_kernels(name):
         assert g.stats()["missing_cone_lookups"] == 0
 
 
+MIXED_TOL = 2e-5  # mixed pipeline vs the FP64 pipeline, relative 2-norm
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", list(KERNELS))
+def test_mixed_precision_matches_fp64(name):
+    n = 6000
+    pts = W.sphere_points(n, seed=0)
+    w = densities_for(name, n)
+    dxs = [-1, 1] if name == "grad_helmholtz" else [-1]
+    for dx in dxs:
+        g = make_gpu_op(name, leaf=50, order=8, dx=dx)
+        init_op(g, name, pts, pts)
+        u64 = g.mult(w)
+        g.set_precision("mixed")
+        u32 = g.mult(w)
+        assert rel2(u32, u64) <= MIXED_TOL, (name, dx, rel2(u32, u64))
+        g.set_precision("fp64")
+        assert rel2(g.mult(w), u64) <= 1e-15  # switching back restores FP64 exactly
+        assert g.stats()["missing_cone_lookups"] == 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,order", [("helmholtz", 10), ("laplace", 12)])
+def test_high_orders(name, order):
+    """p=10: 700 nodes per cone (two node chunks per CTA row); Laplace p=12:
+    1296 nodes and low order (6,9,9) on the runtime-order code path."""
+    n = 3000
+    pts = W.sphere_points(n, seed=0)
+    w = densities_for(name, n)
+    g = make_gpu_op(name, leaf=60, order=order)
+    o = make_oracle_op(name, leaf=60, order=order)
+    g.init(pts, pts)
+    o.init(pts, pts)
+    assert rel2(g.mult(w), o.mult(w)) <= PARITY_TOL
+    g.set_precision("mixed")
+    assert rel2(g.mult(w), o.mult(w)) <= MIXED_TOL
+
+
 @pytest.mark.gpu
 def test_config1_laplace_20k():
     """Plain Laplace, N=20,000 on the unit sphere, leaf 100, p=8 (high (5,8,8),
