@@ -63,17 +63,26 @@ struct LevelLists
     const int* leaf_idx; // coarse cones of leaf boxes (indices into cc_*)
     const int* up_idx;   // coarse cones of boxes with children, ordered by element
     const int* up_slot;  // element slot of each up_idx entry (geometry table row)
-    const UpGeo64* geo64; // [slot][octant][node]
+    const UpGeo64* geo64; // [slot][octant][up_pad entries]
     const UpGeo32* geo32;
     int n_leaf, n_up;
+    int up_pad; // row stride of the geometry tables
 };
 
-// Builds the upward geometry tables of one level (device, FP64).
-// slot_el: element id of each slot; off: 8 child-centre offsets (24 doubles).
+// Upward geometry tables of one level, built on the device in two passes:
+// upgeo_row_max measures every (slot, octant) row's padded length (row_len
+// scratch of 8 n_slots ints) and returns the longest, the row stride P_pad;
+// launch_build_upgeo fills tables pre-set to all-ones bytes (skipped
+// entries).  slot_el: element id of each slot; off: 8 child-centre offsets.
+template <int KIND>
+int upgeo_row_max(const LevelGeom& PG, const LevelGeom& CG, double pH, double cH,
+                  const double* off_dev, const int* slot_el, int n_slots, const double* hi_nodes,
+                  int P_hi, KParams kp, int* row_len_dev, int* row_len_host);
 template <int KIND>
 void launch_build_upgeo(const LevelGeom& PG, const LevelGeom& CG, double pH, double cH,
                         const double* off_dev, const int* slot_el, int n_slots,
-                        const double* hi_nodes, int P_hi, KParams kp, UpGeo64* g64, UpGeo32* g32);
+                        const double* hi_nodes, int P_hi, KParams kp, int P_pad, UpGeo64* g64,
+                        UpGeo32* g32);
 
 // Everything one matvec launch needs (device pointers, sizes, orders).
 struct MultPtrs

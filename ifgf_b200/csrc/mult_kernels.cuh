@@ -220,6 +220,7 @@ struct UpArgs
     const int* __restrict__ slot;
     const UpGeo64* __restrict__ geo64;
     const UpGeo32* __restrict__ geo32;
+    int P_pad;
     const double* __restrict__ hi_nodes;
     const int* __restrict__ fmap;
     const double2* __restrict__ fcoef;
@@ -266,68 +267,31 @@ __device__ __forceinline__ bool upward_fallback64(const UpArgs& a, int box, int 
     return true;
 }
 
-template <int KIND, int N0, int N1, int N2>
-__global__ void __launch_bounds__(NODE_THREADS) upward_kernel(UpArgs a)
-{
-    extern __shared__ double2 acc64[]; // one accumulator per node of the cone
-    const int c = a.idx[blockIdx.x];
-    const int slot = a.slot[blockIdx.x];
-    const int box = a.cc_box[c], el = a.cc_el[c];
-    for (int n = threadIdx.x; n < a.P_hi; n += blockDim.x)
-        acc64[n] = make_double2(0.0, 0.0);
-    const LevelGeom& C = a.GC;
-    const long long nf = (long long)C.nf[0] * C.nf[1] * C.nf[2];
-    for (int o = 0; o < 8; o++)
-    {
-        const int cb = a.T.box_child[8 * box + o];
-        if (cb < 0)
-            continue;
-        __syncthreads(); // every node is updated once per octant
-        const int* fm = a.fmap + C.fmap_off + (long long)(cb - C.box_off) * nf;
-        const UpGeo64* row = a.geo64 + ((size_t)slot * 8 + o) * a.P_hi;
-        for (int i = threadIdx.x; i < a.P_hi; i += blockDim.x)
-        {
-            const UpGeo64& g = row[i];
-            if (g.fe < 0)
-                continue;
-            const int gf = fm[g.fe];
-            cplx<double> v;
-            if (gf < 0)
-            {
-                if (!upward_fallback64<KIND, N0, N1, N2>(a, box, el, g.node, cb, fm, v))
-                    continue;
-            }
-            else
-                v = cmul(Cheb<N0, N1, N2>::eval(a.fcoef + (size_t)gf * a.P_lo, g.loc, a.lo),
-                         cplx<double>{g.tr, g.ti});
-            double2 s = acc64[g.node];
-            s.x += v.re;
-            s.y += v.im;
-            acc64[g.node] = s;
-        }
-    }
-    __syncthreads();
-    for (int n = threadIdx.x; n < a.P_hi; n += blockDim.x)
-        a.cvals[(size_t)c * a.P_hi + n] = acc64[n];
-}
-
 // Builds one level's upward geometry (FP64 values and their FP32 copies):
 // the parent box is centred at the origin, child o at off[o].  One CTA per
-// (slot, octant) row; the row is sorted by child element (then node).
+// (slot, octant) row.  The row lists the nodes that fall inside the child's
+// domain, sorted by child element, each element's run padded with skipped
+// entries to a multiple of UPGEO_RUN so that a group of UPGEO_RUN entries
+// always shares one element.  fill = 0 only measures the padded row length.
+constexpr int UPGEO_RUN = 4;
+
 template <int KIND>
 __global__ void __launch_bounds__(256) build_upgeo_kernel(LevelGeom PG, LevelGeom CG, double pH,
                                                           double cH, const double* __restrict__ off,
                                                           const int* __restrict__ slot_el,
                                                           const double* __restrict__ hi_nodes,
-                                                          int P_hi, KParams kp, UpGeo64* g64,
-                                                          UpGeo32* g32)
+                                                          int P_hi, KParams kp, int fill, int P_pad,
+                                                          int* row_len, UpGeo64* g64, UpGeo32* g32)
 {
     using P = Plugin<KIND>;
-    extern __shared__ int key[]; // sort key per node: element (outside -> last), then node
-    const int slot = blockIdx.x >> 3, o = blockIdx.x & 7;
+    extern __shared__ int sh[]; // key[P_hi] | sorted node[P_hi] | padded position[P_hi]
+    int* key = sh;
+    int* snode = sh + P_hi;
+    int* pos = snode + P_hi;
+    const int row = blockIdx.x;
+    const int slot = row >> 3, o = row & 7;
     const int el = slot_el[slot];
     const double zero[3] = {0.0, 0.0, 0.0};
-    const size_t base = ((size_t)slot * 8 + o) * P_hi;
     for (int n = threadIdx.x; n < P_hi; n += blockDim.x)
     {
         double y[3], s[3];
@@ -340,7 +304,6 @@ __global__ void __launch_bounds__(256) build_upgeo_kernel(LevelGeom PG, LevelGeo
     __syncthreads();
     for (int n = threadIdx.x; n < P_hi; n += blockDim.x)
     {
-        // rank of (key, n) among the row
         const int kn = key[n];
         int rank = 0;
         for (int m = 0; m < P_hi; m++)
@@ -348,24 +311,61 @@ __global__ void __launch_bounds__(256) build_upgeo_kernel(LevelGeom PG, LevelGeo
             const int km = key[m];
             rank += (km < kn) || (km == kn && m < n);
         }
+        snode[rank] = n;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        int off_run = 0, start = 0;
+        for (int i = 0; i <= P_hi; i++)
+        {
+            const bool end = i == P_hi || key[snode[i]] != key[snode[start]];
+            if (end)
+            {
+                if (key[snode[start]] == 0x7fffffff)
+                    break; // the nodes outside the domain sort last and are dropped
+                const int len = i - start;
+                for (int j = 0; j < len; j++)
+                    pos[start + j] = off_run + j;
+                off_run += (len + UPGEO_RUN - 1) / UPGEO_RUN * UPGEO_RUN;
+                start = i;
+            }
+            if (i < P_hi && key[snode[i]] == 0x7fffffff)
+            {
+                for (int j = i; j < P_hi; j++)
+                    pos[j] = -1;
+                break;
+            }
+        }
+        if (!fill)
+            row_len[row] = off_run;
+    }
+    __syncthreads();
+    if (!fill)
+        return;
+    // entry (group g, member r) lives at r * (P_pad / UPGEO_RUN) + g, so the
+    // threads of a warp (consecutive groups) read consecutive entries
+    const size_t base = (size_t)row * P_pad;
+    const int ngroups = P_pad / UPGEO_RUN;
+    for (int i = threadIdx.x; i < P_hi; i += blockDim.x)
+    {
+        if (pos[i] < 0)
+            continue;
+        const size_t at = base + (size_t)(pos[i] % UPGEO_RUN) * ngroups + pos[i] / UPGEO_RUN;
+        const int n = snode[i];
         double y[3], s[3];
         node_position(PG, el, n, hi_nodes, zero, pH, y);
         const double dp2 = y[0] * y[0] + y[1] * y[1] + y[2] * y[2];
         const double p0 = y[0] - off[3 * o], p1 = y[1] - off[3 * o + 1], p2 = y[2] - off[3 * o + 2];
         cart_to_interp(p0, p1, p2, cH, s);
         UpGeo64 g;
-        g.fe = element_for_point(s, CG.dmin, CG.dmax, CG.hf, CG.nf);
+        g.fe = key[n];
         g.node = n;
-        g.loc[0] = g.loc[1] = g.loc[2] = 0.0;
-        g.tr = g.ti = 0.0;
-        if (g.fe >= 0)
-        {
-            to_local(g.fe, s, CG.dmin, CG.hf, CG.nf, g.loc);
-            const cplx<double> tf = P::transfer(p0 * p0 + p1 * p1 + p2 * p2, dp2, kp);
-            g.tr = tf.re;
-            g.ti = tf.im;
-        }
-        g64[base + rank] = g;
+        to_local(g.fe, s, CG.dmin, CG.hf, CG.nf, g.loc);
+        const cplx<double> tf = P::transfer(p0 * p0 + p1 * p1 + p2 * p2, dp2, kp);
+        g.tr = tf.re;
+        g.ti = tf.im;
+        g64[at] = g;
         UpGeo32 h;
         h.fe = g.fe;
         h.node = n;
@@ -375,19 +375,41 @@ __global__ void __launch_bounds__(256) build_upgeo_kernel(LevelGeom PG, LevelGeo
         h.loc[2] = (float)g.loc[2];
         h.tr = (float)g.tr;
         h.ti = (float)g.ti;
-        g32[base + rank] = h;
+        g32[at] = h;
     }
+}
+
+template <int KIND>
+int upgeo_row_max(const LevelGeom& PG, const LevelGeom& CG, double pH, double cH,
+                  const double* off_dev, const int* slot_el, int n_slots, const double* hi_nodes,
+                  int P_hi, KParams kp, int* row_len_dev, int* row_len_host)
+{
+    if (n_slots <= 0)
+        return 0;
+    build_upgeo_kernel<KIND><<<n_slots * 8, 256, 3 * P_hi * sizeof(int)>>>(
+        PG, CG, pH, cH, off_dev, slot_el, hi_nodes, P_hi, kp, 0, 0, row_len_dev, nullptr, nullptr);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess)
+        e = cudaMemcpy(row_len_host, row_len_dev, (size_t)n_slots * 8 * sizeof(int),
+                       cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess)
+        throw Error(2, std::string("build_upgeo_kernel: ") + cudaGetErrorString(e));
+    int mx = 0;
+    for (int i = 0; i < n_slots * 8; i++)
+        mx = row_len_host[i] > mx ? row_len_host[i] : mx;
+    return mx;
 }
 
 template <int KIND>
 void launch_build_upgeo(const LevelGeom& PG, const LevelGeom& CG, double pH, double cH,
                         const double* off_dev, const int* slot_el, int n_slots,
-                        const double* hi_nodes, int P_hi, KParams kp, UpGeo64* g64, UpGeo32* g32)
+                        const double* hi_nodes, int P_hi, KParams kp, int P_pad, UpGeo64* g64,
+                        UpGeo32* g32)
 {
-    if (n_slots <= 0)
+    if (n_slots <= 0 || P_pad <= 0)
         return;
-    build_upgeo_kernel<KIND><<<n_slots * 8, 256, P_hi * sizeof(int)>>>(
-        PG, CG, pH, cH, off_dev, slot_el, hi_nodes, P_hi, kp, g64, g32);
+    build_upgeo_kernel<KIND><<<n_slots * 8, 256, 3 * P_hi * sizeof(int)>>>(
+        PG, CG, pH, cH, off_dev, slot_el, hi_nodes, P_hi, kp, 1, P_pad, nullptr, g64, g32);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess)
         throw Error(2, std::string("build_upgeo_kernel: ") + cudaGetErrorString(e));
@@ -940,10 +962,196 @@ __global__ void __launch_bounds__(NODE_THREADS) leaf_sample_mixed_kernel(LeafArg
     }
 }
 
-template <int KIND, int N0, int N1, int N2>
-__global__ void __launch_bounds__(NODE_THREADS) upward_mixed_kernel(UpArgs a)
+// Chebyshev sums of R points sharing one coefficient block: every coefficient
+// is loaded once and used R times.  N0 = 0 selects the runtime-order path.
+template <typename T> struct VecOf;
+template <> struct VecOf<double>
 {
-    extern __shared__ float2 acc32[]; // one accumulator per node of the cone
+    using type = double2;
+};
+template <> struct VecOf<float>
+{
+    using type = float2;
+};
+
+template <typename T, int N> __device__ __forceinline__ void cheb_basis(T x, T* t)
+{
+    t[0] = T(1);
+    if (N > 1)
+        t[1] = x;
+#pragma unroll
+    for (int i = 2; i < N; i++)
+        t[i] = fma(T(2) * x, t[i - 1], -t[i - 2]);
+}
+
+template <typename T, int N0, int N1, int N2, int R> struct ChebMulti
+{
+    using V = typename VecOf<T>::type;
+    __device__ static __forceinline__ void eval(const V* __restrict__ c, const T (&x)[R][3],
+                                                const int*, T (&ore)[R], T (&oim)[R])
+    {
+        T t0[R][N0], t1[R][N1], t2[R][N2];
+#pragma unroll
+        for (int r = 0; r < R; r++)
+        {
+            cheb_basis<T, N0>(x[r][0], t0[r]);
+            cheb_basis<T, N1>(x[r][1], t1[r]);
+            cheb_basis<T, N2>(x[r][2], t2[r]);
+            ore[r] = oim[r] = T(0);
+        }
+#pragma unroll
+        for (int k = 0; k < N2; k++)
+        {
+            T br[R], bi[R];
+#pragma unroll
+            for (int r = 0; r < R; r++)
+                br[r] = bi[r] = T(0);
+#pragma unroll
+            for (int j = 0; j < N1; j++)
+            {
+                T cr[R], ci[R];
+#pragma unroll
+                for (int r = 0; r < R; r++)
+                    cr[r] = ci[r] = T(0);
+#pragma unroll
+                for (int i = 0; i < N0; i++)
+                {
+                    const V v = __ldg(c + i + N0 * (j + N1 * k));
+#pragma unroll
+                    for (int r = 0; r < R; r++)
+                    {
+                        cr[r] = fma(v.x, t0[r][i], cr[r]);
+                        ci[r] = fma(v.y, t0[r][i], ci[r]);
+                    }
+                }
+#pragma unroll
+                for (int r = 0; r < R; r++)
+                {
+                    br[r] = fma(cr[r], t1[r][j], br[r]);
+                    bi[r] = fma(ci[r], t1[r][j], bi[r]);
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < R; r++)
+            {
+                ore[r] = fma(br[r], t2[r][k], ore[r]);
+                oim[r] = fma(bi[r], t2[r][k], oim[r]);
+            }
+        }
+    }
+};
+
+template <int R> struct ChebMulti<double, 0, 0, 0, R>
+{
+    __device__ static __forceinline__ void eval(const double2* __restrict__ c,
+                                                const double (&x)[R][3], const int* n,
+                                                double (&ore)[R], double (&oim)[R])
+    {
+        for (int r = 0; r < R; r++)
+        {
+            const cplx<double> v = cheb_eval3<16>(c, x[r], n);
+            ore[r] = v.re;
+            oim[r] = v.im;
+        }
+    }
+};
+
+template <int R> struct ChebMulti<float, 0, 0, 0, R>
+{
+    __device__ static __forceinline__ void eval(const float2* __restrict__ c,
+                                                const float (&x)[R][3], const int* n,
+                                                float (&ore)[R], float (&oim)[R])
+    {
+        for (int r = 0; r < R; r++)
+        {
+            const cplx<float> v = ChebF<0, 0, 0>::eval(c, x[r], n);
+            ore[r] = v.re;
+            oim[r] = v.im;
+        }
+    }
+};
+
+constexpr int UP_THREADS = 128;
+
+// One CTA per coarse cone of a box with children (CTAs ordered by cone
+// element, so consecutive CTAs share their geometry-table rows in L2).  For
+// every child, the cone's nodes inside the child's domain come from the
+// level's geometry table in groups of R sharing one child cone: one
+// coefficient gather serves R nodes.  Each node is updated once per child,
+// so the per-node sums in shared memory need no atomics.
+template <int KIND, int N0, int N1, int N2>
+__global__ void __launch_bounds__(UP_THREADS) upward_kernel(UpArgs a)
+{
+    constexpr int R = 2;
+    extern __shared__ double2 acc64[];
+    const int c = a.idx[blockIdx.x];
+    const int slot = a.slot[blockIdx.x];
+    const int box = a.cc_box[c], el = a.cc_el[c];
+    for (int n = threadIdx.x; n < a.P_hi; n += blockDim.x)
+        acc64[n] = make_double2(0.0, 0.0);
+    const LevelGeom& C = a.GC;
+    const long long nf = (long long)C.nf[0] * C.nf[1] * C.nf[2];
+    for (int o = 0; o < 8; o++)
+    {
+        const int cb = a.T.box_child[8 * box + o];
+        if (cb < 0)
+            continue;
+        __syncthreads();
+        const int* fm = a.fmap + C.fmap_off + (long long)(cb - C.box_off) * nf;
+        const UpGeo64* row = a.geo64 + ((size_t)slot * 8 + o) * a.P_pad;
+        const int ngroups = a.P_pad / UPGEO_RUN;
+        // a table group holds UPGEO_RUN entries; FP64 evaluates it as pairs
+        for (int gh = threadIdx.x; gh < ngroups * (UPGEO_RUN / R); gh += blockDim.x)
+        {
+            const int g = gh % ngroups, h = gh / ngroups;
+            UpGeo64 e[R];
+#pragma unroll
+            for (int r = 0; r < R; r++)
+                e[r] = row[(size_t)(h * R + r) * ngroups + g];
+            if (e[0].fe < 0)
+                continue;
+            const int gf = fm[e[0].fe];
+            if (gf < 0)
+            {
+#pragma unroll
+                for (int r = 0; r < R; r++)
+                {
+                    cplx<double> v;
+                    if (e[r].node >= 0 &&
+                        upward_fallback64<KIND, N0, N1, N2>(a, box, el, e[r].node, cb, fm, v))
+                    {
+                        acc64[e[r].node].x += v.re;
+                        acc64[e[r].node].y += v.im;
+                    }
+                }
+                continue;
+            }
+            double x[R][3], vr[R], vi[R];
+#pragma unroll
+            for (int r = 0; r < R; r++)
+                for (int d = 0; d < 3; d++)
+                    x[r][d] = e[r].loc[d];
+            ChebMulti<double, N0, N1, N2, R>::eval(a.fcoef + (size_t)gf * a.P_lo, x, a.lo, vr, vi);
+#pragma unroll
+            for (int r = 0; r < R; r++)
+                if (e[r].node >= 0)
+                {
+                    const double2 s = acc64[e[r].node];
+                    acc64[e[r].node] = make_double2(s.x + (vr[r] * e[r].tr - vi[r] * e[r].ti),
+                                                    s.y + (vr[r] * e[r].ti + vi[r] * e[r].tr));
+                }
+        }
+    }
+    __syncthreads();
+    for (int n = threadIdx.x; n < a.P_hi; n += blockDim.x)
+        a.cvals[(size_t)c * a.P_hi + n] = acc64[n];
+}
+
+template <int KIND, int N0, int N1, int N2>
+__global__ void __launch_bounds__(UP_THREADS) upward_mixed_kernel(UpArgs a)
+{
+    constexpr int R = UPGEO_RUN;
+    extern __shared__ float2 acc32[];
     const int c = a.idx[blockIdx.x];
     const int slot = a.slot[blockIdx.x];
     const int box = a.cc_box[c], el = a.cc_el[c];
@@ -957,41 +1165,61 @@ __global__ void __launch_bounds__(NODE_THREADS) upward_mixed_kernel(UpArgs a)
         const int cb = a.T.box_child[8 * box + o];
         if (cb < 0)
             continue;
-        __syncthreads(); // every node is updated once per octant
+        __syncthreads();
         const int* fm = a.fmap + C.fmap_off + (long long)(cb - C.box_off) * nf;
-        const UpGeo32* row = a.geo32 + ((size_t)slot * 8 + o) * a.P_hi;
-        for (int i = threadIdx.x; i < a.P_hi; i += blockDim.x)
+        const UpGeo32* row = a.geo32 + ((size_t)slot * 8 + o) * a.P_pad;
+        const int ngroups = a.P_pad / R;
+        for (int g = threadIdx.x; g < ngroups; g += blockDim.x)
         {
-            const UpGeo32 g = row[i];
-            if (g.fe < 0)
+            UpGeo32 e[R];
+#pragma unroll
+            for (int r = 0; r < R; r++)
+                e[r] = row[(size_t)r * ngroups + g];
+            if (e[0].fe < 0)
                 continue;
-            const int gf = fm[g.fe];
-            cplx<float> v = {0.f, 0.f};
+            const int gf = fm[e[0].fe];
             if (gf < 0)
             {
                 // tabulated element inactive in this child: absolute coordinates
                 const double xc[3] = {a.T.box_c[3 * box], a.T.box_c[3 * box + 1],
                                       a.T.box_c[3 * box + 2]};
-                double y[3];
-                node_position(a.G, el, g.node, a.hi_nodes, xc, a.T.box_H[box], y);
-                const double p[3] = {y[0] - a.T.box_c[3 * cb], y[1] - a.T.box_c[3 * cb + 1],
-                                     y[2] - a.T.box_c[3 * cb + 2]};
-                float loc[3];
-                const int gf2 = fine_lookup_mixed(C, fm, p, a.T.box_H[cb], loc, a.err);
-                if (gf2 < 0)
-                    continue;
-                const double e0 = y[0] - xc[0], e1 = y[1] - xc[1], e2 = y[2] - xc[2];
-                cfmaf(v, ChebF<N0, N1, N2>::eval(fcf + (size_t)gf2 * a.P_lo, loc, a.lo),
-                      transfer_mixed<KIND>(p[0] * p[0] + p[1] * p[1] + p[2] * p[2],
-                                           e0 * e0 + e1 * e1 + e2 * e2, a.kp));
+#pragma unroll
+                for (int r = 0; r < R; r++)
+                {
+                    if (e[r].node < 0)
+                        continue;
+                    double y[3];
+                    node_position(a.G, el, e[r].node, a.hi_nodes, xc, a.T.box_H[box], y);
+                    const double p[3] = {y[0] - a.T.box_c[3 * cb], y[1] - a.T.box_c[3 * cb + 1],
+                                         y[2] - a.T.box_c[3 * cb + 2]};
+                    float loc[3];
+                    const int gf2 = fine_lookup_mixed(C, fm, p, a.T.box_H[cb], loc, a.err);
+                    if (gf2 < 0)
+                        continue;
+                    const double e0 = y[0] - xc[0], e1 = y[1] - xc[1], e2 = y[2] - xc[2];
+                    cplx<float> v = {0.f, 0.f};
+                    cfmaf(v, ChebF<N0, N1, N2>::eval(fcf + (size_t)gf2 * a.P_lo, loc, a.lo),
+                          transfer_mixed<KIND>(p[0] * p[0] + p[1] * p[1] + p[2] * p[2],
+                                               e0 * e0 + e1 * e1 + e2 * e2, a.kp));
+                    acc32[e[r].node].x += v.re;
+                    acc32[e[r].node].y += v.im;
+                }
+                continue;
             }
-            else
-                cfmaf(v, ChebF<N0, N1, N2>::eval(fcf + (size_t)gf * a.P_lo, g.loc, a.lo),
-                      cplx<float>{g.tr, g.ti});
-            float2 s = acc32[g.node];
-            s.x += v.re;
-            s.y += v.im;
-            acc32[g.node] = s;
+            float x[R][3], vr[R], vi[R];
+#pragma unroll
+            for (int r = 0; r < R; r++)
+                for (int d = 0; d < 3; d++)
+                    x[r][d] = e[r].loc[d];
+            ChebMulti<float, N0, N1, N2, R>::eval(fcf + (size_t)gf * a.P_lo, x, a.lo, vr, vi);
+#pragma unroll
+            for (int r = 0; r < R; r++)
+                if (e[r].node >= 0)
+                {
+                    const float2 s = acc32[e[r].node];
+                    acc32[e[r].node] = make_float2(s.x + (vr[r] * e[r].tr - vi[r] * e[r].ti),
+                                                   s.y + (vr[r] * e[r].ti + vi[r] * e[r].tr));
+                }
         }
     }
     __syncthreads();
@@ -999,6 +1227,7 @@ __global__ void __launch_bounds__(NODE_THREADS) upward_mixed_kernel(UpArgs a)
     for (int n = threadIdx.x; n < a.P_hi; n += blockDim.x)
         cv[(size_t)c * a.P_hi + n] = acc32[n];
 }
+
 
 static __global__ void __launch_bounds__(256) coarse_to_fine_mixed_kernel(C2FArgs a)
 {
@@ -1242,7 +1471,7 @@ static bool launch_c2f_fixed(const C2FArgs& fa, unsigned grid, cudaStream_t st)
 // coordinates relative to the leaf's first target, far-field Chebyshev sums
 // in FP32, every contribution accumulated in FP64.
 template <int KIND, int N0, int N1, int N2>
-__global__ void __launch_bounds__(EVAL_THREADS) target_eval_mixed_kernel(EvalArgs a)
+__global__ void __launch_bounds__(EVAL_THREADS, 6) target_eval_mixed_kernel(EvalArgs a)
 {
     using P = PluginF<KIND>;
     // kernels with normals stage FP64 coordinates (see PluginF::kernel_d)
@@ -1454,6 +1683,7 @@ static int run_mult(const MultPtrs& m, const void* d_w, void* d_u, bool real, cu
             ua.slot = LL.up_slot;
             ua.geo64 = LL.geo64;
             ua.geo32 = LL.geo32;
+            ua.P_pad = LL.up_pad;
             ua.hi_nodes = m.hi_nodes;
             ua.fmap = m.fmap;
             ua.fcoef = m.fcoef;
@@ -1468,10 +1698,10 @@ static int run_mult(const MultPtrs& m, const void* d_w, void* d_u, bool real, cu
                 hk->begin(PROF_UPWARD);
             if (MIXED)
                 upward_mixed_kernel<KIND, N0, N1, N2>
-                    <<<LL.n_up, NODE_THREADS, m.P_hi * sizeof(float2), st>>>(ua);
+                    <<<LL.n_up, UP_THREADS, m.P_hi * sizeof(float2), st>>>(ua);
             else
                 upward_kernel<KIND, N0, N1, N2>
-                    <<<LL.n_up, NODE_THREADS, m.P_hi * sizeof(double2), st>>>(ua);
+                    <<<LL.n_up, UP_THREADS, m.P_hi * sizeof(double2), st>>>(ua);
             IFGF_CHECK_LAUNCH();
             if (hk)
                 hk->end();
@@ -1590,6 +1820,9 @@ void launch_direct_kernel(const MultPtrs& m, const int* tpos, int nt, double2* o
     template void permute_only<K>(const MultPtrs&, const void*, bool, cudaStream_t);         \
     template void launch_build_upgeo<K>(const LevelGeom&, const LevelGeom&, double, double,   \
                                         const double*, const int*, int, const double*, int,     \
-                                        KParams, UpGeo64*, UpGeo32*);
+                                        KParams, int, UpGeo64*, UpGeo32*);                      \
+    template int upgeo_row_max<K>(const LevelGeom&, const LevelGeom&, double, double,         \
+                                  const double*, const int*, int, const double*, int, KParams,  \
+                                  int*, int*);
 
 } // namespace ifgf

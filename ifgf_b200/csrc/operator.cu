@@ -631,6 +631,8 @@ void Operator::setup_device(const double* normals)
     D.geo64.resize(L);
     D.geo32.resize(L);
     std::vector<std::vector<int>> up_host(L);
+    std::vector<int> up_pad(L, 0);
+    upgeo_bytes_ = 0;
     int64_t coarse_tot = 0, fine_tot = 0;
     leaf_evals_ = upward_evals_ = 0;
     for (int l = 0; l < L; l++)
@@ -766,16 +768,28 @@ void Operator::setup_device(const double* normals)
             doff.upload(off, 24);
             DevBuf<int> dslot_el;
             dslot_el.upload(slot_el);
-            const size_t n_ent = slot_el.size() * 8 * (size_t)P_hi;
-            D.geo64[l].alloc(n_ent);
-            D.geo32[l].alloc(n_ent);
             const KParams kp = make_kparams(kr_, ki_, dx_);
             const double pH = S.levels[l].side, cH = S.levels[l + 1].side;
+            const int ns = (int)slot_el.size();
+            DevBuf<int> drow;
+            drow.alloc((size_t)ns * 8);
+            std::vector<int> hrow((size_t)ns * 8);
+            int pad = 0;
+            IFGF_DISPATCH(kind_, pad = upgeo_row_max<KK>(lv_[l], lv_[l + 1], pH, cH, doff.p,
+                                                          dslot_el.p, ns, D.hi_nodes.p, P_hi, kp,
+                                                          drow.p, hrow.data()));
+            up_pad[l] = pad;
+            const size_t n_ent = (size_t)ns * 8 * (size_t)std::max(pad, 1);
+            D.geo64[l].alloc(n_ent);
+            D.geo32[l].alloc(n_ent);
+            // all-ones bytes: element -1 and node -1 mark skipped entries
+            IFGF_CUDA(cudaMemset(D.geo64[l].p, 0xff, n_ent * sizeof(UpGeo64)));
+            IFGF_CUDA(cudaMemset(D.geo32[l].p, 0xff, n_ent * sizeof(UpGeo32)));
             IFGF_DISPATCH(kind_, launch_build_upgeo<KK>(lv_[l], lv_[l + 1], pH, cH, doff.p,
-                                                         dslot_el.p, (int)slot_el.size(),
-                                                         D.hi_nodes.p, P_hi, kp, D.geo64[l].p,
-                                                         D.geo32[l].p));
+                                                         dslot_el.p, ns, D.hi_nodes.p, P_hi, kp,
+                                                         pad, D.geo64[l].p, D.geo32[l].p));
             IFGF_CUDA(cudaDeviceSynchronize());
+            upgeo_bytes_ += (double)n_ent * (sizeof(UpGeo64) + sizeof(UpGeo32));
         }
         D.up_idx[l].upload(uidx);
         D.up_slot[l].upload(slot_of);
@@ -784,7 +798,7 @@ void Operator::setup_device(const double* normals)
     for (int l = 0; l < L; l++)
         D.lists[l] = LevelLists{D.cc_box[l].p, D.cc_el[l].p, D.leaf_idx[l].p, D.up_idx[l].p,
                                 D.up_slot[l].p, D.geo64[l].p, D.geo32[l].p,
-                                (int)D.leaf_idx[l].n, (int)D.up_idx[l].n};
+                                (int)D.leaf_idx[l].n, (int)D.up_idx[l].n, up_pad[l]};
     n_coarse_total_ = coarse_tot;
     n_fine_total_ = fine_tot;
     D.lv.upload(lv_);
@@ -1112,6 +1126,7 @@ std::string Operator::stats_json() const
       << ",\"far_target_evals\":" << plan_.far_target_evals
       << ",\"leaf_factor_evals\":" << leaf_evals_ << ",\"upward_node_evals\":" << upward_evals_
       << ",\"coarse_cones_total\":" << n_coarse_total_ << ",\"fine_cones_total\":" << n_fine_total_
+      << ",\"upward_geometry_bytes\":" << upgeo_bytes_
       << ",\"target_leaves\":" << dev_->n_tleaf << ",\"missing_cone_lookups\":" << missing_
       << ",\"init_ms\":" << init_ms_ << ",\"launches_per_mult\":" << launches_per_mult_
       << ",\"last_mult_ms\":{\"permute\":" << last_.permute << ",\"leaf_sample\":" << last_.coarse

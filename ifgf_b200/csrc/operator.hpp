@@ -89,6 +89,7 @@ class Operator
     StageTimes last_;
     int64_t n_coarse_total_ = 0, n_fine_total_ = 0;
     double leaf_evals_ = 0, upward_evals_ = 0;
+    double upgeo_bytes_ = 0; // device bytes of the upward geometry tables
     unsigned long long missing_ = 0;
     bool profiling_ = false;
     // per kernel class: launches and accumulated milliseconds
