@@ -50,6 +50,8 @@ struct LevelGeom
     double dmax[3];    // interpolation domain max: (smax, pi, pi)
     double hc[3];      // coarse (step 1) element widths
     double hf[3];      // fine (step 0) element widths
+    double hci[3];     // 1 / hc
+    double hfi[3];     // 1 / hf
     int nc[3];         // coarse cones per dimension
     int nf[3];         // fine cones per dimension
     int nbox;          // boxes at this level

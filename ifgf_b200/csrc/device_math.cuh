@@ -104,9 +104,11 @@ __device__ __forceinline__ void interp_to_cart(const double* s, const double* xc
 }
 
 // ConeDomain::elementForPoint (cone_domain.hpp:232-256): element id or -1
-// when the point lies outside the interpolation domain.
+// when the point lies outside the interpolation domain.  hinv = 1 / width:
+// floor((s - min) * hinv) equals the reference's floor((s - min) / h) except
+// within one rounding of an element boundary.
 __device__ __forceinline__ int element_for_point(const double* s, const double* dmin,
-                                                 const double* dmax, const double* h,
+                                                 const double* dmax, const double* hinv,
                                                  const int* n)
 {
     double d2 = 0;
@@ -130,7 +132,7 @@ __device__ __forceinline__ int element_for_point(const double* s, const double* 
 #pragma unroll
     for (int j = 0; j < 3; j++)
     {
-        int q = (int)floor((s[j] - dmin[j]) / h[j]);
+        int q = (int)floor((s[j] - dmin[j]) * hinv[j]);
         q = min(max(q, 0), n[j] - 1);
         id += q * stride;
         stride *= n[j];
@@ -138,9 +140,11 @@ __device__ __forceinline__ int element_for_point(const double* s, const double* 
     return id;
 }
 
-// ConeDomain::transformBackwards (cone_domain.hpp:173-184)
+// ConeDomain::transformBackwards (cone_domain.hpp:173-184), with the division
+// by the half width replaced by a multiplication with 2 / width
 __device__ __forceinline__ void to_local(int el, const double* s, const double* dmin,
-                                         const double* h, const int* n, double* loc)
+                                         const double* h, const double* hinv, const int* n,
+                                         double* loc)
 {
     int i0 = el % n[0];
     int r = el / n[0];
@@ -150,9 +154,9 @@ __device__ __forceinline__ void to_local(int el, const double* s, const double* 
 #pragma unroll
     for (int d = 0; d < 3; d++)
     {
-        const double a = 0.5 * h[d];
+        const double a2 = 2.0 * hinv[d]; // 1 / (h / 2)
         const double b = dmin[d] + ((double)idx[d] + 0.5) * h[d];
-        loc[d] = (s[d] - b) / a;
+        loc[d] = (s[d] - b) * a2;
     }
 }
 
@@ -704,7 +708,7 @@ template <int KIND>
 __device__ __forceinline__ cplx<float> cf_mixed(double d2, const KParams& p)
 {
     const double d = sqrt(d2);
-    const float id = (float)(1.0 / d) * INV4PIF;
+    const float id = rsqrtf((float)d2) * INV4PIF;
     if (KIND == K_LAPLACE)
         return {id, 0.f};
     if (KIND == K_HELMHOLTZ || KIND == K_COMBINEDFIELD)
@@ -720,7 +724,7 @@ template <int KIND>
 __device__ __forceinline__ cplx<float> transfer_mixed(double d2, double dp2, const KParams& p)
 {
     const double d = sqrt(d2), dp = sqrt(dp2);
-    const float ratio = (float)(dp / d);
+    const float ratio = __fdividef((float)dp, (float)d);
     if (KIND == K_LAPLACE)
         return {ratio, 0.f};
     if (KIND == K_HELMHOLTZ || KIND == K_COMBINEDFIELD)

@@ -100,6 +100,7 @@ struct MultPtrs
     const long long* tgt_perm;
     const double* hi_nodes;
     const double* A;
+    const double* A_host; // host copy of A (fixed-order kernels take it by value)
     const int* fmap;
     const int* tl_first;
     const int* tl_last;
@@ -112,7 +113,11 @@ struct MultPtrs
     double2* w;
     double2* cvals;
     double2* fcoef;
+    double2* unear; // near-field sums per sorted target
     unsigned long long* err;
+    // second stream for the near field, which overlaps the level loop
+    cudaStream_t side;
+    cudaEvent_t ev_fork, ev_join;
     int lo[3], hi[3], fct[3];
     int P_lo, P_hi;
     size_t c2f_smem; // for FP64 buffers (half of it in mixed precision)
@@ -126,8 +131,9 @@ enum ProfClass
     PROF_PERMUTE = 0,
     PROF_COARSE = 1, // leaf sampling
     PROF_C2F = 2,
-    PROF_EVAL = 3,
-    PROF_UPWARD = 4
+    PROF_EVAL = 3, // far field (+ the near sums)
+    PROF_UPWARD = 4,
+    PROF_NEAR = 5
 };
 
 struct LaunchHooks

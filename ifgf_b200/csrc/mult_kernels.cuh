@@ -251,7 +251,7 @@ __device__ __forceinline__ bool upward_fallback64(const UpArgs& a, int box, int 
                  p2 = y[2] - a.T.box_c[3 * cb + 2];
     double s[3], loc[3];
     cart_to_interp(p0, p1, p2, a.T.box_H[cb], s);
-    const int fe = element_for_point(s, C.dmin, C.dmax, C.hf, C.nf);
+    const int fe = element_for_point(s, C.dmin, C.dmax, C.hfi, C.nf);
     if (fe < 0)
         return false;
     const int gf = fm[fe];
@@ -260,7 +260,7 @@ __device__ __forceinline__ bool upward_fallback64(const UpArgs& a, int box, int 
         atomicAdd(a.err, 1ull);
         return false;
     }
-    to_local(fe, s, C.dmin, C.hf, C.nf, loc);
+    to_local(fe, s, C.dmin, C.hf, C.hfi, C.nf, loc);
     const cplx<double> v = Cheb<N0, N1, N2>::eval(a.fcoef + (size_t)gf * a.P_lo, loc, a.lo);
     const double e0 = y[0] - xc[0], e1 = y[1] - xc[1], e2 = y[2] - xc[2];
     v_out = cmul(v, P::transfer(p0 * p0 + p1 * p1 + p2 * p2, e0 * e0 + e1 * e1 + e2 * e2, a.kp));
@@ -298,7 +298,7 @@ __global__ void __launch_bounds__(256) build_upgeo_kernel(LevelGeom PG, LevelGeo
         node_position(PG, el, n, hi_nodes, zero, pH, y);
         const double p0 = y[0] - off[3 * o], p1 = y[1] - off[3 * o + 1], p2 = y[2] - off[3 * o + 2];
         cart_to_interp(p0, p1, p2, cH, s);
-        const int fe = element_for_point(s, CG.dmin, CG.dmax, CG.hf, CG.nf);
+        const int fe = element_for_point(s, CG.dmin, CG.dmax, CG.hfi, CG.nf);
         key[n] = fe < 0 ? 0x7fffffff : fe;
     }
     __syncthreads();
@@ -361,7 +361,7 @@ __global__ void __launch_bounds__(256) build_upgeo_kernel(LevelGeom PG, LevelGeo
         UpGeo64 g;
         g.fe = key[n];
         g.node = n;
-        to_local(g.fe, s, CG.dmin, CG.hf, CG.nf, g.loc);
+        to_local(g.fe, s, CG.dmin, CG.hf, CG.hfi, CG.nf, g.loc);
         const cplx<double> tf = P::transfer(p0 * p0 + p1 * p1 + p2 * p2, dp2, kp);
         g.tr = tf.re;
         g.ti = tf.im;
@@ -535,7 +535,8 @@ struct EvalArgs
     const double2* __restrict__ w;
     const int* __restrict__ fmap;
     const double2* __restrict__ fcoef;
-    double* out; // complex (interleaved) or real for Laplace
+    double* out;     // complex (interleaved) or real for Laplace
+    double2* unear;  // near-field sums per sorted target (written by the near pass)
     int real_out;
     unsigned long long* err;
     int P_lo;
@@ -544,11 +545,12 @@ struct EvalArgs
 };
 
 constexpr int EVAL_THREADS = 128;
+constexpr int EVAL_NEAR = 0, EVAL_FAR = 1; // the two passes of target evaluation
 
 // One CTA per target leaf.  A leaf holds fewer targets than threads, so
 // thread (ti, si) takes target ti and every S-th near source / far box
 // (S = threads / targets); the S partial sums are added in a fixed order.
-template <int KIND, int N0, int N1, int N2>
+template <int KIND, int N0, int N1, int N2, int PART>
 __global__ void __launch_bounds__(EVAL_THREADS) target_eval_kernel(EvalArgs a)
 {
     using P = Plugin<KIND>;
@@ -559,8 +561,8 @@ __global__ void __launch_bounds__(EVAL_THREADS) target_eval_kernel(EvalArgs a)
     __shared__ double rr[EVAL_THREADS], ri[EVAL_THREADS];
     const int tl = blockIdx.x;
     const int tf = a.tl_first[tl], tlast = a.tl_last[tl];
-    const long long nb0 = a.near_off[tl], nb1 = a.near_off[tl + 1];
-    const long long fb0 = a.far_off[tl], fb1 = a.far_off[tl + 1];
+    const long long nb0 = a.near_off[tl], nb1 = PART == EVAL_NEAR ? a.near_off[tl + 1] : nb0;
+    const long long fb0 = a.far_off[tl], fb1 = PART == EVAL_FAR ? a.far_off[tl + 1] : fb0;
     for (int base = tf; base < tlast; base += EVAL_THREADS)
     {
         const int cnt = min(EVAL_THREADS, tlast - base);
@@ -615,7 +617,7 @@ __global__ void __launch_bounds__(EVAL_THREADS) target_eval_kernel(EvalArgs a)
                                      y2 - a.T.box_c[3 * sb + 2]};
                 double s[3], loc[3];
                 cart_to_interp(p[0], p[1], p[2], a.T.box_H[sb], s);
-                const int fe = element_for_point(s, G.dmin, G.dmax, G.hf, G.nf);
+                const int fe = element_for_point(s, G.dmin, G.dmax, G.hfi, G.nf);
                 if (fe < 0)
                     continue;
                 const long long nft = (long long)G.nf[0] * G.nf[1] * G.nf[2];
@@ -625,7 +627,7 @@ __global__ void __launch_bounds__(EVAL_THREADS) target_eval_kernel(EvalArgs a)
                     atomicAdd(a.err, 1ull);
                     continue;
                 }
-                to_local(fe, s, G.dmin, G.hf, G.nf, loc);
+                to_local(fe, s, G.dmin, G.hf, G.hfi, G.nf, loc);
                 const cplx<double> v = Cheb<N0, N1, N2>::eval(a.fcoef + (size_t)gf * a.P_lo, loc, a.lo);
                 cfma(acc, v, P::cf(p, a.kp));
             }
@@ -641,13 +643,21 @@ __global__ void __launch_bounds__(EVAL_THREADS) target_eval_kernel(EvalArgs a)
                 sr += rr[ti + s * cnt];
                 sim += ri[ti + s * cnt];
             }
-            const long long o = a.tgt_perm[t];
-            if (a.real_out)
-                a.out[o] = sr;
+            if (PART == EVAL_NEAR)
+                a.unear[t] = make_double2(sr, sim);
             else
             {
-                a.out[2 * o] = sr;
-                a.out[2 * o + 1] = sim;
+                const double2 nr = a.unear[t];
+                sr += nr.x;
+                sim += nr.y;
+                const long long o = a.tgt_perm[t];
+                if (a.real_out)
+                    a.out[o] = sr;
+                else
+                {
+                    a.out[2 * o] = sr;
+                    a.out[2 * o + 1] = sim;
+                }
             }
         }
     }
@@ -810,7 +820,7 @@ __device__ __forceinline__ int fine_lookup_mixed(const LevelGeom& G, const int* 
         {
             const float lo = (float)G.dmin[j], hi = (float)G.dmax[j];
             inside = inside && sf[j] >= lo && sf[j] <= hi;
-            int q = (int)floorf((sf[j] - lo) / (float)G.hf[j]);
+            int q = (int)floorf((sf[j] - lo) * (float)G.hfi[j]);
             q = min(max(q, 0), G.nf[j] - 1);
             id += q * stride;
             stride *= G.nf[j];
@@ -829,15 +839,15 @@ __device__ __forceinline__ int fine_lookup_mixed(const LevelGeom& G, const int* 
 #pragma unroll
         for (int d = 0; d < 3; d++)
         {
-            const float a = 0.5f * (float)G.hf[d];
+            const float a2 = 2.f * (float)G.hfi[d];
             const float b = (float)(G.dmin[d] + ((double)idx[d] + 0.5) * G.hf[d]);
-            loc[d] = (sf[d] - b) / a;
+            loc[d] = (sf[d] - b) * a2;
         }
         return gf;
     }
     double s[3], ld[3];
     cart_to_interp(p[0], p[1], p[2], H, s);
-    fe = element_for_point(s, G.dmin, G.dmax, G.hf, G.nf);
+    fe = element_for_point(s, G.dmin, G.dmax, G.hfi, G.nf);
     if (fe < 0)
         return -1;
     gf = fm[fe];
@@ -846,7 +856,7 @@ __device__ __forceinline__ int fine_lookup_mixed(const LevelGeom& G, const int* 
         atomicAdd(err, 1ull);
         return -1;
     }
-    to_local(fe, s, G.dmin, G.hf, G.nf, ld);
+    to_local(fe, s, G.dmin, G.hf, G.hfi, G.nf, ld);
     loc[0] = (float)ld[0];
     loc[1] = (float)ld[1];
     loc[2] = (float)ld[2];
@@ -1332,101 +1342,140 @@ template <> struct Vec2<float>
     using type = float2;
 };
 
+// The three per-dimension matrices as a kernel parameter: with every loop
+// unrolled, each entry is a compile-time offset into the parameter bank and
+// enters its FMA as a constant operand, so the contraction reads only the
+// data operand from shared memory.
 template <int H0, int H1, int H2, int L0, int L1, int L2, int F, typename T>
-__global__ void __launch_bounds__(256) coarse_to_fine_fixed_kernel(C2FArgs a)
+struct C2FMats
+{
+    T a0[F * L0 * H0];
+    T a1[F * L1 * H1];
+    T a2[F * L2 * H2];
+};
+
+// Row stride of the second intermediate: F0 F1 rounded up so that the rows
+// of consecutive m2 start F0 banks apart (conflict-free stage-2 stores).
+template <int F0, int F1>
+__host__ __device__ constexpr int c2f_row_stride()
+{
+    int s = F0 * F1;
+    while (s % 16 != F0 % 16)
+        s++;
+    return s;
+}
+
+template <int H0, int H1, int H2, int L0, int L1, int L2, int F>
+constexpr int c2f_fixed_threads()
+{
+    return (F * L0 * F * L1 + 31) / 32 * 32;
+}
+
+// Coarse-to-fine with compile-time orders and refinement factor F (the same
+// in every dimension), one coarse cone per block, register-tiled: every
+// thread loads one input vector of a mode product into registers once and
+// produces all output rows that use it.
+//   stage 1 (thread = (m1, m2)):  Y1[i0][m1][m2] = sum_m A0[i0][m] X[m][m1][m2]
+//   stage 2 (thread = (i0, m2)):  Y2[m2][i0 + F0 i1] = sum_m A1[i1][m] Y1[i0][m][m2]
+//   stage 3 (thread = i0 + F0 i1): C[j2 L2 + i2] = sum_m A2[j2 L2 + i2][m] Y2[m][.]
+// Stage 3 writes the coefficients of every active sub-cone straight to
+// global memory.  T is the working precision (double, or float in the mixed
+// pipeline).
+template <int H0, int H1, int H2, int L0, int L1, int L2, int F, typename T>
+__global__ void __launch_bounds__(c2f_fixed_threads<H0, H1, H2, L0, L1, L2, F>())
+    coarse_to_fine_fixed_kernel(C2FArgs a, const C2FMats<H0, H1, H2, L0, L1, L2, F, T> M)
 {
     using V = typename Vec2<T>::type;
-    constexpr int F0 = F * L0, F1 = F * L1, F2 = F * L2;
+    constexpr int F0 = F * L0, F1 = F * L1;
     constexpr int P_HI = H0 * H1 * H2, P_LO = L0 * L1 * L2;
-    constexpr int SZ2 = (F0 * H1 * H2 > F0 * F1 * L2) ? F0 * H1 * H2 : F0 * F1 * L2;
-    constexpr int SZ1 = F0 * F1 * H2;
-    constexpr int NA0 = F0 * H0, NA1 = F1 * H1, NA2 = F2 * H2;
+    constexpr int S2 = c2f_row_stride<F0, F1>();
     extern __shared__ __align__(16) unsigned char c2f_raw[];
-    V* B0 = reinterpret_cast<V*>(c2f_raw);
-    V* B2 = B0 + P_HI;
-    V* B1 = B2 + SZ2;
-    T* A0 = reinterpret_cast<T*>(B1 + SZ1);
-    T* A1 = A0 + NA0;
-    T* A2 = A1 + NA1;
-    __shared__ int gsub[F * F];
+    V* Y1 = reinterpret_cast<V*>(c2f_raw); // [m2][m1][i0], i0 fastest
+    V* Y2 = Y1 + F0 * H1 * H2;             // [m2][S2]
+    __shared__ int gsub[F * F * F];
     const int c = blockIdx.x;
+    const int t = threadIdx.x;
     const int box = a.cc_box[c], el = a.cc_el[c];
-    const V* cv = reinterpret_cast<const V*>(a.cvals) + (size_t)c * P_HI;
-    V* fco = reinterpret_cast<V*>(a.fcoef);
-    for (int i = threadIdx.x; i < NA0 + NA1 + NA2; i += blockDim.x)
-        A0[i] = (T)a.A[i];
-    for (int i = threadIdx.x; i < P_HI; i += blockDim.x)
-        B0[i] = cv[i];
-    __syncthreads();
-    for (int o = threadIdx.x; o < F0 * H1 * H2; o += blockDim.x)
+    if (t < F * F * F)
     {
-        const int i0 = o % F0, r = o / F0;
-        T re = 0, im = 0;
+        const int nc0 = a.G.nc[0], nc1 = a.G.nc[1];
+        const int hid0 = el % nc0, hid1 = (el / nc0) % nc1, hid2 = el / (nc0 * nc1);
+        const int nf0 = a.G.nf[0], nf1 = a.G.nf[1];
+        const long long nft = (long long)nf0 * nf1 * a.G.nf[2];
+        const int* fm = a.fmap + a.G.fmap_off + (long long)(box - a.G.box_off) * nft;
+        const int j0 = t % F, j1 = (t / F) % F, j2 = t / (F * F);
+        gsub[t] = fm[((hid2 * F + j2) * nf1 + (hid1 * F + j1)) * nf0 + (hid0 * F + j0)];
+    }
+    if (t < H1 * H2)
+    {
+        const V* src = reinterpret_cast<const V*>(a.cvals) + (size_t)c * P_HI + H0 * t;
+        V x[H0];
 #pragma unroll
         for (int m = 0; m < H0; m++)
-        {
-            const T av = A0[i0 * H0 + m];
-            const V v = B0[m + H0 * r];
-            re = fma(av, v.x, re);
-            im = fma(av, v.y, im);
-        }
-        B2[o] = V{re, im};
-    }
-    __syncthreads();
-    for (int o = threadIdx.x; o < SZ1; o += blockDim.x)
-    {
-        const int i0 = o % F0, r = o / F0;
-        const int i1 = r % F1, m2 = r / F1;
-        T re = 0, im = 0;
+            x[m] = src[m];
 #pragma unroll
-        for (int m = 0; m < H1; m++)
+        for (int i0 = 0; i0 < F0; i0++)
         {
-            const T av = A1[i1 * H1 + m];
-            const V v = B2[i0 + F0 * (m + H1 * m2)];
-            re = fma(av, v.x, re);
-            im = fma(av, v.y, im);
-        }
-        B1[o] = V{re, im};
-    }
-    const int nc0 = a.G.nc[0], nc1 = a.G.nc[1];
-    const int hid0 = el % nc0, hid1 = (el / nc0) % nc1, hid2 = el / (nc0 * nc1);
-    const int nf0 = a.G.nf[0], nf1 = a.G.nf[1];
-    const long long nft = (long long)nf0 * nf1 * a.G.nf[2];
-    const int* fm = a.fmap + a.G.fmap_off + (long long)(box - a.G.box_off) * nft;
-    for (int j2 = 0; j2 < F; j2++)
-    {
-        __syncthreads();
-        if (threadIdx.x < F * F)
-        {
-            const int j0 = threadIdx.x % F, j1 = threadIdx.x / F;
-            gsub[threadIdx.x] =
-                fm[((hid2 * F + j2) * nf1 + (hid1 * F + j1)) * nf0 + (hid0 * F + j0)];
-        }
-        for (int o = threadIdx.x; o < F0 * F1 * L2; o += blockDim.x)
-        {
-            const int i01 = o % (F0 * F1), i2 = o / (F0 * F1);
-            const int row = j2 * L2 + i2;
             T re = 0, im = 0;
 #pragma unroll
-            for (int m = 0; m < H2; m++)
+            for (int m = 0; m < H0; m++)
             {
-                const T av = A2[row * H2 + m];
-                const V v = B1[i01 + F0 * F1 * m];
-                re = fma(av, v.x, re);
-                im = fma(av, v.y, im);
+                re = fma(M.a0[i0 * H0 + m], x[m].x, re);
+                im = fma(M.a0[i0 * H0 + m], x[m].y, im);
             }
-            B2[o] = V{re, im};
+            Y1[i0 + F0 * t] = V{re, im};
         }
-        __syncthreads();
-        for (int o = threadIdx.x; o < F * F * P_LO; o += blockDim.x)
+    }
+    __syncthreads();
+    if (t < F0 * H2)
+    {
+        const int i0 = t % F0, m2 = t / F0;
+        V x[H1];
+#pragma unroll
+        for (int m = 0; m < H1; m++)
+            x[m] = Y1[i0 + F0 * (m + H1 * m2)];
+#pragma unroll
+        for (int i1 = 0; i1 < F1; i1++)
         {
-            const int sub = o / P_LO, q = o % P_LO;
-            const int gf = gsub[sub];
+            T re = 0, im = 0;
+#pragma unroll
+            for (int m = 0; m < H1; m++)
+            {
+                re = fma(M.a1[i1 * H1 + m], x[m].x, re);
+                im = fma(M.a1[i1 * H1 + m], x[m].y, im);
+            }
+            Y2[i0 + F0 * i1 + S2 * m2] = V{re, im};
+        }
+    }
+    __syncthreads();
+    if (t < F0 * F1)
+    {
+        const int i0f = t % F0, i1f = t / F0;
+        const int j0 = i0f / L0, i0 = i0f % L0, j1 = i1f / L1, i1 = i1f % L1;
+        V x[H2];
+#pragma unroll
+        for (int m = 0; m < H2; m++)
+            x[m] = Y2[t + S2 * m];
+        V* fco = reinterpret_cast<V*>(a.fcoef);
+#pragma unroll
+        for (int j2 = 0; j2 < F; j2++)
+        {
+            const int gf = gsub[j0 + F * (j1 + F * j2)];
             if (gf < 0)
                 continue;
-            const int j0 = sub % F, j1 = sub / F;
-            const int i0 = q % L0, i1 = (q / L0) % L1, i2 = q / (L0 * L1);
-            fco[(size_t)gf * P_LO + q] = B2[(j0 * L0 + i0) + F0 * ((j1 * L1 + i1) + F1 * i2)];
+            V* dst = fco + (size_t)gf * P_LO + i0 + L0 * i1;
+#pragma unroll
+            for (int i2 = 0; i2 < L2; i2++)
+            {
+                T re = 0, im = 0;
+#pragma unroll
+                for (int m = 0; m < H2; m++)
+                {
+                    re = fma(M.a2[(j2 * L2 + i2) * H2 + m], x[m].x, re);
+                    im = fma(M.a2[(j2 * L2 + i2) * H2 + m], x[m].y, im);
+                }
+                dst[L0 * L1 * i2] = V{re, im};
+            }
         }
     }
 }
@@ -1434,30 +1483,35 @@ __global__ void __launch_bounds__(256) coarse_to_fine_fixed_kernel(C2FArgs a)
 template <int H0, int H1, int H2, int L0, int L1, int L2, int F, typename T>
 constexpr size_t c2f_fixed_smem()
 {
-    constexpr int F0 = F * L0, F1 = F * L1, F2 = F * L2;
-    constexpr int SZ2 = (F0 * H1 * H2 > F0 * F1 * L2) ? F0 * H1 * H2 : F0 * F1 * L2;
-    return (size_t)(H0 * H1 * H2 + SZ2 + F0 * F1 * H2) * 2 * sizeof(T) +
-           (size_t)(F0 * H0 + F1 * H1 + F2 * H2) * sizeof(T);
+    constexpr int F0 = F * L0, F1 = F * L1;
+    return (size_t)(F0 * H1 * H2 + c2f_row_stride<F0, F1>() * H2) * 2 * sizeof(T);
 }
 
 // Launches the fixed-size coarse-to-fine kernel when (hi, lo, f) is one of the
 // instantiated shapes; returns false otherwise.
 template <typename T>
-static bool launch_c2f_fixed(const C2FArgs& fa, unsigned grid, cudaStream_t st)
+static bool launch_c2f_fixed(const C2FArgs& fa, const double* A_host, unsigned grid,
+                             cudaStream_t st)
 {
     const int* h = fa.hi;
     const int* l = fa.lo;
     const int f = fa.f[0];
-    if (fa.f[1] != f || fa.f[2] != f || f != 3)
+    if (fa.f[1] != f || fa.f[2] != f || f != 3 || A_host == nullptr)
         return false;
 #define IFGF_C2F_CASE(A, B, C, D, E, G)                                                       \
     if (h[0] == A && h[1] == B && h[2] == C && l[0] == D && l[1] == E && l[2] == G)            \
     {                                                                                          \
+        C2FMats<A, B, C, D, E, G, 3, T> mats;                                                  \
+        T* dst = mats.a0;                                                                      \
+        constexpr int NA = 3 * (D * A + E * B + G * C);                                        \
+        static_assert(sizeof(mats) == NA * sizeof(T), "matrix block layout");                  \
+        for (int i = 0; i < NA; i++)                                                           \
+            dst[i] = (T)A_host[i];                                                             \
         constexpr size_t sm = c2f_fixed_smem<A, B, C, D, E, G, 3, T>();                        \
         auto kern = coarse_to_fine_fixed_kernel<A, B, C, D, E, G, 3, T>;                       \
         if (sm > 48 * 1024)                                                                    \
             cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);  \
-        kern<<<grid, 256, sm, st>>>(fa);                                                       \
+        kern<<<grid, c2f_fixed_threads<A, B, C, D, E, G, 3>(), sm, st>>>(fa, mats);            \
         return true;                                                                           \
     }
     IFGF_C2F_CASE(5, 8, 8, 2, 5, 5)
@@ -1470,7 +1524,7 @@ static bool launch_c2f_fixed(const C2FArgs& fa, unsigned grid, cudaStream_t st)
 // Mixed-precision target leaf evaluation: near-field terms in FP32 on
 // coordinates relative to the leaf's first target, far-field Chebyshev sums
 // in FP32, every contribution accumulated in FP64.
-template <int KIND, int N0, int N1, int N2>
+template <int KIND, int N0, int N1, int N2, int PART>
 __global__ void __launch_bounds__(EVAL_THREADS, 6) target_eval_mixed_kernel(EvalArgs a)
 {
     using P = PluginF<KIND>;
@@ -1486,8 +1540,8 @@ __global__ void __launch_bounds__(EVAL_THREADS, 6) target_eval_mixed_kernel(Eval
     const int tl = blockIdx.x;
     const int tf = a.tl_first[tl], tlast = a.tl_last[tl];
     const double r0 = a.tx[tf], r1 = a.ty[tf], r2 = a.tz[tf]; // local origin
-    const long long nb0 = a.near_off[tl], nb1 = a.near_off[tl + 1];
-    const long long fb0 = a.far_off[tl], fb1 = a.far_off[tl + 1];
+    const long long nb0 = a.near_off[tl], nb1 = PART == EVAL_NEAR ? a.near_off[tl + 1] : nb0;
+    const long long fb0 = a.far_off[tl], fb1 = PART == EVAL_FAR ? a.far_off[tl + 1] : fb0;
     for (int base = tf; base < tlast; base += EVAL_THREADS)
     {
         const int cnt = min(EVAL_THREADS, tlast - base);
@@ -1579,17 +1633,33 @@ __global__ void __launch_bounds__(EVAL_THREADS, 6) target_eval_mixed_kernel(Eval
                 sr += rr[ti + s * cnt];
                 sim += ri[ti + s * cnt];
             }
-            const long long o = a.tgt_perm[t];
-            if (a.real_out)
-                a.out[o] = sr;
+            if (PART == EVAL_NEAR)
+                a.unear[t] = make_double2(sr, sim);
             else
             {
-                a.out[2 * o] = sr;
-                a.out[2 * o + 1] = sim;
+                const double2 nr = a.unear[t];
+                sr += nr.x;
+                sim += nr.y;
+                const long long o = a.tgt_perm[t];
+                if (a.real_out)
+                    a.out[o] = sr;
+                else
+                {
+                    a.out[2 * o] = sr;
+                    a.out[2 * o + 1] = sim;
+                }
             }
         }
     }
 }
+
+#define IFGF_CHECK(x)                                                                         \
+    do                                                                                         \
+    {                                                                                          \
+        cudaError_t e_ = (x);                                                                  \
+        if (e_ != cudaSuccess)                                                                 \
+            throw Error(2, std::string(#x) + ": " + cudaGetErrorString(e_));                   \
+    } while (0)
 
 #define IFGF_CHECK_LAUNCH()                                                                   \
     do                                                                                         \
@@ -1644,6 +1714,57 @@ static int run_mult(const MultPtrs& m, const void* d_w, void* d_u, bool real, cu
         IFGF_CHECK_LAUNCH();
         if (hk)
             hk->end();
+        launches++;
+    }
+    // target evaluation arguments; the near pass needs only the permuted
+    // densities, so without per-kernel timing it runs on the side stream
+    // while the level loop builds the interpolants
+    EvalArgs ea;
+    ea.lv = m.lv_dev;
+    ea.T = m.T;
+    ea.S = m.S;
+    ea.tx = m.tx;
+    ea.ty = m.ty;
+    ea.tz = m.tz;
+    ea.tgt_perm = m.tgt_perm;
+    ea.tl_first = m.tl_first;
+    ea.tl_last = m.tl_last;
+    ea.far_off = m.tl_far_off;
+    ea.far_src = m.tl_far_src;
+    ea.near_off = m.tl_near_off;
+    ea.near_src = m.tl_near_src;
+    ea.w = m.w;
+    ea.fmap = m.fmap;
+    ea.fcoef = m.fcoef;
+    ea.out = (double*)d_u;
+    ea.unear = m.unear;
+    ea.real_out = real ? 1 : 0;
+    ea.err = m.err;
+    ea.P_lo = m.P_lo;
+    for (int d = 0; d < 3; d++)
+        ea.lo[d] = m.lo[d];
+    ea.kp = m.kp;
+    const bool overlap = hk == nullptr && m.side != nullptr;
+    if (m.n_tleaf > 0)
+    {
+        cudaStream_t ns = st;
+        if (overlap)
+        {
+            IFGF_CHECK(cudaEventRecord(m.ev_fork, st));
+            IFGF_CHECK(cudaStreamWaitEvent(m.side, m.ev_fork, 0));
+            ns = m.side;
+        }
+        if (hk)
+            hk->begin(PROF_NEAR);
+        if (MIXED)
+            target_eval_mixed_kernel<KIND, 0, 0, 0, EVAL_NEAR><<<m.n_tleaf, EVAL_THREADS, 0, ns>>>(ea);
+        else
+            target_eval_kernel<KIND, 0, 0, 0, EVAL_NEAR><<<m.n_tleaf, EVAL_THREADS, 0, ns>>>(ea);
+        IFGF_CHECK_LAUNCH();
+        if (hk)
+            hk->end();
+        if (overlap)
+            IFGF_CHECK(cudaEventRecord(m.ev_join, m.side));
         launches++;
     }
     const int nthr = node_threads(m.P_hi);
@@ -1726,7 +1847,7 @@ static int run_mult(const MultPtrs& m, const void* d_w, void* d_u, bool real, cu
         if (hk)
             hk->begin(PROF_C2F);
         if (launch_c2f_fixed<typename std::conditional<MIXED, float, double>::type>(
-                fa, (unsigned)G.n_coarse, st))
+                fa, m.A_host, (unsigned)G.n_coarse, st))
         {
         }
         else if (MIXED)
@@ -1740,36 +1861,14 @@ static int run_mult(const MultPtrs& m, const void* d_w, void* d_u, bool real, cu
     }
     if (m.n_tleaf > 0)
     {
-        EvalArgs ea;
-        ea.lv = m.lv_dev;
-        ea.T = m.T;
-        ea.S = m.S;
-        ea.tx = m.tx;
-        ea.ty = m.ty;
-        ea.tz = m.tz;
-        ea.tgt_perm = m.tgt_perm;
-        ea.tl_first = m.tl_first;
-        ea.tl_last = m.tl_last;
-        ea.far_off = m.tl_far_off;
-        ea.far_src = m.tl_far_src;
-        ea.near_off = m.tl_near_off;
-        ea.near_src = m.tl_near_src;
-        ea.w = m.w;
-        ea.fmap = m.fmap;
-        ea.fcoef = m.fcoef;
-        ea.out = (double*)d_u;
-        ea.real_out = real ? 1 : 0;
-        ea.err = m.err;
-        ea.P_lo = m.P_lo;
-        for (int d = 0; d < 3; d++)
-            ea.lo[d] = m.lo[d];
-        ea.kp = m.kp;
+        if (overlap)
+            IFGF_CHECK(cudaStreamWaitEvent(st, m.ev_join, 0));
         if (hk)
             hk->begin(PROF_EVAL);
         if (MIXED)
-            target_eval_mixed_kernel<KIND, N0, N1, N2><<<m.n_tleaf, EVAL_THREADS, 0, st>>>(ea);
+            target_eval_mixed_kernel<KIND, N0, N1, N2, EVAL_FAR><<<m.n_tleaf, EVAL_THREADS, 0, st>>>(ea);
         else
-            target_eval_kernel<KIND, N0, N1, N2><<<m.n_tleaf, EVAL_THREADS, 0, st>>>(ea);
+            target_eval_kernel<KIND, N0, N1, N2, EVAL_FAR><<<m.n_tleaf, EVAL_THREADS, 0, st>>>(ea);
         IFGF_CHECK_LAUNCH();
         if (hk)
             hk->end();

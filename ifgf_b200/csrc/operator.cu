@@ -101,18 +101,27 @@ struct DeviceState
     std::vector<LevelLists> lists;                         // per level views of the above
     DevBuf<int> fmap;
     DevBuf<double> hi_nodes, A;
+    std::vector<double> A_host; // host copy of A
     DevBuf<int> tl_first, tl_last, tl_far_src, tl_near_src;
     DevBuf<long long> tl_far_off, tl_near_off;
-    DevBuf<double2> w, cvals, fcoef;
+    DevBuf<double2> w, cvals, fcoef, unear;
     DevBuf<unsigned long long> err;
     DevBuf<double> io_w, io_u; // staging for host-buffer mult
     std::vector<cudaEvent_t> prof_ev;
+    cudaStream_t side = nullptr; // near-field stream
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     int n_tleaf = 0;
     size_t c2f_smem = 0;
     ~DeviceState()
     {
         for (auto& e : prof_ev)
             cudaEventDestroy(e);
+        if (ev_fork)
+            cudaEventDestroy(ev_fork);
+        if (ev_join)
+            cudaEventDestroy(ev_join);
+        if (side)
+            cudaStreamDestroy(side);
     }
 };
 
@@ -138,8 +147,8 @@ __global__ void mark_far_kernel(LevelGeom G, TreeArgs T, const int* __restrict__
     {
         double s[3];
         cart_to_interp(tx[t] - xc0, ty[t] - xc1, tz[t] - xc2, H, s);
-        const int fe = element_for_point(s, G.dmin, G.dmax, G.hf, G.nf);
-        const int ce = element_for_point(s, G.dmin, G.dmax, G.hc, G.nc);
+        const int fe = element_for_point(s, G.dmin, G.dmax, G.hfi, G.nf);
+        const int ce = element_for_point(s, G.dmin, G.dmax, G.hci, G.nc);
         if (fe >= 0)
             fmark[G.fmap_off + lb * nf + fe] = 1;
         if (ce >= 0)
@@ -177,8 +186,8 @@ __global__ void mark_parent_kernel(LevelGeom PG, LevelGeom G, TreeArgs T,
             double s2[3];
             cart_to_interp(x[0] - T.box_c[3 * cb], x[1] - T.box_c[3 * cb + 1],
                            x[2] - T.box_c[3 * cb + 2], T.box_H[cb], s2);
-            const int fe = element_for_point(s2, G.dmin, G.dmax, G.hf, G.nf);
-            const int ce = element_for_point(s2, G.dmin, G.dmax, G.hc, G.nc);
+            const int fe = element_for_point(s2, G.dmin, G.dmax, G.hfi, G.nf);
+            const int ce = element_for_point(s2, G.dmin, G.dmax, G.hci, G.nc);
             if (fe >= 0)
                 fmark[G.fmap_off + lb * nf + fe] = 1;
             if (ce >= 0)
@@ -452,6 +461,8 @@ void Operator::init(const double* srcs, int64_t ns, const double* tgts, int64_t 
             G.nc[d] = (int)nc[d];
             G.hf[d] = (G.dmax[d] - G.dmin[d]) / (double)nf[d];
             G.hc[d] = (G.dmax[d] - G.dmin[d]) / (double)nc[d];
+            G.hfi[d] = 1.0 / G.hf[d];
+            G.hci[d] = 1.0 / G.hc[d];
         }
         if (l == 0)
             for (int d = 0; d < 3; d++)
@@ -565,6 +576,7 @@ void Operator::setup_device(const double* normals)
             A.insert(A.end(), m.begin(), m.end());
         }
         D.A.upload(A);
+        D.A_host = A;
     }
     // target leaves
     {
@@ -809,8 +821,15 @@ void Operator::setup_device(const double* normals)
     D.fcoef.alloc((size_t)std::max<int64_t>(fine_tot, 1) * P_lo);
     D.fcoef.zero(); // fine cones without an active coarse parent stay zero
     D.w.alloc(S.n);
+    D.unear.alloc(Tt.n);
     D.err.alloc(1);
     D.err.zero();
+    if (!D.side)
+        IFGF_CUDA(cudaStreamCreateWithFlags(&D.side, cudaStreamNonBlocking));
+    if (!D.ev_fork)
+        IFGF_CUDA(cudaEventCreateWithFlags(&D.ev_fork, cudaEventDisableTiming));
+    if (!D.ev_join)
+        IFGF_CUDA(cudaEventCreateWithFlags(&D.ev_join, cudaEventDisableTiming));
     const int F0 = fct_[0] * lo_[0], F1 = fct_[1] * lo_[1];
     const size_t sz2 = std::max<size_t>((size_t)F0 * hi_[1] * hi_[2], (size_t)F0 * F1 * lo_[2]);
     D.c2f_smem = (P_hi + sz2 + (size_t)F0 * F1 * hi_[2]) * sizeof(double2);
@@ -861,6 +880,7 @@ void Operator::fill_mult_ptrs(MultPtrs& m) const
     m.tgt_perm = D.tgt_perm.p;
     m.hi_nodes = D.hi_nodes.p;
     m.A = D.A.p;
+    m.A_host = D.A_host.data();
     m.fmap = D.fmap.p;
     m.tl_first = D.tl_first.p;
     m.tl_last = D.tl_last.p;
@@ -873,7 +893,11 @@ void Operator::fill_mult_ptrs(MultPtrs& m) const
     m.w = D.w.p;
     m.cvals = D.cvals.p;
     m.fcoef = D.fcoef.p;
+    m.unear = D.unear.p;
     m.err = D.err.p;
+    m.side = D.side;
+    m.ev_fork = D.ev_fork;
+    m.ev_join = D.ev_join;
     for (int d = 0; d < 3; d++)
     {
         m.lo[d] = lo_[d];
@@ -907,7 +931,7 @@ void Operator::launch_mult(const void* d_w, void* d_u, void* stream, bool timed)
     if (on && log.n > 0)
     {
         IFGF_CUDA(cudaEventSynchronize(D.prof_ev[2 * log.n - 1]));
-        double cls_ms[NPROF] = {0, 0, 0, 0, 0};
+        double cls_ms[NPROF] = {};
         for (int i = 0; i < log.n; i++)
         {
             float ms = 0;
@@ -928,6 +952,7 @@ void Operator::launch_mult(const void* d_w, void* d_u, void* stream, bool timed)
         last_.c2f = cls_ms[PROF_C2F];
         last_.eval = cls_ms[PROF_EVAL];
         last_.upward = cls_ms[PROF_UPWARD];
+        last_.near = cls_ms[PROF_NEAR];
         last_.total = tot;
     }
 }
@@ -967,7 +992,7 @@ void Operator::mult_host(const void* w, void* u, int64_t batch)
     {
         IFGF_CUDA(cudaMemcpy(D.io_w.p, (const double*)w + b * nw, nw * sizeof(double),
                              cudaMemcpyHostToDevice));
-        launch_mult(D.io_w.p, D.io_u.p, nullptr, true);
+        launch_mult(D.io_w.p, D.io_u.p, nullptr, false);
         IFGF_CUDA(cudaMemcpy((double*)u + b * nu, D.io_u.p, nu * sizeof(double),
                              cudaMemcpyDeviceToHost));
     }
@@ -984,8 +1009,8 @@ void Operator::mult_device_external_scratch(const void* d_w, void* d_u, void* st
     DeviceState& D = *dev_;
     auto up = [](size_t b) { return (b + 255) / 256 * 256; };
     const size_t bw = up(D.w.n * sizeof(double2)), bc = up(D.cvals.n * sizeof(double2)),
-                 bf = up(D.fcoef.n * sizeof(double2));
-    const size_t need = bw + bc + bf;
+                 bf = up(D.fcoef.n * sizeof(double2)), bn = up(D.unear.n * sizeof(double2));
+    const size_t need = bw + bc + bf + bn;
     if (need > scratch_bytes)
         throw Error(ERR_INVALID, "this operator needs " + std::to_string(need) +
                                      " bytes of matvec scratch; the fixed no-allocation scratch "
@@ -995,6 +1020,7 @@ void Operator::mult_device_external_scratch(const void* d_w, void* d_u, void* st
     double2* w = reinterpret_cast<double2*>(base);
     double2* cv = reinterpret_cast<double2*>(base + bw);
     double2* fc = reinterpret_cast<double2*>(base + bw + bc);
+    double2* un = reinterpret_cast<double2*>(base + bw + bc + bf);
     cudaStream_t st = (cudaStream_t)stream;
     // fine cones without an active coarse parent must read as zero; the
     // shared scratch still holds the previous call's coefficients
@@ -1004,17 +1030,19 @@ void Operator::mult_device_external_scratch(const void* d_w, void* d_u, void* st
     struct Redirect
     {
         DeviceState& D;
-        double2 *w, *cv, *fc;
+        double2 *w, *cv, *fc, *un;
         ~Redirect()
         {
             D.w.p = w;
             D.cvals.p = cv;
             D.fcoef.p = fc;
+            D.unear.p = un;
         }
-    } restore{D, D.w.p, D.cvals.p, D.fcoef.p};
+    } restore{D, D.w.p, D.cvals.p, D.fcoef.p, D.unear.p};
     D.w.p = w;
     D.cvals.p = cv;
     D.fcoef.p = fc;
+    D.unear.p = un;
     MultPtrs m;
     fill_mult_ptrs(m); // no hooks: this path creates no events
     IFGF_DISPATCH(kind_, launch_mult_kernels<KK>(m, d_w, d_u, is_real(), st, nullptr));
@@ -1131,9 +1159,11 @@ std::string Operator::stats_json() const
       << ",\"init_ms\":" << init_ms_ << ",\"launches_per_mult\":" << launches_per_mult_
       << ",\"last_mult_ms\":{\"permute\":" << last_.permute << ",\"leaf_sample\":" << last_.coarse
       << ",\"upward\":" << last_.upward << ",\"coarse_to_fine\":" << last_.c2f
-      << ",\"target_eval\":" << last_.eval << ",\"total\":" << last_.total
+      << ",\"target_eval\":" << last_.eval << ",\"near\":" << last_.near
+      << ",\"total\":" << last_.total
       << "},\"profile\":{\"mults\":" << mults_profiled_;
-    const char* names[NPROF] = {"permute", "leaf_sample", "coarse_to_fine", "target_eval", "upward"};
+    const char* names[NPROF] = {"permute", "leaf_sample", "coarse_to_fine", "target_eval",
+                                "upward",  "near"};
     for (int i = 0; i < NPROF; i++)
         o << ",\"" << names[i] << "\":{\"launches\":" << prof_launches_[i] << ",\"ms\":" << prof_ms_[i]
           << "}";

@@ -19,7 +19,7 @@ struct MultPtrs;    // kernel launch view, defined in mult.hpp
 
 struct StageTimes
 {
-    double permute = 0, coarse = 0, c2f = 0, eval = 0, upward = 0, total = 0;
+    double permute = 0, coarse = 0, c2f = 0, eval = 0, upward = 0, near = 0, total = 0;
 };
 
 class Operator
@@ -94,9 +94,9 @@ class Operator
     bool profiling_ = false;
     // per kernel class: launches and accumulated milliseconds
     // permute, leaf_sample, coarse_to_fine, target_eval, upward
-    static constexpr int NPROF = 5;
-    int64_t prof_launches_[NPROF] = {0, 0, 0, 0, 0};
-    double prof_ms_[NPROF] = {0, 0, 0, 0, 0};
+    static constexpr int NPROF = 6;
+    int64_t prof_launches_[NPROF] = {};
+    double prof_ms_[NPROF] = {};
     int64_t mults_profiled_ = 0;
     int launches_per_mult_ = 0;
 };
