@@ -381,6 +381,8 @@ def run_ours(a):
             "model": "survey flop model: transcendental = 1 flop, FMA = 2"}
     breakdown = {k: v["ms"] / max(prof["mults"], 1) for k, v in kernels.items()}
     breakdown["serialised_total"] = sum(breakdown.values())
+    per_level = {k: [round(x / max(prof["mults"], 1), 3) for x in v["level_ms"]]
+                 for k, v in kernels.items() if any(v.get("level_ms", []))}
 
     line = {
         "metric": METRIC, "value": ms, "unit": UNIT, "n_gpus": ws, "steps": a.steps,
@@ -389,14 +391,15 @@ def run_ours(a):
         "data": "synthetic", "config": workload_config(a, precision),
         "rel_err_vs_fp64_direct": err, "tol": TOL, "meets_tol": err <= TOL,
         "fp64_pipeline": fp64,
-        "init_ms": init_ms, "kernel_ms_per_step": breakdown,
+        "init_ms": init_ms, "kernel_ms_per_step": breakdown, "kernel_ms_per_level": per_level,
         "gpu_launches": int(stats["launches_per_mult"] * a.steps),
         "e2e": {"value": e2e_ms, "unit": UNIT, "h2d_bytes_per_step": int(w.nbytes),
                 "d2h_bytes_per_step": int(u.nbytes)},
         "roofline": roof, "clocks": clk,
         "work": {k: stats[k] for k in ("near_point_pairs", "far_target_evals",
                                        "leaf_factor_evals", "upward_node_evals",
-                                       "coarse_cones_total", "fine_cones_total")},
+                                       "coarse_cones_total", "fine_cones_total",
+                                       "upward_runs_max", "upward_levels")},
     }
     if rank == 0 and ws == 1 and not a.no_cpu_baseline:
         opc, boxes, scale, threads, init_s, rec, nb = cpu_sample_setup(a, pts, w)

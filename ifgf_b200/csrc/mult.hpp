@@ -67,22 +67,27 @@ struct LevelLists
     const UpGeo32* geo32;
     int n_leaf, n_up;
     int up_pad; // row stride of the geometry tables
+    const int2* fe_list; // [slot][octant][fe_pad]: (child element, first group) of each run
+    int fe_pad;         // longest run list of a row
 };
 
 // Upward geometry tables of one level, built on the device in two passes:
-// upgeo_row_max measures every (slot, octant) row's padded length (row_len
-// scratch of 8 n_slots ints) and returns the longest, the row stride P_pad;
-// launch_build_upgeo fills tables pre-set to all-ones bytes (skipped
-// entries).  slot_el: element id of each slot; off: 8 child-centre offsets.
+// upgeo_row_max measures every (slot, octant) row's padded length and number
+// of element runs (row_len scratch of 16 n_slots ints) and returns the
+// longest row, the row stride P_pad, with the most runs of a row in
+// *runs_max; launch_build_upgeo fills tables pre-set to all-ones bytes
+// (skipped entries) and the per-row element lists (fe_pad entries a row,
+// pre-set to -1).  slot_el: element id of each slot; off: 8 child-centre
+// offsets.
 template <int KIND>
 int upgeo_row_max(const LevelGeom& PG, const LevelGeom& CG, double pH, double cH,
                   const double* off_dev, const int* slot_el, int n_slots, const double* hi_nodes,
-                  int P_hi, KParams kp, int* row_len_dev, int* row_len_host);
+                  int P_hi, KParams kp, int* row_len_dev, int* row_len_host, int* runs_max);
 template <int KIND>
 void launch_build_upgeo(const LevelGeom& PG, const LevelGeom& CG, double pH, double cH,
                         const double* off_dev, const int* slot_el, int n_slots,
                         const double* hi_nodes, int P_hi, KParams kp, int P_pad, UpGeo64* g64,
-                        UpGeo32* g32);
+                        UpGeo32* g32, int fe_pad, int2* fe_list);
 
 // Everything one matvec launch needs (device pointers, sizes, orders).
 struct MultPtrs
@@ -138,7 +143,8 @@ enum ProfClass
 
 struct LaunchHooks
 {
-    virtual void begin(int cls) = 0;
+    // cls: ProfClass; level: source-tree level of a per-level launch, else -1
+    virtual void begin(int cls, int level = -1) = 0;
     virtual void end() = 0;
     virtual ~LaunchHooks() = default;
 };

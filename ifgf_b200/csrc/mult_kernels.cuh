@@ -221,6 +221,9 @@ struct UpArgs
     const UpGeo64* __restrict__ geo64;
     const UpGeo32* __restrict__ geo32;
     int P_pad;
+    const int2* __restrict__ fe_list; // [slot][octant][fe_pad]: (element, first group) per run
+    int fe_pad;
+    int rch; // runs staged at a time by the staged kernel
     const double* __restrict__ hi_nodes;
     const int* __restrict__ fmap;
     const double2* __restrict__ fcoef;
@@ -272,7 +275,12 @@ __device__ __forceinline__ bool upward_fallback64(const UpArgs& a, int box, int 
 // (slot, octant) row.  The row lists the nodes that fall inside the child's
 // domain, sorted by child element, each element's run padded with skipped
 // entries to a multiple of UPGEO_RUN so that a group of UPGEO_RUN entries
-// always shares one element.  fill = 0 only measures the padded row length.
+// always shares one element.  fill = 0 only measures the row: its padded
+// length and its number of element runs (row_len[2 row], row_len[2 row + 1]).
+// fill = 1 also lists each row's distinct elements in run order
+// with the group at which each run starts (fe_list[row fe_pad + r] =
+// (element, first group)) and stores the run index r of every entry in
+// UpGeo32::pad, so that a kernel can stage one coefficient block per run.
 constexpr int UPGEO_RUN = 4;
 
 template <int KIND>
@@ -281,13 +289,16 @@ __global__ void __launch_bounds__(256) build_upgeo_kernel(LevelGeom PG, LevelGeo
                                                           const int* __restrict__ slot_el,
                                                           const double* __restrict__ hi_nodes,
                                                           int P_hi, KParams kp, int fill, int P_pad,
-                                                          int* row_len, UpGeo64* g64, UpGeo32* g32)
+                                                          int* row_len, UpGeo64* g64, UpGeo32* g32,
+                                                          int fe_pad, int2* fe_list)
 {
     using P = Plugin<KIND>;
-    extern __shared__ int sh[]; // key[P_hi] | sorted node[P_hi] | padded position[P_hi]
+    // key[P_hi] | sorted node[P_hi] | padded position[P_hi] | run index[P_hi]
+    extern __shared__ int sh[];
     int* key = sh;
     int* snode = sh + P_hi;
     int* pos = snode + P_hi;
+    int* runid = pos + P_hi;
     const int row = blockIdx.x;
     const int slot = row >> 3, o = row & 7;
     const int el = slot_el[slot];
@@ -316,7 +327,7 @@ __global__ void __launch_bounds__(256) build_upgeo_kernel(LevelGeom PG, LevelGeo
     __syncthreads();
     if (threadIdx.x == 0)
     {
-        int off_run = 0, start = 0;
+        int off_run = 0, start = 0, nrun = 0;
         for (int i = 0; i <= P_hi; i++)
         {
             const bool end = i == P_hi || key[snode[i]] != key[snode[start]];
@@ -326,7 +337,14 @@ __global__ void __launch_bounds__(256) build_upgeo_kernel(LevelGeom PG, LevelGeo
                     break; // the nodes outside the domain sort last and are dropped
                 const int len = i - start;
                 for (int j = 0; j < len; j++)
+                {
                     pos[start + j] = off_run + j;
+                    runid[start + j] = nrun;
+                }
+                if (fill && nrun < fe_pad)
+                    fe_list[(size_t)row * fe_pad + nrun] =
+                        make_int2(key[snode[start]], off_run / UPGEO_RUN);
+                nrun++;
                 off_run += (len + UPGEO_RUN - 1) / UPGEO_RUN * UPGEO_RUN;
                 start = i;
             }
@@ -338,7 +356,10 @@ __global__ void __launch_bounds__(256) build_upgeo_kernel(LevelGeom PG, LevelGeo
             }
         }
         if (!fill)
-            row_len[row] = off_run;
+        {
+            row_len[2 * row] = off_run;
+            row_len[2 * row + 1] = nrun;
+        }
     }
     __syncthreads();
     if (!fill)
@@ -369,7 +390,7 @@ __global__ void __launch_bounds__(256) build_upgeo_kernel(LevelGeom PG, LevelGeo
         UpGeo32 h;
         h.fe = g.fe;
         h.node = n;
-        h.pad = 0;
+        h.pad = runid[i];
         h.loc[0] = (float)g.loc[0];
         h.loc[1] = (float)g.loc[1];
         h.loc[2] = (float)g.loc[2];
@@ -382,21 +403,27 @@ __global__ void __launch_bounds__(256) build_upgeo_kernel(LevelGeom PG, LevelGeo
 template <int KIND>
 int upgeo_row_max(const LevelGeom& PG, const LevelGeom& CG, double pH, double cH,
                   const double* off_dev, const int* slot_el, int n_slots, const double* hi_nodes,
-                  int P_hi, KParams kp, int* row_len_dev, int* row_len_host)
+                  int P_hi, KParams kp, int* row_len_dev, int* row_len_host, int* runs_max)
 {
+    *runs_max = 0;
     if (n_slots <= 0)
         return 0;
-    build_upgeo_kernel<KIND><<<n_slots * 8, 256, 3 * P_hi * sizeof(int)>>>(
-        PG, CG, pH, cH, off_dev, slot_el, hi_nodes, P_hi, kp, 0, 0, row_len_dev, nullptr, nullptr);
+    build_upgeo_kernel<KIND><<<n_slots * 8, 256, 4 * P_hi * sizeof(int)>>>(
+        PG, CG, pH, cH, off_dev, slot_el, hi_nodes, P_hi, kp, 0, 0, row_len_dev, nullptr, nullptr,
+        0, nullptr);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess)
-        e = cudaMemcpy(row_len_host, row_len_dev, (size_t)n_slots * 8 * sizeof(int),
+        e = cudaMemcpy(row_len_host, row_len_dev, (size_t)n_slots * 16 * sizeof(int),
                        cudaMemcpyDeviceToHost);
     if (e != cudaSuccess)
         throw Error(2, std::string("build_upgeo_kernel: ") + cudaGetErrorString(e));
-    int mx = 0;
+    int mx = 0, rx = 0;
     for (int i = 0; i < n_slots * 8; i++)
-        mx = row_len_host[i] > mx ? row_len_host[i] : mx;
+    {
+        mx = row_len_host[2 * i] > mx ? row_len_host[2 * i] : mx;
+        rx = row_len_host[2 * i + 1] > rx ? row_len_host[2 * i + 1] : rx;
+    }
+    *runs_max = rx;
     return mx;
 }
 
@@ -404,12 +431,13 @@ template <int KIND>
 void launch_build_upgeo(const LevelGeom& PG, const LevelGeom& CG, double pH, double cH,
                         const double* off_dev, const int* slot_el, int n_slots,
                         const double* hi_nodes, int P_hi, KParams kp, int P_pad, UpGeo64* g64,
-                        UpGeo32* g32)
+                        UpGeo32* g32, int fe_pad, int2* fe_list)
 {
     if (n_slots <= 0 || P_pad <= 0)
         return;
-    build_upgeo_kernel<KIND><<<n_slots * 8, 256, 3 * P_hi * sizeof(int)>>>(
-        PG, CG, pH, cH, off_dev, slot_el, hi_nodes, P_hi, kp, 1, P_pad, nullptr, g64, g32);
+    build_upgeo_kernel<KIND><<<n_slots * 8, 256, 4 * P_hi * sizeof(int)>>>(
+        PG, CG, pH, cH, off_dev, slot_el, hi_nodes, P_hi, kp, 1, P_pad, nullptr, g64, g32, fe_pad,
+        fe_list);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess)
         throw Error(2, std::string("build_upgeo_kernel: ") + cudaGetErrorString(e));
@@ -713,6 +741,37 @@ __global__ void __launch_bounds__(256) direct_eval_kernel(SrcArgs S, const doubl
 // Mixed-precision variants.  Buffers are reused as float2: permuted
 // densities, coarse nodal values and fine coefficients in FP32.
 // ===========================================================================
+// Loads of FP32 coefficient rows (N0 consecutive float2) as 16-byte vectors:
+// one row when N0 is even, two rows when N0 is odd and N1 even (the pair
+// then starts on a 16-byte boundary), else one float2 at a time.  Blocks
+// start on 16-byte boundaries whenever N0 N1 N2 is even.  SHARED selects
+// plain loads (shared memory) instead of read-only global loads.
+template <int N0, int N1, bool SHARED = false> struct CoefRows
+{
+    static constexpr bool VEC = (N0 % 2 == 0) || (N1 % 2 == 0);
+    static constexpr int ROWS = (N0 % 2 == 0) ? 1 : (N1 % 2 == 0 ? 2 : 1);
+    __device__ static __forceinline__ void load(const float2* __restrict__ p, float2* v)
+    {
+        if constexpr (VEC)
+        {
+            const float4* q = reinterpret_cast<const float4*>(p);
+#pragma unroll
+            for (int h = 0; h < ROWS * N0 / 2; h++)
+            {
+                const float4 u = SHARED ? q[h] : __ldg(q + h);
+                v[2 * h] = make_float2(u.x, u.y);
+                v[2 * h + 1] = make_float2(u.z, u.w);
+            }
+        }
+        else
+        {
+#pragma unroll
+            for (int h = 0; h < ROWS * N0; h++)
+                v[h] = SHARED ? p[h] : __ldg(p + h);
+        }
+    }
+};
+
 template <int N0, int N1, int N2> struct ChebF
 {
     __device__ static __forceinline__ cplx<float> eval(const float2* __restrict__ c, const float* x,
@@ -741,18 +800,23 @@ template <int N0, int N1, int N2> struct ChebF
         {
             float br = 0, bi = 0;
 #pragma unroll
-            for (int j = 0; j < N1; j++)
+            for (int j = 0; j < N1; j += CoefRows<N0, N1>::ROWS)
             {
-                float cr = 0, ci = 0;
+                float2 v[CoefRows<N0, N1>::ROWS * N0];
+                CoefRows<N0, N1>::load(c + N0 * (j + N1 * k), v);
 #pragma unroll
-                for (int i = 0; i < N0; i++)
+                for (int jj = 0; jj < CoefRows<N0, N1>::ROWS; jj++)
                 {
-                    const float2 v = __ldg(c + i + N0 * (j + N1 * k));
-                    cr = fmaf(v.x, t0[i], cr);
-                    ci = fmaf(v.y, t0[i], ci);
+                    float cr = 0, ci = 0;
+#pragma unroll
+                    for (int i = 0; i < N0; i++)
+                    {
+                        cr = fmaf(v[jj * N0 + i].x, t0[i], cr);
+                        ci = fmaf(v[jj * N0 + i].y, t0[i], ci);
+                    }
+                    br = fmaf(cr, t1[j + jj], br);
+                    bi = fmaf(ci, t1[j + jj], bi);
                 }
-                br = fmaf(cr, t1[j], br);
-                bi = fmaf(ci, t1[j], bi);
             }
             ar = fmaf(br, t2[k], ar);
             ai = fmaf(bi, t2[k], ai);
@@ -994,9 +1058,23 @@ template <typename T, int N> __device__ __forceinline__ void cheb_basis(T x, T* 
         t[i] = fma(T(2) * x, t[i - 1], -t[i - 2]);
 }
 
-template <typename T, int N0, int N1, int N2, int R> struct ChebMulti
+template <typename T, int N0, int N1, int N2, int R, bool SHARED = false> struct ChebMulti
 {
     using V = typename VecOf<T>::type;
+    // SHARED: c points into shared memory (plain loads); else read-only
+    // global.  FP32 rows are read as 16-byte vectors (CoefRows).
+    static constexpr int ROWS = std::is_same<T, float>::value ? CoefRows<N0, N1>::ROWS : 1;
+    __device__ static __forceinline__ void load_rows(const V* __restrict__ c, V* v)
+    {
+        if constexpr (std::is_same<T, float>::value)
+            CoefRows<N0, N1, SHARED>::load(c, v);
+        else
+        {
+#pragma unroll
+            for (int i = 0; i < N0; i++)
+                v[i] = SHARED ? c[i] : __ldg(c + i);
+        }
+    }
     __device__ static __forceinline__ void eval(const V* __restrict__ c, const T (&x)[R][3],
                                                 const int*, T (&ore)[R], T (&oim)[R])
     {
@@ -1017,28 +1095,33 @@ template <typename T, int N0, int N1, int N2, int R> struct ChebMulti
             for (int r = 0; r < R; r++)
                 br[r] = bi[r] = T(0);
 #pragma unroll
-            for (int j = 0; j < N1; j++)
+            for (int j = 0; j < N1; j += ROWS)
             {
-                T cr[R], ci[R];
+                V v[ROWS * N0];
+                load_rows(c + N0 * (j + N1 * k), v);
 #pragma unroll
-                for (int r = 0; r < R; r++)
-                    cr[r] = ci[r] = T(0);
-#pragma unroll
-                for (int i = 0; i < N0; i++)
+                for (int jj = 0; jj < ROWS; jj++)
                 {
-                    const V v = __ldg(c + i + N0 * (j + N1 * k));
+                    T cr[R], ci[R];
+#pragma unroll
+                    for (int r = 0; r < R; r++)
+                        cr[r] = ci[r] = T(0);
+#pragma unroll
+                    for (int i = 0; i < N0; i++)
+                    {
+#pragma unroll
+                        for (int r = 0; r < R; r++)
+                        {
+                            cr[r] = fma(v[jj * N0 + i].x, t0[r][i], cr[r]);
+                            ci[r] = fma(v[jj * N0 + i].y, t0[r][i], ci[r]);
+                        }
+                    }
 #pragma unroll
                     for (int r = 0; r < R; r++)
                     {
-                        cr[r] = fma(v.x, t0[r][i], cr[r]);
-                        ci[r] = fma(v.y, t0[r][i], ci[r]);
+                        br[r] = fma(cr[r], t1[r][j + jj], br[r]);
+                        bi[r] = fma(ci[r], t1[r][j + jj], bi[r]);
                     }
-                }
-#pragma unroll
-                for (int r = 0; r < R; r++)
-                {
-                    br[r] = fma(cr[r], t1[r][j], br[r]);
-                    bi[r] = fma(ci[r], t1[r][j], bi[r]);
                 }
             }
 #pragma unroll
@@ -1051,7 +1134,7 @@ template <typename T, int N0, int N1, int N2, int R> struct ChebMulti
     }
 };
 
-template <int R> struct ChebMulti<double, 0, 0, 0, R>
+template <int R> struct ChebMulti<double, 0, 0, 0, R, false>
 {
     __device__ static __forceinline__ void eval(const double2* __restrict__ c,
                                                 const double (&x)[R][3], const int* n,
@@ -1066,7 +1149,7 @@ template <int R> struct ChebMulti<double, 0, 0, 0, R>
     }
 };
 
-template <int R> struct ChebMulti<float, 0, 0, 0, R>
+template <int R> struct ChebMulti<float, 0, 0, 0, R, false>
 {
     __device__ static __forceinline__ void eval(const float2* __restrict__ c,
                                                 const float (&x)[R][3], const int* n,
@@ -1082,6 +1165,7 @@ template <int R> struct ChebMulti<float, 0, 0, 0, R>
 };
 
 constexpr int UP_THREADS = 128;
+constexpr size_t UP_STAGED_SMEM_MAX = 96 * 1024;
 
 // One CTA per coarse cone of a box with children (CTAs ordered by cone
 // element, so consecutive CTAs share their geometry-table rows in L2).  For
@@ -1155,6 +1239,173 @@ __global__ void __launch_bounds__(UP_THREADS) upward_kernel(UpArgs a)
     __syncthreads();
     for (int n = threadIdx.x; n < a.P_hi; n += blockDim.x)
         a.cvals[(size_t)c * a.P_hi + n] = acc64[n];
+}
+
+// Stride (in float2) of a staged coefficient block: at least P_lo, a
+// multiple of 2 (16-byte rows for cp.async) and 2 mod 4, so that the blocks
+// of eight consecutive runs start in eight different bank pairs.
+__host__ __device__ constexpr int up_block_stride(int p_lo)
+{
+    return p_lo + ((2 - p_lo % 4) + 4) % 4;
+}
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all()
+{
+    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+
+// Shared memory of the staged upward kernel staging rch runs at a time.
+template <int N0, int N1, int N2>
+size_t upward_staged_smem(int P_hi, int rch)
+{
+    constexpr int P_LO = N0 * N1 * N2;
+    return ((size_t)((P_hi + 1) & ~1) + (size_t)rch * up_block_stride(P_LO)) * sizeof(float2) +
+           (size_t)rch * sizeof(int);
+}
+
+// Runs staged at a time: all of a row's runs when they fit in about 36 KB.
+template <int N0, int N1, int N2>
+int upward_staged_rch(int fe_pad)
+{
+    constexpr int per = up_block_stride(N0 * N1 * N2) * (int)sizeof(float2);
+    const int fit = 36 * 1024 / per;
+    return fe_pad < fit ? fe_pad : (fit > 0 ? fit : 1);
+}
+
+// Mixed-precision upward transfer with the coefficient blocks in shared
+// memory.  Per child, every run of the (slot, octant) geometry row needs one
+// child fine cone; its block (P_lo coefficients) is copied once into shared
+// memory with cp.async (one warp per block), rch runs at a time, after which
+// the Chebyshev sums of those runs' groups read only shared memory.
+// Compile-time orders only (P_lo even, so that a block is a whole number of
+// 16-byte chunks).
+template <int KIND, int N0, int N1, int N2>
+__global__ void __launch_bounds__(UP_THREADS, 5) upward_staged_kernel(UpArgs a)
+{
+    constexpr int R = UPGEO_RUN;
+    constexpr int P_LO = N0 * N1 * N2;
+    constexpr int BS = up_block_stride(P_LO);
+    constexpr int CH = P_LO * (int)sizeof(float2) / 16; // 16-byte chunks per block
+    static_assert(P_LO % 2 == 0, "staged blocks need an even number of coefficients");
+    extern __shared__ __align__(16) float2 up_sh[];
+    float2* acc = up_sh;
+    float2* blk = up_sh + ((a.P_hi + 1) & ~1);
+    int* blk_gf = reinterpret_cast<int*>(blk + (size_t)a.rch * BS);
+    const int c = a.idx[blockIdx.x];
+    const int slot = a.slot[blockIdx.x];
+    const int box = a.cc_box[c], el = a.cc_el[c];
+    const float2* fcf = reinterpret_cast<const float2*>(a.fcoef);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int n = threadIdx.x; n < a.P_hi; n += blockDim.x)
+        acc[n] = make_float2(0.f, 0.f);
+    const LevelGeom& C = a.GC;
+    const long long nf = (long long)C.nf[0] * C.nf[1] * C.nf[2];
+    const int ngroups = a.P_pad / R;
+    for (int o = 0; o < 8; o++)
+    {
+        const int cb = a.T.box_child[8 * box + o];
+        if (cb < 0)
+            continue;
+        const int* fm = a.fmap + C.fmap_off + (long long)(cb - C.box_off) * nf;
+        const int2* fl = a.fe_list + ((size_t)slot * 8 + o) * a.fe_pad;
+        const UpGeo32* row = a.geo32 + ((size_t)slot * 8 + o) * a.P_pad;
+        for (int r0 = 0; r0 < a.fe_pad; r0 += a.rch)
+        {
+            const int2 first = fl[r0];
+            if (first.x < 0)
+                break; // past the row's last run
+            const int r1 = min(r0 + a.rch, a.fe_pad);
+            int g_end = ngroups;
+            if (r1 < a.fe_pad)
+            {
+                const int2 next = fl[r1];
+                if (next.x >= 0)
+                    g_end = next.y;
+            }
+            __syncthreads(); // the previous runs' blocks are no longer read
+            for (int r = r0 + warp; r < r1; r += UP_THREADS / 32)
+            {
+                int gf = -1;
+                if (lane == 0)
+                {
+                    const int fe = fl[r].x;
+                    gf = fe >= 0 ? fm[fe] : -1;
+                    blk_gf[r - r0] = gf;
+                }
+                gf = __shfl_sync(0xffffffffu, gf, 0);
+                if (gf < 0)
+                    continue;
+                const float2* src = fcf + (size_t)gf * P_LO;
+                float2* dst = blk + (size_t)(r - r0) * BS;
+                for (int ch = lane; ch < CH; ch += 32)
+                    cp_async16(dst + 2 * ch, src + 2 * ch);
+            }
+            cp_async_wait_all();
+            __syncthreads();
+            for (int g = first.y + threadIdx.x; g < g_end; g += blockDim.x)
+            {
+                UpGeo32 e[R];
+#pragma unroll
+                for (int r = 0; r < R; r++)
+                    e[r] = row[(size_t)r * ngroups + g];
+                if (e[0].fe < 0)
+                    continue;
+                const int rl = e[0].pad - r0;
+                if (blk_gf[rl] < 0)
+                {
+                    // tabulated element inactive in this child: absolute coordinates
+                    const double xc[3] = {a.T.box_c[3 * box], a.T.box_c[3 * box + 1],
+                                          a.T.box_c[3 * box + 2]};
+#pragma unroll
+                    for (int r = 0; r < R; r++)
+                    {
+                        if (e[r].node < 0)
+                            continue;
+                        double y[3];
+                        node_position(a.G, el, e[r].node, a.hi_nodes, xc, a.T.box_H[box], y);
+                        const double p[3] = {y[0] - a.T.box_c[3 * cb],
+                                             y[1] - a.T.box_c[3 * cb + 1],
+                                             y[2] - a.T.box_c[3 * cb + 2]};
+                        float loc[3];
+                        const int gf2 = fine_lookup_mixed(C, fm, p, a.T.box_H[cb], loc, a.err);
+                        if (gf2 < 0)
+                            continue;
+                        const double e0 = y[0] - xc[0], e1 = y[1] - xc[1], e2 = y[2] - xc[2];
+                        cplx<float> v = {0.f, 0.f};
+                        cfmaf(v, ChebF<N0, N1, N2>::eval(fcf + (size_t)gf2 * P_LO, loc, a.lo),
+                              transfer_mixed<KIND>(p[0] * p[0] + p[1] * p[1] + p[2] * p[2],
+                                                   e0 * e0 + e1 * e1 + e2 * e2, a.kp));
+                        acc[e[r].node].x += v.re;
+                        acc[e[r].node].y += v.im;
+                    }
+                    continue;
+                }
+                float x[R][3], vr[R], vi[R];
+#pragma unroll
+                for (int r = 0; r < R; r++)
+                    for (int d = 0; d < 3; d++)
+                        x[r][d] = e[r].loc[d];
+                ChebMulti<float, N0, N1, N2, R, true>::eval(blk + (size_t)rl * BS, x, a.lo, vr, vi);
+#pragma unroll
+                for (int r = 0; r < R; r++)
+                    if (e[r].node >= 0)
+                    {
+                        const float2 s = acc[e[r].node];
+                        acc[e[r].node] = make_float2(s.x + (vr[r] * e[r].tr - vi[r] * e[r].ti),
+                                                     s.y + (vr[r] * e[r].ti + vi[r] * e[r].tr));
+                    }
+            }
+        }
+    }
+    __syncthreads();
+    float2* cv = reinterpret_cast<float2*>(a.cvals);
+    for (int n = threadIdx.x; n < a.P_hi; n += blockDim.x)
+        cv[(size_t)c * a.P_hi + n] = acc[n];
 }
 
 template <int KIND, int N0, int N1, int N2>
@@ -1535,6 +1786,10 @@ __global__ void __launch_bounds__(EVAL_THREADS, 6) target_eval_mixed_kernel(Eval
     __shared__ double n0[P::needs_normals ? EVAL_THREADS : 1], n1[P::needs_normals ? EVAL_THREADS : 1],
         n2[P::needs_normals ? EVAL_THREADS : 1];
     __shared__ double rr[EVAL_THREADS], ri[EVAL_THREADS];
+    constexpr int NF = PART == EVAL_FAR ? EVAL_THREADS : 1;
+    __shared__ double fcx[NF], fcy[NF], fcz[NF], fH[NF];
+    __shared__ long long ffm[NF];
+    __shared__ int flev[NF];
     const float2* wf = reinterpret_cast<const float2*>(a.w);
     const float2* fcf = reinterpret_cast<const float2*>(a.fcoef);
     const int tl = blockIdx.x;
@@ -1603,17 +1858,34 @@ __global__ void __launch_bounds__(EVAL_THREADS, 6) target_eval_mixed_kernel(Eval
                 }
             }
         }
-        if (active)
-            for (long long e = fb0 + si; e < fb1; e += S)
+        // far sources in chunks of EVAL_THREADS boxes, whose centre, size,
+        // level and fine-map row are staged in shared memory first
+        for (long long e0 = fb0; e0 < fb1; e0 += EVAL_THREADS)
+        {
+            const int fcnt = (int)min((long long)EVAL_THREADS, fb1 - e0);
+            __syncthreads();
+            if (threadIdx.x < fcnt)
             {
-                const int sb = a.far_src[e];
-                const LevelGeom& G = a.lv[a.T.box_level[sb]];
-                const double p[3] = {y0 - a.T.box_c[3 * sb], y1 - a.T.box_c[3 * sb + 1],
-                                     y2 - a.T.box_c[3 * sb + 2]};
+                const int sb = a.far_src[e0 + threadIdx.x];
+                const int lev = a.T.box_level[sb];
+                const LevelGeom& G = a.lv[lev];
                 const long long nft = (long long)G.nf[0] * G.nf[1] * G.nf[2];
-                const int* fm = a.fmap + G.fmap_off + (long long)(sb - G.box_off) * nft;
+                fcx[threadIdx.x] = a.T.box_c[3 * sb];
+                fcy[threadIdx.x] = a.T.box_c[3 * sb + 1];
+                fcz[threadIdx.x] = a.T.box_c[3 * sb + 2];
+                fH[threadIdx.x] = a.T.box_H[sb];
+                ffm[threadIdx.x] = G.fmap_off + (long long)(sb - G.box_off) * nft;
+                flev[threadIdx.x] = lev;
+            }
+            __syncthreads();
+            if (!active)
+                continue;
+            for (int i = si; i < fcnt; i += S)
+            {
+                const LevelGeom& G = a.lv[flev[i]];
+                const double p[3] = {y0 - fcx[i], y1 - fcy[i], y2 - fcz[i]};
                 float loc[3];
-                const int gf = fine_lookup_mixed(G, fm, p, a.T.box_H[sb], loc, a.err);
+                const int gf = fine_lookup_mixed(G, a.fmap + ffm[i], p, fH[i], loc, a.err);
                 if (gf < 0)
                     continue;
                 const cplx<float> v = ChebF<N0, N1, N2>::eval(fcf + (size_t)gf * a.P_lo, loc, a.lo);
@@ -1621,6 +1893,7 @@ __global__ void __launch_bounds__(EVAL_THREADS, 6) target_eval_mixed_kernel(Eval
                 accr += (double)(v.re * cf.re - v.im * cf.im);
                 acci += (double)(v.re * cf.im + v.im * cf.re);
             }
+        }
         __syncthreads();
         rr[threadIdx.x] = accr;
         ri[threadIdx.x] = acci;
@@ -1780,7 +2053,7 @@ static int run_mult(const MultPtrs& m, const void* d_w, void* d_u, bool real, cu
             LeafArgs la{G, m.T, m.S, LL.cc_box, LL.cc_el, LL.leaf_idx, m.hi_nodes, m.w, m.cvals,
                         m.P_hi, m.kp};
             if (hk)
-                hk->begin(PROF_COARSE);
+                hk->begin(PROF_COARSE, l);
             if (MIXED)
                 leaf_sample_mixed_kernel<KIND>
                     <<<dim3(LL.n_leaf, nchk), nthr, 9 * nthr * sizeof(float), st>>>(la);
@@ -1805,6 +2078,9 @@ static int run_mult(const MultPtrs& m, const void* d_w, void* d_u, bool real, cu
             ua.geo64 = LL.geo64;
             ua.geo32 = LL.geo32;
             ua.P_pad = LL.up_pad;
+            ua.fe_list = LL.fe_list;
+            ua.rch = 0;
+            ua.fe_pad = LL.fe_pad;
             ua.hi_nodes = m.hi_nodes;
             ua.fmap = m.fmap;
             ua.fcoef = m.fcoef;
@@ -1816,8 +2092,26 @@ static int run_mult(const MultPtrs& m, const void* d_w, void* d_u, bool real, cu
                 ua.lo[d] = m.lo[d];
             ua.kp = m.kp;
             if (hk)
-                hk->begin(PROF_UPWARD);
-            if (MIXED)
+                hk->begin(PROF_UPWARD, l);
+            bool staged = false;
+            if constexpr (MIXED && N0 > 0 && (N0 * N1 * N2) % 2 == 0)
+            {
+                ua.rch = upward_staged_rch<N0, N1, N2>(LL.fe_pad);
+                const size_t sm = upward_staged_smem<N0, N1, N2>(m.P_hi, ua.rch);
+                if (LL.fe_pad > 0 && sm <= UP_STAGED_SMEM_MAX)
+                {
+                    auto kern = upward_staged_kernel<KIND, N0, N1, N2>;
+                    if (sm > 48 * 1024)
+                        IFGF_CHECK(cudaFuncSetAttribute(
+                            kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+                    kern<<<LL.n_up, UP_THREADS, sm, st>>>(ua);
+                    staged = true;
+                }
+            }
+            if (staged)
+            {
+            }
+            else if (MIXED)
                 upward_mixed_kernel<KIND, N0, N1, N2>
                     <<<LL.n_up, UP_THREADS, m.P_hi * sizeof(float2), st>>>(ua);
             else
@@ -1845,7 +2139,7 @@ static int run_mult(const MultPtrs& m, const void* d_w, void* d_u, bool real, cu
         fa.P_hi = m.P_hi;
         fa.P_lo = m.P_lo;
         if (hk)
-            hk->begin(PROF_C2F);
+            hk->begin(PROF_C2F, l);
         if (launch_c2f_fixed<typename std::conditional<MIXED, float, double>::type>(
                 fa, m.A_host, (unsigned)G.n_coarse, st))
         {
@@ -1919,9 +2213,9 @@ void launch_direct_kernel(const MultPtrs& m, const int* tpos, int nt, double2* o
     template void permute_only<K>(const MultPtrs&, const void*, bool, cudaStream_t);         \
     template void launch_build_upgeo<K>(const LevelGeom&, const LevelGeom&, double, double,   \
                                         const double*, const int*, int, const double*, int,     \
-                                        KParams, int, UpGeo64*, UpGeo32*);                      \
+                                        KParams, int, UpGeo64*, UpGeo32*, int, int2*);          \
     template int upgeo_row_max<K>(const LevelGeom&, const LevelGeom&, double, double,         \
                                   const double*, const int*, int, const double*, int, KParams,  \
-                                  int*, int*);
+                                  int*, int*, int*);
 
 } // namespace ifgf

@@ -98,6 +98,7 @@ struct DeviceState
     std::vector<DevBuf<int>> leaf_idx, up_idx, up_slot;    // per level coarse-cone partition
     std::vector<DevBuf<UpGeo64>> geo64;                    // per level upward geometry
     std::vector<DevBuf<UpGeo32>> geo32;
+    std::vector<DevBuf<int2>> fe_list; // per-row (child element, first group) of each run
     std::vector<LevelLists> lists;                         // per level views of the above
     DevBuf<int> fmap;
     DevBuf<double> hi_nodes, A;
@@ -642,8 +643,11 @@ void Operator::setup_device(const double* normals)
     D.up_slot.resize(L);
     D.geo64.resize(L);
     D.geo32.resize(L);
+    D.fe_list.resize(L);
     std::vector<std::vector<int>> up_host(L);
     std::vector<int> up_pad(L, 0);
+    fe_pad_.assign(L, 0);
+    up_stats_.assign(L, UpwardLevelStats{});
     upgeo_bytes_ = 0;
     int64_t coarse_tot = 0, fine_tot = 0;
     leaf_evals_ = upward_evals_ = 0;
@@ -784,13 +788,36 @@ void Operator::setup_device(const double* normals)
             const double pH = S.levels[l].side, cH = S.levels[l + 1].side;
             const int ns = (int)slot_el.size();
             DevBuf<int> drow;
-            drow.alloc((size_t)ns * 8);
-            std::vector<int> hrow((size_t)ns * 8);
-            int pad = 0;
+            drow.alloc((size_t)ns * 16);
+            std::vector<int> hrow((size_t)ns * 16);
+            int pad = 0, runs = 0;
             IFGF_DISPATCH(kind_, pad = upgeo_row_max<KK>(lv_[l], lv_[l + 1], pH, cH, doff.p,
                                                           dslot_el.p, ns, D.hi_nodes.p, P_hi, kp,
-                                                          drow.p, hrow.data()));
+                                                          drow.p, hrow.data(), &runs));
             up_pad[l] = pad;
+            fe_pad_[l] = runs;
+            {
+                // work of this level's upward transfer: node evaluations,
+                // child coefficient blocks (runs) and padded table entries
+                UpwardLevelStats& us = up_stats_[l];
+                us.cones = (int64_t)uidx.size();
+                us.slots = ns;
+                std::vector<int> cbox(lv_[l].n_coarse);
+                IFGF_CUDA(cudaMemcpy(cbox.data(), D.cc_box[l].p, cbox.size() * sizeof(int),
+                                     cudaMemcpyDeviceToHost));
+                for (size_t i = 0; i < uidx.size(); i++)
+                {
+                    const int g = cbox[uidx[i]];
+                    for (int o = 0; o < 8; o++)
+                        if (bch[8 * g + o] >= 0)
+                        {
+                            us.blocks += hrow[2 * ((size_t)slot_of[i] * 8 + o) + 1];
+                            us.entries += hrow[2 * ((size_t)slot_of[i] * 8 + o)];
+                        }
+                }
+            }
+            D.fe_list[l].alloc((size_t)ns * 8 * std::max(runs, 1));
+            IFGF_CUDA(cudaMemset(D.fe_list[l].p, 0xff, D.fe_list[l].n * sizeof(int2)));
             const size_t n_ent = (size_t)ns * 8 * (size_t)std::max(pad, 1);
             D.geo64[l].alloc(n_ent);
             D.geo32[l].alloc(n_ent);
@@ -799,7 +826,8 @@ void Operator::setup_device(const double* normals)
             IFGF_CUDA(cudaMemset(D.geo32[l].p, 0xff, n_ent * sizeof(UpGeo32)));
             IFGF_DISPATCH(kind_, launch_build_upgeo<KK>(lv_[l], lv_[l + 1], pH, cH, doff.p,
                                                          dslot_el.p, ns, D.hi_nodes.p, P_hi, kp,
-                                                         pad, D.geo64[l].p, D.geo32[l].p));
+                                                         pad, D.geo64[l].p, D.geo32[l].p, runs,
+                                                         D.fe_list[l].p));
             IFGF_CUDA(cudaDeviceSynchronize());
             upgeo_bytes_ += (double)n_ent * (sizeof(UpGeo64) + sizeof(UpGeo32));
         }
@@ -810,7 +838,8 @@ void Operator::setup_device(const double* normals)
     for (int l = 0; l < L; l++)
         D.lists[l] = LevelLists{D.cc_box[l].p, D.cc_el[l].p, D.leaf_idx[l].p, D.up_idx[l].p,
                                 D.up_slot[l].p, D.geo64[l].p, D.geo32[l].p,
-                                (int)D.leaf_idx[l].n, (int)D.up_idx[l].n, up_pad[l]};
+                                (int)D.leaf_idx[l].n, (int)D.up_idx[l].n, up_pad[l],
+                                D.fe_list[l].p, fe_pad_[l]};
     n_coarse_total_ = coarse_tot;
     n_fine_total_ = fine_tot;
     D.lv.upload(lv_);
@@ -845,8 +874,10 @@ struct EventHooks : LaunchHooks
     std::vector<int> cls;
     int n = 0;
     EventHooks(DeviceState& d, cudaStream_t s) : D(d), st(s) {}
-    void begin(int c) override
+    std::vector<int> lev;
+    void begin(int c, int level) override
     {
+        lev.push_back(level);
         while ((int)D.prof_ev.size() < 2 * (n + 1))
         {
             cudaEvent_t e;
@@ -941,6 +972,8 @@ void Operator::launch_mult(const void* d_w, void* d_u, void* stream, bool timed)
             {
                 prof_ms_[log.cls[i]] += ms;
                 prof_launches_[log.cls[i]]++;
+                if (log.lev[i] >= 0 && log.lev[i] < MAX_LEVELS)
+                    prof_level_ms_[log.cls[i]][log.lev[i]] += ms;
             }
         }
         float tot = 0;
@@ -964,6 +997,8 @@ void Operator::set_profiling(bool on)
     {
         prof_launches_[i] = 0;
         prof_ms_[i] = 0;
+        for (int l = 0; l < MAX_LEVELS; l++)
+            prof_level_ms_[i][l] = 0;
     }
     mults_profiled_ = 0;
 }
@@ -1154,7 +1189,15 @@ std::string Operator::stats_json() const
       << ",\"far_target_evals\":" << plan_.far_target_evals
       << ",\"leaf_factor_evals\":" << leaf_evals_ << ",\"upward_node_evals\":" << upward_evals_
       << ",\"coarse_cones_total\":" << n_coarse_total_ << ",\"fine_cones_total\":" << n_fine_total_
-      << ",\"upward_geometry_bytes\":" << upgeo_bytes_
+      << ",\"upward_geometry_bytes\":" << upgeo_bytes_ << ",\"upward_runs_max\":[";
+    for (size_t l = 0; l < fe_pad_.size(); l++)
+        o << (l ? "," : "") << fe_pad_[l];
+    o << "],\"upward_levels\":[";
+    for (size_t l = 0; l < up_stats_.size(); l++)
+        o << (l ? "," : "") << "{\"cones\":" << up_stats_[l].cones << ",\"slots\":"
+          << up_stats_[l].slots << ",\"blocks\":" << up_stats_[l].blocks
+          << ",\"padded_entries\":" << up_stats_[l].entries << "}";
+    o << "]"
       << ",\"target_leaves\":" << dev_->n_tleaf << ",\"missing_cone_lookups\":" << missing_
       << ",\"init_ms\":" << init_ms_ << ",\"launches_per_mult\":" << launches_per_mult_
       << ",\"last_mult_ms\":{\"permute\":" << last_.permute << ",\"leaf_sample\":" << last_.coarse
@@ -1165,8 +1208,13 @@ std::string Operator::stats_json() const
     const char* names[NPROF] = {"permute", "leaf_sample", "coarse_to_fine", "target_eval",
                                 "upward",  "near"};
     for (int i = 0; i < NPROF; i++)
+    {
         o << ",\"" << names[i] << "\":{\"launches\":" << prof_launches_[i] << ",\"ms\":" << prof_ms_[i]
-          << "}";
+          << ",\"level_ms\":[";
+        for (size_t l = 0; l < lv_.size(); l++)
+            o << (l ? "," : "") << prof_level_ms_[i][l];
+        o << "]}";
+    }
     o << "}}";
     return o.str();
 }

@@ -90,6 +90,12 @@ class Operator
     int64_t n_coarse_total_ = 0, n_fine_total_ = 0;
     double leaf_evals_ = 0, upward_evals_ = 0;
     double upgeo_bytes_ = 0; // device bytes of the upward geometry tables
+    std::vector<int> fe_pad_; // per level: most element runs in one upward geometry row
+    struct UpwardLevelStats
+    {
+        int64_t cones = 0, slots = 0, blocks = 0, entries = 0;
+    };
+    std::vector<UpwardLevelStats> up_stats_;
     unsigned long long missing_ = 0;
     bool profiling_ = false;
     // per kernel class: launches and accumulated milliseconds
@@ -97,6 +103,7 @@ class Operator
     static constexpr int NPROF = 6;
     int64_t prof_launches_[NPROF] = {};
     double prof_ms_[NPROF] = {};
+    double prof_level_ms_[NPROF][MAX_LEVELS] = {}; // per-level launches only
     int64_t mults_profiled_ = 0;
     int launches_per_mult_ = 0;
 };
