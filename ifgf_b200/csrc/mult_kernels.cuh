@@ -1268,14 +1268,19 @@ size_t upward_staged_smem(int P_hi, int rch)
            (size_t)rch * sizeof(int);
 }
 
-// Runs staged at a time: all of a row's runs when they fit in about 36 KB.
+// Runs staged at a time: all of a row's runs when they fit in about 16 KB
+// (rows average a handful of runs; the longest ones take several chunks).
 template <int N0, int N1, int N2>
 int upward_staged_rch(int fe_pad)
 {
     constexpr int per = up_block_stride(N0 * N1 * N2) * (int)sizeof(float2);
-    const int fit = 36 * 1024 / per;
+    const int fit = 16 * 1024 / per;
     return fe_pad < fit ? fe_pad : (fit > 0 ? fit : 1);
 }
+
+// Threads of the staged upward kernel: an average geometry row has a few
+// dozen groups, so small CTAs keep most threads busy.
+constexpr int UPS_THREADS = 64;
 
 // Mixed-precision upward transfer with the coefficient blocks in shared
 // memory.  Per child, every run of the (slot, octant) geometry row needs one
@@ -1285,7 +1290,7 @@ int upward_staged_rch(int fe_pad)
 // Compile-time orders only (P_lo even, so that a block is a whole number of
 // 16-byte chunks).
 template <int KIND, int N0, int N1, int N2>
-__global__ void __launch_bounds__(UP_THREADS, 5) upward_staged_kernel(UpArgs a)
+__global__ void __launch_bounds__(UPS_THREADS, 10) upward_staged_kernel(UpArgs a)
 {
     constexpr int R = UPGEO_RUN;
     constexpr int P_LO = N0 * N1 * N2;
@@ -1328,7 +1333,7 @@ __global__ void __launch_bounds__(UP_THREADS, 5) upward_staged_kernel(UpArgs a)
                     g_end = next.y;
             }
             __syncthreads(); // the previous runs' blocks are no longer read
-            for (int r = r0 + warp; r < r1; r += UP_THREADS / 32)
+            for (int r = r0 + warp; r < r1; r += UPS_THREADS / 32)
             {
                 int gf = -1;
                 if (lane == 0)
@@ -1345,14 +1350,25 @@ __global__ void __launch_bounds__(UP_THREADS, 5) upward_staged_kernel(UpArgs a)
                 for (int ch = lane; ch < CH; ch += 32)
                     cp_async16(dst + 2 * ch, src + 2 * ch);
             }
-            cp_async_wait_all();
-            __syncthreads();
-            for (int g = first.y + threadIdx.x; g < g_end; g += blockDim.x)
+            // the first group's table entries load while the blocks arrive
+            const int g0 = first.y + threadIdx.x;
+            UpGeo32 e[R];
+            if (g0 < g_end)
             {
-                UpGeo32 e[R];
 #pragma unroll
                 for (int r = 0; r < R; r++)
-                    e[r] = row[(size_t)r * ngroups + g];
+                    e[r] = row[(size_t)r * ngroups + g0];
+            }
+            cp_async_wait_all();
+            __syncthreads();
+            for (int g = g0; g < g_end; g += blockDim.x)
+            {
+                if (g != g0)
+                {
+#pragma unroll
+                    for (int r = 0; r < R; r++)
+                        e[r] = row[(size_t)r * ngroups + g];
+                }
                 if (e[0].fe < 0)
                     continue;
                 const int rl = e[0].pad - r0;
@@ -2104,7 +2120,7 @@ static int run_mult(const MultPtrs& m, const void* d_w, void* d_u, bool real, cu
                     if (sm > 48 * 1024)
                         IFGF_CHECK(cudaFuncSetAttribute(
                             kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-                    kern<<<LL.n_up, UP_THREADS, sm, st>>>(ua);
+                    kern<<<LL.n_up, UPS_THREADS, sm, st>>>(ua);
                     staged = true;
                 }
             }
