@@ -548,6 +548,7 @@ static __global__ void __launch_bounds__(256) coarse_to_fine_kernel(C2FArgs a)
 struct EvalArgs
 {
     const LevelGeom* __restrict__ lv;
+    int L; // levels
     TreeArgs T;
     SrcArgs S;
     const double* __restrict__ tx;
@@ -915,6 +916,80 @@ __device__ __forceinline__ int fine_lookup_mixed(const LevelGeom& G, const int* 
     if (fe < 0)
         return -1;
     gf = fm[fe];
+    if (gf < 0)
+    {
+        atomicAdd(err, 1ull);
+        return -1;
+    }
+    to_local(fe, s, G.dmin, G.hf, G.hfi, G.nf, ld);
+    loc[0] = (float)ld[0];
+    loc[1] = (float)ld[1];
+    loc[2] = (float)ld[2];
+    return gf;
+}
+
+// FP32 cone-lookup parameters of one level, made once per CTA in shared
+// memory so that the far-field lookups read no level data from global memory.
+struct LookupF
+{
+    float lo[3], hi[3], hinv[3], top[3]; // domain, 1 / fine width, nf - 1
+    int nf[3];
+};
+
+__device__ __forceinline__ void make_lookupf(const LevelGeom& G, LookupF& L)
+{
+#pragma unroll
+    for (int d = 0; d < 3; d++)
+    {
+        L.lo[d] = (float)G.dmin[d];
+        L.hi[d] = (float)G.dmax[d];
+        L.hinv[d] = (float)G.hfi[d];
+        L.top[d] = (float)(G.nf[d] - 1);
+        L.nf[d] = G.nf[d];
+    }
+}
+
+// fine_lookup_mixed with the level's FP32 parameters at hand: with
+// t = (s - lo) / h the element index is q = floor(t) (clamped) and the local
+// coordinate 2 (t - q) - 1, the same quantities as (s - centre) / (h / 2).
+// The FP64 fallback (outside the FP32 domain or an inactive cone) is that of
+// fine_lookup_mixed.
+__device__ __forceinline__ int fine_lookup_fast(const LookupF& L, const LevelGeom& G,
+                                                const int* __restrict__ fm, const double* p,
+                                                double H, float* loc, unsigned long long* err)
+{
+    float sf[3];
+    cart_to_interp_f((float)p[0], (float)p[1], (float)p[2], (float)H, sf);
+    bool inside = true;
+    int id = 0, stride = 1;
+    float fr[3];
+#pragma unroll
+    for (int j = 0; j < 3; j++)
+    {
+        inside = inside && sf[j] >= L.lo[j] && sf[j] <= L.hi[j];
+        const float t = (sf[j] - L.lo[j]) * L.hinv[j];
+        const float q = fminf(fmaxf(floorf(t), 0.f), L.top[j]);
+        fr[j] = t - q;
+        id += __float2int_rz(q) * stride;
+        stride *= L.nf[j];
+    }
+    if (inside)
+    {
+        const int gf = fm[id];
+        if (gf >= 0)
+        {
+#pragma unroll
+            for (int d = 0; d < 3; d++)
+                loc[d] = fmaf(2.f, fr[d], -1.f);
+            return gf;
+        }
+    }
+    double s[3], ld[3];
+    cart_to_interp(p[0], p[1], p[2], H, s);
+    const int fe = element_for_point(s, G.dmin, G.dmax, G.hfi, G.nf);
+    if (fe < 0)
+        return -1;
+    const int gf = fm[fe];
     if (gf < 0)
     {
         atomicAdd(err, 1ull);
@@ -1806,6 +1881,10 @@ __global__ void __launch_bounds__(EVAL_THREADS, 6) target_eval_mixed_kernel(Eval
     __shared__ double fcx[NF], fcy[NF], fcz[NF], fH[NF];
     __shared__ long long ffm[NF];
     __shared__ int flev[NF];
+    __shared__ LookupF lfs[PART == EVAL_FAR ? MAX_LEVELS : 1];
+    if (PART == EVAL_FAR)
+        for (int l = threadIdx.x; l < a.L; l += blockDim.x)
+            make_lookupf(a.lv[l], lfs[l]); // read after the first chunk's barriers
     const float2* wf = reinterpret_cast<const float2*>(a.w);
     const float2* fcf = reinterpret_cast<const float2*>(a.fcoef);
     const int tl = blockIdx.x;
@@ -1898,10 +1977,11 @@ __global__ void __launch_bounds__(EVAL_THREADS, 6) target_eval_mixed_kernel(Eval
                 continue;
             for (int i = si; i < fcnt; i += S)
             {
-                const LevelGeom& G = a.lv[flev[i]];
+                const int lev = flev[i];
                 const double p[3] = {y0 - fcx[i], y1 - fcy[i], y2 - fcz[i]};
                 float loc[3];
-                const int gf = fine_lookup_mixed(G, a.fmap + ffm[i], p, fH[i], loc, a.err);
+                const int gf =
+                    fine_lookup_fast(lfs[lev], a.lv[lev], a.fmap + ffm[i], p, fH[i], loc, a.err);
                 if (gf < 0)
                     continue;
                 const cplx<float> v = ChebF<N0, N1, N2>::eval(fcf + (size_t)gf * a.P_lo, loc, a.lo);
@@ -2010,6 +2090,7 @@ static int run_mult(const MultPtrs& m, const void* d_w, void* d_u, bool real, cu
     // while the level loop builds the interpolants
     EvalArgs ea;
     ea.lv = m.lv_dev;
+    ea.L = m.L;
     ea.T = m.T;
     ea.S = m.S;
     ea.tx = m.tx;
