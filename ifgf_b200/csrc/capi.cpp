@@ -143,6 +143,31 @@ extern "C"
         });
     }
 
+    int ifgf_direct_eval_dk(ifgf_operator* h, const void* w, const long* tidx, long nt,
+                            void* out)
+    {
+        if (!h)
+            return null_handle();
+        return guarded([&] {
+            std::vector<int64_t> t(tidx, tidx + (tidx ? nt : 0));
+            h->op.direct_eval(w, t.data(), nt, out, true);
+        });
+    }
+
+    int ifgf_mult_dk(ifgf_operator* h, const void* w, void* u, long batch)
+    {
+        if (!h)
+            return null_handle();
+        return guarded([&] { h->op.mult_dk_host(w, u, batch); });
+    }
+
+    int ifgf_mult_dk_device(ifgf_operator* h, const void* d_w, void* d_u, void* stream)
+    {
+        if (!h)
+            return null_handle();
+        return guarded([&] { h->op.mult_dk_device(d_w, d_u, stream); });
+    }
+
     int ifgf_set_profiling(ifgf_operator* h, int on)
     {
         if (!h)

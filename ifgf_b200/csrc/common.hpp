@@ -21,7 +21,11 @@ enum KernelKind : int
     K_MODHELMHOLTZ = 2,
     K_GRADHELMHOLTZ = 3,
     K_DOUBLELAYER = 4,
-    K_COMBINEDFIELD = 5
+    K_COMBINEDFIELD = 5,
+    // wavenumber derivatives dG/dk of kernels 1 and 5 (no reference
+    // counterpart; same tree, cones and orders as the base kernel)
+    K_HELMHOLTZ_DK = 6,
+    K_COMBINEDFIELD_DK = 7
 };
 
 enum Precision : int

@@ -447,6 +447,84 @@ template <> struct Plugin<K_COMBINEDFIELD>
     }
 };
 
+// d/dk of the Helmholtz kernel, i e^{ikr} / (4 pi).  Centred factor
+// e^{ik r_c} / (4 pi) (no 1/r_c: the factored kernel i e^{ik(r - r_c)} is then
+// as smooth in the cone coordinates as the Helmholtz one), centre shift
+// e^{ik(r - r_p)}.
+template <> struct Plugin<K_HELMHOLTZ_DK>
+{
+    static constexpr bool needs_normals = false;
+    __device__ static cplx<double> kernel(const double* x, const double*, const KParams& p)
+    {
+        const double d = sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
+        if (d == 0)
+            return {0.0, 0.0};
+        const cplx<double> e = exp_ik(p.kr, d);
+        return {-e.im * INV4PI, e.re * INV4PI};
+    }
+    __device__ static cplx<double> cf(const double* x, const KParams& p)
+    {
+        const double d = sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
+        return cscale(exp_ik(p.kr, d), INV4PI);
+    }
+    __device__ static cplx<double> transfer(double d2, double dp2, const KParams& p)
+    {
+        return exp_ik(p.kr, sqrt(d2) - sqrt(dp2));
+    }
+    __device__ static cplx<double> factored(const double* a, const double*, cplx<double> w,
+                                            const double*, double dc, const KParams& p)
+    {
+        const double d = sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+        const cplx<double> v = cmul(w, exp_ik(p.kr, d - dc));
+        return {-v.im, v.re};
+    }
+};
+
+// d/dkappa of the combined-field kernel e^{i kap d} / (4 pi d^3)
+// (nxy (1 - i kap d) - i kap d^2):  e^{i kap d} / (4 pi d) (kap (nxy + d) - i),
+// nxy = -n . x.  Centred factor and centre shift as for K_HELMHOLTZ_DK.
+template <> struct Plugin<K_COMBINEDFIELD_DK>
+{
+    static constexpr bool needs_normals = true;
+    __device__ static cplx<double> kernel(const double* x, const double* n, const KParams& p)
+    {
+        const double kap = p.kr;
+        const double d2 = x[0] * x[0] + x[1] * x[1] + x[2] * x[2];
+        if (d2 < 1e-14)
+            return {0.0, 0.0};
+        const double invd = 1.0 / sqrt(d2);
+        const double d = d2 * invd;
+        const double nxy = -(n[0] * x[0] + n[1] * x[1] + n[2] * x[2]);
+        const cplx<double> e = exp_ik(kap, d);
+        const double f = INV4PI * invd;
+        const double g = kap * (nxy + d); // (g - i) e
+        return {f * (g * e.re + e.im), f * (g * e.im - e.re)};
+    }
+    __device__ static cplx<double> cf(const double* x, const KParams& p)
+    {
+        const double d = sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
+        return cscale(exp_ik(p.kr, d), INV4PI);
+    }
+    __device__ static cplx<double> transfer(double d2, double dp2, const KParams& p)
+    {
+        return exp_ik(p.kr, sqrt(d2) - sqrt(dp2));
+    }
+    __device__ static cplx<double> factored(const double* a, const double* n, cplx<double> w,
+                                            const double*, double dc, const KParams& p)
+    {
+        const double d2 = a[0] * a[0] + a[1] * a[1] + a[2] * a[2];
+        if (!(d2 > 1e-14))
+            return {0.0, 0.0};
+        const double kap = p.kr;
+        const double nxy = -(a[0] * n[0] + a[1] * n[1] + a[2] * n[2]);
+        const double invd = 1.0 / sqrt(d2);
+        const double d = d2 * invd;
+        const cplx<double> v = cmul(w, exp_ik(kap, d - dc));
+        const double g = kap * (nxy + d);
+        return {invd * (g * v.re + v.im), invd * (g * v.im - v.re)};
+    }
+};
+
 // ===========================================================================
 // Mixed precision: FP32 arithmetic on coordinates relative to a nearby box
 // centre, with the phase k*r formed and reduced modulo 2 pi in FP64 and the
@@ -701,6 +779,59 @@ template <> struct PluginF<K_COMBINEDFIELD>
     }
 };
 
+template <> struct PluginF<K_HELMHOLTZ_DK>
+{
+    static constexpr bool needs_normals = false;
+    __device__ static cplx<float> kernel(const float* x, const float*, const KParams& p)
+    {
+        const float d2 = x[0] * x[0] + x[1] * x[1] + x[2] * x[2];
+        if (d2 == 0.f)
+            return {0.f, 0.f};
+        const cplx<float> e = exp_ik_ff(p, d2 * rsqrtf(d2));
+        return {-e.im * INV4PIF, e.re * INV4PIF};
+    }
+    __device__ static cplx<float> factored(const float* a, float aa, const float* b, const float*,
+                                           cplx<float> w, float dc, const KParams& p)
+    {
+        float inv, d, dd, d2;
+        factored_geom(a, aa, b, dc, inv, d, dd, d2);
+        const cplx<float> e = exp_ik_ff(p, dd);
+        return {-(w.re * e.im + w.im * e.re), w.re * e.re - w.im * e.im};
+    }
+};
+template <> struct PluginF<K_COMBINEDFIELD_DK>
+{
+    static constexpr bool needs_normals = true;
+    __device__ static cplx<float> kernel_d(const double* x, const double* n, const KParams& p)
+    {
+        const double d2d = x[0] * x[0] + x[1] * x[1] + x[2] * x[2];
+        if (!(d2d >= 1e-14))
+            return {0.f, 0.f};
+        const float kap = p.krh;
+        const float nxy = (float)-(n[0] * x[0] + n[1] * x[1] + n[2] * x[2]);
+        const float d2 = (float)d2d;
+        const float inv = rsqrtf(d2), d = d2 * inv;
+        const cplx<float> e = exp_ik_ff(p, d);
+        const float f = INV4PIF * inv, g = kap * (nxy + d);
+        return {f * (g * e.re + e.im), f * (g * e.im - e.re)};
+    }
+    __device__ static cplx<float> factored(const float* a, float aa, const float* b, const float* n,
+                                           cplx<float> w, float dc, const KParams& p)
+    {
+        float inv, d, dd, d2;
+        factored_geom(a, aa, b, dc, inv, d, dd, d2);
+        if (!(d2 > 1e-14f))
+            return {0.f, 0.f};
+        const float kap = p.krh;
+        // z = y - x = b - a, nxy = z . n
+        const float nxy = (b[0] - a[0]) * n[0] + (b[1] - a[1]) * n[1] + (b[2] - a[2]) * n[2];
+        const cplx<float> e = exp_ik_ff(p, dd);
+        const float vr = w.re * e.re - w.im * e.im, vi = w.re * e.im + w.im * e.re;
+        const float g = kap * (nxy + d);
+        return {inv * (g * vr + vi), inv * (g * vi - vr)};
+    }
+};
+
 
 // Centred factor CF(y - xc) and centre-shift factor G(y, xc)/G(y, pxc) in
 // mixed precision: distances in FP64 (d2 given), phases reduced in FP64.
@@ -708,6 +839,11 @@ template <int KIND>
 __device__ __forceinline__ cplx<float> cf_mixed(double d2, const KParams& p)
 {
     const double d = sqrt(d2);
+    if (KIND == K_HELMHOLTZ_DK || KIND == K_COMBINEDFIELD_DK)
+    {
+        const cplx<float> e = exp_ik_f(p.kr, d);
+        return {e.re * INV4PIF, e.im * INV4PIF};
+    }
     const float id = rsqrtf((float)d2) * INV4PIF;
     if (KIND == K_LAPLACE)
         return {id, 0.f};
@@ -724,6 +860,8 @@ template <int KIND>
 __device__ __forceinline__ cplx<float> transfer_mixed(double d2, double dp2, const KParams& p)
 {
     const double d = sqrt(d2), dp = sqrt(dp2);
+    if (KIND == K_HELMHOLTZ_DK || KIND == K_COMBINEDFIELD_DK)
+        return exp_ik_f(p.kr, d - dp);
     const float ratio = __fdividef((float)dp, (float)d);
     if (KIND == K_LAPLACE)
         return {ratio, 0.f};

@@ -27,6 +27,8 @@ static constexpr int ERR_INVALID = 1, ERR_CUDA = 2, ERR_STATE = 3, ERR_OOM = 4;
     case K_GRADHELMHOLTZ: { constexpr int KK = K_GRADHELMHOLTZ; CALL; } break;                \
     case K_DOUBLELAYER: { constexpr int KK = K_DOUBLELAYER; CALL; } break;                    \
     case K_COMBINEDFIELD: { constexpr int KK = K_COMBINEDFIELD; CALL; } break;                \
+    case K_HELMHOLTZ_DK: { constexpr int KK = K_HELMHOLTZ_DK; CALL; } break;                  \
+    case K_COMBINEDFIELD_DK: { constexpr int KK = K_COMBINEDFIELD_DK; CALL; } break;          \
     }
 
 #define IFGF_CUDA(x)                                                                          \
@@ -99,6 +101,15 @@ struct DeviceState
     std::vector<DevBuf<UpGeo64>> geo64;                    // per level upward geometry
     std::vector<DevBuf<UpGeo32>> geo32;
     std::vector<DevBuf<int2>> fe_list; // per-row (child element, first group) of each run
+    // what the upward geometry of a level is built from (kept for variants)
+    std::vector<DevBuf<int>> slot_el;      // element of each slot
+    std::vector<DevBuf<double>> child_off; // 8 child-centre offsets
+    std::vector<double> up_pH, up_cH;      // parent / child side lengths
+    // variant kernel (k-derivative) geometry tables and list views
+    int vkind = -1;
+    std::vector<DevBuf<UpGeo64>> vgeo64;
+    std::vector<DevBuf<UpGeo32>> vgeo32;
+    std::vector<LevelLists> vlists;
     std::vector<LevelLists> lists;                         // per level views of the above
     DevBuf<int> fmap;
     DevBuf<double> hi_nodes, A;
@@ -644,6 +655,14 @@ void Operator::setup_device(const double* normals)
     D.geo64.resize(L);
     D.geo32.resize(L);
     D.fe_list.resize(L);
+    D.slot_el.resize(L);
+    D.child_off.resize(L);
+    D.up_pH.assign(L, 0.0);
+    D.up_cH.assign(L, 0.0);
+    D.vkind = -1;
+    D.vgeo64.clear();
+    D.vgeo32.clear();
+    D.vlists.clear();
     std::vector<std::vector<int>> up_host(L);
     std::vector<int> up_pad(L, 0);
     fe_pad_.assign(L, 0);
@@ -780,12 +799,14 @@ void Operator::setup_device(const double* normals)
                     const double cmn = mn + size * (double)((o >> d) & 1), cmx = cmn + size;
                     off[3 * o + d] = (cmx + cmn) / 2.0 - (mx + mn) / 2.0;
                 }
-            DevBuf<double> doff;
+            DevBuf<double>& doff = D.child_off[l];
             doff.upload(off, 24);
-            DevBuf<int> dslot_el;
+            DevBuf<int>& dslot_el = D.slot_el[l];
             dslot_el.upload(slot_el);
             const KParams kp = make_kparams(kr_, ki_, dx_);
             const double pH = S.levels[l].side, cH = S.levels[l + 1].side;
+            D.up_pH[l] = pH;
+            D.up_cH[l] = cH;
             const int ns = (int)slot_el.size();
             DevBuf<int> drow;
             drow.alloc((size_t)ns * 16);
@@ -894,13 +915,13 @@ struct EventHooks : LaunchHooks
     }
 };
 
-void Operator::fill_mult_ptrs(MultPtrs& m) const
+void Operator::fill_mult_ptrs(MultPtrs& m, bool variant) const
 {
     const DeviceState& D = *dev_;
     m.L = (int)lv_.size();
     m.lv_host = lv_.data();
     m.lv_dev = D.lv.p;
-    m.lists = D.lists.data();
+    m.lists = variant ? D.vlists.data() : D.lists.data();
     m.T = TreeArgs{D.box_c.p, D.box_H.p, D.box_first.p, D.box_last.p, D.box_child.p,
                    D.box_level.p, D.box_leaf.p};
     m.S = SrcArgs{D.sx.p, D.sy.p, D.sz.p, D.nx.p, D.ny.p, D.nz.p};
@@ -943,7 +964,71 @@ void Operator::fill_mult_ptrs(MultPtrs& m) const
 }
 
 
-void Operator::launch_mult(const void* d_w, void* d_u, void* stream, bool timed)
+int Operator::dk_kind() const
+{
+    return kind_ == K_HELMHOLTZ ? K_HELMHOLTZ_DK : kind_ == K_COMBINEDFIELD ? K_COMBINEDFIELD_DK : -1;
+}
+
+// Upward geometry tables of another kernel on the same tree and cones: the
+// rows (elements, nodes, local coordinates, runs) are the base kernel's and
+// only the centre-shift factors differ, so the fill pass simply runs again
+// with the variant kernel.
+void Operator::ensure_variant_tables(int vkind)
+{
+    DeviceState& D = *dev_;
+    if (D.vkind == vkind)
+        return;
+    const int L = (int)lv_.size();
+    const int P_hi = hi_[0] * hi_[1] * hi_[2];
+    const KParams kp = make_kparams(kr_, ki_, dx_);
+    D.vkind = -1;
+    D.vgeo64.clear();
+    D.vgeo32.clear();
+    D.vgeo64.resize(L);
+    D.vgeo32.resize(L);
+    D.vlists = D.lists;
+    for (int l = 0; l + 1 < L; l++)
+    {
+        const LevelLists& LL = D.lists[l];
+        const int ns = (int)D.slot_el[l].n;
+        if (ns == 0 || LL.up_pad <= 0)
+            continue;
+        const size_t n_ent = (size_t)ns * 8 * (size_t)LL.up_pad;
+        D.vgeo64[l].alloc(n_ent);
+        D.vgeo32[l].alloc(n_ent);
+        IFGF_CUDA(cudaMemset(D.vgeo64[l].p, 0xff, n_ent * sizeof(UpGeo64)));
+        IFGF_CUDA(cudaMemset(D.vgeo32[l].p, 0xff, n_ent * sizeof(UpGeo32)));
+        IFGF_DISPATCH(vkind, launch_build_upgeo<KK>(lv_[l], lv_[l + 1], D.up_pH[l], D.up_cH[l],
+                                                     D.child_off[l].p, D.slot_el[l].p, ns,
+                                                     D.hi_nodes.p, P_hi, kp, LL.up_pad,
+                                                     D.vgeo64[l].p, D.vgeo32[l].p, LL.fe_pad,
+                                                     D.fe_list[l].p));
+        IFGF_CUDA(cudaDeviceSynchronize());
+        D.vlists[l].geo64 = D.vgeo64[l].p;
+        D.vlists[l].geo32 = D.vgeo32[l].p;
+    }
+    D.vkind = vkind;
+}
+
+void Operator::mult_dk_device(const void* d_w, void* d_u, void* stream)
+{
+    const int vk = dk_kind();
+    if (vk < 0)
+        throw Error(ERR_INVALID, "the k-derivative exists for the Helmholtz and combined-field "
+                                 "kernels only");
+    launch_mult(d_w, d_u, stream, false, vk);
+}
+
+void Operator::mult_dk_host(const void* w, void* u, int64_t batch)
+{
+    const int vk = dk_kind();
+    if (vk < 0)
+        throw Error(ERR_INVALID, "the k-derivative exists for the Helmholtz and combined-field "
+                                 "kernels only");
+    host_mult_loop(w, u, batch, vk);
+}
+
+void Operator::launch_mult(const void* d_w, void* d_u, void* stream, bool timed, int vkind)
 {
     if (!initialized_)
         throw Error(ERR_STATE, "mult called before init");
@@ -951,13 +1036,16 @@ void Operator::launch_mult(const void* d_w, void* d_u, void* stream, bool timed)
         throw Error(ERR_INVALID, "null density or result buffer");
     cudaStream_t st = (cudaStream_t)stream;
     DeviceState& D = *dev_;
+    if (vkind >= 0)
+        ensure_variant_tables(vkind);
     MultPtrs m;
-    fill_mult_ptrs(m);
+    fill_mult_ptrs(m, vkind >= 0);
     EventHooks log(D, st);
     const bool on = profiling_ || timed;
     int launches = 0;
-    IFGF_DISPATCH(kind_, launches = launch_mult_kernels<KK>(m, d_w, d_u, is_real(), st,
-                                                             on ? &log : nullptr));
+    IFGF_DISPATCH(vkind >= 0 ? vkind : kind_,
+                  launches = launch_mult_kernels<KK>(m, d_w, d_u, is_real(), st,
+                                                     on ? &log : nullptr));
     launches_per_mult_ = launches;
     if (on && log.n > 0)
     {
@@ -1010,6 +1098,11 @@ void Operator::mult_device(const void* d_w, void* d_u, void* stream)
 
 void Operator::mult_host(const void* w, void* u, int64_t batch)
 {
+    host_mult_loop(w, u, batch, -1);
+}
+
+void Operator::host_mult_loop(const void* w, void* u, int64_t batch, int vkind)
+{
     if (!initialized_)
         throw Error(ERR_STATE, "mult called before init");
     if (!w || !u)
@@ -1027,7 +1120,7 @@ void Operator::mult_host(const void* w, void* u, int64_t batch)
     {
         IFGF_CUDA(cudaMemcpy(D.io_w.p, (const double*)w + b * nw, nw * sizeof(double),
                              cudaMemcpyHostToDevice));
-        launch_mult(D.io_w.p, D.io_u.p, nullptr, false);
+        launch_mult(D.io_w.p, D.io_u.p, nullptr, false, vkind);
         IFGF_CUDA(cudaMemcpy((double*)u + b * nu, D.io_u.p, nu * sizeof(double),
                              cudaMemcpyDeviceToHost));
     }
@@ -1083,8 +1176,12 @@ void Operator::mult_device_external_scratch(const void* d_w, void* d_u, void* st
     IFGF_DISPATCH(kind_, launch_mult_kernels<KK>(m, d_w, d_u, is_real(), st, nullptr));
 }
 
-void Operator::direct_eval(const void* w, const int64_t* tidx, int64_t nt, void* out)
+void Operator::direct_eval(const void* w, const int64_t* tidx, int64_t nt, void* out, bool dk)
 {
+    const int ek = dk ? dk_kind() : kind_;
+    if (ek < 0)
+        throw Error(ERR_INVALID, "the k-derivative exists for the Helmholtz and combined-field "
+                                 "kernels only");
     if (!initialized_)
         throw Error(ERR_STATE, "direct_eval called before init");
     if (!w || !out || (nt > 0 && !tidx))
@@ -1115,7 +1212,7 @@ void Operator::direct_eval(const void* w, const int64_t* tidx, int64_t nt, void*
     dout.alloc(nt);
     MultPtrs m;
     fill_mult_ptrs(m);
-    IFGF_DISPATCH(kind_, permute_only<KK>(m, D.io_w.p, is_real(), nullptr);
+    IFGF_DISPATCH(ek, permute_only<KK>(m, D.io_w.p, is_real(), nullptr);
                   launch_direct_kernel<KK>(m, dpos.p, (int)nt, dout.p, nullptr));
     std::vector<double2> h(nt);
     IFGF_CUDA(cudaMemcpy(h.data(), dout.p, nt * sizeof(double2), cudaMemcpyDeviceToHost));

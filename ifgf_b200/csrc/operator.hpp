@@ -44,8 +44,16 @@ class Operator
     // of the buffers allocated at init; allocates nothing
     void mult_device_external_scratch(const void* d_w, void* d_u, void* stream, void* scratch,
                                       size_t scratch_bytes);
-    // FP64 direct sum at selected targets (original indices), host buffers
-    void direct_eval(const void* w, const int64_t* tidx, int64_t nt, void* out);
+    // (dA/dk) w for the Helmholtz and combined-field kernels: the same tree,
+    // cones and orders, with the k-derivative kernel (K_HELMHOLTZ_DK,
+    // K_COMBINEDFIELD_DK); its upward geometry is tabulated on first use
+    void mult_dk_device(const void* d_w, void* d_u, void* stream);
+    void mult_dk_host(const void* w, void* u, int64_t batch);
+    // kernel of the k-derivative, or -1 when the kernel has none
+    int dk_kind() const;
+    // FP64 direct sum at selected targets (original indices), host buffers;
+    // with dk, of the k-derivative kernel
+    void direct_eval(const void* w, const int64_t* tidx, int64_t nt, void* out, bool dk = false);
     void set_profiling(bool on);
 
     int kind() const { return kind_; }
@@ -65,8 +73,11 @@ class Operator
     void elements_for_box(double H, int step, int64_t* out) const;
     double cutoff_limit(double H) const;
     void setup_device(const double* normals);
-    void launch_mult(const void* d_w, void* d_u, void* stream, bool timed);
-    void fill_mult_ptrs(MultPtrs& m) const;
+    // vkind >= 0: run that kernel with the variant geometry tables
+    void launch_mult(const void* d_w, void* d_u, void* stream, bool timed, int vkind = -1);
+    void fill_mult_ptrs(MultPtrs& m, bool variant = false) const;
+    void ensure_variant_tables(int vkind);
+    void host_mult_loop(const void* w, void* u, int64_t batch, int vkind);
 
     int kind_;
     double kr_, ki_;

@@ -130,13 +130,31 @@ class IfgfOperator:
         check(lib.ifgf_mult_device(self._h, C.c_void_p(w_ptr), C.c_void_p(u_ptr),
                                    C.c_void_p(stream_ptr)))
 
-    def direct_eval(self, weights, targets):
-        """FP64 dense direct sum at the given target indices (on the GPU)."""
+    def mult_dk(self, weights):
+        """(dA/dk) . w, the matvec of the wavenumber derivative of the kernel
+        (Helmholtz and combined field); a (batch, N) array gives (batch, M)."""
+        w = np.ascontiguousarray(np.asarray(weights, dtype=self._dtype()))
+        batch = w.shape[0] if w.ndim == 2 else 1
+        if w.shape[-1] != self._n_src or w.ndim > 2:
+            raise ValueError(f"weights must have shape ([batch,] {self._n_src})")
+        u = np.empty(w.shape[:-1] + (self._n_tgt,), dtype=self._dtype())
+        check(lib.ifgf_mult_dk(self._h, w.ctypes.data, u.ctypes.data, batch))
+        return u
+
+    def mult_dk_device(self, w_ptr, u_ptr, stream_ptr=0):
+        """Enqueue (dA/dk) . w on device buffers (raw pointers)."""
+        check(lib.ifgf_mult_dk_device(self._h, C.c_void_p(w_ptr), C.c_void_p(u_ptr),
+                                      C.c_void_p(stream_ptr)))
+
+    def direct_eval(self, weights, targets, dk=False):
+        """FP64 dense direct sum at the given target indices (on the GPU);
+        dk=True sums the k-derivative kernel."""
         w = np.ascontiguousarray(np.asarray(weights, dtype=self._dtype()))
         t = np.ascontiguousarray(np.asarray(targets, dtype=np.int64))
         out = np.empty(len(t), dtype=self._dtype())
-        check(lib.ifgf_direct_eval(self._h, w.ctypes.data, t.ctypes.data_as(C.POINTER(C.c_long)),
-                                   len(t), out.ctypes.data))
+        fn = lib.ifgf_direct_eval_dk if dk else lib.ifgf_direct_eval
+        check(fn(self._h, w.ctypes.data, t.ctypes.data_as(C.POINTER(C.c_long)), len(t),
+                 out.ctypes.data))
         return out
 
     def set_profiling(self, on=True):

@@ -112,11 +112,25 @@ int ifgf_mult_device(ifgf_operator* op, const void* d_w, void* d_u, void* stream
  * overlaps race and must be serialised.  No reference counterpart. */
 int ifgf_mult_device_noalloc(ifgf_operator* op, const void* d_w, void* d_u, void* stream);
 
+/* u = (dA/dk) w: the matvec of the wavenumber derivative of the kernel,
+ * for the Helmholtz kernel (dG/dk = i e^{ikr}/(4 pi)) and the combined-field
+ * kernel (e^{i kap r}/(4 pi r) (kap (n.(y - x) + r) - i)); other kernels
+ * return IFGF_ERR_INVALID_ARG.  It runs on the operator's tree, cones and
+ * orders with the derivative kernel factored by e^{ik r_c}/(4 pi); the first
+ * call tabulates its upward geometry.  Buffers as in ifgf_mult_batch (host)
+ * and ifgf_mult_device (device).  No reference counterpart: the reference
+ * has no k-derivative; gradients with respect to k of a matvec are
+ * (dA/dk) w. */
+int ifgf_mult_dk(ifgf_operator* op, const void* w, void* u, long batch);
+int ifgf_mult_dk_device(ifgf_operator* op, const void* d_w, void* d_u, void* stream);
+
 /* FP64 dense direct sum u(y_t) = sum_s w_s G(x_s - y_t) on the GPU at the
  * targets listed in tidx (caller's target indices), for error estimates:
  * w as in ifgf_mult (host buffer), out receives nt values.  The reference
  * checks its mult the same way on the host (test/test_ifgf.cpp:143-165). */
 int ifgf_direct_eval(ifgf_operator* op, const void* w, const long* tidx, long nt, void* out);
+/* ifgf_direct_eval of the k-derivative kernel (see ifgf_mult_dk). */
+int ifgf_direct_eval_dk(ifgf_operator* op, const void* w, const long* tidx, long nt, void* out);
 
 /* Per-kernel CUDA-event timing of every following mult (on the stream the
  * kernels run on); on != 0 enables and resets the counters.  Results appear

@@ -489,8 +489,20 @@ enum Kind
     MODHELMHOLTZ = 2,   // modified_helmholtz_ifgf.hpp
     GRADHELMHOLTZ = 3,  // grad_helmholtz_ifgf.hpp
     DOUBLELAYER = 4,    // double_layer_helmholtz_ifgf.hpp
-    COMBINEDFIELD = 5   // combined_field_helmholtz_ifgf.hpp
+    COMBINEDFIELD = 5,  // combined_field_helmholtz_ifgf.hpp
+    // wavenumber derivatives of kinds 1 and 5.  Not in the reference: the
+    // kernels are the k-derivatives of helmholtz_ifgf.hpp:94-112 and
+    // combined_field_helmholtz_ifgf.hpp:110-129, factored with the centred
+    // factor e^{ik r_c} / (4 pi); orders and cone grids are the base kernel's
+    HELMHOLTZ_DK = 6,
+    COMBINEDFIELD_DK = 7
 };
+
+// kernel whose orders and cone grids a kind follows
+inline int grid_kind(int kind)
+{
+    return kind == HELMHOLTZ_DK ? HELMHOLTZ : kind == COMBINEDFIELD_DK ? COMBINEDFIELD : kind;
+}
 
 struct KernelDef
 {
@@ -508,7 +520,7 @@ struct KernelDef
             if (step == 0)
             {
                 out[i] = base[i] - 3;
-                if (kind == HELMHOLTZ || kind == GRADHELMHOLTZ)
+                if (grid_kind(kind) == HELMHOLTZ || kind == GRADHELMHOLTZ)
                     out[i] = std::max(out[i], 2);
             }
         }
@@ -518,6 +530,7 @@ struct KernelDef
     // double_layer_helmholtz_ifgf.hpp:190-214, combined_field_helmholtz_ifgf.hpp:201-224)
     void elements_for_box(double H, const long* base_in, int step, long* out) const
     {
+        const int kind = grid_kind(this->kind);
         long base[3] = {base_in[0], base_in[1], base_in[2]};
         if (kind == LAPLACE)
         {
@@ -596,6 +609,16 @@ struct KernelDef
             return cd(f * (c * nxy + s * kap * (dd * nxy + d2)),
                       f * (-c * kap * (dd * nxy + d2) + s * nxy));
         }
+        case HELMHOLTZ_DK: // d/dk e^{ikd}/(4 pi d) = i e^{ikd}/(4 pi)
+            return (d == 0) ? cd(0) : cd(0, 1) * std::exp(cd(0, k.real()) * d) / (4 * PI);
+        case COMBINEDFIELD_DK: // e^{i kap d}/(4 pi d) (kap (nxy + d) - i)
+        {
+            if (d2 < 1e-14)
+                return 0;
+            const double kap = k.real();
+            const double nxy = -(n[0] * x[0] + n[1] * x[1] + n[2] * x[2]);
+            return std::exp(cd(0, kap) * d) / (4 * PI * d) * cd(kap * (nxy + d), -1.0);
+        }
         }
         return 0;
     }
@@ -614,6 +637,9 @@ struct KernelDef
             return std::exp(cd(0, k.real()) * d) * id * (1 / (4.0 * PI));
         case COMBINEDFIELD: // combined_field_helmholtz_ifgf.hpp:81-91
             return std::exp(cd(0., k.real()) * d) * id * (1 / (4.0 * PI));
+        case HELMHOLTZ_DK:
+        case COMBINEDFIELD_DK:
+            return std::exp(cd(0., k.real()) * d) * (1 / (4.0 * PI));
         default: // modified_helmholtz_ifgf.hpp:56-64, grad:87-98, dl:80-89
             return std::exp(-k * d) * id * (1 / (4.0 * PI));
         }
@@ -658,6 +684,9 @@ struct KernelDef
             const double dp = std::sqrt(dp2), d = d2 * invd;
             return std::exp(cd(0., k.real()) * (d - dp)) * (dp * invd);
         }
+        case HELMHOLTZ_DK:
+        case COMBINEDFIELD_DK:
+            return std::exp(cd(0., k.real()) * (std::sqrt(d2) - std::sqrt(dp2)));
         }
         return 0;
     }
@@ -771,6 +800,36 @@ struct KernelDef
                 }
             }
             return cd(re, im);
+        }
+        case HELMHOLTZ_DK: // i e^{ik(d - dc)}
+        {
+            const double kr = k.real();
+            for (size_t i = 0; i < ns; i++)
+            {
+                const double* x = xs + 3 * i;
+                double a = x[0] - y[0], b = x[1] - y[1], c = x[2] - y[2];
+                double d = std::sqrt(a * a + b * b + c * c);
+                res += w[i] * cd(0, 1) * std::exp(cd(0, kr) * (d - dc));
+            }
+            return res;
+        }
+        case COMBINEDFIELD_DK: // e^{i kap (d - dc)} (kap (nxy + d) - i) / d
+        {
+            const double kap = k.real();
+            for (size_t i = 0; i < ns; i++)
+            {
+                const double* x = xs + 3 * i;
+                const double* n = nrm + 3 * i;
+                const double z0 = y[0] - x[0], z1 = y[1] - x[1], z2 = y[2] - x[2];
+                const double d2 = z0 * z0 + z1 * z1 + z2 * z2;
+                if (d2 > 1e-14)
+                {
+                    const double nxy = z0 * n[0] + z1 * n[1] + z2 * n[2];
+                    const double d = std::sqrt(d2);
+                    res += w[i] * std::exp(cd(0, kap) * (d - dc)) * cd(kap * (nxy + d), -1.0) / d;
+                }
+            }
+            return res;
         }
         }
         return res;

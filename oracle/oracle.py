@@ -24,6 +24,9 @@ KINDS = {
     "grad_helmholtz": 3,
     "double_layer": 4,
     "combined_field": 5,
+    # k-derivatives of kinds 1 and 5 (not reference kernels; see the C++ header)
+    "helmholtz_dk": 6,
+    "combined_field_dk": 7,
 }
 
 _dp = C.POINTER(C.c_double)
