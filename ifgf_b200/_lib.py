@@ -57,6 +57,8 @@ def _load():
         "ifgf_direct_eval": [H, C.c_void_p, _lp, C.c_long, C.c_void_p],
         "ifgf_direct_eval_dk": [H, C.c_void_p, _lp, C.c_long, C.c_void_p],
         "ifgf_mult_dk": [H, C.c_void_p, C.c_void_p, C.c_long],
+        "ifgf_mult_adjoint": [H, C.c_void_p, C.c_void_p, C.c_long],
+        "ifgf_mult_adjoint_device": [H, C.c_void_p, C.c_void_p, C.c_void_p],
         "ifgf_mult_dk_device": [H, C.c_void_p, C.c_void_p, C.c_void_p],
         "ifgf_set_profiling": [H, C.c_int],
         "ifgf_num_sources": [H, _lp],
@@ -87,7 +89,8 @@ EXPORTED = [
     "ifgf_create", "ifgf_set_dx", "ifgf_set_precision", "ifgf_init", "ifgf_init_plan_only",
     "ifgf_box_list", "ifgf_mult",
     "ifgf_mult_batch", "ifgf_mult_device", "ifgf_mult_device_noalloc", "ifgf_direct_eval",
-    "ifgf_mult_dk", "ifgf_mult_dk_device", "ifgf_direct_eval_dk",
+    "ifgf_mult_dk", "ifgf_mult_dk_device", "ifgf_direct_eval_dk", "ifgf_mult_adjoint",
+    "ifgf_mult_adjoint_device",
     "ifgf_set_profiling",
     "ifgf_num_sources", "ifgf_num_targets",
     "ifgf_stats_json", "ifgf_tree_levels", "ifgf_tree_num_boxes", "ifgf_tree_permutation",

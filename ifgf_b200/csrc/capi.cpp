@@ -154,6 +154,20 @@ extern "C"
         });
     }
 
+    int ifgf_mult_adjoint(ifgf_operator* h, const void* w, void* u, long batch)
+    {
+        if (!h)
+            return null_handle();
+        return guarded([&] { h->op.mult_adjoint_host(w, u, batch); });
+    }
+
+    int ifgf_mult_adjoint_device(ifgf_operator* h, const void* d_w, void* d_u, void* stream)
+    {
+        if (!h)
+            return null_handle();
+        return guarded([&] { h->op.mult_adjoint_device(d_w, d_u, stream); });
+    }
+
     int ifgf_mult_dk(ifgf_operator* h, const void* w, void* u, long batch)
     {
         if (!h)

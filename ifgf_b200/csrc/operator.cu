@@ -137,6 +137,20 @@ struct DeviceState
     }
 };
 
+// Operators and buffers of the adjoint (see Operator::mult_adjoint_device).
+struct AdjointState
+{
+    // 0: conj(A conj w) on this operator; 1: sign conj(A' conj w) on the
+    // swapped operator; 2: double layer; 3: combined field
+    int mode = -1;
+    double sign = 1;
+    std::vector<std::unique_ptr<Operator>> ops;
+    DevBuf<double2> wc;    // conj(w)
+    DevBuf<double2> z[4];  // results of the swapped operators
+    DevBuf<double> nx, ny, nz; // source normals in the caller's order
+    DevBuf<double> io_w, io_u; // host-buffer staging
+};
+
 // ---------------------------------------------------------------------------
 // Setup kernels: active-cone marking (octree.hpp:571-690) and compaction
 // ---------------------------------------------------------------------------
@@ -321,6 +335,8 @@ void Operator::set_dx(int dx)
 {
     if (dx < -1 || dx > 2)
         throw Error(ERR_INVALID, "dx must be -1, 0, 1 or 2");
+    if (dx != dx_)
+        adj_.reset(); // the adjoint of the gradient kernel follows dx
     dx_ = dx;
 }
 
@@ -333,6 +349,9 @@ void Operator::set_precision(int mode)
     if (mode != precision_ && initialized_)
         dev_->fcoef.zero();
     precision_ = mode;
+    if (adj_)
+        for (auto& op : adj_->ops)
+            op->set_precision(mode);
 }
 
 // orderForBox of each plug-in (helmholtz_ifgf.hpp:158-170, laplace_ifgf.hpp:134-146,
@@ -436,6 +455,15 @@ void Operator::init(const double* srcs, int64_t ns, const double* tgts, int64_t 
         lo_[1] > 16 || lo_[2] > 16)
         throw Error(ERR_INVALID, "interpolation order too high");
 
+    adj_.reset();
+    src_pts_.assign(srcs, srcs + 3 * ns);
+    tgt_pts_.assign(tgts, tgts + 3 * nt);
+    if (normals)
+        normals_.assign(normals, normals + 3 * ns);
+    else
+        normals_.clear();
+    cutoff_ = cutoff;
+    same_points_ = ns == nt && std::equal(srcs, srcs + 3 * ns, tgts);
     plan_ = Plan();
     plan_.src.build(srcs, ns, leaf_);
     plan_.tgt.build(tgts, nt, leaf_);
@@ -963,6 +991,187 @@ void Operator::fill_mult_ptrs(MultPtrs& m, bool variant) const
     m.mixed = precision_ == PREC_MIXED;
 }
 
+
+// ---------------------------------------------------------------------------
+// Adjoint
+// ---------------------------------------------------------------------------
+
+// out = sign conj(in)
+static __global__ void adj_conj_kernel(const double2* __restrict__ in, double2* out, long long n,
+                                       double sign)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+    {
+        const double2 v = in[i];
+        out[i] = make_double2(sign * v.x, -sign * v.y);
+    }
+}
+
+// out = sign conj(sum_d n_d z_d - i kap y)   (y may be null)
+static __global__ void adj_combine_kernel(const double2* __restrict__ z0,
+                                          const double2* __restrict__ z1,
+                                          const double2* __restrict__ z2,
+                                          const double2* __restrict__ y,
+                                          const double* __restrict__ nx,
+                                          const double* __restrict__ ny,
+                                          const double* __restrict__ nz, double kap, double sign,
+                                          double2* out, long long n)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+    {
+        const double a = nx[i], b = ny[i], c = nz[i];
+        double sr = a * z0[i].x + b * z1[i].x + c * z2[i].x;
+        double si = a * z0[i].y + b * z1[i].y + c * z2[i].y;
+        if (y)
+        {
+            sr += kap * y[i].y;
+            si -= kap * y[i].x;
+        }
+        out[i] = make_double2(sign * sr, -sign * si);
+    }
+}
+
+static unsigned elementwise_grid(long long n)
+{
+    return (unsigned)std::max<long long>(1, std::min<long long>((n + 255) / 256, 148 * 16));
+}
+
+void Operator::ensure_adjoint()
+{
+    if (adj_)
+        return;
+    if (!initialized_)
+        throw Error(ERR_STATE, "adjoint called before init");
+    auto A = std::make_unique<AdjointState>();
+    const int64_t ns = n_src(), nt = n_tgt();
+    const bool sym = kind_ == K_LAPLACE || kind_ == K_HELMHOLTZ || kind_ == K_MODHELMHOLTZ;
+    // an operator of kernel `kind` (wavenumber kr + i ki, component dx) from
+    // the targets to the sources
+    auto swapped = [&](int kind, double kr, double ki, int dx) {
+        std::unique_ptr<Operator> op(
+            new Operator(kind, kr, ki, leaf_, order0_, base_n_[0], tol_));
+        op->set_dx(dx);
+        op->set_precision(precision_);
+        op->init(tgt_pts_.data(), nt, src_pts_.data(), ns, nullptr, cutoff_);
+        return op;
+    };
+    if (sym && same_points_)
+        A->mode = 0;
+    else if (sym || kind_ == K_GRADHELMHOLTZ)
+    {
+        A->mode = 1;
+        A->sign = kind_ == K_GRADHELMHOLTZ ? -1.0 : 1.0; // the gradient kernel is odd
+        A->ops.push_back(swapped(kind_, kr_, ki_, dx_));
+    }
+    else if (kind_ == K_DOUBLELAYER)
+    {
+        // G_DL(x, n_s) = sum_d n_s[d] G_grad,d(x) with the same k
+        A->mode = 2;
+        A->sign = -1.0;
+        for (int d = 0; d < 3; d++)
+            A->ops.push_back(swapped(K_GRADHELMHOLTZ, kr_, ki_, d));
+    }
+    else if (kind_ == K_COMBINEDFIELD)
+    {
+        // G_CF = dG/dn_s - i kap G with G = e^{i kap r}/(4 pi r), and
+        // dG/dn_s = -sum_d n_s[d] G_grad,d for the gradient kernel at k = -i kap
+        A->mode = 3;
+        A->sign = 1.0;
+        for (int d = 0; d < 3; d++)
+            A->ops.push_back(swapped(K_GRADHELMHOLTZ, 0.0, -kr_, d));
+        A->ops.push_back(swapped(K_HELMHOLTZ, kr_, 0.0, -1));
+    }
+    else
+        throw Error(ERR_INVALID, "no adjoint for this kernel");
+    if (!is_real())
+        A->wc.alloc(nt);
+    for (size_t i = 0; i < A->ops.size() || (A->mode == 0 && i == 0); i++)
+        if (!is_real())
+            A->z[i].alloc(ns);
+    if (A->mode >= 2)
+    {
+        if (normals_.size() != (size_t)(3 * ns))
+            throw Error(ERR_STATE, "the adjoint of this kernel needs the source normals");
+        std::vector<double> c(ns);
+        DevBuf<double>* dst[3] = {&A->nx, &A->ny, &A->nz};
+        for (int d = 0; d < 3; d++)
+        {
+            for (int64_t i = 0; i < ns; i++)
+                c[i] = normals_[3 * i + d];
+            dst[d]->upload(c);
+        }
+    }
+    adj_ = std::move(A);
+}
+
+void Operator::mult_adjoint_device(const void* d_w, void* d_u, void* stream)
+{
+    if (!d_w || !d_u)
+        throw Error(ERR_INVALID, "null density or result buffer");
+    ensure_adjoint();
+    AdjointState& A = *adj_;
+    cudaStream_t st = (cudaStream_t)stream;
+    const long long ns = n_src(), nt = n_tgt();
+    if (is_real())
+    {
+        // A^H = A^T for the real Laplace kernel
+        if (A.mode == 0)
+            mult_device(d_w, d_u, stream);
+        else
+            A.ops[0]->mult_device(d_w, d_u, stream);
+        return;
+    }
+    adj_conj_kernel<<<elementwise_grid(nt), 256, 0, st>>>((const double2*)d_w, A.wc.p, nt, 1.0);
+    IFGF_CUDA(cudaGetLastError());
+    double2* u = (double2*)d_u;
+    switch (A.mode)
+    {
+    case 0:
+        mult_device(A.wc.p, A.z[0].p, stream);
+        adj_conj_kernel<<<elementwise_grid(ns), 256, 0, st>>>(A.z[0].p, u, ns, A.sign);
+        break;
+    case 1:
+        A.ops[0]->mult_device(A.wc.p, A.z[0].p, stream);
+        adj_conj_kernel<<<elementwise_grid(ns), 256, 0, st>>>(A.z[0].p, u, ns, A.sign);
+        break;
+    default:
+        for (size_t i = 0; i < A.ops.size(); i++)
+            A.ops[i]->mult_device(A.wc.p, A.z[i].p, stream);
+        adj_combine_kernel<<<elementwise_grid(ns), 256, 0, st>>>(
+            A.z[0].p, A.z[1].p, A.z[2].p, A.mode == 3 ? A.z[3].p : nullptr, A.nx.p, A.ny.p,
+            A.nz.p, kr_, A.sign, u, ns);
+        break;
+    }
+    IFGF_CUDA(cudaGetLastError());
+}
+
+void Operator::mult_adjoint_host(const void* w, void* u, int64_t batch)
+{
+    if (!initialized_)
+        throw Error(ERR_STATE, "adjoint called before init");
+    if (!w || !u)
+        throw Error(ERR_INVALID, "null density or result buffer");
+    if (batch < 1)
+        throw Error(ERR_INVALID, "batch must be >= 1");
+    ensure_adjoint();
+    AdjointState& A = *adj_;
+    const size_t per = is_real() ? 1 : 2;
+    const size_t nw = per * (size_t)n_tgt(), nu = per * (size_t)n_src();
+    if (A.io_w.n < nw)
+        A.io_w.alloc(nw);
+    if (A.io_u.n < nu)
+        A.io_u.alloc(nu);
+    for (int64_t b = 0; b < batch; b++)
+    {
+        IFGF_CUDA(cudaMemcpy(A.io_w.p, (const double*)w + b * nw, nw * sizeof(double),
+                             cudaMemcpyHostToDevice));
+        mult_adjoint_device(A.io_w.p, A.io_u.p, nullptr);
+        IFGF_CUDA(cudaMemcpy((double*)u + b * nu, A.io_u.p, nu * sizeof(double),
+                             cudaMemcpyDeviceToHost));
+    }
+}
 
 int Operator::dk_kind() const
 {

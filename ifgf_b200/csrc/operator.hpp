@@ -14,8 +14,9 @@
 namespace ifgf
 {
 
-struct DeviceState; // device buffers, defined in operator.cu
-struct MultPtrs;    // kernel launch view, defined in mult.hpp
+struct DeviceState;  // device buffers, defined in operator.cu
+struct MultPtrs;     // kernel launch view, defined in mult.hpp
+struct AdjointState; // operators and buffers of the adjoint, defined in operator.cu
 
 struct StageTimes
 {
@@ -51,6 +52,17 @@ class Operator
     void mult_dk_host(const void* w, void* u, int64_t batch);
     // kernel of the k-derivative, or -1 when the kernel has none
     int dk_kind() const;
+    // u = A^H w (w over the targets, u over the sources).  Kernels symmetric
+    // under exchanging source and target (Laplace, Helmholtz, modified
+    // Helmholtz) give conj(A' conj(w)) with A' the operator with the roles of
+    // the point sets swapped (A itself when sources and targets are the same
+    // points); the gradient kernel, antisymmetric, the negative of that; the
+    // double-layer and combined-field kernels carry the normal at the new
+    // target and are composed from three swapped gradient operators (plus a
+    // swapped Helmholtz one for the combined field).  The operators are built
+    // on first use from the points, normals and cutoff of init.
+    void mult_adjoint_device(const void* d_w, void* d_u, void* stream);
+    void mult_adjoint_host(const void* w, void* u, int64_t batch);
     // FP64 direct sum at selected targets (original indices), host buffers;
     // with dk, of the k-derivative kernel
     void direct_eval(const void* w, const int64_t* tidx, int64_t nt, void* out, bool dk = false);
@@ -77,6 +89,7 @@ class Operator
     void launch_mult(const void* d_w, void* d_u, void* stream, bool timed, int vkind = -1);
     void fill_mult_ptrs(MultPtrs& m, bool variant = false) const;
     void ensure_variant_tables(int vkind);
+    void ensure_adjoint();
     void host_mult_loop(const void* w, void* u, int64_t batch, int vkind);
 
     int kind_;
@@ -95,6 +108,11 @@ class Operator
     int lo_[3], hi_[3];
     int fct_[3];
     std::unique_ptr<DeviceState> dev_;
+    // init inputs in the caller's order, kept for the adjoint operators
+    std::vector<double> src_pts_, tgt_pts_, normals_;
+    std::function<bool(double)> cutoff_;
+    bool same_points_ = false;
+    std::unique_ptr<AdjointState> adj_;
     // statistics
     double init_ms_ = 0;
     StageTimes last_;

@@ -75,6 +75,9 @@ class IfgfOperator:
                 return 1 if f(dist) else 0
             cb = _lib.CUTOFF_FN(_cb)
         dp = C.POINTER(C.c_double)
+        # the library calls the cutoff again when it builds the adjoint's
+        # operators, so the callback lives as long as the operator
+        self._cutoff_cb = cb
         check(lib.ifgf_init(self._h, s.ctypes.data_as(dp), s.shape[0], t.ctypes.data_as(dp),
                             t.shape[0], n.ctypes.data_as(dp) if n is not None else None, cb, None))
         self._n_src, self._n_tgt = s.shape[0], t.shape[0]
@@ -140,6 +143,22 @@ class IfgfOperator:
         u = np.empty(w.shape[:-1] + (self._n_tgt,), dtype=self._dtype())
         check(lib.ifgf_mult_dk(self._h, w.ctypes.data, u.ctypes.data, batch))
         return u
+
+    def mult_adjoint(self, weights):
+        """A^H . w: one value per target in, one per source out; a (batch, M)
+        array gives (batch, N)."""
+        w = np.ascontiguousarray(np.asarray(weights, dtype=self._dtype()))
+        batch = w.shape[0] if w.ndim == 2 else 1
+        if w.shape[-1] != self._n_tgt or w.ndim > 2:
+            raise ValueError(f"weights must have shape ([batch,] {self._n_tgt})")
+        u = np.empty(w.shape[:-1] + (self._n_src,), dtype=self._dtype())
+        check(lib.ifgf_mult_adjoint(self._h, w.ctypes.data, u.ctypes.data, batch))
+        return u
+
+    def mult_adjoint_device(self, w_ptr, u_ptr, stream_ptr=0):
+        """Enqueue A^H . w on device buffers (raw pointers)."""
+        check(lib.ifgf_mult_adjoint_device(self._h, C.c_void_p(w_ptr), C.c_void_p(u_ptr),
+                                           C.c_void_p(stream_ptr)))
 
     def mult_dk_device(self, w_ptr, u_ptr, stream_ptr=0):
         """Enqueue (dA/dk) . w on device buffers (raw pointers)."""

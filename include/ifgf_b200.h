@@ -124,6 +124,21 @@ int ifgf_mult_device_noalloc(ifgf_operator* op, const void* d_w, void* d_u, void
 int ifgf_mult_dk(ifgf_operator* op, const void* w, void* u, long batch);
 int ifgf_mult_dk_device(ifgf_operator* op, const void* d_w, void* d_u, void* stream);
 
+/* u = A^H w, the adjoint matvec: w has one value per target, u one per
+ * source (u_s = sum_t conj(G(x_s - y_t)) w_t).  Laplace, Helmholtz and
+ * modified Helmholtz: conj(A' conj(w)) with A' the operator with sources and
+ * targets exchanged (A itself when init got the same points twice); the
+ * gradient kernel: minus that; double layer and combined field: composed
+ * from three exchanged gradient operators (dG/dn_s = sum_d n_s[d] G_grad,d)
+ * and, for the combined field, an exchanged Helmholtz operator.  The
+ * operators are built on the first call from init's points, normals and
+ * cutoff callback (which must therefore stay valid).  Buffers as in
+ * ifgf_mult_batch / ifgf_mult_device with the roles of n_src and n_tgt
+ * exchanged.  No reference counterpart: gradients of sum |A w - b|^2 with
+ * respect to w are A^H (A w - b). */
+int ifgf_mult_adjoint(ifgf_operator* op, const void* w, void* u, long batch);
+int ifgf_mult_adjoint_device(ifgf_operator* op, const void* d_w, void* d_u, void* stream);
+
 /* FP64 dense direct sum u(y_t) = sum_s w_s G(x_s - y_t) on the GPU at the
  * targets listed in tidx (caller's target indices), for error estimates:
  * w as in ifgf_mult (host buffer), out receives nt values.  The reference

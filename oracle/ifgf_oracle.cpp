@@ -1795,6 +1795,30 @@ extern "C"
         return 0;
     }
 
+    // Dense kernel matrix A[t][s] = G(x_s - y_t) (complex, row-major nt x ns),
+    // the matrix the direct sum applies; tests form adjoints from it
+    int oracle_dense(int kind, double k_re, double k_im, int dx, const double* srcs, long ns,
+                     const double* normals, const double* tgts, long nt, double* out)
+    {
+        orc::KernelDef K;
+        K.kind = kind;
+        K.k = cd(k_re, k_im);
+        K.dx = dx;
+#pragma omp parallel for schedule(static)
+        for (long t = 0; t < nt; t++)
+        {
+            const double* y = tgts + 3 * t;
+            for (long s = 0; s < ns; s++)
+            {
+                double x[3] = {srcs[3 * s] - y[0], srcs[3 * s + 1] - y[1], srcs[3 * s + 2] - y[2]};
+                const cd v = K.kernel(x, normals ? normals + 3 * s : nullptr);
+                out[2 * (t * ns + s)] = v.real();
+                out[2 * (t * ns + s) + 1] = v.imag();
+            }
+        }
+        return 0;
+    }
+
     // Chebyshev building blocks exposed for closed-form tests
     void oracle_cheb_nodes(int n, double* out)
     {

@@ -66,6 +66,8 @@ def lib():
         L.oracle_orders.argtypes = [C.c_void_p, C.c_int, _ip]
         L.oracle_direct.argtypes = [C.c_int, C.c_double, C.c_double, C.c_int, _dp, C.c_long, _dp,
                                     _dp, _dp, _lp, C.c_long, _dp]
+        L.oracle_dense.argtypes = [C.c_int, C.c_double, C.c_double, C.c_int, _dp, C.c_long, _dp,
+                                   _dp, C.c_long, _dp]
         L.oracle_cheb_nodes.argtypes = [C.c_int, _dp]
         L.oracle_chebtransform3.argtypes = [_ip, _dp, _dp]
         L.oracle_clenshaw3.argtypes = [_ip, _dp, _dp, C.c_long, _dp]
@@ -211,6 +213,21 @@ def direct_sum(kind, k, srcs, w, tgts, tidx, normals=None, dx=-1):
                         _p(n) if n is not None else None, _p(w.view(np.float64)), _p(t),
                         _p(tidx, _lp), len(tidx), _p(out.view(np.float64)))
     return out.real.copy() if kind == 0 else out
+
+
+def dense_matrix(kind, k, srcs, tgts, normals=None, dx=-1):
+    """The kernel matrix A[t, s] = G(x_s - y_t) that direct_sum applies
+    (complex128, shape (M, N)); small cases only."""
+    kind = KINDS[kind] if isinstance(kind, str) else int(kind)
+    k = complex(k)
+    s = _aos(srcs)
+    t = _aos(tgts)
+    n = _aos(normals) if normals is not None else None
+    out = np.zeros((t.shape[0], s.shape[0]), dtype=np.complex128)
+    lib().oracle_dense(kind, k.real, k.imag, dx, _p(s), s.shape[0],
+                       _p(n) if n is not None else None, _p(t), t.shape[0],
+                       _p(out.view(np.float64)))
+    return out
 
 
 def cheb_nodes(n):
