@@ -47,6 +47,8 @@ def _load():
                         C.POINTER(H)],
         "ifgf_set_dx": [H, C.c_int],
         "ifgf_set_precision": [H, C.c_int],
+        "ifgf_set_shard": [H, C.c_int, C.c_int],
+        "ifgf_shard_boxes": [H, _ip, _lp, C.c_long, _lp],
         "ifgf_init": [H, _dp, C.c_long, _dp, C.c_long, _dp, CUTOFF_FN, C.c_void_p],
         "ifgf_init_plan_only": [H, _dp, C.c_long, _dp, C.c_long, CUTOFF_FN, C.c_void_p],
         "ifgf_box_list": [H, C.c_int, C.c_long, C.c_int, _lp, C.c_long, _lp],
@@ -86,7 +88,8 @@ lib = _load()
 
 # Every symbol declared in include/ifgf_b200.h.
 EXPORTED = [
-    "ifgf_create", "ifgf_set_dx", "ifgf_set_precision", "ifgf_init", "ifgf_init_plan_only",
+    "ifgf_create", "ifgf_set_dx", "ifgf_set_precision", "ifgf_set_shard", "ifgf_shard_boxes",
+    "ifgf_init", "ifgf_init_plan_only",
     "ifgf_box_list", "ifgf_mult",
     "ifgf_mult_batch", "ifgf_mult_device", "ifgf_mult_device_noalloc", "ifgf_direct_eval",
     "ifgf_mult_dk", "ifgf_mult_dk_device", "ifgf_direct_eval_dk", "ifgf_mult_adjoint",

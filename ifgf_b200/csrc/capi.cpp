@@ -79,6 +79,28 @@ extern "C"
         return guarded([&] { h->op.set_dx(dx); });
     }
 
+    int ifgf_set_shard(ifgf_operator* h, int rank, int nranks)
+    {
+        if (!h)
+            return null_handle();
+        return guarded([&] { h->op.set_shard(rank, nranks); });
+    }
+
+    int ifgf_shard_boxes(const ifgf_operator* h, int* level, long* boxes, long cap, long* n)
+    {
+        if (!h)
+            return null_handle();
+        return guarded([&] {
+            const std::vector<int64_t> b = h->op.shard_boxes();
+            if (level)
+                *level = h->op.shard_level();
+            if (n)
+                *n = (long)b.size();
+            for (long i = 0; boxes && i < cap && i < (long)b.size(); i++)
+                boxes[i] = (long)b[i];
+        });
+    }
+
     int ifgf_set_precision(ifgf_operator* h, int mode)
     {
         if (!h)

@@ -69,6 +69,8 @@ struct LevelLists
     int up_pad; // row stride of the geometry tables
     const int2* fe_list; // [slot][octant][fe_pad]: (child element, first group) of each run
     int fe_pad;         // longest run list of a row
+    const int* c2f_idx; // coarse cones to refine when n_c2f >= 0 (sharded operators)
+    int n_c2f;          // -1: all of the level's cones
 };
 
 // Upward geometry tables of one level, built on the device in two passes:

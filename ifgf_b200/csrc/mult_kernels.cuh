@@ -447,6 +447,7 @@ void launch_build_upgeo(const LevelGeom& PG, const LevelGeom& CG, double pH, dou
 struct C2FArgs
 {
     LevelGeom G;
+    const int* __restrict__ idx; // coarse cones to refine (null: all of the level)
     const int* __restrict__ cc_box;
     const int* __restrict__ cc_el;
     const double2* __restrict__ cvals;
@@ -461,7 +462,7 @@ struct C2FArgs
 static __global__ void __launch_bounds__(256) coarse_to_fine_kernel(C2FArgs a)
 {
     extern __shared__ double2 s2[];
-    const int c = blockIdx.x;
+    const int c = a.idx ? a.idx[blockIdx.x] : (int)blockIdx.x;
     const int box = a.cc_box[c], el = a.cc_el[c];
     const int h0 = a.hi[0], h1 = a.hi[1], h2 = a.hi[2];
     const int F0 = a.f[0] * a.lo[0], F1 = a.f[1] * a.lo[1];
@@ -1584,7 +1585,7 @@ __global__ void __launch_bounds__(UP_THREADS) upward_mixed_kernel(UpArgs a)
 static __global__ void __launch_bounds__(256) coarse_to_fine_mixed_kernel(C2FArgs a)
 {
     extern __shared__ float2 s2f[];
-    const int c = blockIdx.x;
+    const int c = a.idx ? a.idx[blockIdx.x] : (int)blockIdx.x;
     const int box = a.cc_box[c], el = a.cc_el[c];
     const int h0 = a.hi[0], h1 = a.hi[1], h2 = a.hi[2];
     const int F0 = a.f[0] * a.lo[0], F1 = a.f[1] * a.lo[1];
@@ -1735,7 +1736,7 @@ __global__ void __launch_bounds__(c2f_fixed_threads<H0, H1, H2, L0, L1, L2, F>()
     V* Y1 = reinterpret_cast<V*>(c2f_raw); // [m2][m1][i0], i0 fastest
     V* Y2 = Y1 + F0 * H1 * H2;             // [m2][S2]
     __shared__ int gsub[F * F * F];
-    const int c = blockIdx.x;
+    const int c = a.idx ? a.idx[blockIdx.x] : (int)blockIdx.x;
     const int t = threadIdx.x;
     const int box = a.cc_box[c], el = a.cc_el[c];
     if (t < F * F * F)
@@ -2219,8 +2220,13 @@ static int run_mult(const MultPtrs& m, const void* d_w, void* d_u, bool real, cu
                 hk->end();
             launches++;
         }
+        // a sharded operator refines its own cones only (n_c2f >= 0)
+        const unsigned c2f_grid = LL.n_c2f >= 0 ? (unsigned)LL.n_c2f : (unsigned)G.n_coarse;
+        if (c2f_grid == 0)
+            continue;
         C2FArgs fa;
         fa.G = G;
+        fa.idx = LL.n_c2f >= 0 ? LL.c2f_idx : nullptr;
         fa.cc_box = LL.cc_box;
         fa.cc_el = LL.cc_el;
         fa.cvals = m.cvals;
@@ -2238,13 +2244,13 @@ static int run_mult(const MultPtrs& m, const void* d_w, void* d_u, bool real, cu
         if (hk)
             hk->begin(PROF_C2F, l);
         if (launch_c2f_fixed<typename std::conditional<MIXED, float, double>::type>(
-                fa, m.A_host, (unsigned)G.n_coarse, st))
+                fa, m.A_host, c2f_grid, st))
         {
         }
         else if (MIXED)
-            coarse_to_fine_mixed_kernel<<<(unsigned)G.n_coarse, 256, c2f_smem, st>>>(fa);
+            coarse_to_fine_mixed_kernel<<<c2f_grid, 256, c2f_smem, st>>>(fa);
         else
-            coarse_to_fine_kernel<<<(unsigned)G.n_coarse, 256, c2f_smem, st>>>(fa);
+            coarse_to_fine_kernel<<<c2f_grid, 256, c2f_smem, st>>>(fa);
         IFGF_CHECK_LAUNCH();
         if (hk)
             hk->end();

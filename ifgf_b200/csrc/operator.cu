@@ -101,6 +101,7 @@ struct DeviceState
     std::vector<DevBuf<UpGeo64>> geo64;                    // per level upward geometry
     std::vector<DevBuf<UpGeo32>> geo32;
     std::vector<DevBuf<int2>> fe_list; // per-row (child element, first group) of each run
+    std::vector<DevBuf<int>> c2f_idx;  // per level: coarse cones of a sharded operator
     // what the upward geometry of a level is built from (kept for variants)
     std::vector<DevBuf<int>> slot_el;      // element of each slot
     std::vector<DevBuf<double>> child_off; // 8 child-centre offsets
@@ -340,6 +341,28 @@ void Operator::set_dx(int dx)
     dx_ = dx;
 }
 
+void Operator::set_shard(int rank, int nranks)
+{
+    if (nranks < 1 || rank < 0 || rank >= nranks)
+        throw Error(ERR_INVALID, "shard rank must be in [0, nranks)");
+    shard_rank_ = rank;
+    shard_n_ = nranks;
+    initialized_ = planned_ = false; // takes effect at the next init
+}
+
+std::vector<int64_t> Operator::shard_boxes() const
+{
+    std::vector<int64_t> out;
+    if (!planned_ && !initialized_)
+        throw Error(ERR_STATE, "shard boxes are known after init");
+    const int S = plan_.shard_level;
+    const int64_t off = plan_.src.level_off[S];
+    for (size_t b = 0; b < plan_.src.levels[S].size(); b++)
+        if (plan_.box_rank[off + (int64_t)b] == shard_rank_)
+            out.push_back((int64_t)b);
+    return out;
+}
+
 void Operator::set_precision(int mode)
 {
     if (mode != PREC_FP64 && mode != PREC_MIXED)
@@ -468,7 +491,8 @@ void Operator::init(const double* srcs, int64_t ns, const double* tgts, int64_t 
     plan_.src.build(srcs, ns, leaf_);
     plan_.tgt.build(tgts, nt, leaf_);
     plan_.build_lists(cutoff);
-    plan_.build_target_lists();
+    plan_.assign_shards(shard_n_);
+    plan_.build_target_lists(shard_n_ > 1 ? shard_rank_ : -1);
 
     const int L = plan_.src.num_levels();
     if (L > MAX_LEVELS)
@@ -692,6 +716,10 @@ void Operator::setup_device(const double* normals)
     D.vgeo32.clear();
     D.vlists.clear();
     std::vector<std::vector<int>> up_host(L);
+    // coarse cones each level refines: all of them, or this rank's
+    const bool sharded = shard_n_ > 1;
+    std::vector<std::vector<int>> c2f_host(L);
+    D.c2f_idx.resize(L);
     std::vector<int> up_pad(L, 0);
     fe_pad_.assign(L, 0);
     up_stats_.assign(L, UpwardLevelStats{});
@@ -779,6 +807,9 @@ void Operator::setup_device(const double* normals)
             for (int64_t i = 0; i < G.n_coarse; i++)
             {
                 const int g = cb[i];
+                if (sharded && plan_.box_rank[g] != shard_rank_)
+                    continue; // another rank's subtree
+                c2f_host[l].push_back((int)i);
                 if (bleaf[g])
                 {
                     lidx.push_back((int)i);
@@ -885,10 +916,16 @@ void Operator::setup_device(const double* normals)
     }
     D.lists.assign(L, LevelLists{});
     for (int l = 0; l < L; l++)
+    {
+        if (sharded)
+            D.c2f_idx[l].upload(c2f_host[l]);
         D.lists[l] = LevelLists{D.cc_box[l].p, D.cc_el[l].p, D.leaf_idx[l].p, D.up_idx[l].p,
                                 D.up_slot[l].p, D.geo64[l].p, D.geo32[l].p,
                                 (int)D.leaf_idx[l].n, (int)D.up_idx[l].n, up_pad[l],
-                                D.fe_list[l].p, fe_pad_[l]};
+                                D.fe_list[l].p, fe_pad_[l],
+                                sharded ? D.c2f_idx[l].p : nullptr,
+                                sharded ? (int)c2f_host[l].size() : -1};
+    }
     n_coarse_total_ = coarse_tot;
     n_fine_total_ = fine_tot;
     D.lv.upload(lv_);

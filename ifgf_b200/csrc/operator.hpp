@@ -32,6 +32,14 @@ class Operator
     ~Operator();
 
     void set_dx(int dx);
+    // Take share `rank` of `nranks` of the matvec (before init): mult then
+    // returns the contribution of this rank's source subtrees to every
+    // target, and the ranks' results sum to the full matvec (see
+    // Plan::assign_shards).
+    void set_shard(int rank, int nranks);
+    // recursive level of the shards and this rank's boxes on it
+    int shard_level() const { return plan_.shard_level; }
+    std::vector<int64_t> shard_boxes() const;
     void set_precision(int mode);
     // IfgfOperator::init (ifgfoperator.hpp:65-106)
     void init(const double* srcs, int64_t ns, const double* tgts, int64_t nt,
@@ -113,6 +121,7 @@ class Operator
     std::function<bool(double)> cutoff_;
     bool same_points_ = false;
     std::unique_ptr<AdjointState> adj_;
+    int shard_rank_ = 0, shard_n_ = 1;
     // statistics
     double init_ms_ = 0;
     StageTimes last_;

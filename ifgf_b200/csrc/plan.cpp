@@ -272,13 +272,82 @@ void Plan::build_lists(const std::function<bool(double)>& cutoff)
     w.walk(0, 0, 0, 0);
 }
 
-void Plan::build_target_lists()
+void Plan::assign_shards(int nranks)
+{
+    const int L = src.num_levels();
+    const int64_t nsb = src.num_boxes_total();
+    // first level with a far pair (the subtree roots)
+    shard_level = L - 1;
+    for (int l = 0; l < L; l++)
+    {
+        bool any = false;
+        for (size_t b = 0; b < src.levels[l].size() && !any; b++)
+            any = !far[src.level_off[l] + (int64_t)b].empty();
+        if (any)
+        {
+            shard_level = l;
+            break;
+        }
+    }
+    box_rank.assign(nsb, 0);
+    if (nranks <= 1)
+        return;
+    // modelled work of every box: near point pairs + far target evaluations
+    // weighted by the cost of one evaluation relative to one kernel pair
+    auto tsize = [&](int64_t tg) {
+        int l = (int)(std::upper_bound(tgt.level_off.begin(), tgt.level_off.end(), tg) -
+                      tgt.level_off.begin()) - 1;
+        const int64_t b = tg - tgt.level_off[l];
+        return (double)(tgt.levels[l].last[b] - tgt.levels[l].first[b]);
+    };
+    std::vector<double> work(nsb, 0.0);
+    for (int l = L - 1; l >= 0; l--)
+        for (size_t b = 0; b < src.levels[l].size(); b++)
+        {
+            const int64_t g = src.level_off[l] + (int64_t)b;
+            const double ns = (double)(src.levels[l].last[b] - src.levels[l].first[b]);
+            for (int64_t t : near[g])
+                work[g] += ns * tsize(t);
+            for (int64_t t : far[g])
+                work[g] += 20.0 * tsize(t);
+            if (l > 0)
+                work[src.level_off[l - 1] + src.levels[l].parent[b]] += work[g];
+        }
+    const TreeLevel& S = src.levels[shard_level];
+    const int64_t nr = (int64_t)S.size();
+    double total = 0;
+    for (int64_t b = 0; b < nr; b++)
+        total += work[src.level_off[shard_level] + b];
+    // contiguous ranges: rank r ends where the running work passes
+    // (r + 1) / nranks of the total
+    std::vector<int32_t> root_rank(nr, 0);
+    double run = 0;
+    int r = 0;
+    for (int64_t b = 0; b < nr; b++)
+    {
+        const double wb = work[src.level_off[shard_level] + b];
+        while (r < nranks - 1 && run + 0.5 * wb > total * (double)(r + 1) / nranks)
+            r++;
+        root_rank[b] = r;
+        run += wb;
+    }
+    for (int64_t b = 0; b < nr; b++)
+        box_rank[src.level_off[shard_level] + b] = root_rank[b];
+    for (int l = shard_level + 1; l < L; l++)
+        for (size_t b = 0; b < src.levels[l].size(); b++)
+            box_rank[src.level_off[l] + (int64_t)b] =
+                box_rank[src.level_off[l - 1] + src.levels[l].parent[b]];
+}
+
+void Plan::build_target_lists(int rank)
 {
     const int64_t ntb = tgt.num_boxes_total();
     std::vector<std::vector<int32_t>> far_in(ntb), near_in(ntb);
     const int64_t nsb = src.num_boxes_total();
     for (int64_t s = 0; s < nsb; s++)
     {
+        if (rank >= 0 && box_rank[s] != rank)
+            continue;
         for (int64_t t : far[s])
             far_in[t].push_back((int32_t)s);
         for (int64_t t : near[s])

@@ -56,9 +56,19 @@ struct Plan
     // counters (octree.hpp:265-268)
     int64_t n_far_pairs = 0, n_near_pairs = 0, n_dropped = 0;
     int64_t far_target_evals = 0, near_point_pairs = 0;
+    // Sharding of the matvec over ranks.  No source box above shard_level
+    // has far targets, so the subtrees rooted at shard_level are
+    // independent: each rank takes a contiguous (Morton-ordered) range of
+    // them, balanced by modelled work, and computes their contribution to
+    // every target.  box_rank: owning rank of every source box (boxes above
+    // shard_level, whose only work is near-field leaves, belong to rank 0).
+    int shard_level = 0;
+    std::vector<int32_t> box_rank;
 
     void build_lists(const std::function<bool(double)>& cutoff);
-    void build_target_lists();
+    void assign_shards(int nranks);
+    // target-leaf lists of the sources owned by `rank` (all when rank < 0)
+    void build_target_lists(int rank = -1);
 };
 
 // Morton key of a point normalised to the root box: 42 bits per dimension,

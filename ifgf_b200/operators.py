@@ -100,6 +100,21 @@ class IfgfOperator:
                                       t.ctypes.data_as(dp), t.shape[0], cb, None))
         self._n_src, self._n_tgt = s.shape[0], t.shape[0]
 
+    def set_shard(self, rank, nranks):
+        """Take share `rank` of `nranks` of the matvec (call before init); the
+        ranks' mult results sum to the full matvec (see ifgf_b200.distributed)."""
+        check(lib.ifgf_set_shard(self._h, int(rank), int(nranks)))
+
+    def shard_boxes(self):
+        """(level, boxes): the shard level and this rank's boxes on it."""
+        lev = C.c_int(0)
+        n = C.c_long(0)
+        check(lib.ifgf_shard_boxes(self._h, C.byref(lev), None, 0, C.byref(n)))
+        out = np.zeros(n.value, dtype=np.int64)
+        check(lib.ifgf_shard_boxes(self._h, C.byref(lev), out.ctypes.data_as(C.POINTER(C.c_long)),
+                                   n.value, C.byref(n)))
+        return lev.value, out
+
     def set_precision(self, mode):
         """"fp64" (default) or "mixed"."""
         m = {"fp64": _lib.PREC_FP64, "mixed": _lib.PREC_MIXED}.get(mode, mode)

@@ -68,6 +68,21 @@ int ifgf_set_dx(ifgf_operator* op, int dx);
  * counterpart (the reference is FP64 only). */
 int ifgf_set_precision(ifgf_operator* op, int mode);
 
+/* Multi-GPU sharding, called before ifgf_init: the operator takes share
+ * `rank` of `nranks` -- a contiguous Morton range, balanced by modelled work,
+ * of the source subtrees rooted at the first level that has far pairs (no
+ * box above it has far targets, so the subtrees are independent).  Its
+ * matvec returns the contribution of those subtrees to every target, and the
+ * ranks' results sum to the full matvec (one all-reduce of n_tgt values).
+ * Each rank builds the whole tree and cone maps.  No reference counterpart:
+ * the reference runs those subtrees as parallel tasks on one host
+ * (ifgfoperator.hpp:330-340). */
+int ifgf_set_shard(ifgf_operator* op, int rank, int nranks);
+
+/* After init: the shard level and this rank's boxes on it (level-local box
+ * indices, *n of them, at most cap written). */
+int ifgf_shard_boxes(const ifgf_operator* op, int* level, long* boxes, long cap, long* n);
+
 /* Far-interaction drop predicate of IfgfOperator::init
  * (ifgfoperator.hpp:65-67, octree.hpp:282-297): return nonzero to drop an
  * admissible pair at exterior distance `dist`.  May be NULL. */

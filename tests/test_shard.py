@@ -1,0 +1,122 @@
+"""Multi-GPU sharding of the matvec.
+
+CPU: the shard assignment (host planner, plan-only init) covers the subtree
+roots once, in contiguous balanced ranges; a world-size-2 gloo run sums the
+ranks' partial results with the library's reduction (the partials come from
+the oracle's subtree matvec over the boxes the library assigned).  GPU: the
+shards' matvecs, run one after another on one GPU, sum to the unsharded
+matvec and to the oracle.
+"""
+import os
+import socket
+
+import numpy as np
+import pytest
+
+from ifgf_b200 import workloads as W
+
+from .helpers import densities_for, rel2
+
+
+def _plan(n, nranks, rank, leaf=40, order=8):
+    import ifgf_b200 as G
+
+    pts = W.sphere_points(n, seed=0)
+    op = G.HelmholtzIfgfOperator(20.0, leaf, order)
+    op.set_shard(rank, nranks)
+    op.init_plan_only(pts, pts)
+    return op
+
+
+@pytest.mark.parametrize("nranks", [2, 3, 5])
+def test_shard_assignment_partitions_the_subtrees(nranks):
+    n = 20000
+    got = []
+    level = None
+    for r in range(nranks):
+        lev, boxes = _plan(n, nranks, r).shard_boxes()
+        level = lev if level is None else level
+        assert lev == level and lev >= 1
+        if len(boxes):
+            assert np.all(np.diff(boxes) == 1)  # contiguous Morton range
+        got.append(boxes)
+    allb = np.concatenate(got)
+    nb = _plan(n, 1, 0).num_boxes(level)
+    assert np.array_equal(np.sort(allb), np.arange(nb))  # each root exactly once
+    assert sum(len(b) > 0 for b in got) == min(nranks, nb)
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _gloo_rank(rank, world, port, n, out_dir):
+    import torch
+    import torch.distributed as dist
+
+    from ifgf_b200.distributed import reduce_partial
+    from oracle import oracle as O
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        pts = W.sphere_points(n, seed=0)
+        w = densities_for("helmholtz", n)
+        op = _plan(n, world, rank)
+        level, boxes = op.shard_boxes()
+        o = O.OracleOperator("helmholtz", 20.0, 40, 8)
+        o.init(pts, pts)
+        part = o.mult_sample(w, level, boxes) if len(boxes) else np.zeros(n, complex)
+        u = torch.from_numpy(np.ascontiguousarray(part))
+        reduce_partial(u)
+        np.save(os.path.join(out_dir, f"u{rank}.npy"), u.numpy())
+    finally:
+        dist.destroy_process_group()
+
+
+def test_gloo_two_ranks_sum_to_the_full_matvec(tmp_path):
+    import torch.multiprocessing as mp
+
+    from oracle import oracle as O
+
+    n = 12000
+    port = _free_port()
+    mp.start_processes(_gloo_rank, args=(2, port, n, str(tmp_path)), nprocs=2, join=True,
+                       start_method="spawn")
+    pts = W.sphere_points(n, seed=0)
+    w = densities_for("helmholtz", n)
+    o = O.OracleOperator("helmholtz", 20.0, 40, 8)
+    o.init(pts, pts)
+    full = o.mult(w)
+    for r in range(2):
+        u = np.load(tmp_path / f"u{r}.npy")
+        assert rel2(u, full) <= 1e-13
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,nranks", [("helmholtz", 3), ("combined_field", 2), ("laplace", 4)])
+def test_shards_sum_to_the_matvec_on_one_gpu(name, nranks):
+    from oracle import oracle as O
+
+    from .helpers import KERNELS, init_op, make_gpu_op, make_oracle_op
+
+    n = 20000
+    pts = W.sphere_points(n, seed=0)
+    w = densities_for(name, n)
+    full = make_gpu_op(name, leaf=50, order=8)
+    init_op(full, name, pts, pts)
+    uf = full.mult(w)
+    parts = []
+    for r in range(nranks):
+        g = make_gpu_op(name, leaf=50, order=8)
+        g.set_shard(r, nranks)
+        init_op(g, name, pts, pts)
+        parts.append(g.mult(w))
+        assert g.stats()["missing_cone_lookups"] == 0
+    assert rel2(sum(parts), uf) <= 1e-13
+    o = make_oracle_op(name, leaf=50, order=8)
+    init_op(o, name, pts, pts)
+    assert rel2(sum(parts), o.mult(w)) <= 1e-12
