@@ -55,6 +55,7 @@ def _load():
         "ifgf_mult": [H, C.c_void_p, C.c_void_p],
         "ifgf_mult_batch": [H, C.c_void_p, C.c_void_p, C.c_long],
         "ifgf_mult_device": [H, C.c_void_p, C.c_void_p, C.c_void_p],
+        "ifgf_mult_batch_device": [H, C.c_void_p, C.c_void_p, C.c_long, C.c_void_p],
         "ifgf_mult_device_noalloc": [H, C.c_void_p, C.c_void_p, C.c_void_p],
         "ifgf_direct_eval": [H, C.c_void_p, _lp, C.c_long, C.c_void_p],
         "ifgf_direct_eval_dk": [H, C.c_void_p, _lp, C.c_long, C.c_void_p],
@@ -91,7 +92,8 @@ EXPORTED = [
     "ifgf_create", "ifgf_set_dx", "ifgf_set_precision", "ifgf_set_shard", "ifgf_shard_boxes",
     "ifgf_init", "ifgf_init_plan_only",
     "ifgf_box_list", "ifgf_mult",
-    "ifgf_mult_batch", "ifgf_mult_device", "ifgf_mult_device_noalloc", "ifgf_direct_eval",
+    "ifgf_mult_batch", "ifgf_mult_batch_device", "ifgf_mult_device", "ifgf_mult_device_noalloc",
+    "ifgf_direct_eval",
     "ifgf_mult_dk", "ifgf_mult_dk_device", "ifgf_direct_eval_dk", "ifgf_mult_adjoint",
     "ifgf_mult_adjoint_device",
     "ifgf_set_profiling",

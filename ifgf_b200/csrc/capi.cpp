@@ -148,6 +148,14 @@ extern "C"
         return guarded([&] { h->op.mult_host(w, u, batch); });
     }
 
+    int ifgf_mult_batch_device(ifgf_operator* h, const void* d_w, void* d_u, long batch,
+                               void* stream)
+    {
+        if (!h)
+            return null_handle();
+        return guarded([&] { h->op.mult_batch_device(d_w, d_u, batch, stream); });
+    }
+
     int ifgf_mult_device(ifgf_operator* h, const void* d_w, void* d_u, void* stream)
     {
         if (!h)

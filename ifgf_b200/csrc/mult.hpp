@@ -156,6 +156,28 @@ template <int KIND>
 int launch_mult_kernels(const MultPtrs& m, const void* d_w, void* d_u, bool real, cudaStream_t st,
                         LaunchHooks* hooks);
 
+// Planes of the batched mixed matvec (mult_batch.cuh): right-hand side b of
+// a group lives at offset b * plane of each buffer.
+constexpr int BATCH_NB = 4;
+struct BatchPtrs
+{
+    float2* w;      // BATCH_NB planes of n_src permuted densities
+    float2* cvals;  // BATCH_NB planes of cv_plane coarse values
+    float2* fcoef;  // BATCH_NB planes of fc_plane fine coefficients
+    double2* unear; // BATCH_NB planes of n_tgt near-field sums
+    long long cv_plane, fc_plane;
+    long long n_src, n_tgt;
+    int nrhs;                      // planes holding right-hand sides (the rest are zero)
+    long long in_plane, out_plane; // caller's density / result strides (in doubles)
+};
+
+// Enqueues the mixed matvec of bp.nrhs <= BATCH_NB right-hand sides sharing
+// the kernel and geometry work; returns the kernels launched, or -1 when the
+// operator's orders or upward rows have no batched path.
+template <int KIND>
+int launch_mult_batch_kernels(const MultPtrs& m, const BatchPtrs& bp, const void* d_w, void* d_u,
+                              bool real, cudaStream_t st, LaunchHooks* hooks);
+
 // Only the density permutation into m.w (for direct sums).
 template <int KIND>
 void permute_only(const MultPtrs& m, const void* d_w, bool real, cudaStream_t st);

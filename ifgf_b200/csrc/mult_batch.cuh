@@ -1,0 +1,567 @@
+// Mixed-precision matvec of several right-hand sides at once (included by
+// mult_kernels.cuh).  BATCH_NB densities share every geometry- and
+// kernel-dependent quantity of the pipeline -- the factored-kernel values at
+// the cone nodes, the near-field kernel values, the far-field cone lookups and
+// centred factors -- and keep their own interpolant planes: buffers hold
+// BATCH_NB planes (right-hand side b at offset b * plane).  The upward
+// transfer and the coarse-to-fine step run the single-right-hand-side kernels
+// with blockIdx.y selecting the plane.
+// Included inside namespace ifgf, after the single-right-hand-side kernels.
+#pragma once
+
+
+// Permuted FP32 densities of nrhs right-hand sides; planes past nrhs zero.
+static __global__ void permute_batch_kernel(const double* __restrict__ in, int real_in,
+                                            const long long* __restrict__ perm, float2* w,
+                                            long long n, int nrhs, long long in_plane)
+{
+    const int b = blockIdx.y;
+    float2* wb = w + (size_t)b * n;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+    {
+        if (b >= nrhs)
+        {
+            wb[i] = make_float2(0.f, 0.f);
+            continue;
+        }
+        const long long j = perm[i];
+        const double* src = in + (size_t)b * in_plane;
+        if (real_in)
+            wb[i] = make_float2((float)src[j], 0.f);
+        else
+        {
+            const double2 v = reinterpret_cast<const double2*>(src)[j];
+            wb[i] = make_float2((float)v.x, (float)v.y);
+        }
+    }
+}
+
+// Leaf sampling of BATCH_NB right-hand sides: the factored kernel at a
+// (node, source) pair is evaluated once with unit density and applied to
+// every plane's density (the kernels are linear in the density).
+template <int KIND>
+__global__ void __launch_bounds__(NODE_THREADS) leaf_sample_batch_kernel(LeafArgs a, BatchPtrs bp)
+{
+    using P = PluginF<KIND>;
+    constexpr int NB = BATCH_NB;
+    extern __shared__ float smb[];
+    const int c = a.idx[blockIdx.x];
+    const int node0 = blockIdx.y * NPT * blockDim.x;
+    const int box = a.cc_box[c], el = a.cc_el[c];
+    const double xc[3] = {a.T.box_c[3 * box], a.T.box_c[3 * box + 1], a.T.box_c[3 * box + 2]};
+    const double H = a.T.box_H[box];
+    float b[NPT][3], dc[NPT];
+    cplx<float> acc[NPT][NB];
+#pragma unroll
+    for (int q = 0; q < NPT; q++)
+    {
+        const int n = node0 + threadIdx.x + q * blockDim.x;
+#pragma unroll
+        for (int r = 0; r < NB; r++)
+            acc[q][r] = {0.f, 0.f};
+        b[q][0] = b[q][1] = b[q][2] = 0.f;
+        dc[q] = 1.f;
+        if (n < a.P_hi)
+        {
+            double y[3];
+            node_position(a.G, el, n, a.hi_nodes, xc, H, y);
+            const double e0 = y[0] - xc[0], e1 = y[1] - xc[1], e2 = y[2] - xc[2];
+            b[q][0] = (float)e0;
+            b[q][1] = (float)e1;
+            b[q][2] = (float)e2;
+            dc[q] = (float)sqrt(e0 * e0 + e1 * e1 + e2 * e2);
+        }
+    }
+    const int nt = blockDim.x;
+    float* ax = smb;
+    float* ay = ax + nt;
+    float* az = ay + nt;
+    float* aa = az + nt;
+    float* n0 = aa + nt;
+    float* n1 = n0 + nt;
+    float* n2 = n1 + nt;
+    float2* wv = reinterpret_cast<float2*>(n2 + nt); // [NB][nt]
+    const int f = a.T.box_first[box], l = a.T.box_last[box];
+    for (int cs = f; cs < l; cs += nt)
+    {
+        const int cnt = min(nt, l - cs);
+        __syncthreads();
+        if (threadIdx.x < cnt)
+        {
+            const int i = cs + threadIdx.x;
+            const double a0 = a.S.sx[i] - xc[0], a1 = a.S.sy[i] - xc[1], a2 = a.S.sz[i] - xc[2];
+            ax[threadIdx.x] = (float)a0;
+            ay[threadIdx.x] = (float)a1;
+            az[threadIdx.x] = (float)a2;
+            aa[threadIdx.x] = (float)(a0 * a0 + a1 * a1 + a2 * a2);
+#pragma unroll
+            for (int r = 0; r < NB; r++)
+                wv[r * nt + threadIdx.x] = bp.w[(size_t)r * bp.n_src + i];
+            if (P::needs_normals)
+            {
+                n0[threadIdx.x] = (float)a.S.nx[i];
+                n1[threadIdx.x] = (float)a.S.ny[i];
+                n2[threadIdx.x] = (float)a.S.nz[i];
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < NPT; q++)
+        {
+            if (node0 + threadIdx.x + q * blockDim.x >= a.P_hi)
+                continue;
+            for (int i = 0; i < cnt; i++)
+            {
+                const float av[3] = {ax[i], ay[i], az[i]};
+                const float nv[3] = {P::needs_normals ? n0[i] : 0.f, P::needs_normals ? n1[i] : 0.f,
+                                     P::needs_normals ? n2[i] : 0.f};
+                const cplx<float> v = P::factored(av, aa[i], b[q], nv, {1.f, 0.f}, dc[q], a.kp);
+#pragma unroll
+                for (int r = 0; r < NB; r++)
+                {
+                    const float2 wr = wv[r * nt + i];
+                    acc[q][r].re = fmaf(wr.x, v.re, fmaf(-wr.y, v.im, acc[q][r].re));
+                    acc[q][r].im = fmaf(wr.x, v.im, fmaf(wr.y, v.re, acc[q][r].im));
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < NPT; q++)
+    {
+        const int n = node0 + threadIdx.x + q * blockDim.x;
+        if (n < a.P_hi)
+#pragma unroll
+            for (int r = 0; r < NB; r++)
+                bp.cvals[(size_t)r * bp.cv_plane + (size_t)c * a.P_hi + n] =
+                    make_float2(acc[q][r].re, acc[q][r].im);
+    }
+}
+
+// Near field of BATCH_NB right-hand sides: one kernel value per (target,
+// source) pair, applied to every plane; FP32 per source chunk, FP64 across
+// chunks and threads, written to the near-sum planes.
+template <int KIND>
+__global__ void __launch_bounds__(EVAL_THREADS) near_batch_kernel(EvalArgs a, BatchPtrs bp)
+{
+    using P = PluginF<KIND>;
+    constexpr int NB = BATCH_NB;
+    using CT = typename std::conditional<P::needs_normals, double, float>::type;
+    __shared__ CT xs[EVAL_THREADS], ys[EVAL_THREADS], zs[EVAL_THREADS];
+    __shared__ float2 ws[NB][EVAL_THREADS];
+    __shared__ double n0[P::needs_normals ? EVAL_THREADS : 1], n1[P::needs_normals ? EVAL_THREADS : 1],
+        n2[P::needs_normals ? EVAL_THREADS : 1];
+    __shared__ double rr[NB][EVAL_THREADS], ri[NB][EVAL_THREADS];
+    const long long nsrc = bp.n_src;
+    const int tl = blockIdx.x;
+    const int tf = a.tl_first[tl], tlast = a.tl_last[tl];
+    const double r0 = a.tx[tf], r1 = a.ty[tf], r2 = a.tz[tf];
+    const long long nb0 = a.near_off[tl], nb1 = a.near_off[tl + 1];
+    for (int base = tf; base < tlast; base += EVAL_THREADS)
+    {
+        const int cnt = min(EVAL_THREADS, tlast - base);
+        const int S = EVAL_THREADS / cnt;
+        const int ti = threadIdx.x % cnt, si = threadIdx.x / cnt;
+        const bool active = si < S;
+        const int t = base + ti;
+        const double y0 = a.tx[t], y1 = a.ty[t], y2 = a.tz[t];
+        const float yl0 = (float)(y0 - r0), yl1 = (float)(y1 - r1), yl2 = (float)(y2 - r2);
+        double accr[NB], acci[NB];
+#pragma unroll
+        for (int r = 0; r < NB; r++)
+            accr[r] = acci[r] = 0.0;
+        for (long long e = nb0; e < nb1; e++)
+        {
+            const int sb = a.near_src[e];
+            const int sf = a.T.box_first[sb], sl = a.T.box_last[sb];
+            for (int cs = sf; cs < sl; cs += EVAL_THREADS)
+            {
+                const int ccnt = min(EVAL_THREADS, sl - cs);
+                __syncthreads();
+                if (threadIdx.x < ccnt)
+                {
+                    const int i = cs + threadIdx.x;
+                    xs[threadIdx.x] = (CT)(a.S.sx[i] - r0);
+                    ys[threadIdx.x] = (CT)(a.S.sy[i] - r1);
+                    zs[threadIdx.x] = (CT)(a.S.sz[i] - r2);
+#pragma unroll
+                    for (int r = 0; r < NB; r++)
+                        ws[r][threadIdx.x] = bp.w[(size_t)r * nsrc + i];
+                    if (P::needs_normals)
+                    {
+                        n0[threadIdx.x] = a.S.nx[i];
+                        n1[threadIdx.x] = a.S.ny[i];
+                        n2[threadIdx.x] = a.S.nz[i];
+                    }
+                }
+                __syncthreads();
+                if (!active)
+                    continue;
+                cplx<float> acc[NB];
+#pragma unroll
+                for (int r = 0; r < NB; r++)
+                    acc[r] = {0.f, 0.f};
+                for (int i = si; i < ccnt; i += S)
+                {
+                    cplx<float> kv;
+                    if constexpr (P::needs_normals)
+                    {
+                        const double yd0 = y0 - r0, yd1 = y1 - r1, yd2 = y2 - r2;
+                        const double x[3] = {xs[i] - yd0, ys[i] - yd1, zs[i] - yd2};
+                        const double nv[3] = {n0[i], n1[i], n2[i]};
+                        kv = P::kernel_d(x, nv, a.kp);
+                    }
+                    else
+                    {
+                        const float x[3] = {xs[i] - yl0, ys[i] - yl1, zs[i] - yl2};
+                        kv = P::kernel(x, nullptr, a.kp);
+                    }
+#pragma unroll
+                    for (int r = 0; r < NB; r++)
+                        cfmaf(acc[r], cplx<float>{ws[r][i].x, ws[r][i].y}, kv);
+                }
+#pragma unroll
+                for (int r = 0; r < NB; r++)
+                {
+                    accr[r] += acc[r].re;
+                    acci[r] += acc[r].im;
+                }
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < NB; r++)
+        {
+            rr[r][threadIdx.x] = accr[r];
+            ri[r][threadIdx.x] = acci[r];
+        }
+        __syncthreads();
+        if (active && si == 0)
+        {
+#pragma unroll
+            for (int r = 0; r < NB; r++)
+            {
+                double sr = 0, sim = 0;
+                for (int s = 0; s < S; s++)
+                {
+                    sr += rr[r][ti + s * cnt];
+                    sim += ri[r][ti + s * cnt];
+                }
+                bp.unear[(size_t)r * bp.n_tgt + t] = make_double2(sr, sim);
+            }
+        }
+    }
+}
+
+// Far field of BATCH_NB right-hand sides: the cone lookup and the centred
+// factor of a (target, far box) pair are computed once; each plane's
+// Chebyshev sum uses its own coefficient block.  Adds the near sums and
+// writes the caller's result planes (the first nrhs).
+template <int KIND, int N0, int N1, int N2>
+__global__ void __launch_bounds__(EVAL_THREADS, 4) far_batch_kernel(EvalArgs a, BatchPtrs bp)
+{
+    constexpr int NB = BATCH_NB;
+    __shared__ double fcx[EVAL_THREADS], fcy[EVAL_THREADS], fcz[EVAL_THREADS], fH[EVAL_THREADS];
+    __shared__ long long ffm[EVAL_THREADS];
+    __shared__ int flev[EVAL_THREADS];
+    __shared__ LookupF lfs[MAX_LEVELS];
+    __shared__ double rr[NB][EVAL_THREADS], ri[NB][EVAL_THREADS];
+    for (int l = threadIdx.x; l < a.L; l += blockDim.x)
+        make_lookupf(a.lv[l], lfs[l]); // read after the first chunk's barriers
+    const int tl = blockIdx.x;
+    const int tf = a.tl_first[tl], tlast = a.tl_last[tl];
+    const long long fb0 = a.far_off[tl], fb1 = a.far_off[tl + 1];
+    for (int base = tf; base < tlast; base += EVAL_THREADS)
+    {
+        const int cnt = min(EVAL_THREADS, tlast - base);
+        const int S = EVAL_THREADS / cnt;
+        const int ti = threadIdx.x % cnt, si = threadIdx.x / cnt;
+        const bool active = si < S;
+        const int t = base + ti;
+        const double y0 = a.tx[t], y1 = a.ty[t], y2 = a.tz[t];
+        double accr[NB], acci[NB];
+#pragma unroll
+        for (int r = 0; r < NB; r++)
+            accr[r] = acci[r] = 0.0;
+        for (long long e0 = fb0; e0 < fb1; e0 += EVAL_THREADS)
+        {
+            const int fcnt = (int)min((long long)EVAL_THREADS, fb1 - e0);
+            __syncthreads();
+            if (threadIdx.x < fcnt)
+            {
+                const int sb = a.far_src[e0 + threadIdx.x];
+                const int lev = a.T.box_level[sb];
+                const LevelGeom& G = a.lv[lev];
+                const long long nft = (long long)G.nf[0] * G.nf[1] * G.nf[2];
+                fcx[threadIdx.x] = a.T.box_c[3 * sb];
+                fcy[threadIdx.x] = a.T.box_c[3 * sb + 1];
+                fcz[threadIdx.x] = a.T.box_c[3 * sb + 2];
+                fH[threadIdx.x] = a.T.box_H[sb];
+                ffm[threadIdx.x] = G.fmap_off + (long long)(sb - G.box_off) * nft;
+                flev[threadIdx.x] = lev;
+            }
+            __syncthreads();
+            if (!active)
+                continue;
+            for (int i = si; i < fcnt; i += S)
+            {
+                const int lev = flev[i];
+                const double p[3] = {y0 - fcx[i], y1 - fcy[i], y2 - fcz[i]};
+                float loc[3];
+                const int gf =
+                    fine_lookup_fast(lfs[lev], a.lv[lev], a.fmap + ffm[i], p, fH[i], loc, a.err);
+                if (gf < 0)
+                    continue;
+                const cplx<float> cf =
+                    cf_mixed<KIND>(p[0] * p[0] + p[1] * p[1] + p[2] * p[2], a.kp);
+#pragma unroll
+                for (int r = 0; r < NB; r++)
+                {
+                    const cplx<float> v = ChebF<N0, N1, N2>::eval(
+                        bp.fcoef + (size_t)r * bp.fc_plane + (size_t)gf * a.P_lo, loc, a.lo);
+                    accr[r] += (double)(v.re * cf.re - v.im * cf.im);
+                    acci[r] += (double)(v.re * cf.im + v.im * cf.re);
+                }
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < NB; r++)
+        {
+            rr[r][threadIdx.x] = accr[r];
+            ri[r][threadIdx.x] = acci[r];
+        }
+        __syncthreads();
+        if (active && si == 0)
+        {
+            const long long o = a.tgt_perm[t];
+            for (int r = 0; r < bp.nrhs; r++)
+            {
+                double sr = 0, sim = 0;
+                for (int s = 0; s < S; s++)
+                {
+                    sr += rr[r][ti + s * cnt];
+                    sim += ri[r][ti + s * cnt];
+                }
+                const double2 nr = bp.unear[(size_t)r * bp.n_tgt + t];
+                sr += nr.x;
+                sim += nr.y;
+                double* out = a.out + (size_t)r * bp.out_plane;
+                if (a.real_out)
+                    out[o] = sr;
+                else
+                {
+                    out[2 * o] = sr;
+                    out[2 * o + 1] = sim;
+                }
+            }
+        }
+    }
+}
+
+// Enqueues the batched mixed matvec of bp.nrhs (<= BATCH_NB) right-hand
+// sides; returns the number of kernels launched, or -1 when this operator's
+// shape has no batched path (runtime orders, or a level whose upward runs
+// do not fit the staged kernel) and the right-hand sides must run one by one.
+template <int KIND, int N0, int N1, int N2>
+static int run_mult_batch(const MultPtrs& m, const BatchPtrs& bp, const void* d_w, void* d_u,
+                          bool real, cudaStream_t st, LaunchHooks* hk)
+{
+    if constexpr (N0 == 0 || (N0 * N1 * N2) % 2 != 0)
+        return -1;
+    else
+    {
+        for (int l = 0; l + 1 < m.L; l++)
+        {
+            const LevelLists& LL = m.lists[l];
+            if (LL.n_up > 0 && (LL.fe_pad <= 0 || upward_staged_smem<N0, N1, N2>(
+                                                      m.P_hi, upward_staged_rch<N0, N1, N2>(
+                                                                  LL.fe_pad)) >
+                                                      UP_STAGED_SMEM_MAX))
+                return -1;
+        }
+        if (m.lo[0] != N0 || m.fct[0] != 3 || m.fct[1] != 3 || m.fct[2] != 3)
+            return -1;
+        int launches = 0;
+        {
+            const int thr = 256;
+            const int blocks = (int)std::min<long long>((m.n_src + thr - 1) / thr, 148 * 4);
+            if (hk)
+                hk->begin(PROF_PERMUTE);
+            permute_batch_kernel<<<dim3(blocks, BATCH_NB), thr, 0, st>>>(
+                (const double*)d_w, real ? 1 : 0, m.src_perm, bp.w, m.n_src, bp.nrhs, bp.in_plane);
+            IFGF_CHECK_LAUNCH();
+            if (hk)
+                hk->end();
+            launches++;
+        }
+        EvalArgs ea;
+        ea.lv = m.lv_dev;
+        ea.L = m.L;
+        ea.T = m.T;
+        ea.S = m.S;
+        ea.tx = m.tx;
+        ea.ty = m.ty;
+        ea.tz = m.tz;
+        ea.tgt_perm = m.tgt_perm;
+        ea.tl_first = m.tl_first;
+        ea.tl_last = m.tl_last;
+        ea.far_off = m.tl_far_off;
+        ea.far_src = m.tl_far_src;
+        ea.near_off = m.tl_near_off;
+        ea.near_src = m.tl_near_src;
+        ea.w = reinterpret_cast<const double2*>(bp.w);
+        ea.fmap = m.fmap;
+        ea.fcoef = reinterpret_cast<const double2*>(bp.fcoef);
+        ea.out = (double*)d_u;
+        ea.unear = bp.unear;
+        ea.real_out = real ? 1 : 0;
+        ea.err = m.err;
+        ea.P_lo = m.P_lo;
+        for (int d = 0; d < 3; d++)
+            ea.lo[d] = m.lo[d];
+        ea.kp = m.kp;
+        const bool overlap = hk == nullptr && m.side != nullptr;
+        if (m.n_tleaf > 0)
+        {
+            cudaStream_t ns = st;
+            if (overlap)
+            {
+                IFGF_CHECK(cudaEventRecord(m.ev_fork, st));
+                IFGF_CHECK(cudaStreamWaitEvent(m.side, m.ev_fork, 0));
+                ns = m.side;
+            }
+            if (hk)
+                hk->begin(PROF_NEAR);
+            near_batch_kernel<KIND><<<m.n_tleaf, EVAL_THREADS, 0, ns>>>(ea, bp);
+            IFGF_CHECK_LAUNCH();
+            if (hk)
+                hk->end();
+            if (overlap)
+                IFGF_CHECK(cudaEventRecord(m.ev_join, m.side));
+            launches++;
+        }
+        const int nthr = node_threads(m.P_hi);
+        const int nchk = node_chunks(m.P_hi);
+        for (int l = m.L - 1; l >= 0; l--)
+        {
+            const LevelGeom& G = m.lv_host[l];
+            if (G.n_coarse == 0)
+                continue;
+            const LevelLists& LL = m.lists[l];
+            if (LL.n_leaf > 0)
+            {
+                LeafArgs la{G,      m.T,     m.S,  LL.cc_box, LL.cc_el, LL.leaf_idx, m.hi_nodes,
+                            m.w,    m.cvals, m.P_hi, m.kp};
+                if (hk)
+                    hk->begin(PROF_COARSE, l);
+                leaf_sample_batch_kernel<KIND>
+                    <<<dim3(LL.n_leaf, nchk), nthr,
+                       (7 * nthr + 2 * BATCH_NB * nthr) * sizeof(float), st>>>(la, bp);
+                IFGF_CHECK_LAUNCH();
+                if (hk)
+                    hk->end();
+                launches++;
+            }
+            if (LL.n_up > 0)
+            {
+                UpArgs ua;
+                ua.G = G;
+                ua.GC = l + 1 < m.L ? m.lv_host[l + 1] : G;
+                ua.T = m.T;
+                ua.cc_box = LL.cc_box;
+                ua.cc_el = LL.cc_el;
+                ua.idx = LL.up_idx;
+                ua.slot = LL.up_slot;
+                ua.geo64 = LL.geo64;
+                ua.geo32 = LL.geo32;
+                ua.P_pad = LL.up_pad;
+                ua.fe_list = LL.fe_list;
+                ua.fe_pad = LL.fe_pad;
+                ua.rch = upward_staged_rch<N0, N1, N2>(LL.fe_pad);
+                ua.cv_plane = bp.cv_plane;
+                ua.fc_plane = bp.fc_plane;
+                ua.hi_nodes = m.hi_nodes;
+                ua.fmap = m.fmap;
+                ua.fcoef = reinterpret_cast<const double2*>(bp.fcoef);
+                ua.cvals = reinterpret_cast<double2*>(bp.cvals);
+                ua.err = m.err;
+                ua.P_hi = m.P_hi;
+                ua.P_lo = m.P_lo;
+                for (int d = 0; d < 3; d++)
+                    ua.lo[d] = m.lo[d];
+                ua.kp = m.kp;
+                const size_t sm = upward_staged_smem<N0, N1, N2>(m.P_hi, ua.rch);
+                auto kern = upward_staged_kernel<KIND, N0, N1, N2>;
+                if (sm > 48 * 1024)
+                    IFGF_CHECK(cudaFuncSetAttribute(
+                        kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+                if (hk)
+                    hk->begin(PROF_UPWARD, l);
+                kern<<<dim3(LL.n_up, BATCH_NB), UPS_THREADS, sm, st>>>(ua);
+                IFGF_CHECK_LAUNCH();
+                if (hk)
+                    hk->end();
+                launches++;
+            }
+            const unsigned c2f_grid = LL.n_c2f >= 0 ? (unsigned)LL.n_c2f : (unsigned)G.n_coarse;
+            if (c2f_grid == 0)
+                continue;
+            C2FArgs fa;
+            fa.G = G;
+            fa.idx = LL.n_c2f >= 0 ? LL.c2f_idx : nullptr;
+            fa.cv_plane = bp.cv_plane;
+            fa.fc_plane = bp.fc_plane;
+            fa.cc_box = LL.cc_box;
+            fa.cc_el = LL.cc_el;
+            fa.cvals = reinterpret_cast<const double2*>(bp.cvals);
+            fa.A = m.A;
+            fa.fmap = m.fmap;
+            fa.fcoef = reinterpret_cast<double2*>(bp.fcoef);
+            for (int d = 0; d < 3; d++)
+            {
+                fa.hi[d] = m.hi[d];
+                fa.lo[d] = m.lo[d];
+                fa.f[d] = m.fct[d];
+            }
+            fa.P_hi = m.P_hi;
+            fa.P_lo = m.P_lo;
+            if (hk)
+                hk->begin(PROF_C2F, l);
+            if (!launch_c2f_fixed<float>(fa, m.A_host, c2f_grid, st, BATCH_NB))
+                throw Error(6, "batched coarse-to-fine needs one of the fixed order shapes");
+            IFGF_CHECK_LAUNCH();
+            if (hk)
+                hk->end();
+            launches++;
+        }
+        if (m.n_tleaf > 0)
+        {
+            if (overlap)
+                IFGF_CHECK(cudaStreamWaitEvent(st, m.ev_join, 0));
+            if (hk)
+                hk->begin(PROF_EVAL);
+            far_batch_kernel<KIND, N0, N1, N2><<<m.n_tleaf, EVAL_THREADS, 0, st>>>(ea, bp);
+            IFGF_CHECK_LAUNCH();
+            if (hk)
+                hk->end();
+            launches++;
+        }
+        return launches;
+    }
+}
+
+template <int KIND>
+int launch_mult_batch_kernels(const MultPtrs& m, const BatchPtrs& bp, const void* d_w, void* d_u,
+                              bool real, cudaStream_t st, LaunchHooks* hk)
+{
+    const int* lo = m.lo;
+    if (lo[0] == 2 && lo[1] == 5 && lo[2] == 5)
+        return run_mult_batch<KIND, 2, 5, 5>(m, bp, d_w, d_u, real, st, hk);
+    if (lo[0] == 3 && lo[1] == 6 && lo[2] == 6)
+        return run_mult_batch<KIND, 3, 6, 6>(m, bp, d_w, d_u, real, st, hk);
+    if (lo[0] == 4 && lo[1] == 7 && lo[2] == 7)
+        return run_mult_batch<KIND, 4, 7, 7>(m, bp, d_w, d_u, real, st, hk);
+    return -1;
+}

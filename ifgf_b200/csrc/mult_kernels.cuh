@@ -224,6 +224,8 @@ struct UpArgs
     const int2* __restrict__ fe_list; // [slot][octant][fe_pad]: (element, first group) per run
     int fe_pad;
     int rch; // runs staged at a time by the staged kernel
+    // batched right-hand sides (staged kernel): blockIdx.y selects the plane
+    long long cv_plane, fc_plane;
     const double* __restrict__ hi_nodes;
     const int* __restrict__ fmap;
     const double2* __restrict__ fcoef;
@@ -448,6 +450,8 @@ struct C2FArgs
 {
     LevelGeom G;
     const int* __restrict__ idx; // coarse cones to refine (null: all of the level)
+    // batched right-hand sides (fixed-order kernel): blockIdx.y selects the plane
+    long long cv_plane, fc_plane;
     const int* __restrict__ cc_box;
     const int* __restrict__ cc_el;
     const double2* __restrict__ cvals;
@@ -1380,7 +1384,7 @@ __global__ void __launch_bounds__(UPS_THREADS, 10) upward_staged_kernel(UpArgs a
     const int c = a.idx[blockIdx.x];
     const int slot = a.slot[blockIdx.x];
     const int box = a.cc_box[c], el = a.cc_el[c];
-    const float2* fcf = reinterpret_cast<const float2*>(a.fcoef);
+    const float2* fcf = reinterpret_cast<const float2*>(a.fcoef) + blockIdx.y * a.fc_plane;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int n = threadIdx.x; n < a.P_hi; n += blockDim.x)
         acc[n] = make_float2(0.f, 0.f);
@@ -1495,7 +1499,7 @@ __global__ void __launch_bounds__(UPS_THREADS, 10) upward_staged_kernel(UpArgs a
         }
     }
     __syncthreads();
-    float2* cv = reinterpret_cast<float2*>(a.cvals);
+    float2* cv = reinterpret_cast<float2*>(a.cvals) + blockIdx.y * a.cv_plane;
     for (int n = threadIdx.x; n < a.P_hi; n += blockDim.x)
         cv[(size_t)c * a.P_hi + n] = acc[n];
 }
@@ -1751,7 +1755,8 @@ __global__ void __launch_bounds__(c2f_fixed_threads<H0, H1, H2, L0, L1, L2, F>()
     }
     if (t < H1 * H2)
     {
-        const V* src = reinterpret_cast<const V*>(a.cvals) + (size_t)c * P_HI + H0 * t;
+        const V* src = reinterpret_cast<const V*>(a.cvals) + blockIdx.y * a.cv_plane +
+                       (size_t)c * P_HI + H0 * t;
         V x[H0];
 #pragma unroll
         for (int m = 0; m < H0; m++)
@@ -1799,7 +1804,7 @@ __global__ void __launch_bounds__(c2f_fixed_threads<H0, H1, H2, L0, L1, L2, F>()
 #pragma unroll
         for (int m = 0; m < H2; m++)
             x[m] = Y2[t + S2 * m];
-        V* fco = reinterpret_cast<V*>(a.fcoef);
+        V* fco = reinterpret_cast<V*>(a.fcoef) + blockIdx.y * a.fc_plane;
 #pragma unroll
         for (int j2 = 0; j2 < F; j2++)
         {
@@ -1834,7 +1839,7 @@ constexpr size_t c2f_fixed_smem()
 // instantiated shapes; returns false otherwise.
 template <typename T>
 static bool launch_c2f_fixed(const C2FArgs& fa, const double* A_host, unsigned grid,
-                             cudaStream_t st)
+                             cudaStream_t st, unsigned planes = 1)
 {
     const int* h = fa.hi;
     const int* l = fa.lo;
@@ -1854,7 +1859,7 @@ static bool launch_c2f_fixed(const C2FArgs& fa, const double* A_host, unsigned g
         auto kern = coarse_to_fine_fixed_kernel<A, B, C, D, E, G, 3, T>;                       \
         if (sm > 48 * 1024)                                                                    \
             cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);  \
-        kern<<<grid, c2f_fixed_threads<A, B, C, D, E, G, 3>(), sm, st>>>(fa, mats);            \
+        kern<<<dim3(grid, planes), c2f_fixed_threads<A, B, C, D, E, G, 3>(), sm, st>>>(fa, mats); \
         return true;                                                                           \
     }
     IFGF_C2F_CASE(5, 8, 8, 2, 5, 5)
@@ -2178,6 +2183,7 @@ static int run_mult(const MultPtrs& m, const void* d_w, void* d_u, bool real, cu
             ua.P_pad = LL.up_pad;
             ua.fe_list = LL.fe_list;
             ua.rch = 0;
+            ua.cv_plane = ua.fc_plane = 0;
             ua.fe_pad = LL.fe_pad;
             ua.hi_nodes = m.hi_nodes;
             ua.fmap = m.fmap;
@@ -2227,6 +2233,7 @@ static int run_mult(const MultPtrs& m, const void* d_w, void* d_u, bool real, cu
         C2FArgs fa;
         fa.G = G;
         fa.idx = LL.n_c2f >= 0 ? LL.c2f_idx : nullptr;
+        fa.cv_plane = fa.fc_plane = 0;
         fa.cc_box = LL.cc_box;
         fa.cc_el = LL.cc_el;
         fa.cvals = m.cvals;
@@ -2309,9 +2316,13 @@ void launch_direct_kernel(const MultPtrs& m, const int* tpos, int nt, double2* o
     IFGF_CHECK_LAUNCH();
 }
 
+#include "mult_batch.cuh"
+
 #define IFGF_INSTANTIATE_KIND(K)                                                              \
     template int launch_mult_kernels<K>(const MultPtrs&, const void*, void*, bool, cudaStream_t, \
                                         LaunchHooks*);                                         \
+    template int launch_mult_batch_kernels<K>(const MultPtrs&, const BatchPtrs&, const void*,  \
+                                              void*, bool, cudaStream_t, LaunchHooks*);        \
     template void launch_direct_kernel<K>(const MultPtrs&, const int*, int, double2*, cudaStream_t); \
     template void permute_only<K>(const MultPtrs&, const void*, bool, cudaStream_t);         \
     template void launch_build_upgeo<K>(const LevelGeom&, const LevelGeom&, double, double,   \

@@ -118,6 +118,9 @@ struct DeviceState
     DevBuf<int> tl_first, tl_last, tl_far_src, tl_near_src;
     DevBuf<long long> tl_far_off, tl_near_off;
     DevBuf<double2> w, cvals, fcoef, unear;
+    // planes of the batched mixed matvec, allocated on first use
+    DevBuf<float2> bw, bcv, bfc;
+    DevBuf<double2> bun;
     DevBuf<unsigned long long> err;
     DevBuf<double> io_w, io_u; // staging for host-buffer mult
     std::vector<cudaEvent_t> prof_ev;
@@ -1294,6 +1297,14 @@ void Operator::launch_mult(const void* d_w, void* d_u, void* stream, bool timed,
                                                      on ? &log : nullptr));
     launches_per_mult_ = launches;
     if (on && log.n > 0)
+        finish_profile(log, 1);
+}
+
+// Per-kernel times of the launches recorded in `log` (one matvec, or one
+// batched group of `rhs` right-hand sides).
+void Operator::finish_profile(EventHooks& log, int rhs)
+{
+    DeviceState& D = *dev_;
     {
         IFGF_CUDA(cudaEventSynchronize(D.prof_ev[2 * log.n - 1]));
         double cls_ms[NPROF] = {};
@@ -1313,7 +1324,7 @@ void Operator::launch_mult(const void* d_w, void* d_u, void* stream, bool timed,
         float tot = 0;
         IFGF_CUDA(cudaEventElapsedTime(&tot, D.prof_ev[0], D.prof_ev[2 * log.n - 1]));
         if (profiling_)
-            mults_profiled_++;
+            mults_profiled_ += rhs;
         last_.permute = cls_ms[PROF_PERMUTE];
         last_.coarse = cls_ms[PROF_COARSE];
         last_.c2f = cls_ms[PROF_C2F];
@@ -1344,7 +1355,84 @@ void Operator::mult_device(const void* d_w, void* d_u, void* stream)
 
 void Operator::mult_host(const void* w, void* u, int64_t batch)
 {
+    if (batch > 1 && precision_ == PREC_MIXED)
+    {
+        // the batched device pipeline on staged copies of all right-hand sides
+        DeviceState& D = *dev_;
+        if (!w || !u)
+            throw Error(ERR_INVALID, "null density or result buffer");
+        const size_t per = is_real() ? 1 : 2;
+        const size_t nw = per * (size_t)n_src() * batch, nu = per * (size_t)n_tgt() * batch;
+        if (D.io_w.n < nw)
+            D.io_w.alloc(nw);
+        if (D.io_u.n < nu)
+            D.io_u.alloc(nu);
+        IFGF_CUDA(cudaMemcpy(D.io_w.p, w, nw * sizeof(double), cudaMemcpyHostToDevice));
+        mult_batch_device(D.io_w.p, D.io_u.p, batch, nullptr);
+        IFGF_CUDA(cudaMemcpy(u, D.io_u.p, nu * sizeof(double), cudaMemcpyDeviceToHost));
+        IFGF_CUDA(cudaMemcpy(&missing_, D.err.p, sizeof(unsigned long long),
+                             cudaMemcpyDeviceToHost));
+        return;
+    }
     host_mult_loop(w, u, batch, -1);
+}
+
+void Operator::mult_batch_device(const void* d_w, void* d_u, int64_t batch, void* stream)
+{
+    if (!initialized_)
+        throw Error(ERR_STATE, "mult called before init");
+    if (!d_w || !d_u)
+        throw Error(ERR_INVALID, "null density or result buffer");
+    if (batch < 1)
+        throw Error(ERR_INVALID, "batch must be >= 1");
+    DeviceState& D = *dev_;
+    const size_t per = is_real() ? 1 : 2;
+    const long long in_plane = (long long)(per * n_src()), out_plane = (long long)(per * n_tgt());
+    int64_t done = 0;
+    if (precision_ == PREC_MIXED && batch > 1)
+    {
+        if (D.bw.n == 0)
+        {
+            D.bw.alloc((size_t)BATCH_NB * n_src());
+            D.bcv.alloc((size_t)BATCH_NB * D.cvals.n);
+            D.bfc.alloc((size_t)BATCH_NB * D.fcoef.n);
+            D.bfc.zero(); // fine cones without an active coarse parent read zero
+            D.bun.alloc((size_t)BATCH_NB * n_tgt());
+        }
+        BatchPtrs bp;
+        bp.w = D.bw.p;
+        bp.cvals = D.bcv.p;
+        bp.fcoef = D.bfc.p;
+        bp.unear = D.bun.p;
+        bp.cv_plane = (long long)D.cvals.n;
+        bp.fc_plane = (long long)D.fcoef.n;
+        bp.n_src = n_src();
+        bp.n_tgt = n_tgt();
+        bp.in_plane = in_plane;
+        bp.out_plane = out_plane;
+        MultPtrs m;
+        fill_mult_ptrs(m);
+        cudaStream_t st = (cudaStream_t)stream;
+        while (done < batch)
+        {
+            bp.nrhs = (int)std::min<int64_t>(BATCH_NB, batch - done);
+            EventHooks log(D, st);
+            int r = -1;
+            IFGF_DISPATCH(kind_, r = launch_mult_batch_kernels<KK>(
+                                     m, bp, (const double*)d_w + done * in_plane,
+                                     (double*)d_u + done * out_plane, is_real(), st,
+                                     profiling_ ? &log : nullptr));
+            if (r < 0)
+                break; // no batched path for this shape
+            launches_per_mult_ = r;
+            if (profiling_ && log.n > 0)
+                finish_profile(log, bp.nrhs);
+            done += bp.nrhs;
+        }
+    }
+    for (; done < batch; done++)
+        launch_mult((const double*)d_w + done * in_plane, (double*)d_u + done * out_plane, stream,
+                    false);
 }
 
 void Operator::host_mult_loop(const void* w, void* u, int64_t batch, int vkind)

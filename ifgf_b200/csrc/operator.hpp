@@ -17,6 +17,7 @@ namespace ifgf
 struct DeviceState;  // device buffers, defined in operator.cu
 struct MultPtrs;     // kernel launch view, defined in mult.hpp
 struct AdjointState; // operators and buffers of the adjoint, defined in operator.cu
+struct EventHooks;   // per-launch CUDA events, defined in operator.cu
 
 struct StageTimes
 {
@@ -49,6 +50,11 @@ class Operator
     void mult_device(const void* d_w, void* d_u, void* stream);
     // host buffers, `batch` right-hand sides
     void mult_host(const void* w, void* u, int64_t batch);
+    // `batch` right-hand sides on device buffers (batch x n_src in, batch x
+    // n_tgt out).  The mixed pipeline runs them BATCH_NB at a time through
+    // the batched kernels (one kernel / geometry evaluation for the group);
+    // FP64 and shapes without a batched path run them one by one.
+    void mult_batch_device(const void* d_w, void* d_u, int64_t batch, void* stream);
     // mult_device with its scratch in a caller-provided device region instead
     // of the buffers allocated at init; allocates nothing
     void mult_device_external_scratch(const void* d_w, void* d_u, void* stream, void* scratch,
@@ -98,6 +104,7 @@ class Operator
     void fill_mult_ptrs(MultPtrs& m, bool variant = false) const;
     void ensure_variant_tables(int vkind);
     void ensure_adjoint();
+    void finish_profile(EventHooks& log, int rhs);
     void host_mult_loop(const void* w, void* u, int64_t batch, int vkind);
 
     int kind_;

@@ -142,6 +142,12 @@ class IfgfOperator:
         check(lib.ifgf_mult_batch(self._h, w.ctypes.data, u.ctypes.data, w.shape[0]))
         return u
 
+    def mult_batch_device(self, w_ptr, u_ptr, batch, stream_ptr=0):
+        """Enqueue A . w for `batch` right-hand sides on device buffers
+        (batch x N in, batch x M out; raw pointers)."""
+        check(lib.ifgf_mult_batch_device(self._h, C.c_void_p(w_ptr), C.c_void_p(u_ptr),
+                                         int(batch), C.c_void_p(stream_ptr)))
+
     def mult_device(self, w_ptr, u_ptr, stream_ptr=0):
         """Enqueue A . w on device buffers given as raw pointers (torch:
         tensor.data_ptr(), torch.cuda.current_stream().cuda_stream)."""

@@ -107,8 +107,16 @@ int ifgf_init_plan_only(ifgf_operator* op, const double* srcs, long n_src, const
 int ifgf_mult(ifgf_operator* op, const void* w, void* u);
 
 /* Same as ifgf_mult for `batch` right-hand sides stored one after another
- * (w: batch x n_src, u: batch x n_tgt).  No reference counterpart. */
+ * (w: batch x n_src, u: batch x n_tgt).  In the mixed-precision pipeline the
+ * right-hand sides run four at a time through batched kernels that share the
+ * kernel, cone-lookup and centred-factor evaluations of the group (each
+ * right-hand side keeps its own interpolants); FP64 runs them one by one.
+ * No reference counterpart. */
 int ifgf_mult_batch(ifgf_operator* op, const void* w, void* u, long batch);
+
+/* ifgf_mult_batch on device buffers enqueued on `stream`. */
+int ifgf_mult_batch_device(ifgf_operator* op, const void* d_w, void* d_u, long batch,
+                           void* stream);
 
 /* ifgf_mult on device buffers (complex128 / float64 as above) enqueued on
  * `stream` (a cudaStream_t, NULL = legacy default stream).  Returns after
