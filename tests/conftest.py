@@ -10,6 +10,11 @@ if ROOT not in sys.path:
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200); parity tests of the CUDA path")
+    # build (or find current) the CUDA library and the oracle before the test
+    # modules are collected: they import the package, which needs the library
+    import __graft_entry__
+
+    __graft_entry__.build()
 
 
 _HAS_GPU = None
@@ -31,14 +36,3 @@ def pytest_collection_modifyitems(config, items):
     for item in items:
         if "gpu" in item.keywords and not has_gpu():
             item.add_marker(pytest.mark.skip(reason="no CUDA device visible"))
-
-
-@pytest.fixture(scope="session", autouse=True)
-def _built():
-    """Build the oracle and the CUDA library once per session (no-ops when current)."""
-    from oracle.build import build_oracle
-
-    build_oracle()
-    from ifgf_b200 import build as b
-
-    b.build()
