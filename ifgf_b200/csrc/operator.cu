@@ -491,9 +491,27 @@ void Operator::init(const double* srcs, int64_t ns, const double* tgts, int64_t 
     cutoff_ = cutoff;
     same_points_ = ns == nt && std::equal(srcs, srcs + 3 * ns, tgts);
     plan_ = Plan();
-    plan_.src.build(srcs, ns, leaf_);
-    plan_.tgt.build(tgts, nt, leaf_);
+    // the octrees on the GPU; a plan-only init (no GPU needed) on the host,
+    // with the same result
+    const auto tt0 = std::chrono::steady_clock::now();
+    if (plan_only)
+    {
+        plan_.src.build(srcs, ns, leaf_);
+        plan_.tgt.build(tgts, nt, leaf_);
+    }
+    else
+    {
+        plan_.src.build_gpu(srcs, ns, leaf_);
+        if (same_points_ && ns == nt)
+            plan_.tgt = plan_.src;
+        else
+            plan_.tgt.build_gpu(tgts, nt, leaf_);
+    }
+    const auto tt1 = std::chrono::steady_clock::now();
+    tree_ms_ = std::chrono::duration<double, std::milli>(tt1 - tt0).count();
     plan_.build_lists(cutoff);
+    lists_ms_ = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tt1)
+                    .count();
     plan_.assign_shards(shard_n_);
     plan_.build_target_lists(shard_n_ > 1 ? shard_rank_ : -1);
 
@@ -1630,7 +1648,8 @@ std::string Operator::stats_json() const
           << ",\"padded_entries\":" << up_stats_[l].entries << "}";
     o << "]"
       << ",\"target_leaves\":" << dev_->n_tleaf << ",\"missing_cone_lookups\":" << missing_
-      << ",\"init_ms\":" << init_ms_ << ",\"launches_per_mult\":" << launches_per_mult_
+      << ",\"init_ms\":" << init_ms_ << ",\"init_tree_ms\":" << tree_ms_
+      << ",\"init_lists_ms\":" << lists_ms_ << ",\"launches_per_mult\":" << launches_per_mult_
       << ",\"last_mult_ms\":{\"permute\":" << last_.permute << ",\"leaf_sample\":" << last_.coarse
       << ",\"upward\":" << last_.upward << ",\"coarse_to_fine\":" << last_.c2f
       << ",\"target_eval\":" << last_.eval << ",\"near\":" << last_.near

@@ -56,6 +56,27 @@ static bool box_contains(const double* mn, const double* mx, const double* p)
     return true;
 }
 
+void Tree::inflate_bbox(double* mn, double* mx)
+{
+    const double nmn = std::sqrt(mn[0] * mn[0] + mn[1] * mn[1] + mn[2] * mn[2]);
+    const double nmx = std::sqrt(mx[0] * mx[0] + mx[1] * mx[1] + mx[2] * mx[2]);
+    for (int d = 0; d < 3; d++)
+    {
+        mn[d] -= 1e-8 * nmn;
+        mx[d] += 1e-8 * nmx;
+    }
+}
+
+void Tree::child_box(const TreeLevel& L, size_t b, int j, double* cmn, double* cmx)
+{
+    for (int d = 0; d < 3; d++)
+    {
+        const double size = 0.5 * (L.bbmax[3 * b + d] - L.bbmin[3 * b + d]);
+        cmn[d] = L.bbmin[3 * b + d] + size * (double)((j >> d) & 1);
+        cmx[d] = cmn[d] + size;
+    }
+}
+
 void Tree::build(const double* p, int64_t n_pts, int64_t leaf_size)
 {
     n = n_pts;
@@ -70,13 +91,7 @@ void Tree::build(const double* p, int64_t n_pts, int64_t leaf_size)
             mn[d] = std::min(mn[d], p[3 * i + d]);
             mx[d] = std::max(mx[d], p[3 * i + d]);
         }
-    const double nmn = std::sqrt(mn[0] * mn[0] + mn[1] * mn[1] + mn[2] * mn[2]);
-    const double nmx = std::sqrt(mx[0] * mx[0] + mx[1] * mx[1] + mx[2] * mx[2]);
-    for (int d = 0; d < 3; d++)
-    {
-        mn[d] -= 1e-8 * nmn;
-        mx[d] += 1e-8 * nmx;
-    }
+    inflate_bbox(mn, mx);
     double c[3], diam[3];
     for (int d = 0; d < 3; d++)
     {
@@ -112,7 +127,27 @@ void Tree::build(const double* p, int64_t n_pts, int64_t leaf_size)
     }
     keys.clear();
     keys.shrink_to_fit();
+    // children's point ranges by the greedy scan over the sorted points
+    make_levels(mn, mx, [&](const TreeLevel& L, std::vector<int64_t>& ends) {
+        for (size_t b = 0; b < L.size(); b++)
+        {
+            if (L.last[b] - L.first[b] <= max_leaf)
+                continue;
+            int64_t pidx = L.first[b];
+            for (int j = 0; j < 8; j++)
+            {
+                double cmn[3], cmx[3];
+                child_box(L, b, j, cmn, cmx);
+                while (pidx < L.last[b] && box_contains(cmn, cmx, &pts[3 * pidx]))
+                    ++pidx;
+                ends[8 * b + j] = pidx;
+            }
+        }
+    });
+}
 
+void Tree::make_levels(const double* mn, const double* mx, const SplitFn& split)
+{
     // Level-synchronous construction.  Visiting the boxes of a level in id
     // order and their children in octant order hands out the same per-level
     // ids as the depth-first construction of octree.hpp:1106-1184.
@@ -138,10 +173,13 @@ void Tree::build(const double* p, int64_t n_pts, int64_t leaf_size)
     levels.emplace_back();
     if (n > 0)
         push_box(levels[0], 0, n, -1, mn, mx);
+    std::vector<int64_t> ends;
     for (size_t l = 0; l < levels.size(); l++)
     {
         TreeLevel next;
         TreeLevel& L = levels[l];
+        ends.assign(8 * L.size(), -1);
+        split(L, ends);
         for (size_t b = 0; b < L.size(); b++)
         {
             const int64_t cnt = L.last[b] - L.first[b];
@@ -151,15 +189,8 @@ void Tree::build(const double* p, int64_t n_pts, int64_t leaf_size)
             for (int j = 0; j < 8; j++)
             {
                 double cmn[3], cmx[3];
-                for (int d = 0; d < 3; d++)
-                {
-                    const double size = 0.5 * (L.bbmax[3 * b + d] - L.bbmin[3 * b + d]);
-                    cmn[d] = L.bbmin[3 * b + d] + size * (double)((j >> d) & 1);
-                    cmx[d] = cmn[d] + size;
-                }
-                int64_t end = pidx;
-                while (end < L.last[b] && box_contains(cmn, cmx, &pts[3 * end]))
-                    ++end;
+                child_box(L, b, j, cmn, cmx);
+                const int64_t end = ends[8 * b + j];
                 if (end > pidx)
                 {
                     L.child[8 * b + j] = (int32_t)next.size();

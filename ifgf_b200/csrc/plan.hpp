@@ -38,8 +38,26 @@ struct Tree
     int num_levels() const { return (int)levels.size(); }
     int64_t num_boxes_total() const { return level_off.empty() ? 0 : level_off.back(); }
 
-    // Octree::build (octree.hpp:202-238)
+    // Octree::build (octree.hpp:202-238) on the host
     void build(const double* p, int64_t n_pts, int64_t leaf_size);
+    // The same tree built on the current GPU (gpu_tree.cu): Morton keys,
+    // radix sort, and the children's point ranges of every level found by
+    // one warp per box; the result equals build()'s bit for bit.
+    void build_gpu(const double* p, int64_t n_pts, int64_t leaf_size);
+
+    // Inflated bounding box of the points (octree.hpp:207-218), as build
+    // computes it, from the plain coordinate minima and maxima.
+    static void inflate_bbox(double* mn, double* mx);
+    // Creates the levels from the sorted points (pts, perm set) and the root
+    // box: the boxes of a level are split in id order, children in octant
+    // order.  `split` fills, for every box b of the level with more than
+    // max_leaf points, ends[8 b + j] = one past the last point of child j
+    // (the greedy closed-interval scan of octree.hpp:1139-1170; a child is
+    // empty when its end equals the previous child's).
+    using SplitFn = std::function<void(const TreeLevel&, std::vector<int64_t>& ends)>;
+    void make_levels(const double* mn, const double* mx, const SplitFn& split);
+    // the child bounding box j of box b of level L (octree.hpp:1152-1163)
+    static void child_box(const TreeLevel& L, size_t b, int j, double* cmn, double* cmx);
 };
 
 struct Plan
