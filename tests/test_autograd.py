@@ -68,3 +68,42 @@ def test_autograd_real_kernel_density_gradient():
     u = matvec(op, x)
     (u.sum()).backward()
     assert rel2(x.grad.cpu().numpy(), op.mult_adjoint(np.ones(4000))) <= 1e-12
+
+
+@pytest.mark.gpu
+def test_config5_gradients_against_central_differences():
+    """The differentiation workload: combined field, kappa = 50, N = 500,000
+    points on the unit sphere with outward normals, x and b complex N(0,1);
+    loss 0.5 ||A x - b||^2.  The x-gradient (adjoint kernel) against the
+    central difference of the loss along a random direction, the kappa-
+    gradient (dA/dk kernel) against the central difference in kappa, both
+    with step 1e-6, to 1e-6."""
+    import torch
+
+    from ifgf_b200.autograd import matvec
+
+    n = 500000
+    kappa = 50.0
+    pts = W.sphere_points(n, seed=0)
+    x0 = W.densities(n, seed=1)
+    b0 = W.densities(n, seed=3)
+    v0 = W.densities(n, seed=4)
+    op = _cf(kappa, pts)
+    x = torch.tensor(x0, device="cuda", requires_grad=True)
+    b = torch.tensor(b0, device="cuda")
+    k = torch.tensor(kappa, dtype=torch.float64, device="cuda", requires_grad=True)
+    loss = 0.5 * torch.sum(torch.abs(matvec(op, x, k) - b) ** 2)
+    loss.backward()
+    gx = x.grad.cpu().numpy()
+    h = 1e-6
+
+    def loss_of(o, xx):
+        return 0.5 * float(np.sum(np.abs(o.mult(xx) - b0) ** 2))
+
+    # along v: d/dh L(x + h v) = Re <grad_x, v>
+    fd_x = (loss_of(op, x0 + h * v0) - loss_of(op, x0 - h * v0)) / (2 * h)
+    dir_x = float(np.real(np.vdot(gx, v0)))
+    assert abs(fd_x - dir_x) <= 1e-6 * abs(fd_x), (fd_x, dir_x)
+    fd_k = (loss_of(_cf(kappa + h, pts), x0) - loss_of(_cf(kappa - h, pts), x0)) / (2 * h)
+    assert abs(fd_k - k.grad.item()) <= 1e-6 * abs(fd_k), (fd_k, k.grad.item())
+
