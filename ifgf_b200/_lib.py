@@ -48,6 +48,7 @@ def _load():
         "ifgf_set_dx": [H, C.c_int],
         "ifgf_set_precision": [H, C.c_int],
         "ifgf_set_shard": [H, C.c_int, C.c_int],
+        "ifgf_set_wavenumber": [H, C.c_double, C.c_double],
         "ifgf_shard_boxes": [H, _ip, _lp, C.c_long, _lp],
         "ifgf_init": [H, _dp, C.c_long, _dp, C.c_long, _dp, CUTOFF_FN, C.c_void_p],
         "ifgf_init_plan_only": [H, _dp, C.c_long, _dp, C.c_long, CUTOFF_FN, C.c_void_p],
@@ -90,6 +91,7 @@ lib = _load()
 # Every symbol declared in include/ifgf_b200.h.
 EXPORTED = [
     "ifgf_create", "ifgf_set_dx", "ifgf_set_precision", "ifgf_set_shard", "ifgf_shard_boxes",
+    "ifgf_set_wavenumber",
     "ifgf_init", "ifgf_init_plan_only",
     "ifgf_box_list", "ifgf_mult",
     "ifgf_mult_batch", "ifgf_mult_batch_device", "ifgf_mult_device", "ifgf_mult_device_noalloc",

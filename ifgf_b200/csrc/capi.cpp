@@ -79,6 +79,13 @@ extern "C"
         return guarded([&] { h->op.set_dx(dx); });
     }
 
+    int ifgf_set_wavenumber(ifgf_operator* h, double k_re, double k_im)
+    {
+        if (!h)
+            return null_handle();
+        return guarded([&] { h->op.set_wavenumber(k_re, k_im); });
+    }
+
     int ifgf_set_shard(ifgf_operator* h, int rank, int nranks)
     {
         if (!h)

@@ -344,6 +344,74 @@ void Operator::set_dx(int dx)
     dx_ = dx;
 }
 
+void Operator::set_wavenumber(double k_re, double k_im)
+{
+    if (!std::isfinite(k_re) || !std::isfinite(k_im))
+        throw Error(ERR_INVALID, "wavenumber must be finite");
+    if (!initialized_)
+    {
+        kr_ = k_re;
+        ki_ = k_im;
+        return;
+    }
+    const double okr = kr_, oki = ki_;
+    kr_ = k_re;
+    ki_ = k_im;
+    bool same = true;
+    for (const LevelGeom& G : lv_)
+    {
+        int64_t nf[3], nc[3];
+        elements_for_box(G.H, 0, nf);
+        elements_for_box(G.H, 1, nc);
+        double smin = cutoff_limit(G.H);
+        if (smin >= std::sqrt(3.0) / 3)
+            smin = std::sqrt(3.0) / 3 - 0.05;
+        for (int d = 0; d < 3; d++)
+            same = same && nf[d] == G.nf[d] && nc[d] == G.nc[d];
+        same = same && smin == G.dmin[0];
+    }
+    adj_.reset();
+    if (!same)
+    {
+        // new cone grids: a full init from the stored points
+        const std::vector<double> s = src_pts_, t = tgt_pts_, nrm = normals_;
+        const auto cut = cutoff_;
+        try
+        {
+            init(s.data(), (int64_t)s.size() / 3, t.data(), (int64_t)t.size() / 3,
+                 nrm.empty() ? nullptr : nrm.data(), cut);
+        }
+        catch (...)
+        {
+            kr_ = okr;
+            ki_ = oki;
+            throw;
+        }
+        return;
+    }
+    DeviceState& D = *dev_;
+    const int L = (int)lv_.size();
+    const int P_hi = hi_[0] * hi_[1] * hi_[2];
+    const KParams kp = make_kparams(kr_, ki_, dx_);
+    for (int l = 0; l + 1 < L; l++)
+    {
+        const LevelLists& LL = D.lists[l];
+        const int ns = (int)D.slot_el[l].n;
+        if (ns == 0 || LL.up_pad <= 0)
+            continue;
+        const size_t n_ent = (size_t)ns * 8 * (size_t)LL.up_pad;
+        IFGF_CUDA(cudaMemset(D.geo64[l].p, 0xff, n_ent * sizeof(UpGeo64)));
+        IFGF_CUDA(cudaMemset(D.geo32[l].p, 0xff, n_ent * sizeof(UpGeo32)));
+        IFGF_DISPATCH(kind_, launch_build_upgeo<KK>(lv_[l], lv_[l + 1], D.up_pH[l], D.up_cH[l],
+                                                     D.child_off[l].p, D.slot_el[l].p, ns,
+                                                     D.hi_nodes.p, P_hi, kp, LL.up_pad,
+                                                     D.geo64[l].p, D.geo32[l].p, LL.fe_pad,
+                                                     D.fe_list[l].p));
+    }
+    IFGF_CUDA(cudaDeviceSynchronize());
+    D.vkind = -1; // variant (k-derivative) tables are rebuilt on next use
+}
+
 void Operator::set_shard(int rank, int nranks)
 {
     if (nranks < 1 || rank < 0 || rank >= nranks)

@@ -33,6 +33,13 @@ class Operator
     ~Operator();
 
     void set_dx(int dx);
+    // Change the wavenumber of an initialised operator.  When every level's
+    // cone grids stay the same (elementsForBox), the tree, lists and cone
+    // maps are kept and only the k-dependent centre-shift factors of the
+    // upward geometry are recomputed; otherwise the operator is initialised
+    // again from the points of the last init.  Frequency sets (convolution
+    // quadrature) thus share one tree and one set of cone maps.
+    void set_wavenumber(double k_re, double k_im);
     // Take share `rank` of `nranks` of the matvec (before init): mult then
     // returns the contribution of this rank's source subtrees to every
     // target, and the ranks' results sum to the full matvec (see

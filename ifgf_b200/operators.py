@@ -100,6 +100,13 @@ class IfgfOperator:
                                       t.ctypes.data_as(dp), t.shape[0], cb, None))
         self._n_src, self._n_tgt = s.shape[0], t.shape[0]
 
+    def set_wavenumber(self, k):
+        """Move the operator to wavenumber k (complex for the modified
+        Helmholtz and gradient kernels), keeping the tree and cone maps when
+        the cone grids allow (frequency sets)."""
+        k = complex(k)
+        check(lib.ifgf_set_wavenumber(self._h, k.real, k.imag))
+
     def set_shard(self, rank, nranks):
         """Take share `rank` of `nranks` of the matvec (call before init); the
         ranks' mult results sum to the full matvec (see ifgf_b200.distributed)."""

@@ -64,6 +64,15 @@ int ifgf_create(int kind, double k_re, double k_im, long leaf_size, long order, 
  * py_ifgf.cpp:40): dx in {-1, 0, 1, 2}. */
 int ifgf_set_dx(ifgf_operator* op, int dx);
 
+/* Changes the wavenumber of an operator.  After init, when the new k gives
+ * every level the same cone grids (elementsForBox of the kernel), the tree,
+ * interaction lists and active-cone maps are kept and only the k-dependent
+ * centre-shift factors are recomputed (milliseconds); otherwise the operator
+ * is initialised again from the points, normals and cutoff of its last init.
+ * For frequency sets (convolution quadrature), where the reference builds a
+ * new operator per frequency (test/test_CQIFGF.cpp:117-135). */
+int ifgf_set_wavenumber(ifgf_operator* op, double k_re, double k_im);
+
 /* Selects FP64 (default) or the mixed-precision pipeline.  No reference
  * counterpart (the reference is FP64 only). */
 int ifgf_set_precision(ifgf_operator* op, int mode);
