@@ -67,7 +67,8 @@ struct LevelLists
     const UpGeo32* geo32;
     int n_leaf, n_up;
     int up_pad; // row stride of the geometry tables
-    const int2* fe_list; // [slot][octant][fe_pad]: (child element, first group) of each run
+    const int2* fe_list; // [slot][octant][fe_pad + 1]: (child element, first group) of each
+                         // run, then (-1, groups of the row)
     int fe_pad;         // longest run list of a row
     const int* c2f_idx; // coarse cones to refine when n_c2f >= 0 (sharded operators)
     int n_c2f;          // -1: all of the level's cones

@@ -221,7 +221,9 @@ struct UpArgs
     const UpGeo64* __restrict__ geo64;
     const UpGeo32* __restrict__ geo32;
     int P_pad;
-    const int2* __restrict__ fe_list; // [slot][octant][fe_pad]: (element, first group) per run
+    // [slot][octant][fe_pad + 1]: (element, first group) per run, then a
+    // sentinel (-1, groups of the row)
+    const int2* __restrict__ fe_list;
     int fe_pad;
     int rch; // runs staged at a time by the staged kernel
     // batched right-hand sides (staged kernel): blockIdx.y selects the plane
@@ -280,8 +282,9 @@ __device__ __forceinline__ bool upward_fallback64(const UpArgs& a, int box, int 
 // always shares one element.  fill = 0 only measures the row: its padded
 // length and its number of element runs (row_len[2 row], row_len[2 row + 1]).
 // fill = 1 also lists each row's distinct elements in run order
-// with the group at which each run starts (fe_list[row fe_pad + r] =
-// (element, first group)) and stores the run index r of every entry in
+// with the group at which each run starts (fe_list[row (fe_pad + 1) + r] =
+// (element, first group)), followed by a sentinel (-1, groups of the row),
+// and stores the run index r of every entry in
 // UpGeo32::pad, so that a kernel can stage one coefficient block per run.
 constexpr int UPGEO_RUN = 4;
 
@@ -344,7 +347,7 @@ __global__ void __launch_bounds__(256) build_upgeo_kernel(LevelGeom PG, LevelGeo
                     runid[start + j] = nrun;
                 }
                 if (fill && nrun < fe_pad)
-                    fe_list[(size_t)row * fe_pad + nrun] =
+                    fe_list[(size_t)row * (fe_pad + 1) + nrun] =
                         make_int2(key[snode[start]], off_run / UPGEO_RUN);
                 nrun++;
                 off_run += (len + UPGEO_RUN - 1) / UPGEO_RUN * UPGEO_RUN;
@@ -362,6 +365,9 @@ __global__ void __launch_bounds__(256) build_upgeo_kernel(LevelGeom PG, LevelGeo
             row_len[2 * row] = off_run;
             row_len[2 * row + 1] = nrun;
         }
+        else if (nrun <= fe_pad)
+            // sentinel after the last run: (-1, groups of the row)
+            fe_list[(size_t)row * (fe_pad + 1) + nrun] = make_int2(-1, off_run / UPGEO_RUN);
     }
     __syncthreads();
     if (!fill)
@@ -1397,7 +1403,7 @@ __global__ void __launch_bounds__(UPS_THREADS, 10) upward_staged_kernel(UpArgs a
         if (cb < 0)
             continue;
         const int* fm = a.fmap + C.fmap_off + (long long)(cb - C.box_off) * nf;
-        const int2* fl = a.fe_list + ((size_t)slot * 8 + o) * a.fe_pad;
+        const int2* fl = a.fe_list + ((size_t)slot * 8 + o) * (a.fe_pad + 1);
         const UpGeo32* row = a.geo32 + ((size_t)slot * 8 + o) * a.P_pad;
         for (int r0 = 0; r0 < a.fe_pad; r0 += a.rch)
         {
@@ -1405,13 +1411,9 @@ __global__ void __launch_bounds__(UPS_THREADS, 10) upward_staged_kernel(UpArgs a
             if (first.x < 0)
                 break; // past the row's last run
             const int r1 = min(r0 + a.rch, a.fe_pad);
-            int g_end = ngroups;
-            if (r1 < a.fe_pad)
-            {
-                const int2 next = fl[r1];
-                if (next.x >= 0)
-                    g_end = next.y;
-            }
+            // the next run's first group, or the row's end from its sentinel
+            const int2 next = fl[r1];
+            const int g_end = next.y >= 0 ? next.y : ngroups;
             __syncthreads(); // the previous runs' blocks are no longer read
             for (int r = r0 + warp; r < r1; r += UPS_THREADS / 32)
             {

@@ -985,7 +985,7 @@ void Operator::setup_device(const double* normals)
                         }
                 }
             }
-            D.fe_list[l].alloc((size_t)ns * 8 * std::max(runs, 1));
+            D.fe_list[l].alloc((size_t)ns * 8 * (runs + 1)); // runs and a sentinel per row
             IFGF_CUDA(cudaMemset(D.fe_list[l].p, 0xff, D.fe_list[l].n * sizeof(int2)));
             const size_t n_ent = (size_t)ns * 8 * (size_t)std::max(pad, 1);
             D.geo64[l].alloc(n_ent);
