@@ -189,4 +189,22 @@ template <int KIND>
 void launch_direct_kernel(const MultPtrs& m, const int* tpos, int nt, double2* out,
                           cudaStream_t st);
 
+// Order estimation probe (ifgfoperator.hpp:204-212): the factored kernel of
+// a sample box's sources with unit weights at Cartesian nodes.  Sample s owns
+// sources [src_off[s], src_off[s + 1]) of S and nodes [node_off[s],
+// node_off[s + 1]) of `nodes` (xyz triples); out receives one value per node.
+struct ProbeArgs
+{
+    SrcArgs S;
+    const int* __restrict__ src_off;
+    const double* __restrict__ nodes;
+    const int* __restrict__ node_off;
+    const double* __restrict__ centre; // 3 per sample
+    KParams kp;
+    double2* out;
+};
+
+template <int KIND>
+void launch_order_probe(const ProbeArgs& a, int n_samples, int max_nodes, cudaStream_t st);
+
 } // namespace ifgf

@@ -2318,6 +2318,41 @@ void launch_direct_kernel(const MultPtrs& m, const int* tpos, int nt, double2* o
     IFGF_CHECK_LAUNCH();
 }
 
+// One thread per node, the sample box's sources read through L1: at most
+// 10 samples of (order + 4)^3 nodes x leaf-size sources, once per estimate.
+template <int KIND>
+__global__ void __launch_bounds__(256) order_probe_kernel(ProbeArgs a)
+{
+    using P = Plugin<KIND>;
+    const int s = blockIdx.y;
+    const int n = a.node_off[s] + blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= a.node_off[s + 1])
+        return;
+    const double y[3] = {a.nodes[3 * n], a.nodes[3 * n + 1], a.nodes[3 * n + 2]};
+    const double* xc = a.centre + 3 * s;
+    const double e0 = y[0] - xc[0], e1 = y[1] - xc[1], e2 = y[2] - xc[2];
+    const double dc = sqrt(e0 * e0 + e1 * e1 + e2 * e2);
+    cplx<double> acc = {0.0, 0.0};
+    for (int i = a.src_off[s]; i < a.src_off[s + 1]; i++)
+    {
+        const double av[3] = {a.S.sx[i] - y[0], a.S.sy[i] - y[1], a.S.sz[i] - y[2]};
+        const double nv[3] = {P::needs_normals ? a.S.nx[i] : 0.0,
+                              P::needs_normals ? a.S.ny[i] : 0.0,
+                              P::needs_normals ? a.S.nz[i] : 0.0};
+        acc = cadd(acc, P::factored(av, nv, {1.0, 0.0}, y, dc, a.kp));
+    }
+    a.out[n] = make_double2(acc.re, acc.im);
+}
+
+template <int KIND>
+void launch_order_probe(const ProbeArgs& a, int n_samples, int max_nodes, cudaStream_t st)
+{
+    if (n_samples <= 0 || max_nodes <= 0)
+        return;
+    order_probe_kernel<KIND><<<dim3((max_nodes + 255) / 256, n_samples), 256, 0, st>>>(a);
+    IFGF_CHECK_LAUNCH();
+}
+
 #include "mult_batch.cuh"
 
 #define IFGF_INSTANTIATE_KIND(K)                                                              \
@@ -2327,6 +2362,7 @@ void launch_direct_kernel(const MultPtrs& m, const int* tpos, int nt, double2* o
                                               void*, bool, cudaStream_t, LaunchHooks*);        \
     template void launch_direct_kernel<K>(const MultPtrs&, const int*, int, double2*, cudaStream_t); \
     template void permute_only<K>(const MultPtrs&, const void*, bool, cudaStream_t);         \
+    template void launch_order_probe<K>(const ProbeArgs&, int, int, cudaStream_t);             \
     template void launch_build_upgeo<K>(const LevelGeom&, const LevelGeom&, double, double,   \
                                         const double*, const int*, int, const double*, int,     \
                                         KParams, int, UpGeo64*, UpGeo32*, int, int2*);          \

@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <complex>
 #include <cstring>
 #include <sstream>
 
@@ -370,6 +371,14 @@ void Operator::set_wavenumber(double k_re, double k_im)
             same = same && nf[d] == G.nf[d] && nc[d] == G.nc[d];
         same = same && smin == G.dmin[0];
     }
+    if (same && tol_ > 0)
+    {
+        // estimated orders follow the wavenumber: new orders need a new init
+        int est[3];
+        estimate_orders(est);
+        for (int d = 0; d < 3; d++)
+            same = same && est[d] == base_order_[d];
+    }
     adj_.reset();
     if (!same)
     {
@@ -513,6 +522,201 @@ double Operator::cutoff_limit(double H) const
 
 void Operator::orders(int step, int* o) const { order_for_box(step, o); }
 
+// Low (step 0) and high (step 1) orders from base_order_, within what the
+// kernels support.
+void Operator::set_orders()
+{
+    order_for_box(0, lo_);
+    order_for_box(1, hi_);
+    for (int i = 0; i < 3; i++)
+        if (lo_[i] < 1 || hi_[i] < 1)
+            throw Error(ERR_INVALID, "interpolation order too low for this kernel (the low-order "
+                                     "grid would have order < 1; use order >= 7)");
+    if (lo_[0] * lo_[1] * lo_[2] > 4096 || hi_[0] * hi_[1] * hi_[2] > 2048 || lo_[0] > 16 ||
+        lo_[1] > 16 || lo_[2] > 16)
+        throw Error(ERR_INVALID, "interpolation order too high");
+}
+
+// estimateRefinement / estimateRefinementOnBox with RefineP
+// (ifgfoperator.hpp:108-244).  Ten boxes spaced Nboxes/10 apart on the
+// deepest source level; in each, the order of a dimension grows by one while
+// the Chebyshev layer n - 3 of the order + 4 expansion of the box's factored
+// kernel (unit weights) on coarse cone 0 holds more than tol of the
+// coefficient norm, at most 10 times; the result is the component-wise
+// maximum over the boxes.  Kernel values come from order_probe_kernel (all
+// live samples in one launch per step); the transform and the norms are a
+// few thousand host operations per step.
+// The reference draws the cone as (n_elements * Random()) / SIZE_MAX in
+// size_t arithmetic, which is 0 for every draw (the product stays below
+// SIZE_MAX or wraps below it); its TBB reduction keeps only the last box of
+// each subrange it is handed, which equals the maximum over all ten boxes
+// when every subrange holds one box.
+void Operator::estimate_orders(int* out) const
+{
+    constexpr int SAMPLES = 10, MAX_R = 10, LAYERS = 3;
+    const Tree& S = plan_.src;
+    const TreeLevel& TL = S.levels[S.num_levels() - 1];
+    const int64_t stride = (int64_t)TL.size() / SAMPLES;
+    const bool need_n = kind_ == K_DOUBLELAYER || kind_ == K_COMBINEDFIELD;
+    if (need_n && normals_.size() != 3 * (size_t)S.n)
+        throw Error(ERR_INVALID, "this kernel needs source normals");
+    std::vector<double> sc[6];
+    std::vector<int> src_off(SAMPLES + 1, 0);
+    std::vector<double> centre(3 * SAMPLES);
+    double H[SAMPLES];
+    for (int i = 0; i < SAMPLES; i++)
+    {
+        const int64_t b = i * stride;
+        for (int d = 0; d < 3; d++)
+            centre[3 * i + d] = TL.center[3 * b + d];
+        H[i] = TL.sides[b];
+        for (int64_t j = TL.first[b]; j < TL.last[b]; j++)
+            for (int d = 0; d < 3; d++)
+            {
+                sc[d].push_back(S.pts[3 * j + d]);
+                sc[3 + d].push_back(need_n ? normals_[3 * S.perm[j] + d] : 0.0);
+            }
+        src_off[i + 1] = (int)sc[0].size();
+    }
+    DevBuf<double> d_sc[6], d_centre, d_nodes;
+    DevBuf<int> d_src_off, d_node_off;
+    DevBuf<double2> d_vals;
+    for (int d = 0; d < 6; d++)
+        d_sc[d].upload(sc[d].data(), sc[d].size());
+    d_centre.upload(centre.data(), centre.size());
+    d_src_off.upload(src_off.data(), src_off.size());
+
+    int base[SAMPLES][3] = {}, newp[SAMPLES][3], order[SAMPLES][3];
+    double err[SAMPLES][3];
+    bool live[SAMPLES];
+    for (int i = 0; i < SAMPLES; i++)
+    {
+        live[i] = true;
+        for (int d = 0; d < 3; d++)
+            err[i][d] = std::numeric_limits<double>::max();
+    }
+    for (;;)
+    {
+        std::vector<double> nodes;
+        std::vector<int> node_off(SAMPLES + 1, 0);
+        int max_nodes = 0;
+        for (int i = 0; i < SAMPLES; i++)
+        {
+            if (live[i])
+            {
+                for (int d = 0; d < 3; d++)
+                {
+                    newp[i][d] = order0_ + base[i][d];
+                    order[i][d] = newp[i][d] + LAYERS + 1; // orderForBox(step 1) is the identity
+                }
+                int64_t ne[3];
+                elements_for_box(H[i], 1, ne);
+                // interpolation box [cutoff_limit(H), sqrt(3)/3] x [0, pi] x [-pi, pi]; a
+                // reversed one gives unit element sizes (ConeDomain, cone_domain.hpp:72-83)
+                const double mn[3] = {cutoff_limit(H[i]), 0.0, -M_PI};
+                const double mx[3] = {std::sqrt(3.0) / 3, M_PI, M_PI};
+                const bool null_box = mn[0] > mx[0];
+                double a[3], b[3];
+                for (int d = 0; d < 3; d++)
+                {
+                    const double h = null_box ? 1.0 : (mx[d] - mn[d]) / (double)ne[d];
+                    a[d] = 0.5 * h;
+                    b[d] = mn[d] + 0.5 * h; // cone 0
+                }
+                std::vector<double> x[3];
+                for (int d = 0; d < 3; d++)
+                    for (int q = 0; q < order[i][d]; q++)
+                        x[d].push_back(std::cos((2. * q + 1.0) / (2. * order[i][d]) * M_PI));
+                for (int i2 = 0; i2 < order[i][2]; i2++)
+                    for (int i1 = 0; i1 < order[i][1]; i1++)
+                        for (int i0 = 0; i0 < order[i][0]; i0++)
+                        {
+                            const double s0 = x[0][i0] * a[0] + b[0], s1 = x[1][i1] * a[1] + b[1],
+                                         s2 = x[2][i2] * a[2] + b[2];
+                            const double r = H[i] / s0; // util.hpp:96-116
+                            nodes.push_back(centre[3 * i] + r * std::cos(s2) * std::sin(s1));
+                            nodes.push_back(centre[3 * i + 1] + r * std::sin(s2) * std::sin(s1));
+                            nodes.push_back(centre[3 * i + 2] + r * std::cos(s1));
+                        }
+            }
+            node_off[i + 1] = (int)(nodes.size() / 3);
+            max_nodes = std::max(max_nodes, node_off[i + 1] - node_off[i]);
+        }
+        if (max_nodes == 0)
+            break;
+        d_nodes.upload(nodes.data(), nodes.size());
+        d_node_off.upload(node_off.data(), node_off.size());
+        d_vals.alloc(nodes.size() / 3);
+        ProbeArgs pa;
+        pa.S = SrcArgs{d_sc[0].p, d_sc[1].p, d_sc[2].p, d_sc[3].p, d_sc[4].p, d_sc[5].p};
+        pa.src_off = d_src_off.p;
+        pa.nodes = d_nodes.p;
+        pa.node_off = d_node_off.p;
+        pa.centre = d_centre.p;
+        pa.kp = make_kparams(kr_, ki_, dx_);
+        pa.out = d_vals.p;
+        IFGF_DISPATCH(kind_, launch_order_probe<KK>(pa, SAMPLES, max_nodes, 0));
+        std::vector<double2> vals(nodes.size() / 3);
+        IFGF_CUDA(cudaMemcpy(vals.data(), d_vals.p, vals.size() * sizeof(double2),
+                             cudaMemcpyDeviceToHost));
+        for (int i = 0; i < SAMPLES; i++)
+        {
+            if (!live[i])
+                continue;
+            const int* n = order[i];
+            const size_t np = (size_t)n[0] * n[1] * n[2];
+            // chebtransform (chebinterp.hpp:176-250): one dimension at a time,
+            // c_k = (k ? 2 : 1) / n sum_j v_j cos(k pi (2 j + 1) / (2 n))
+            std::vector<std::complex<double>> c(np), t(np);
+            for (size_t q = 0; q < np; q++)
+                c[q] = {vals[node_off[i] + q].x, vals[node_off[i] + q].y};
+            size_t inner = 1;
+            for (int d = 0; d < 3; d++)
+            {
+                const int nd = n[d];
+                const size_t outer = np / (inner * nd);
+                for (size_t o = 0; o < outer; o++)
+                    for (size_t in = 0; in < inner; in++)
+                        for (int k = 0; k < nd; k++)
+                        {
+                            std::complex<double> acc = 0;
+                            for (int j = 0; j < nd; j++)
+                                acc += c[(o * nd + j) * inner + in] *
+                                       std::cos(k * M_PI * (2. * j + 1) / (2. * nd));
+                            t[(o * nd + k) * inner + in] = acc * ((k ? 2.0 : 1.0) / nd);
+                        }
+                std::swap(c, t);
+                inner *= nd;
+            }
+            // Util::compute_slice_norm (util.hpp:214-234)
+            double v1 = 0, v2[3] = {0, 0, 0};
+            for (size_t q = 0; q < np; q++)
+            {
+                const double m2 = std::norm(c[q]);
+                v1 += m2;
+                const size_t id[3] = {q % n[0], (q / n[0]) % n[1], q / ((size_t)n[0] * n[1])};
+                for (int d = 0; d < 3; d++)
+                    if ((int)id[d] == n[d] - LAYERS)
+                        v2[d] += m2;
+            }
+            for (int d = 0; d < 3; d++)
+            {
+                err[i][d] = std::sqrt(v2[d]) / std::max(1., std::sqrt(v1));
+                if (err[i][d] > tol_)
+                    base[i][d] += 1;
+            }
+            live[i] = std::max(err[i][0], std::max(err[i][1], err[i][2])) > tol_ &&
+                      std::max(base[i][0], std::max(base[i][1], base[i][2])) < MAX_R;
+        }
+    }
+    for (int d = 0; d < 3; d++)
+    {
+        out[d] = 0;
+        for (int i = 0; i < SAMPLES; i++)
+            out[d] = std::max(out[d], newp[i][d]);
+    }
+}
+
 void Operator::init(const double* srcs, int64_t ns, const double* tgts, int64_t nt,
                     const double* normals, const std::function<bool(double)>& cutoff,
                     bool plan_only)
@@ -536,18 +740,16 @@ void Operator::init(const double* srcs, int64_t ns, const double* tgts, int64_t 
         for (int64_t i = 0; i < 3 * ns; i++)
             if (!std::isfinite(normals[i]))
                 throw Error(ERR_INVALID, "non-finite normal");
-    // radial order reset of ifgfoperator.hpp:90 (fixed-order path), taken from
-    // the constructor's order so that a repeated init does not compound it
+    if (tol_ > 0 && plan_only)
+        throw Error(ERR_INVALID, "order estimation (tol > 0) samples the kernel on the GPU; a "
+                                 "plan-only init needs tol <= 0");
+    // fixed-order path: radial order reset of ifgfoperator.hpp:90, taken from
+    // the constructor's order so that a repeated init does not compound it;
+    // with tol > 0 the orders are estimated once the source octree exists
     base_order_[0] = std::max(order0_ - 3, 2);
-    order_for_box(0, lo_);
-    order_for_box(1, hi_);
-    for (int i = 0; i < 3; i++)
-        if (lo_[i] < 1 || hi_[i] < 1)
-            throw Error(ERR_INVALID, "interpolation order too low for this kernel (the low-order "
-                                     "grid would have order < 1; use order >= 7)");
-    if (lo_[0] * lo_[1] * lo_[2] > 4096 || hi_[0] * hi_[1] * hi_[2] > 2048 || lo_[0] > 16 ||
-        lo_[1] > 16 || lo_[2] > 16)
-        throw Error(ERR_INVALID, "interpolation order too high");
+    base_order_[1] = base_order_[2] = order0_;
+    if (tol_ <= 0)
+        set_orders();
 
     adj_.reset();
     src_pts_.assign(srcs, srcs + 3 * ns);
@@ -582,6 +784,11 @@ void Operator::init(const double* srcs, int64_t ns, const double* tgts, int64_t 
                     .count();
     plan_.assign_shards(shard_n_);
     plan_.build_target_lists(shard_n_ > 1 ? shard_rank_ : -1);
+    if (tol_ > 0) // ifgfoperator.hpp:80-85
+    {
+        estimate_orders(base_order_);
+        set_orders();
+    }
 
     const int L = plan_.src.num_levels();
     if (L > MAX_LEVELS)

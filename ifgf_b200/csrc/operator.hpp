@@ -105,6 +105,8 @@ class Operator
     void order_for_box(int step, int* out) const;
     void elements_for_box(double H, int step, int64_t* out) const;
     double cutoff_limit(double H) const;
+    void set_orders();
+    void estimate_orders(int* out) const;
     void setup_device(const double* normals);
     // vkind >= 0: run that kernel with the variant geometry tables
     void launch_mult(const void* d_w, void* d_u, void* stream, bool timed, int vkind = -1);

@@ -54,9 +54,12 @@ typedef struct ifgf_operator ifgf_operator;
  * combined_field_helmholtz_ifgf.hpp:13-20) as bound at py_ifgf.cpp:19, :46.
  * k = k_re + i k_im is the wavenumber (ignored by Laplace; the imaginary part
  * is ignored by the real-wavenumber Helmholtz and combined-field kernels).
- * tol <= 0 selects the fixed-order path (ifgfoperator.hpp:88-91); tol > 0 is
- * accepted and, as in the reference, only changes the gradient kernel's
- * cutoff (grad_helmholtz_ifgf.hpp:294-304) -- order estimation is not run. */
+ * tol <= 0 selects the fixed orders (max(order - 3, 2), order, order)
+ * (ifgfoperator.hpp:88-91).  tol > 0 makes ifgf_init estimate the orders
+ * (estimateRefinement, ifgfoperator.hpp:80-85, 108-244: ten boxes of the
+ * deepest source level, kernel samples on the GPU) and also sets the gradient
+ * kernel's cutoff (grad_helmholtz_ifgf.hpp:294-304); ifgf_orders reports
+ * the result.  A plan-only init refuses tol > 0. */
 int ifgf_create(int kind, double k_re, double k_im, long leaf_size, long order, long n_elem,
                 double tol, ifgf_operator** out);
 

@@ -1076,8 +1076,106 @@ struct Operator
         }
         n_src = ns;
         n_tgt = nt;
-        base_order[0] = std::max(base_order[0] - 3, 2); // ifgfoperator.hpp:90
+        if (K.tol > 0) // ifgfoperator.hpp:80-85
+            estimate_orders(K.tol, base_order);
+        else
+            base_order[0] = std::max(base_order[0] - 3, 2); // ifgfoperator.hpp:90
         interpolation_range();
+    }
+
+    // estimateRefinementOnBox with RefineP (ifgfoperator.hpp:152-244): raise
+    // the order of each dimension whose Chebyshev layer n-3 of the order+4
+    // expansion of the box's factored kernel (unit weights) on coarse cone 0
+    // still carries more than tol of the coefficient norm; at most 10 steps.
+    // The reference draws the cone as (n_elements * Random()) / SIZE_MAX in
+    // size_t arithmetic, which is 0 for every draw (the product is below
+    // SIZE_MAX, or wraps below it), so cone 0 is restated directly.
+    void estimate_on_box(double tol, int level, long id, int* out) const
+    {
+        const int max_r = 10, layers = 3;
+        const Node& nd = src.nodes[level][id];
+        const double H = nd.bbox.side;
+        const size_t s0 = nd.rng.first, nS = nd.rng.second - nd.rng.first;
+        Box ib;
+        ib.mn[0] = K.cutoff_limit(H);
+        ib.mx[0] = std::sqrt(3.0) / 3;
+        ib.mn[1] = 0;
+        ib.mx[1] = PI;
+        ib.mn[2] = -PI;
+        ib.mx[2] = PI;
+        int base[3] = {0, 0, 0}, new_p[3] = {base_order[0], base_order[1], base_order[2]};
+        double err[3];
+        std::fill(err, err + 3, std::numeric_limits<double>::max());
+        const std::vector<cd> w(nS, cd(1.0));
+        auto max3 = [](const auto* v) { return std::max(v[0], std::max(v[1], v[2])); };
+        while (max3(err) > tol && max3(base) < max_r)
+        {
+            int wide[3], order[3];
+            for (int d = 0; d < 3; d++)
+            {
+                new_p[d] = base_order[d] + base[d];
+                wide[d] = new_p[d] + layers + 1;
+            }
+            K.order_for_box(wide, 1, order);
+            long ne[3];
+            K.elements_for_box(H, base_n, 1, ne);
+            const ConeDomain grid(ne, ib);
+            const auto nodes = cheb_nodes_3d(order);
+            const size_t np = nodes.size() / 3;
+            std::vector<cd> vals(np), coef(np);
+            double loc[3], y[3];
+            for (size_t i = 0; i < np; i++)
+            {
+                grid.transform(0, &nodes[3 * i], loc);
+                interp_to_cart(loc, nd.bbox.c, H, y);
+                vals[i] = K.factored(&src.pts[3 * s0],
+                                     normals.empty() ? nullptr : &normals[3 * s0], w.data(), nS,
+                                     y, nd.bbox.c);
+            }
+            chebtransform<cd>(vals.data(), coef.data(), order, 3);
+            for (int d = 0; d < 3; d++) // Util::compute_slice_norm (util.hpp:214-234)
+            {
+                double v1 = 0, v2 = 0;
+                for (size_t i = 0; i < np; i++)
+                {
+                    size_t r = i;
+                    for (int e = 0; e < d; e++)
+                        r /= (size_t)order[e];
+                    const double n2 = std::norm(coef[i]);
+                    v1 += n2;
+                    if ((int)(r % (size_t)order[d]) == order[d] - layers)
+                        v2 += n2;
+                }
+                err[d] = std::sqrt(v2) / std::max(1., std::sqrt(v1));
+            }
+            for (int d = 0; d < 3; d++)
+                if (err[d] > tol)
+                    base[d] += 1;
+        }
+        for (int d = 0; d < 3; d++)
+            out[d] = new_p[d];
+    }
+
+    // estimateRefinement (ifgfoperator.hpp:108-150): the component-wise
+    // maximum over 10 boxes spaced Nboxes/10 apart on the deepest level.
+    // (The reference's TBB reduction keeps only the last box of each
+    // subrange it is handed, so its result depends on the partitioning; the
+    // restatement takes the maximum over all ten, which is what it computes
+    // when every subrange holds one box.)
+    void estimate_orders(double tol, int* out) const
+    {
+        const int level = src.levels() - 1;
+        const long stride = (long)src.num_boxes(level) / 10;
+        int best[3] = {0, 0, 0};
+        for (long i = 0; i < 10; i++)
+        {
+            int p[3];
+            estimate_on_box(tol, level, i * stride, p);
+            for (int d = 0; d < 3; d++)
+                best[d] = std::max(best[d], p[d]);
+        }
+        for (int d = 0; d < 3; d++)
+            out[d] = best[d];
     }
 
     // Octree::calculateInterpolationRange (octree.hpp:351-816), TwoGrid mode
