@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--order", type=int, default=9)
     ap.add_argument("--leaf", type=int, default=100)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-freq-set", action="store_true",
+                    help="skip the convolution-quadrature frequency-set measurement")
     ap.add_argument("--batch", type=int, default=8,
                     help="right-hand sides per step of the mixed pipeline (1: single matvec)")
     ap.add_argument("--sample-boxes", type=int, default=0,
@@ -270,6 +272,96 @@ def run_reference(a):
     print(json.dumps(line), flush=True)
 
 
+def frequency_set(a, dev):
+    """Convolution-quadrature frequency set on one GPU: N = 1e5 points on the
+    unit sphere, the modified Helmholtz kernel e^{-s r}/(4 pi r) at the 64
+    wavenumbers s_l = (1 - 0.5 z_l)/dt, z_l = 0.9 e^{2 pi i l / 64}, dt = 0.01,
+    one density each (leaf 100, order 8), and 16 right-hand sides of the
+    Helmholtz kernel at k = 20 (leaf 100, order 9), in mixed precision.  The 64 wavenumbers run as
+    one multi-wavenumber batch and, for comparison, as the per-frequency loop
+    of set_wavenumber + matvec; errors against the FP64 direct sum at 1000
+    sampled targets."""
+    import torch
+
+    import ifgf_b200 as G
+
+    n, L, R = 100_000, 64, 16
+    pts = W.sphere_points(n, seed=0)
+    ks = (1.0 - 0.5 * 0.9 * np.exp(2j * np.pi * np.arange(L) / L)) / 0.01
+    wl = np.stack([W.densities(n, seed=10 + l) for l in range(L)])
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+
+    def timed(fn, steps):
+        for _ in range(a.warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    op = G.ModifiedHelmholtzIfgfOperator(ks[0], 100, 8)
+    op.init(pts, pts)
+    op.set_precision("mixed")
+    dW = torch.from_numpy(wl).to(dev)
+    dU = torch.empty_like(dW)
+    dU2 = torch.empty_like(dW)
+    nb = n * 16  # bytes per complex128 plane
+
+    def one_pass():
+        op.mult_wavenumbers_device(ks, dW.data_ptr(), dU.data_ptr(), sp)
+
+    ms_pass = timed(one_pass, a.steps)
+    launches = op.stats()["launches_per_mult"]
+
+    def per_frequency():
+        for l in range(L):
+            op.set_wavenumber(ks[l])
+            op.mult_device(dW.data_ptr() + l * nb, dU2.data_ptr() + l * nb, sp)
+
+    ms_loop = timed(per_frequency, 1)
+    one_pass()
+    torch.cuda.synchronize()
+    u, u2 = dU.cpu().numpy(), dU2.cpu().numpy()
+    idx = W.sample_targets(n, 1000, seed=2)
+    errs = []
+    for l in range(0, L, 4):
+        op.set_wavenumber(ks[l])
+        d = op.direct_eval(wl[l], idx)
+        errs.append(float(np.linalg.norm(u[l][idx] - d) / np.linalg.norm(d)))
+    loop_vs_pass = max(float(np.linalg.norm(u[l] - u2[l]) / np.linalg.norm(u2[l]))
+                       for l in range(L))
+
+    oph = G.HelmholtzIfgfOperator(20.0, 100, 9)
+    oph.init(pts, pts)
+    oph.set_precision("mixed")
+    wr = np.stack([W.densities(n, seed=200 + r) for r in range(R)])
+    dWr = torch.from_numpy(wr).to(dev)
+    dUr = torch.empty_like(dWr)
+    ms_rhs = timed(lambda: oph.mult_batch_device(dWr.data_ptr(), dUr.data_ptr(), R, sp), a.steps)
+    torch.cuda.synchronize()
+    d = oph.direct_eval(wr[0], idx)
+    err_h = float(np.linalg.norm(dUr[0].cpu().numpy()[idx] - d) / np.linalg.norm(d))
+    return {
+        "workload": "modified Helmholtz CQ set, 64 wavenumbers s_l = (1 - 0.45 e^{2 pi i l/64})"
+                    "/0.01, N=100000 unit sphere, (order 8) + 16 Helmholtz k=20 right-hand "
+                    "sides (order 9); leaf 100, mixed",
+        "ms_64_wavenumbers_one_batch": ms_pass,
+        "launches_per_batch": launches,
+        "ms_64_wavenumbers_set_wavenumber_loop": ms_loop,
+        "speedup_batch_vs_loop": ms_loop / ms_pass,
+        "max_rel_err_vs_fp64_direct_every_4th": max(errs),
+        "max_rel_diff_batch_vs_loop": loop_vs_pass,
+        "ms_16_rhs_helmholtz_k20_one_batch": ms_rhs,
+        "rel_err_helmholtz_k20_rhs0": err_h,
+        "ms_all_80": ms_pass + ms_rhs,
+    }
+
+
 def run_ours(a):
     import torch
 
@@ -431,7 +523,9 @@ def run_ours(a):
     breakdown["serialised_total"] = sum(breakdown.values())
     per_level = {k: [round(x / max(prof["mults"], 1), 3) for x in v["level_ms"]]
                  for k, v in kernels.items() if any(v.get("level_ms", []))}
-    groups = -(-batch // 4) if batch > 1 else 1
+    # passes per step: one launch sequence covers up to batch_planes
+    # right-hand sides
+    passes = -(-batch // max(stats.get("batch_planes", 4), 1)) if batch > 1 else 1
 
     cfg = workload_config(a, precision)
     cfg["batch"] = batch
@@ -447,7 +541,7 @@ def run_ours(a):
         "rel_err_vs_fp64_direct": err, "tol": TOL, "meets_tol": err <= TOL,
         "fp64_pipeline": fp64,
         "init_ms": init_ms, "kernel_ms_per_matvec": breakdown, "kernel_ms_per_level": per_level,
-        "gpu_launches": int(stats["launches_per_mult"] * groups * a.steps),
+        "gpu_launches": int(stats["launches_per_mult"] * passes * a.steps),
         "e2e": {"value": e2e_ms, "unit": UNIT, "h2d_bytes_per_step": int(wb.nbytes),
                 "d2h_bytes_per_step": int(wb.nbytes), "note": "ms per matvec"},
         "roofline": roof, "clocks": clk,
@@ -456,6 +550,8 @@ def run_ours(a):
                                        "coarse_cones_total", "fine_cones_total",
                                        "upward_runs_max", "upward_levels")},
     }
+    if ws == 1 and not a.no_freq_set:
+        line["frequency_set"] = frequency_set(a, dev)
     if rank == 0 and ws == 1 and not a.no_cpu_baseline:
         opc, boxes, scale, threads, init_s, rec, nb = cpu_sample_setup(a, pts, w)
         v = cpu_sample_ms(opc, boxes, w, threads) * scale

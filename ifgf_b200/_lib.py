@@ -58,6 +58,8 @@ def _load():
         "ifgf_mult_device": [H, C.c_void_p, C.c_void_p, C.c_void_p],
         "ifgf_mult_batch_device": [H, C.c_void_p, C.c_void_p, C.c_long, C.c_void_p],
         "ifgf_mult_device_noalloc": [H, C.c_void_p, C.c_void_p, C.c_void_p],
+        "ifgf_mult_wavenumbers": [H, _dp, C.c_long, C.c_void_p, C.c_void_p],
+        "ifgf_mult_wavenumbers_device": [H, _dp, C.c_long, C.c_void_p, C.c_void_p, C.c_void_p],
         "ifgf_direct_eval": [H, C.c_void_p, _lp, C.c_long, C.c_void_p],
         "ifgf_direct_eval_dk": [H, C.c_void_p, _lp, C.c_long, C.c_void_p],
         "ifgf_mult_dk": [H, C.c_void_p, C.c_void_p, C.c_long],
@@ -95,6 +97,7 @@ EXPORTED = [
     "ifgf_init", "ifgf_init_plan_only",
     "ifgf_box_list", "ifgf_mult",
     "ifgf_mult_batch", "ifgf_mult_batch_device", "ifgf_mult_device", "ifgf_mult_device_noalloc",
+    "ifgf_mult_wavenumbers", "ifgf_mult_wavenumbers_device",
     "ifgf_direct_eval",
     "ifgf_mult_dk", "ifgf_mult_dk_device", "ifgf_direct_eval_dk", "ifgf_mult_adjoint",
     "ifgf_mult_adjoint_device",

@@ -163,6 +163,22 @@ extern "C"
         return guarded([&] { h->op.mult_batch_device(d_w, d_u, batch, stream); });
     }
 
+    int ifgf_mult_wavenumbers(ifgf_operator* h, const double* k, long n_k, const void* w,
+                              void* u)
+    {
+        if (!h)
+            return null_handle();
+        return guarded([&] { h->op.mult_wavenumbers_host(k, n_k, w, u); });
+    }
+
+    int ifgf_mult_wavenumbers_device(ifgf_operator* h, const double* k, long n_k,
+                                     const void* d_w, void* d_u, void* stream)
+    {
+        if (!h)
+            return null_handle();
+        return guarded([&] { h->op.mult_wavenumbers_device(k, n_k, d_w, d_u, stream); });
+    }
+
     int ifgf_mult_device(ifgf_operator* h, const void* d_w, void* d_u, void* stream)
     {
         if (!h)

@@ -874,6 +874,21 @@ __device__ __forceinline__ cplx<float> transfer_mixed(double d2, double dp2, con
     return {e.re * ratio, e.im * ratio};
 }
 
+// The same factor from a tabulated delta = d - d_parent (FP64 difference
+// rounded to FP32) and ratio = d_parent / d: the distance tables of
+// multi-wavenumber batches, which serve every wavenumber of the batch.
+template <int KIND>
+__device__ __forceinline__ cplx<float> transfer_delta(float delta, float ratio, const KParams& p)
+{
+    if (KIND == K_HELMHOLTZ_DK || KIND == K_COMBINEDFIELD_DK)
+        return exp_ik_ff(p, delta);
+    if (KIND == K_LAPLACE)
+        return {ratio, 0.f};
+    const cplx<float> e = (KIND == K_HELMHOLTZ || KIND == K_COMBINEDFIELD) ? exp_ik_ff(p, delta)
+                                                                          : exp_mk_ff(p, delta);
+    return {e.re * ratio, e.im * ratio};
+}
+
 // FP32 coordinates: (s, theta, phi) from an FP32 difference vector
 __device__ __forceinline__ void cart_to_interp_f(float p0, float p1, float p2, float H, float* s)
 {

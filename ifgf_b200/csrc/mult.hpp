@@ -81,7 +81,8 @@ struct LevelLists
 // *runs_max; launch_build_upgeo fills tables pre-set to all-ones bytes
 // (skipped entries) and the per-row element lists (fe_pad entries a row,
 // pre-set to -1).  slot_el: element id of each slot; off: 8 child-centre
-// offsets.
+// offsets.  With g64 null it fills g32 as a distance table (tr = d - d_parent,
+// ti = d_parent / d) for multi-wavenumber batches.
 template <int KIND>
 int upgeo_row_max(const LevelGeom& PG, const LevelGeom& CG, double pH, double cH,
                   const double* off_dev, const int* slot_el, int n_slots, const double* hi_nodes,
@@ -157,24 +158,33 @@ template <int KIND>
 int launch_mult_kernels(const MultPtrs& m, const void* d_w, void* d_u, bool real, cudaStream_t st,
                         LaunchHooks* hooks);
 
-// Planes of the batched mixed matvec (mult_batch.cuh): right-hand side b of
-// a group lives at offset b * plane of each buffer.
+// Planes of the batched mixed matvec (mult_batch.cuh): a launch covers
+// `groups` groups of BATCH_NB planes; plane p (group p / BATCH_NB) lives at
+// offset p * plane of each buffer.
 constexpr int BATCH_NB = 4;
 struct BatchPtrs
 {
-    float2* w;      // BATCH_NB planes of n_src permuted densities
-    float2* cvals;  // BATCH_NB planes of cv_plane coarse values
-    float2* fcoef;  // BATCH_NB planes of fc_plane fine coefficients
-    double2* unear; // BATCH_NB planes of n_tgt near-field sums
+    float2* w;      // planes of n_src permuted densities
+    float2* cvals;  // planes of cv_plane coarse values
+    float2* fcoef;  // planes of fc_plane fine coefficients
+    double2* unear; // planes of n_tgt near-field sums
     long long cv_plane, fc_plane;
     long long n_src, n_tgt;
     int nrhs;                      // planes holding right-hand sides (the rest are zero)
+    int groups = 1;                // plane groups in one launch (nrhs <= groups * BATCH_NB)
     long long in_plane, out_plane; // caller's density / result strides (in doubles)
+    // wavenumber of every plane (device, groups * BATCH_NB entries), or null
+    // when all planes share the operator's; with it the upward transfer reads
+    // the distance tables (UpGeo32::tr = d - d_parent, ::ti = d_parent / d)
+    const KParams* kp_plane = nullptr;
+    const UpGeo32* const* dgeo32 = nullptr; // per level (host array)
 };
 
-// Enqueues the mixed matvec of bp.nrhs <= BATCH_NB right-hand sides sharing
-// the kernel and geometry work; returns the kernels launched, or -1 when the
-// operator's orders or upward rows have no batched path.
+// Enqueues the mixed matvec of bp.nrhs <= bp.groups * BATCH_NB right-hand
+// sides, one launch per stage and level for all of them; planes of a group
+// share the kernel and geometry work (with kp_plane: the geometry only).
+// Returns the kernels launched, or -1 when the operator's orders or upward
+// rows have no batched path.
 template <int KIND>
 int launch_mult_batch_kernels(const MultPtrs& m, const BatchPtrs& bp, const void* d_w, void* d_u,
                               bool real, cudaStream_t st, LaunchHooks* hooks);

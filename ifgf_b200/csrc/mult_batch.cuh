@@ -1,11 +1,16 @@
 // Mixed-precision matvec of several right-hand sides at once (included by
-// mult_kernels.cuh).  BATCH_NB densities share every geometry- and
-// kernel-dependent quantity of the pipeline -- the factored-kernel values at
-// the cone nodes, the near-field kernel values, the far-field cone lookups and
-// centred factors -- and keep their own interpolant planes: buffers hold
-// BATCH_NB planes (right-hand side b at offset b * plane).  The upward
-// transfer and the coarse-to-fine step run the single-right-hand-side kernels
-// with blockIdx.y selecting the plane.
+// mult_kernels.cuh).  The BATCH_NB densities of a plane group share every
+// geometry- and kernel-dependent quantity of the pipeline -- the
+// factored-kernel values at the cone nodes, the near-field kernel values, the
+// far-field cone lookups and centred factors -- and keep their own
+// interpolant planes (plane p at offset p * plane of each buffer).  One
+// launch per stage and level covers all groups (a grid dimension selects the
+// group).  The upward transfer and the coarse-to-fine step run the
+// single-right-hand-side kernels with blockIdx.y selecting the plane.
+// Multi-wavenumber batches (MK): every plane has its own wavenumber
+// (BatchPtrs::kp_plane); the planes then share the geometry only -- node and
+// source positions, cone lookups, Chebyshev bases -- and evaluate their
+// kernel values, centred and centre-shift factors each.
 // Included inside namespace ifgf, after the single-right-hand-side kernels.
 #pragma once
 
@@ -37,15 +42,21 @@ static __global__ void permute_batch_kernel(const double* __restrict__ in, int r
     }
 }
 
-// Leaf sampling of BATCH_NB right-hand sides: the factored kernel at a
+// Leaf sampling of a plane group (blockIdx.z): the factored kernel at a
 // (node, source) pair is evaluated once with unit density and applied to
-// every plane's density (the kernels are linear in the density).
-template <int KIND>
+// every plane's density (the kernels are linear in the density); with MK once
+// per plane, at its wavenumber.
+template <int KIND, bool MK>
 __global__ void __launch_bounds__(NODE_THREADS) leaf_sample_batch_kernel(LeafArgs a, BatchPtrs bp)
 {
     using P = PluginF<KIND>;
     constexpr int NB = BATCH_NB;
     extern __shared__ float smb[];
+    __shared__ KParams kps[MK ? NB : 1];
+    const int pb = blockIdx.z * NB; // first plane of the group
+    if constexpr (MK)
+        if (threadIdx.x < NB)
+            kps[threadIdx.x] = bp.kp_plane[pb + threadIdx.x]; // read after the chunk barriers
     const int c = a.idx[blockIdx.x];
     const int node0 = blockIdx.y * NPT * blockDim.x;
     const int box = a.cc_box[c], el = a.cc_el[c];
@@ -97,7 +108,7 @@ __global__ void __launch_bounds__(NODE_THREADS) leaf_sample_batch_kernel(LeafArg
             aa[threadIdx.x] = (float)(a0 * a0 + a1 * a1 + a2 * a2);
 #pragma unroll
             for (int r = 0; r < NB; r++)
-                wv[r * nt + threadIdx.x] = bp.w[(size_t)r * bp.n_src + i];
+                wv[r * nt + threadIdx.x] = bp.w[(size_t)(pb + r) * bp.n_src + i];
             if (P::needs_normals)
             {
                 n0[threadIdx.x] = (float)a.S.nx[i];
@@ -116,13 +127,29 @@ __global__ void __launch_bounds__(NODE_THREADS) leaf_sample_batch_kernel(LeafArg
                 const float av[3] = {ax[i], ay[i], az[i]};
                 const float nv[3] = {P::needs_normals ? n0[i] : 0.f, P::needs_normals ? n1[i] : 0.f,
                                      P::needs_normals ? n2[i] : 0.f};
-                const cplx<float> v = P::factored(av, aa[i], b[q], nv, {1.f, 0.f}, dc[q], a.kp);
-#pragma unroll
-                for (int r = 0; r < NB; r++)
+                if constexpr (MK)
                 {
-                    const float2 wr = wv[r * nt + i];
-                    acc[q][r].re = fmaf(wr.x, v.re, fmaf(-wr.y, v.im, acc[q][r].re));
-                    acc[q][r].im = fmaf(wr.x, v.im, fmaf(wr.y, v.re, acc[q][r].im));
+#pragma unroll
+                    for (int r = 0; r < NB; r++)
+                    {
+                        const cplx<float> v =
+                            P::factored(av, aa[i], b[q], nv, {1.f, 0.f}, dc[q], kps[r]);
+                        const float2 wr = wv[r * nt + i];
+                        acc[q][r].re = fmaf(wr.x, v.re, fmaf(-wr.y, v.im, acc[q][r].re));
+                        acc[q][r].im = fmaf(wr.x, v.im, fmaf(wr.y, v.re, acc[q][r].im));
+                    }
+                }
+                else
+                {
+                    const cplx<float> v =
+                        P::factored(av, aa[i], b[q], nv, {1.f, 0.f}, dc[q], a.kp);
+#pragma unroll
+                    for (int r = 0; r < NB; r++)
+                    {
+                        const float2 wr = wv[r * nt + i];
+                        acc[q][r].re = fmaf(wr.x, v.re, fmaf(-wr.y, v.im, acc[q][r].re));
+                        acc[q][r].im = fmaf(wr.x, v.im, fmaf(wr.y, v.re, acc[q][r].im));
+                    }
                 }
             }
         }
@@ -134,19 +161,25 @@ __global__ void __launch_bounds__(NODE_THREADS) leaf_sample_batch_kernel(LeafArg
         if (n < a.P_hi)
 #pragma unroll
             for (int r = 0; r < NB; r++)
-                bp.cvals[(size_t)r * bp.cv_plane + (size_t)c * a.P_hi + n] =
+                bp.cvals[(size_t)(pb + r) * bp.cv_plane + (size_t)c * a.P_hi + n] =
                     make_float2(acc[q][r].re, acc[q][r].im);
     }
 }
 
-// Near field of BATCH_NB right-hand sides: one kernel value per (target,
-// source) pair, applied to every plane; FP32 per source chunk, FP64 across
-// chunks and threads, written to the near-sum planes.
-template <int KIND>
+// Near field of a plane group (blockIdx.y): one kernel value per (target,
+// source) pair, applied to every plane (with MK one per plane); FP32 per
+// source chunk, FP64 across chunks and threads, written to the near-sum
+// planes.
+template <int KIND, bool MK>
 __global__ void __launch_bounds__(EVAL_THREADS) near_batch_kernel(EvalArgs a, BatchPtrs bp)
 {
     using P = PluginF<KIND>;
     constexpr int NB = BATCH_NB;
+    __shared__ KParams kps[MK ? NB : 1];
+    const int pb = blockIdx.y * NB;
+    if constexpr (MK)
+        if (threadIdx.x < NB)
+            kps[threadIdx.x] = bp.kp_plane[pb + threadIdx.x]; // read after the chunk barriers
     using CT = typename std::conditional<P::needs_normals, double, float>::type;
     __shared__ CT xs[EVAL_THREADS], ys[EVAL_THREADS], zs[EVAL_THREADS];
     __shared__ float2 ws[NB][EVAL_THREADS];
@@ -187,7 +220,7 @@ __global__ void __launch_bounds__(EVAL_THREADS) near_batch_kernel(EvalArgs a, Ba
                     zs[threadIdx.x] = (CT)(a.S.sz[i] - r2);
 #pragma unroll
                     for (int r = 0; r < NB; r++)
-                        ws[r][threadIdx.x] = bp.w[(size_t)r * nsrc + i];
+                        ws[r][threadIdx.x] = bp.w[(size_t)(pb + r) * nsrc + i];
                     if (P::needs_normals)
                     {
                         n0[threadIdx.x] = a.S.nx[i];
@@ -204,22 +237,44 @@ __global__ void __launch_bounds__(EVAL_THREADS) near_batch_kernel(EvalArgs a, Ba
                     acc[r] = {0.f, 0.f};
                 for (int i = si; i < ccnt; i += S)
                 {
-                    cplx<float> kv;
                     if constexpr (P::needs_normals)
                     {
                         const double yd0 = y0 - r0, yd1 = y1 - r1, yd2 = y2 - r2;
                         const double x[3] = {xs[i] - yd0, ys[i] - yd1, zs[i] - yd2};
                         const double nv[3] = {n0[i], n1[i], n2[i]};
-                        kv = P::kernel_d(x, nv, a.kp);
+                        if constexpr (MK)
+                        {
+#pragma unroll
+                            for (int r = 0; r < NB; r++)
+                                cfmaf(acc[r], cplx<float>{ws[r][i].x, ws[r][i].y},
+                                      P::kernel_d(x, nv, kps[r]));
+                        }
+                        else
+                        {
+                            const cplx<float> kv = P::kernel_d(x, nv, a.kp);
+#pragma unroll
+                            for (int r = 0; r < NB; r++)
+                                cfmaf(acc[r], cplx<float>{ws[r][i].x, ws[r][i].y}, kv);
+                        }
                     }
                     else
                     {
                         const float x[3] = {xs[i] - yl0, ys[i] - yl1, zs[i] - yl2};
-                        kv = P::kernel(x, nullptr, a.kp);
-                    }
+                        if constexpr (MK)
+                        {
 #pragma unroll
-                    for (int r = 0; r < NB; r++)
-                        cfmaf(acc[r], cplx<float>{ws[r][i].x, ws[r][i].y}, kv);
+                            for (int r = 0; r < NB; r++)
+                                cfmaf(acc[r], cplx<float>{ws[r][i].x, ws[r][i].y},
+                                      P::kernel(x, nullptr, kps[r]));
+                        }
+                        else
+                        {
+                            const cplx<float> kv = P::kernel(x, nullptr, a.kp);
+#pragma unroll
+                            for (int r = 0; r < NB; r++)
+                                cfmaf(acc[r], cplx<float>{ws[r][i].x, ws[r][i].y}, kv);
+                        }
+                    }
                 }
 #pragma unroll
                 for (int r = 0; r < NB; r++)
@@ -248,20 +303,25 @@ __global__ void __launch_bounds__(EVAL_THREADS) near_batch_kernel(EvalArgs a, Ba
                     sr += rr[r][ti + s * cnt];
                     sim += ri[r][ti + s * cnt];
                 }
-                bp.unear[(size_t)r * bp.n_tgt + t] = make_double2(sr, sim);
+                bp.unear[(size_t)(pb + r) * bp.n_tgt + t] = make_double2(sr, sim);
             }
         }
     }
 }
 
-// Far field of BATCH_NB right-hand sides: the cone lookup and the centred
-// factor of a (target, far box) pair are computed once; each plane's
-// Chebyshev sum uses its own coefficient block.  Adds the near sums and
-// writes the caller's result planes (the first nrhs).
-template <int KIND, int N0, int N1, int N2>
+// Far field of a plane group (blockIdx.y): the cone lookup and the centred
+// factor of a (target, far box) pair are computed once (with MK the factor
+// once per plane); each plane's Chebyshev sum uses its own coefficient block.
+// Adds the near sums and writes the caller's result planes (the first nrhs).
+template <int KIND, int N0, int N1, int N2, bool MK>
 __global__ void __launch_bounds__(EVAL_THREADS, 4) far_batch_kernel(EvalArgs a, BatchPtrs bp)
 {
     constexpr int NB = BATCH_NB;
+    __shared__ KParams kps[MK ? NB : 1];
+    const int pb = blockIdx.y * NB;
+    if constexpr (MK)
+        if (threadIdx.x < NB)
+            kps[threadIdx.x] = bp.kp_plane[pb + threadIdx.x]; // read after the chunk barriers
     __shared__ double fcx[EVAL_THREADS], fcy[EVAL_THREADS], fcz[EVAL_THREADS], fH[EVAL_THREADS];
     __shared__ long long ffm[EVAL_THREADS];
     __shared__ int flev[EVAL_THREADS];
@@ -313,13 +373,17 @@ __global__ void __launch_bounds__(EVAL_THREADS, 4) far_batch_kernel(EvalArgs a, 
                     fine_lookup_fast(lfs[lev], a.lv[lev], a.fmap + ffm[i], p, fH[i], loc, a.err);
                 if (gf < 0)
                     continue;
-                const cplx<float> cf =
-                    cf_mixed<KIND>(p[0] * p[0] + p[1] * p[1] + p[2] * p[2], a.kp);
+                const double d2 = p[0] * p[0] + p[1] * p[1] + p[2] * p[2];
+                cplx<float> cf;
+                if constexpr (!MK)
+                    cf = cf_mixed<KIND>(d2, a.kp);
 #pragma unroll
                 for (int r = 0; r < NB; r++)
                 {
+                    if constexpr (MK)
+                        cf = cf_mixed<KIND>(d2, kps[r]);
                     const cplx<float> v = ChebF<N0, N1, N2>::eval(
-                        bp.fcoef + (size_t)r * bp.fc_plane + (size_t)gf * a.P_lo, loc, a.lo);
+                        bp.fcoef + (size_t)(pb + r) * bp.fc_plane + (size_t)gf * a.P_lo, loc, a.lo);
                     accr[r] += (double)(v.re * cf.re - v.im * cf.im);
                     acci[r] += (double)(v.re * cf.im + v.im * cf.re);
                 }
@@ -336,7 +400,7 @@ __global__ void __launch_bounds__(EVAL_THREADS, 4) far_batch_kernel(EvalArgs a, 
         if (active && si == 0)
         {
             const long long o = a.tgt_perm[t];
-            for (int r = 0; r < bp.nrhs; r++)
+            for (int r = 0; r < NB && pb + r < bp.nrhs; r++)
             {
                 double sr = 0, sim = 0;
                 for (int s = 0; s < S; s++)
@@ -344,10 +408,10 @@ __global__ void __launch_bounds__(EVAL_THREADS, 4) far_batch_kernel(EvalArgs a, 
                     sr += rr[r][ti + s * cnt];
                     sim += ri[r][ti + s * cnt];
                 }
-                const double2 nr = bp.unear[(size_t)r * bp.n_tgt + t];
+                const double2 nr = bp.unear[(size_t)(pb + r) * bp.n_tgt + t];
                 sr += nr.x;
                 sim += nr.y;
-                double* out = a.out + (size_t)r * bp.out_plane;
+                double* out = a.out + (size_t)(pb + r) * bp.out_plane;
                 if (a.real_out)
                     out[o] = sr;
                 else
@@ -360,11 +424,12 @@ __global__ void __launch_bounds__(EVAL_THREADS, 4) far_batch_kernel(EvalArgs a, 
     }
 }
 
-// Enqueues the batched mixed matvec of bp.nrhs (<= BATCH_NB) right-hand
-// sides; returns the number of kernels launched, or -1 when this operator's
-// shape has no batched path (runtime orders, or a level whose upward runs
-// do not fit the staged kernel) and the right-hand sides must run one by one.
-template <int KIND, int N0, int N1, int N2>
+// Enqueues the batched mixed matvec of bp.nrhs (<= bp.groups * BATCH_NB)
+// right-hand sides, one launch per stage and level; returns the number of
+// kernels launched, or -1 when this operator's shape has no batched path
+// (runtime orders, or a level whose upward runs do not fit the staged kernel)
+// and the right-hand sides must run one by one.
+template <int KIND, int N0, int N1, int N2, bool MK>
 static int run_mult_batch(const MultPtrs& m, const BatchPtrs& bp, const void* d_w, void* d_u,
                           bool real, cudaStream_t st, LaunchHooks* hk)
 {
@@ -381,7 +446,8 @@ static int run_mult_batch(const MultPtrs& m, const BatchPtrs& bp, const void* d_
                                                       UP_STAGED_SMEM_MAX))
                 return -1;
         }
-        if (m.lo[0] != N0 || m.fct[0] != 3 || m.fct[1] != 3 || m.fct[2] != 3)
+        if (m.lo[0] != N0 || m.fct[1] != m.fct[0] || m.fct[2] != m.fct[0] ||
+            (m.fct[0] != 3 && m.fct[0] != 1))
             return -1;
         int launches = 0;
         {
@@ -389,7 +455,7 @@ static int run_mult_batch(const MultPtrs& m, const BatchPtrs& bp, const void* d_
             const int blocks = (int)std::min<long long>((m.n_src + thr - 1) / thr, 148 * 4);
             if (hk)
                 hk->begin(PROF_PERMUTE);
-            permute_batch_kernel<<<dim3(blocks, BATCH_NB), thr, 0, st>>>(
+            permute_batch_kernel<<<dim3(blocks, bp.groups * BATCH_NB), thr, 0, st>>>(
                 (const double*)d_w, real ? 1 : 0, m.src_perm, bp.w, m.n_src, bp.nrhs, bp.in_plane);
             IFGF_CHECK_LAUNCH();
             if (hk)
@@ -434,7 +500,7 @@ static int run_mult_batch(const MultPtrs& m, const BatchPtrs& bp, const void* d_
             }
             if (hk)
                 hk->begin(PROF_NEAR);
-            near_batch_kernel<KIND><<<m.n_tleaf, EVAL_THREADS, 0, ns>>>(ea, bp);
+            near_batch_kernel<KIND, MK><<<dim3(m.n_tleaf, bp.groups), EVAL_THREADS, 0, ns>>>(ea, bp);
             IFGF_CHECK_LAUNCH();
             if (hk)
                 hk->end();
@@ -456,8 +522,8 @@ static int run_mult_batch(const MultPtrs& m, const BatchPtrs& bp, const void* d_
                             m.w,    m.cvals, m.P_hi, m.kp};
                 if (hk)
                     hk->begin(PROF_COARSE, l);
-                leaf_sample_batch_kernel<KIND>
-                    <<<dim3(LL.n_leaf, nchk), nthr,
+                leaf_sample_batch_kernel<KIND, MK>
+                    <<<dim3(LL.n_leaf, nchk, bp.groups), nthr,
                        (7 * nthr + 2 * BATCH_NB * nthr) * sizeof(float), st>>>(la, bp);
                 IFGF_CHECK_LAUNCH();
                 if (hk)
@@ -475,11 +541,12 @@ static int run_mult_batch(const MultPtrs& m, const BatchPtrs& bp, const void* d_
                 ua.idx = LL.up_idx;
                 ua.slot = LL.up_slot;
                 ua.geo64 = LL.geo64;
-                ua.geo32 = LL.geo32;
+                ua.geo32 = MK ? bp.dgeo32[l] : LL.geo32;
                 ua.P_pad = LL.up_pad;
                 ua.fe_list = LL.fe_list;
                 ua.fe_pad = LL.fe_pad;
                 ua.rch = upward_staged_rch<N0, N1, N2>(LL.fe_pad);
+                ua.kp_plane = bp.kp_plane;
                 ua.cv_plane = bp.cv_plane;
                 ua.fc_plane = bp.fc_plane;
                 ua.hi_nodes = m.hi_nodes;
@@ -493,13 +560,13 @@ static int run_mult_batch(const MultPtrs& m, const BatchPtrs& bp, const void* d_
                     ua.lo[d] = m.lo[d];
                 ua.kp = m.kp;
                 const size_t sm = upward_staged_smem<N0, N1, N2>(m.P_hi, ua.rch);
-                auto kern = upward_staged_kernel<KIND, N0, N1, N2>;
+                auto kern = upward_staged_kernel<KIND, N0, N1, N2, MK>;
                 if (sm > 48 * 1024)
                     IFGF_CHECK(cudaFuncSetAttribute(
                         kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
                 if (hk)
                     hk->begin(PROF_UPWARD, l);
-                kern<<<dim3(LL.n_up, BATCH_NB), UPS_THREADS, sm, st>>>(ua);
+                kern<<<dim3(LL.n_up, bp.groups * BATCH_NB), UPS_THREADS, sm, st>>>(ua);
                 IFGF_CHECK_LAUNCH();
                 if (hk)
                     hk->end();
@@ -529,7 +596,7 @@ static int run_mult_batch(const MultPtrs& m, const BatchPtrs& bp, const void* d_
             fa.P_lo = m.P_lo;
             if (hk)
                 hk->begin(PROF_C2F, l);
-            if (!launch_c2f_fixed<float>(fa, m.A_host, c2f_grid, st, BATCH_NB))
+            if (!launch_c2f_fixed<float>(fa, m.A_host, c2f_grid, st, bp.groups * BATCH_NB))
                 throw Error(6, "batched coarse-to-fine needs one of the fixed order shapes");
             IFGF_CHECK_LAUNCH();
             if (hk)
@@ -542,7 +609,8 @@ static int run_mult_batch(const MultPtrs& m, const BatchPtrs& bp, const void* d_
                 IFGF_CHECK(cudaStreamWaitEvent(st, m.ev_join, 0));
             if (hk)
                 hk->begin(PROF_EVAL);
-            far_batch_kernel<KIND, N0, N1, N2><<<m.n_tleaf, EVAL_THREADS, 0, st>>>(ea, bp);
+            far_batch_kernel<KIND, N0, N1, N2, MK>
+                <<<dim3(m.n_tleaf, bp.groups), EVAL_THREADS, 0, st>>>(ea, bp);
             IFGF_CHECK_LAUNCH();
             if (hk)
                 hk->end();
@@ -557,11 +625,15 @@ int launch_mult_batch_kernels(const MultPtrs& m, const BatchPtrs& bp, const void
                               bool real, cudaStream_t st, LaunchHooks* hk)
 {
     const int* lo = m.lo;
+#define IFGF_RUN_BATCH(A, B, C)                                                               \
+    return bp.kp_plane ? run_mult_batch<KIND, A, B, C, true>(m, bp, d_w, d_u, real, st, hk)     \
+                       : run_mult_batch<KIND, A, B, C, false>(m, bp, d_w, d_u, real, st, hk)
     if (lo[0] == 2 && lo[1] == 5 && lo[2] == 5)
-        return run_mult_batch<KIND, 2, 5, 5>(m, bp, d_w, d_u, real, st, hk);
+        IFGF_RUN_BATCH(2, 5, 5);
     if (lo[0] == 3 && lo[1] == 6 && lo[2] == 6)
-        return run_mult_batch<KIND, 3, 6, 6>(m, bp, d_w, d_u, real, st, hk);
+        IFGF_RUN_BATCH(3, 6, 6);
     if (lo[0] == 4 && lo[1] == 7 && lo[2] == 7)
-        return run_mult_batch<KIND, 4, 7, 7>(m, bp, d_w, d_u, real, st, hk);
+        IFGF_RUN_BATCH(4, 7, 7);
+#undef IFGF_RUN_BATCH
     return -1;
 }

@@ -236,6 +236,9 @@ struct UpArgs
     int P_hi, P_lo;
     int lo[3];
     KParams kp;
+    // staged kernel with MK: wavenumber of plane blockIdx.y, and geo32 holds
+    // distance tables (tr = d - d_parent, ti = d_parent / d)
+    const KParams* kp_plane = nullptr;
 };
 
 // One CTA per coarse cone of a box with children (CTAs ordered by cone
@@ -279,7 +282,9 @@ __device__ __forceinline__ bool upward_fallback64(const UpArgs& a, int box, int 
 // (slot, octant) row.  The row lists the nodes that fall inside the child's
 // domain, sorted by child element, each element's run padded with skipped
 // entries to a multiple of UPGEO_RUN so that a group of UPGEO_RUN entries
-// always shares one element.  fill = 0 only measures the row: its padded
+// always shares one element.  fill = 2 writes distance tables instead of
+// centre-shift factors (UpGeo32 tr = d - d_parent, ti = d_parent / d; no
+// UpGeo64 table).  fill = 0 only measures the row: its padded
 // length and its number of element runs (row_len[2 row], row_len[2 row + 1]).
 // fill = 1 also lists each row's distinct elements in run order
 // with the group at which each run starts (fe_list[row (fe_pad + 1) + r] =
@@ -391,10 +396,20 @@ __global__ void __launch_bounds__(256) build_upgeo_kernel(LevelGeom PG, LevelGeo
         g.fe = key[n];
         g.node = n;
         to_local(g.fe, s, CG.dmin, CG.hf, CG.hfi, CG.nf, g.loc);
-        const cplx<double> tf = P::transfer(p0 * p0 + p1 * p1 + p2 * p2, dp2, kp);
-        g.tr = tf.re;
-        g.ti = tf.im;
-        g64[at] = g;
+        if (fill == 2)
+        {
+            // distance table: d - d_parent and d_parent / d for every wavenumber
+            const double d = sqrt(p0 * p0 + p1 * p1 + p2 * p2), dp = sqrt(dp2);
+            g.tr = d - dp;
+            g.ti = dp / d;
+        }
+        else
+        {
+            const cplx<double> tf = P::transfer(p0 * p0 + p1 * p1 + p2 * p2, dp2, kp);
+            g.tr = tf.re;
+            g.ti = tf.im;
+            g64[at] = g;
+        }
         UpGeo32 h;
         h.fe = g.fe;
         h.node = n;
@@ -443,9 +458,10 @@ void launch_build_upgeo(const LevelGeom& PG, const LevelGeom& CG, double pH, dou
 {
     if (n_slots <= 0 || P_pad <= 0)
         return;
+    // without an FP64 table (g64 null): the distance table
     build_upgeo_kernel<KIND><<<n_slots * 8, 256, 4 * P_hi * sizeof(int)>>>(
-        PG, CG, pH, cH, off_dev, slot_el, hi_nodes, P_hi, kp, 1, P_pad, nullptr, g64, g32, fe_pad,
-        fe_list);
+        PG, CG, pH, cH, off_dev, slot_el, hi_nodes, P_hi, kp, g64 ? 1 : 2, P_pad, nullptr, g64,
+        g32, fe_pad, fe_list);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess)
         throw Error(2, std::string("build_upgeo_kernel: ") + cudaGetErrorString(e));
@@ -1375,7 +1391,9 @@ constexpr int UPS_THREADS = 64;
 // the Chebyshev sums of those runs' groups read only shared memory.
 // Compile-time orders only (P_lo even, so that a block is a whole number of
 // 16-byte chunks).
-template <int KIND, int N0, int N1, int N2>
+// MK: every plane (blockIdx.y) has its own wavenumber; the centre-shift
+// factor is formed from the distance table per plane.
+template <int KIND, int N0, int N1, int N2, bool MK = false>
 __global__ void __launch_bounds__(UPS_THREADS, 10) upward_staged_kernel(UpArgs a)
 {
     constexpr int R = UPGEO_RUN;
@@ -1477,7 +1495,8 @@ __global__ void __launch_bounds__(UPS_THREADS, 10) upward_staged_kernel(UpArgs a
                         cplx<float> v = {0.f, 0.f};
                         cfmaf(v, ChebF<N0, N1, N2>::eval(fcf + (size_t)gf2 * P_LO, loc, a.lo),
                               transfer_mixed<KIND>(p[0] * p[0] + p[1] * p[1] + p[2] * p[2],
-                                                   e0 * e0 + e1 * e1 + e2 * e2, a.kp));
+                                                   e0 * e0 + e1 * e1 + e2 * e2,
+                                                   MK ? a.kp_plane[blockIdx.y] : a.kp));
                         acc[e[r].node].x += v.re;
                         acc[e[r].node].y += v.im;
                     }
@@ -1489,6 +1508,18 @@ __global__ void __launch_bounds__(UPS_THREADS, 10) upward_staged_kernel(UpArgs a
                     for (int d = 0; d < 3; d++)
                         x[r][d] = e[r].loc[d];
                 ChebMulti<float, N0, N1, N2, R, true>::eval(blk + (size_t)rl * BS, x, a.lo, vr, vi);
+                if constexpr (MK)
+                {
+#pragma unroll
+                    for (int r = 0; r < R; r++)
+                        if (e[r].node >= 0)
+                        {
+                            const cplx<float> t =
+                                transfer_delta<KIND>(e[r].tr, e[r].ti, a.kp_plane[blockIdx.y]);
+                            e[r].tr = t.re;
+                            e[r].ti = t.im;
+                        }
+                }
 #pragma unroll
                 for (int r = 0; r < R; r++)
                     if (e[r].node >= 0)
@@ -1714,10 +1745,13 @@ __host__ __device__ constexpr int c2f_row_stride()
     return s;
 }
 
+// one thread per row vector of the widest of the three stages
 template <int H0, int H1, int H2, int L0, int L1, int L2, int F>
 constexpr int c2f_fixed_threads()
 {
-    return (F * L0 * F * L1 + 31) / 32 * 32;
+    constexpr int s1 = H1 * H2, s2 = F * L0 * H2, s3 = F * L0 * F * L1;
+    constexpr int m = s1 > s2 ? (s1 > s3 ? s1 : s3) : (s2 > s3 ? s2 : s3);
+    return (m + 31) / 32 * 32;
 }
 
 // Coarse-to-fine with compile-time orders and refinement factor F (the same
@@ -1846,28 +1880,38 @@ static bool launch_c2f_fixed(const C2FArgs& fa, const double* A_host, unsigned g
     const int* h = fa.hi;
     const int* l = fa.lo;
     const int f = fa.f[0];
-    if (fa.f[1] != f || fa.f[2] != f || f != 3 || A_host == nullptr)
+    if (fa.f[1] != f || fa.f[2] != f || (f != 3 && f != 1) || A_host == nullptr)
         return false;
-#define IFGF_C2F_CASE(A, B, C, D, E, G)                                                       \
-    if (h[0] == A && h[1] == B && h[2] == C && l[0] == D && l[1] == E && l[2] == G)            \
+    // refinement factor 3 (fine grid 3x the coarse one) or 1 (the modified
+    // Helmholtz kernel: fine = coarse grid)
+#define IFGF_C2F_CASE_F(A, B, C, D, E, G, F)                                                  \
     {                                                                                          \
-        C2FMats<A, B, C, D, E, G, 3, T> mats;                                                  \
+        C2FMats<A, B, C, D, E, G, F, T> mats;                                                  \
         T* dst = mats.a0;                                                                      \
-        constexpr int NA = 3 * (D * A + E * B + G * C);                                        \
+        constexpr int NA = F * (D * A + E * B + G * C);                                        \
         static_assert(sizeof(mats) == NA * sizeof(T), "matrix block layout");                  \
         for (int i = 0; i < NA; i++)                                                           \
             dst[i] = (T)A_host[i];                                                             \
-        constexpr size_t sm = c2f_fixed_smem<A, B, C, D, E, G, 3, T>();                        \
-        auto kern = coarse_to_fine_fixed_kernel<A, B, C, D, E, G, 3, T>;                       \
+        constexpr size_t sm = c2f_fixed_smem<A, B, C, D, E, G, F, T>();                        \
+        auto kern = coarse_to_fine_fixed_kernel<A, B, C, D, E, G, F, T>;                       \
         if (sm > 48 * 1024)                                                                    \
             cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);  \
-        kern<<<dim3(grid, planes), c2f_fixed_threads<A, B, C, D, E, G, 3>(), sm, st>>>(fa, mats); \
+        kern<<<dim3(grid, planes), c2f_fixed_threads<A, B, C, D, E, G, F>(), sm, st>>>(fa, mats); \
         return true;                                                                           \
+    }
+#define IFGF_C2F_CASE(A, B, C, D, E, G)                                                       \
+    if (h[0] == A && h[1] == B && h[2] == C && l[0] == D && l[1] == E && l[2] == G)            \
+    {                                                                                          \
+        if (f == 3)                                                                            \
+            IFGF_C2F_CASE_F(A, B, C, D, E, G, 3)                                               \
+        else                                                                                   \
+            IFGF_C2F_CASE_F(A, B, C, D, E, G, 1)                                               \
     }
     IFGF_C2F_CASE(5, 8, 8, 2, 5, 5)
     IFGF_C2F_CASE(6, 9, 9, 3, 6, 6)
     IFGF_C2F_CASE(7, 10, 10, 4, 7, 7)
 #undef IFGF_C2F_CASE
+#undef IFGF_C2F_CASE_F
     return false;
 }
 

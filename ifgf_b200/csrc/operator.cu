@@ -119,9 +119,19 @@ struct DeviceState
     DevBuf<int> tl_first, tl_last, tl_far_src, tl_near_src;
     DevBuf<long long> tl_far_off, tl_near_off;
     DevBuf<double2> w, cvals, fcoef, unear;
-    // planes of the batched mixed matvec, allocated on first use
+    // planes of the batched mixed matvec, allocated on first use for
+    // b_planes planes of the plane sizes recorded beside them
     DevBuf<float2> bw, bcv, bfc;
     DevBuf<double2> bun;
+    int b_planes = 0;
+    size_t b_cv = 0, b_fc = 0;
+    int64_t b_ns = 0, b_nt = 0;
+    // multi-wavenumber batches: per-plane wavenumbers and the per-level
+    // distance tables (built on first use after an init)
+    DevBuf<KParams> kp_plane;
+    std::vector<DevBuf<UpGeo32>> dgeo32;
+    std::vector<const UpGeo32*> dgeo32_ptr;
+    bool dgeo_ready = false;
     DevBuf<unsigned long long> err;
     DevBuf<double> io_w, io_u; // staging for host-buffer mult
     std::vector<cudaEvent_t> prof_ev;
@@ -356,21 +366,9 @@ void Operator::set_wavenumber(double k_re, double k_im)
         return;
     }
     const double okr = kr_, oki = ki_;
+    bool same = grids_match(k_re, k_im);
     kr_ = k_re;
     ki_ = k_im;
-    bool same = true;
-    for (const LevelGeom& G : lv_)
-    {
-        int64_t nf[3], nc[3];
-        elements_for_box(G.H, 0, nf);
-        elements_for_box(G.H, 1, nc);
-        double smin = cutoff_limit(G.H);
-        if (smin >= std::sqrt(3.0) / 3)
-            smin = std::sqrt(3.0) / 3 - 0.05;
-        for (int d = 0; d < 3; d++)
-            same = same && nf[d] == G.nf[d] && nc[d] == G.nc[d];
-        same = same && smin == G.dmin[0];
-    }
     if (same && tol_ > 0)
     {
         // estimated orders follow the wavenumber: new orders need a new init
@@ -419,6 +417,31 @@ void Operator::set_wavenumber(double k_re, double k_im)
     }
     IFGF_CUDA(cudaDeviceSynchronize());
     D.vkind = -1; // variant (k-derivative) tables are rebuilt on next use
+}
+
+// Whether wavenumber k_re + i k_im gives every level the cone grids and
+// interpolation domain the operator was initialised with.
+bool Operator::grids_match(double k_re, double k_im)
+{
+    const double okr = kr_, oki = ki_;
+    kr_ = k_re;
+    ki_ = k_im;
+    bool same = true;
+    for (const LevelGeom& G : lv_)
+    {
+        int64_t nf[3], nc[3];
+        elements_for_box(G.H, 0, nf);
+        elements_for_box(G.H, 1, nc);
+        double smin = cutoff_limit(G.H);
+        if (smin >= std::sqrt(3.0) / 3)
+            smin = std::sqrt(3.0) / 3 - 0.05;
+        for (int d = 0; d < 3; d++)
+            same = same && nf[d] == G.nf[d] && nc[d] == G.nc[d];
+        same = same && smin == G.dmin[0];
+    }
+    kr_ = okr;
+    ki_ = oki;
+    return same;
 }
 
 void Operator::set_shard(int rank, int nranks)
@@ -851,6 +874,9 @@ void Operator::init(const double* srcs, int64_t ns, const double* tgts, int64_t 
 void Operator::setup_device(const double* normals)
 {
     DeviceState& D = *dev_;
+    D.dgeo32.clear();
+    D.dgeo32_ptr.clear();
+    D.dgeo_ready = false;
     const Tree& S = plan_.src;
     const Tree& Tt = plan_.tgt;
     const int L = S.num_levels();
@@ -1684,31 +1710,15 @@ void Operator::mult_batch_device(const void* d_w, void* d_u, int64_t batch, void
     int64_t done = 0;
     if (precision_ == PREC_MIXED && batch > 1)
     {
-        if (D.bw.n == 0)
-        {
-            D.bw.alloc((size_t)BATCH_NB * n_src());
-            D.bcv.alloc((size_t)BATCH_NB * D.cvals.n);
-            D.bfc.alloc((size_t)BATCH_NB * D.fcoef.n);
-            D.bfc.zero(); // fine cones without an active coarse parent read zero
-            D.bun.alloc((size_t)BATCH_NB * n_tgt());
-        }
-        BatchPtrs bp;
-        bp.w = D.bw.p;
-        bp.cvals = D.bcv.p;
-        bp.fcoef = D.bfc.p;
-        bp.unear = D.bun.p;
-        bp.cv_plane = (long long)D.cvals.n;
-        bp.fc_plane = (long long)D.fcoef.n;
-        bp.n_src = n_src();
-        bp.n_tgt = n_tgt();
-        bp.in_plane = in_plane;
-        bp.out_plane = out_plane;
+        const int planes = ensure_batch_planes(batch);
+        BatchPtrs bp = batch_ptrs(in_plane, out_plane);
         MultPtrs m;
         fill_mult_ptrs(m);
         cudaStream_t st = (cudaStream_t)stream;
         while (done < batch)
         {
-            bp.nrhs = (int)std::min<int64_t>(BATCH_NB, batch - done);
+            bp.nrhs = (int)std::min<int64_t>(planes, batch - done);
+            bp.groups = (bp.nrhs + BATCH_NB - 1) / BATCH_NB;
             EventHooks log(D, st);
             int r = -1;
             IFGF_DISPATCH(kind_, r = launch_mult_batch_kernels<KK>(
@@ -1726,6 +1736,184 @@ void Operator::mult_batch_device(const void* d_w, void* d_u, int64_t batch, void
     for (; done < batch; done++)
         launch_mult((const double*)d_w + done * in_plane, (double*)d_u + done * out_plane, stream,
                     false);
+}
+
+// Plane buffers of the batched pipeline for up to `want` right-hand sides
+// (whole groups of BATCH_NB, within a 16 GB budget and 64 planes), sized for
+// the current tree; returns the planes one launch may use.
+int Operator::ensure_batch_planes(int64_t want)
+{
+    DeviceState& D = *dev_;
+    const size_t plane_bytes = sizeof(float2) * ((size_t)n_src() + D.cvals.n + D.fcoef.n) +
+                               sizeof(double2) * (size_t)n_tgt();
+    const int64_t budget = (int64_t)(16ull << 30) / (int64_t)std::max<size_t>(plane_bytes, 1);
+    int cap = (int)std::min<int64_t>(64, budget) / BATCH_NB * BATCH_NB;
+    cap = std::max(cap, BATCH_NB);
+    const int planes =
+        (int)std::min<int64_t>(cap, (want + BATCH_NB - 1) / BATCH_NB * BATCH_NB);
+    if (D.b_planes >= planes && D.b_cv == D.cvals.n && D.b_fc == D.fcoef.n && D.b_ns == n_src() &&
+        D.b_nt == n_tgt())
+        return std::min(planes, D.b_planes);
+    D.bw.alloc((size_t)planes * n_src());
+    D.bcv.alloc((size_t)planes * D.cvals.n);
+    D.bfc.alloc((size_t)planes * D.fcoef.n);
+    D.bfc.zero(); // fine cones without an active coarse parent read zero
+    D.bun.alloc((size_t)planes * n_tgt());
+    D.b_planes = planes;
+    D.b_cv = D.cvals.n;
+    D.b_fc = D.fcoef.n;
+    D.b_ns = n_src();
+    D.b_nt = n_tgt();
+    return planes;
+}
+
+BatchPtrs Operator::batch_ptrs(long long in_plane, long long out_plane) const
+{
+    const DeviceState& D = *dev_;
+    BatchPtrs bp;
+    bp.w = D.bw.p;
+    bp.cvals = D.bcv.p;
+    bp.fcoef = D.bfc.p;
+    bp.unear = D.bun.p;
+    bp.cv_plane = (long long)D.cvals.n;
+    bp.fc_plane = (long long)D.fcoef.n;
+    bp.n_src = n_src();
+    bp.n_tgt = n_tgt();
+    bp.in_plane = in_plane;
+    bp.out_plane = out_plane;
+    return bp;
+}
+
+// Distance tables of every level (UpGeo32 with tr = d - d_parent,
+// ti = d_parent / d): the upward geometry of multi-wavenumber batches.
+void Operator::ensure_distance_tables()
+{
+    DeviceState& D = *dev_;
+    if (D.dgeo_ready)
+        return;
+    const int L = (int)lv_.size();
+    const int P_hi = hi_[0] * hi_[1] * hi_[2];
+    const KParams kp = make_kparams(kr_, ki_, dx_);
+    D.dgeo32.clear();
+    D.dgeo32.resize(L);
+    D.dgeo32_ptr.assign(L, nullptr);
+    for (int l = 0; l + 1 < L; l++)
+    {
+        const LevelLists& LL = D.lists[l];
+        const int ns = (int)D.slot_el[l].n;
+        if (ns == 0 || LL.up_pad <= 0)
+            continue;
+        const size_t n_ent = (size_t)ns * 8 * (size_t)LL.up_pad;
+        D.dgeo32[l].alloc(n_ent);
+        IFGF_CUDA(cudaMemset(D.dgeo32[l].p, 0xff, n_ent * sizeof(UpGeo32)));
+        IFGF_DISPATCH(kind_, launch_build_upgeo<KK>(lv_[l], lv_[l + 1], D.up_pH[l], D.up_cH[l],
+                                                     D.child_off[l].p, D.slot_el[l].p, ns,
+                                                     D.hi_nodes.p, P_hi, kp, LL.up_pad, nullptr,
+                                                     D.dgeo32[l].p, LL.fe_pad, D.fe_list[l].p));
+        D.dgeo32_ptr[l] = D.dgeo32[l].p;
+    }
+    IFGF_CUDA(cudaDeviceSynchronize());
+    D.dgeo_ready = true;
+}
+
+void Operator::mult_wavenumbers_host(const double* k, int64_t nk, const void* w, void* u)
+{
+    if (!initialized_)
+        throw Error(ERR_STATE, "mult called before init");
+    if (!w || !u)
+        throw Error(ERR_INVALID, "null density or result buffer");
+    if (nk < 1)
+        throw Error(ERR_INVALID, "need at least one wavenumber");
+    DeviceState& D = *dev_;
+    const size_t per = is_real() ? 1 : 2;
+    const size_t nw = per * (size_t)n_src() * nk, nu = per * (size_t)n_tgt() * nk;
+    if (D.io_w.n < nw)
+        D.io_w.alloc(nw);
+    if (D.io_u.n < nu)
+        D.io_u.alloc(nu);
+    IFGF_CUDA(cudaMemcpy(D.io_w.p, w, nw * sizeof(double), cudaMemcpyHostToDevice));
+    mult_wavenumbers_device(k, nk, D.io_w.p, D.io_u.p, nullptr);
+    IFGF_CUDA(cudaMemcpy(u, D.io_u.p, nu * sizeof(double), cudaMemcpyDeviceToHost));
+    IFGF_CUDA(cudaMemcpy(&missing_, D.err.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+}
+
+void Operator::mult_wavenumbers_device(const double* k, int64_t nk, const void* d_w, void* d_u,
+                                       void* stream)
+{
+    if (!initialized_)
+        throw Error(ERR_STATE, "mult called before init");
+    if (!k || !d_w || !d_u)
+        throw Error(ERR_INVALID, "null wavenumber, density or result buffer");
+    if (nk < 1)
+        throw Error(ERR_INVALID, "need at least one wavenumber");
+    for (int64_t p = 0; p < nk; p++)
+    {
+        if (!std::isfinite(k[2 * p]) || !std::isfinite(k[2 * p + 1]))
+            throw Error(ERR_INVALID, "wavenumber must be finite");
+        if (!grids_match(k[2 * p], k[2 * p + 1]))
+            throw Error(ERR_INVALID, "wavenumber " + std::to_string(k[2 * p]) + (k[2 * p + 1] < 0 ? "" : "+") +
+                                         std::to_string(k[2 * p + 1]) +
+                                         "i gives other cone grids than the operator's; "
+                                         "use set_wavenumber for it");
+    }
+    DeviceState& D = *dev_;
+    const size_t per = is_real() ? 1 : 2;
+    const long long in_plane = (long long)(per * n_src()), out_plane = (long long)(per * n_tgt());
+    cudaStream_t st = (cudaStream_t)stream;
+    adj_.reset();
+    if (precision_ != PREC_MIXED)
+    {
+        // FP64: the centre-shift factors of each wavenumber, then its matvec
+        const double okr = kr_, oki = ki_;
+        for (int64_t p = 0; p < nk; p++)
+        {
+            IFGF_CUDA(cudaStreamSynchronize(st)); // the tables are rebuilt in place
+            set_wavenumber(k[2 * p], k[2 * p + 1]);
+            launch_mult((const double*)d_w + p * in_plane, (double*)d_u + p * out_plane, stream,
+                        false);
+        }
+        IFGF_CUDA(cudaStreamSynchronize(st));
+        set_wavenumber(okr, oki);
+        return;
+    }
+    ensure_distance_tables();
+    const int planes = ensure_batch_planes(nk);
+    // every plane's wavenumber, padded to whole groups
+    const int64_t nk_pad = (nk + BATCH_NB - 1) / BATCH_NB * BATCH_NB;
+    std::vector<KParams> kps((size_t)nk_pad);
+    for (int64_t p = 0; p < nk_pad; p++)
+    {
+        const int64_t q = std::min(p, nk - 1);
+        kps[(size_t)p] = make_kparams(k[2 * q], k[2 * q + 1], dx_);
+    }
+    if (D.kp_plane.n < kps.size())
+        D.kp_plane.alloc(kps.size());
+    IFGF_CUDA(cudaMemcpyAsync(D.kp_plane.p, kps.data(), kps.size() * sizeof(KParams),
+                              cudaMemcpyHostToDevice, st));
+    BatchPtrs bp = batch_ptrs(in_plane, out_plane);
+    bp.dgeo32 = D.dgeo32_ptr.data();
+    MultPtrs m;
+    fill_mult_ptrs(m);
+    int64_t done = 0;
+    while (done < nk)
+    {
+        bp.nrhs = (int)std::min<int64_t>(planes, nk - done);
+        bp.groups = (bp.nrhs + BATCH_NB - 1) / BATCH_NB;
+        bp.kp_plane = D.kp_plane.p + done;
+        EventHooks log(D, st);
+        int r = -1;
+        IFGF_DISPATCH(kind_, r = launch_mult_batch_kernels<KK>(
+                                 m, bp, (const double*)d_w + done * in_plane,
+                                 (double*)d_u + done * out_plane, is_real(), st,
+                                 profiling_ ? &log : nullptr));
+        if (r < 0)
+            throw Error(ERR_INVALID, "multi-wavenumber batches need one of the batched order "
+                                     "shapes (low orders (2,5,5), (3,6,6) or (4,7,7))");
+        launches_per_mult_ = r;
+        if (profiling_ && log.n > 0)
+            finish_profile(log, bp.nrhs);
+        done += bp.nrhs;
+    }
 }
 
 void Operator::host_mult_loop(const void* w, void* u, int64_t batch, int vkind)
@@ -1925,6 +2113,7 @@ std::string Operator::stats_json() const
       << ",\"target_leaves\":" << dev_->n_tleaf << ",\"missing_cone_lookups\":" << missing_
       << ",\"init_ms\":" << init_ms_ << ",\"init_tree_ms\":" << tree_ms_
       << ",\"init_lists_ms\":" << lists_ms_ << ",\"launches_per_mult\":" << launches_per_mult_
+      << ",\"batch_planes\":" << dev_->b_planes
       << ",\"last_mult_ms\":{\"permute\":" << last_.permute << ",\"leaf_sample\":" << last_.coarse
       << ",\"upward\":" << last_.upward << ",\"coarse_to_fine\":" << last_.c2f
       << ",\"target_eval\":" << last_.eval << ",\"near\":" << last_.near

@@ -18,6 +18,7 @@ struct DeviceState;  // device buffers, defined in operator.cu
 struct MultPtrs;     // kernel launch view, defined in mult.hpp
 struct AdjointState; // operators and buffers of the adjoint, defined in operator.cu
 struct EventHooks;   // per-launch CUDA events, defined in operator.cu
+struct BatchPtrs;    // plane buffers of the batched pipeline, mult.hpp
 
 struct StageTimes
 {
@@ -58,10 +59,21 @@ class Operator
     // host buffers, `batch` right-hand sides
     void mult_host(const void* w, void* u, int64_t batch);
     // `batch` right-hand sides on device buffers (batch x n_src in, batch x
-    // n_tgt out).  The mixed pipeline runs them BATCH_NB at a time through
-    // the batched kernels (one kernel / geometry evaluation for the group);
-    // FP64 and shapes without a batched path run them one by one.
+    // n_tgt out).  The mixed pipeline runs them through the batched kernels,
+    // one launch per stage and level for up to 64 right-hand sides (groups of
+    // BATCH_NB share one kernel / geometry evaluation); FP64 and shapes
+    // without a batched path run them one by one.
     void mult_batch_device(const void* d_w, void* d_u, int64_t batch, void* stream);
+    // Multi-wavenumber batch: right-hand side p (plane p of d_w / d_u) is
+    // multiplied at wavenumber k[2p] + i k[2p+1].  Every wavenumber must give
+    // the operator's cone grids (a convolution-quadrature set does); the
+    // planes share the tree, cone maps and geometry of one pass, one launch
+    // per stage and level for up to 64 planes (mixed precision).  FP64 runs
+    // one set_wavenumber refresh and matvec per plane.
+    void mult_wavenumbers_device(const double* k, int64_t nk, const void* d_w, void* d_u,
+                                 void* stream);
+    // the same with host buffers
+    void mult_wavenumbers_host(const double* k, int64_t nk, const void* w, void* u);
     // mult_device with its scratch in a caller-provided device region instead
     // of the buffers allocated at init; allocates nothing
     void mult_device_external_scratch(const void* d_w, void* d_u, void* stream, void* scratch,
@@ -107,6 +119,10 @@ class Operator
     double cutoff_limit(double H) const;
     void set_orders();
     void estimate_orders(int* out) const;
+    bool grids_match(double k_re, double k_im);
+    int ensure_batch_planes(int64_t want);
+    BatchPtrs batch_ptrs(long long in_plane, long long out_plane) const;
+    void ensure_distance_tables();
     void setup_device(const double* normals);
     // vkind >= 0: run that kernel with the variant geometry tables
     void launch_mult(const void* d_w, void* d_u, void* stream, bool timed, int vkind = -1);

@@ -120,15 +120,33 @@ int ifgf_mult(ifgf_operator* op, const void* w, void* u);
 
 /* Same as ifgf_mult for `batch` right-hand sides stored one after another
  * (w: batch x n_src, u: batch x n_tgt).  In the mixed-precision pipeline the
- * right-hand sides run four at a time through batched kernels that share the
- * kernel, cone-lookup and centred-factor evaluations of the group (each
- * right-hand side keeps its own interpolants); FP64 runs them one by one.
- * No reference counterpart. */
+ * right-hand sides run through batched kernels, one launch per stage and
+ * level for up to 64 of them; groups of four share the kernel, cone-lookup
+ * and centred-factor evaluations (each right-hand side keeps its own
+ * interpolants); FP64 runs them one by one.  No reference counterpart. */
 int ifgf_mult_batch(ifgf_operator* op, const void* w, void* u, long batch);
 
 /* ifgf_mult_batch on device buffers enqueued on `stream`. */
 int ifgf_mult_batch_device(ifgf_operator* op, const void* d_w, void* d_u, long batch,
                            void* stream);
+
+/* Multi-wavenumber batch: u_p = A(k_p) w_p for p < n_k, with
+ * k_p = k[2p] + i k[2p+1] and w / u stored as in ifgf_mult_batch.  Every k_p
+ * must give the cone grids the operator was initialised with (else
+ * IFGF_ERR_INVALID_ARG; a convolution-quadrature frequency set of the
+ * modified Helmholtz kernel does); orders stay the operator's.  The planes
+ * share the tree, cone maps and the geometry of one pass (node and source
+ * positions, cone lookups, Chebyshev bases), each evaluating its own kernel
+ * values and factors: one launch per stage and level for up to 64
+ * wavenumbers (mixed precision, low orders (2,5,5), (3,6,6) or (4,7,7)).
+ * FP64 runs ifgf_set_wavenumber and one matvec per wavenumber.  Replaces the
+ * reference's operator-per-frequency loop (test/test_CQIFGF.cpp:117-135). */
+int ifgf_mult_wavenumbers(ifgf_operator* op, const double* k, long n_k, const void* w, void* u);
+
+/* ifgf_mult_wavenumbers on device buffers enqueued on `stream` (k stays a
+ * host array). */
+int ifgf_mult_wavenumbers_device(ifgf_operator* op, const double* k, long n_k, const void* d_w,
+                                 void* d_u, void* stream);
 
 /* ifgf_mult on device buffers (complex128 / float64 as above) enqueued on
  * `stream` (a cudaStream_t, NULL = legacy default stream).  Returns after

@@ -1,7 +1,8 @@
 """Batched right-hand sides.
 
-The mixed pipeline runs four right-hand sides per pass through kernels that
-share the kernel and geometry evaluations; every right-hand side must equal
+The mixed pipeline runs the right-hand sides in groups of four that share
+the kernel and geometry evaluations, all groups (up to 64 right-hand sides)
+in one launch per stage and level; every right-hand side must equal
 its own single matvec (to FP32 rounding: the leaf factors are evaluated at
 unit density and then scaled) and the FP64 pipeline within the mixed
 tolerance.  The FP64 batch is the loop of single matvecs.
@@ -56,3 +57,37 @@ def test_batched_device_api_and_order_fallback():
         u = du.cpu().numpy()
         for b in range(5):
             assert rel2(u[b], g.mult(w[b])) <= 1e-6
+
+
+@pytest.mark.gpu
+def test_plane_groups_in_one_launch_and_across_launches():
+    # 70 right-hand sides: one launch of 64 planes (16 groups) and one of 6
+    n = 4000
+    pts = W.sphere_points(n, seed=0)
+    g = make_gpu_op("helmholtz", leaf=50, order=8)
+    g.init(pts, pts)
+    g.set_precision("mixed")
+    w = np.stack([densities_for("helmholtz", n, seed=100 + b) for b in range(70)])
+    ub = g.mult_batch(w)
+    for b in (0, 3, 4, 17, 63, 64, 69):
+        assert rel2(ub[b], g.mult(w[b])) <= 1e-6, b
+
+
+@pytest.mark.gpu
+def test_batch_planes_follow_a_reinitialised_tree():
+    # the plane buffers of a batch run before a re-init (finer cone grids,
+    # larger planes) must not be reused at their old size
+    n = 6000
+    pts = W.sphere_points(n, seed=0)
+    g = make_gpu_op("helmholtz", leaf=50, order=8, k=10.0)
+    g.init(pts, pts)
+    g.set_precision("mixed")
+    w = np.stack([densities_for("helmholtz", n, seed=b) for b in range(5)])
+    g.mult_batch(w)
+    g.set_wavenumber(60.0)  # new grids: a full init
+    fresh = make_gpu_op("helmholtz", leaf=50, order=8, k=60.0)
+    fresh.init(pts, pts)
+    fresh.set_precision("mixed")
+    ug, uf = g.mult_batch(w), fresh.mult_batch(w)
+    for b in range(5):
+        assert rel2(ug[b], uf[b]) <= 1e-14, b
