@@ -366,13 +366,15 @@ extern "C"
             if (level < 0 || level >= t.num_levels() || box < 0 || box >= (long)t.levels[level].size())
                 throw ifgf::Error(IFGF_ERR_INVALID_ARG, "box out of range");
             const auto& P = h->op.plan();
-            const auto& v = (far ? P.far : P.near)[t.level_off[level] + box];
+            const ifgf::PairLists& pl = far ? P.far : P.near;
+            const int64_t sg = t.level_off[level] + box;
+            const long cnt = (long)pl.count(sg);
             if (n)
-                *n = (long)v.size();
+                *n = cnt;
             const auto& T = P.tgt;
-            for (long i = 0; out && i < (long)v.size() && i < cap; i++)
+            for (long i = 0; out && i < cnt && i < cap; i++)
             {
-                const int64_t g = v[i];
+                const int64_t g = pl.begin(sg)[i];
                 int lev = (int)(std::upper_bound(T.level_off.begin(), T.level_off.end(), g) -
                                 T.level_off.begin()) - 1;
                 const int64_t b = g - T.level_off[lev];

@@ -802,11 +802,16 @@ void Operator::init(const double* srcs, int64_t ns, const double* tgts, int64_t 
     }
     const auto tt1 = std::chrono::steady_clock::now();
     tree_ms_ = std::chrono::duration<double, std::milli>(tt1 - tt0).count();
-    plan_.build_lists(cutoff);
+    // the walk on the GPU unless a cutoff predicate (host code) takes part
+    if (plan_only || cutoff || !plan_.build_lists_gpu())
+        plan_.build_lists(cutoff);
     lists_ms_ = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tt1)
                     .count();
+    const auto tt2 = std::chrono::steady_clock::now();
     plan_.assign_shards(shard_n_);
     plan_.build_target_lists(shard_n_ > 1 ? shard_rank_ : -1);
+    tlists_ms_ = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tt2)
+                     .count();
     if (tol_ > 0) // ifgfoperator.hpp:80-85
     {
         estimate_orders(base_order_);
@@ -866,7 +871,10 @@ void Operator::init(const double* srcs, int64_t ns, const double* tgts, int64_t 
     planned_ = true;
     if (plan_only)
         return;
+    const auto td = std::chrono::steady_clock::now();
     setup_device(normals);
+    device_ms_ = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - td)
+                     .count();
     initialized_ = true;
     init_ms_ = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
 }
@@ -874,6 +882,22 @@ void Operator::init(const double* srcs, int64_t ns, const double* tgts, int64_t 
 void Operator::setup_device(const double* normals)
 {
     DeviceState& D = *dev_;
+    // wall time of the setup phases (after a device synchronise), summed by name
+    dev_phases_.clear();
+    auto tp = std::chrono::steady_clock::now();
+    auto phase = [&](const char* name) {
+        IFGF_CUDA(cudaDeviceSynchronize());
+        const auto now = std::chrono::steady_clock::now();
+        const double ms = std::chrono::duration<double, std::milli>(now - tp).count();
+        tp = now;
+        for (auto& pr : dev_phases_)
+            if (pr.first == name)
+            {
+                pr.second += ms;
+                return;
+            }
+        dev_phases_.push_back({name, ms});
+    };
     D.dgeo32.clear();
     D.dgeo32_ptr.clear();
     D.dgeo_ready = false;
@@ -988,6 +1012,7 @@ void Operator::setup_device(const double* normals)
         D.n_tleaf = (int)ntl;
     }
 
+    phase("boxes_points_lists_upload");
     // ---- active cones (octree.hpp:351-816) on the GPU ----
     int64_t fmap_total = 0;
     for (auto& G : lv_)
@@ -1038,6 +1063,7 @@ void Operator::setup_device(const double* normals)
     D.vgeo32.clear();
     D.vlists.clear();
     std::vector<std::vector<int>> up_host(L);
+    phase("cone_map_alloc");
     // coarse cones each level refines: all of them, or this rank's
     const bool sharded = shard_n_ > 1;
     std::vector<std::vector<int>> c2f_host(L);
@@ -1055,13 +1081,15 @@ void Operator::setup_device(const double* normals)
         const int64_t nfe = (int64_t)G.nf[0] * G.nf[1] * G.nf[2];
         const int64_t ncm = (int64_t)G.nbox * nce, nfm = (int64_t)G.nbox * nfe;
         IFGF_CUDA(cudaMemset(cmark.p, 0, ncm * sizeof(int)));
+        phase("cone_marks");
         // far pairs of this level
         std::vector<int> fs, f0, f1;
         for (int b = 0; b < G.nbox; b++)
         {
             const int64_t g = G.box_off + b;
-            for (int64_t t : plan_.far[g])
+            for (const int32_t* tp = plan_.far.begin(g); tp != plan_.far.end(g); tp++)
             {
+                const int64_t t = *tp;
                 int lev = (int)(std::upper_bound(Tt.level_off.begin(), Tt.level_off.end(), t) -
                                 Tt.level_off.begin()) - 1;
                 int64_t tb = t - Tt.level_off[lev];
@@ -1070,6 +1098,7 @@ void Operator::setup_device(const double* normals)
                 f1.push_back((int)Tt.levels[lev].last[tb]);
             }
         }
+        phase("far_pairs_host");
         if (!fs.empty())
         {
             DevBuf<int> dfs, df0, df1;
@@ -1089,6 +1118,7 @@ void Operator::setup_device(const double* normals)
             IFGF_CUDA(cudaGetLastError());
             IFGF_CUDA(cudaDeviceSynchronize());
         }
+        phase("mark_far_parent_kernels");
         // compaction
         auto compact = [&](int* map, int64_t n, int64_t n_el, int gbase, DevBuf<int>& lbox,
                            DevBuf<int>& lel) -> int64_t {
@@ -1118,6 +1148,7 @@ void Operator::setup_device(const double* normals)
         fine_tot += G.n_fine;
         if (fine_tot > (1ll << 31) - 1)
             throw Error(ERR_OOM, "too many active fine cones");
+        phase("compaction");
         // leaf / non-leaf partition of the coarse cones and the work counts
         // of the flop model
         std::vector<int> lidx, uidx;
@@ -1149,6 +1180,7 @@ void Operator::setup_device(const double* normals)
         }
         D.leaf_idx[l].upload(lidx);
         up_host[l] = std::move(uidx);
+        phase("cone_partition_host");
     }
     // Upward transfer: order each level's cones of non-leaf boxes by element
     // (stable, so boxes stay ordered within an element), give every distinct
@@ -1193,9 +1225,11 @@ void Operator::setup_device(const double* normals)
             drow.alloc((size_t)ns * 16);
             std::vector<int> hrow((size_t)ns * 16);
             int pad = 0, runs = 0;
+            phase("upward_slots_host");
             IFGF_DISPATCH(kind_, pad = upgeo_row_max<KK>(lv_[l], lv_[l + 1], pH, cH, doff.p,
                                                           dslot_el.p, ns, D.hi_nodes.p, P_hi, kp,
                                                           drow.p, hrow.data(), &runs));
+            phase("upward_row_measure");
             up_pad[l] = pad;
             fe_pad_[l] = runs;
             {
@@ -1218,6 +1252,7 @@ void Operator::setup_device(const double* normals)
                         }
                 }
             }
+            phase("upward_stats_host");
             D.fe_list[l].alloc((size_t)ns * 8 * (runs + 1)); // runs and a sentinel per row
             IFGF_CUDA(cudaMemset(D.fe_list[l].p, 0xff, D.fe_list[l].n * sizeof(int2)));
             const size_t n_ent = (size_t)ns * 8 * (size_t)std::max(pad, 1);
@@ -1232,10 +1267,12 @@ void Operator::setup_device(const double* normals)
                                                          D.fe_list[l].p));
             IFGF_CUDA(cudaDeviceSynchronize());
             upgeo_bytes_ += (double)n_ent * (sizeof(UpGeo64) + sizeof(UpGeo32));
+            phase("upward_table_build");
         }
         D.up_idx[l].upload(uidx);
         D.up_slot[l].upload(slot_of);
     }
+    phase("upward_uploads");
     D.lists.assign(L, LevelLists{});
     for (int l = 0; l < L; l++)
     {
@@ -1272,6 +1309,7 @@ void Operator::setup_device(const double* normals)
     D.c2f_smem = (P_hi + sz2 + (size_t)F0 * F1 * hi_[2]) * sizeof(double2);
     if (D.c2f_smem > 220 * 1024)
         throw Error(ERR_INVALID, "interpolation order too high for the coarse-to-fine kernel");
+    phase("buffers");
 }
 
 // CUDA-event timing of every launch, used when profiling is on.
@@ -2112,7 +2150,11 @@ std::string Operator::stats_json() const
     o << "]"
       << ",\"target_leaves\":" << dev_->n_tleaf << ",\"missing_cone_lookups\":" << missing_
       << ",\"init_ms\":" << init_ms_ << ",\"init_tree_ms\":" << tree_ms_
-      << ",\"init_lists_ms\":" << lists_ms_ << ",\"launches_per_mult\":" << launches_per_mult_
+      << ",\"init_lists_ms\":" << lists_ms_ << ",\"init_target_lists_ms\":" << tlists_ms_
+      << ",\"init_device_ms\":" << device_ms_ << ",\"init_device_phases_ms\":{";
+    for (size_t i = 0; i < dev_phases_.size(); i++)
+        o << (i ? "," : "") << "\"" << dev_phases_[i].first << "\":" << dev_phases_[i].second;
+    o << "},\"launches_per_mult\":" << launches_per_mult_
       << ",\"batch_planes\":" << dev_->b_planes
       << ",\"last_mult_ms\":{\"permute\":" << last_.permute << ",\"leaf_sample\":" << last_.coarse
       << ",\"upward\":" << last_.upward << ",\"coarse_to_fine\":" << last_.c2f

@@ -155,7 +155,8 @@ class Operator
     std::unique_ptr<AdjointState> adj_;
     int shard_rank_ = 0, shard_n_ = 1;
     // statistics
-    double init_ms_ = 0, tree_ms_ = 0, lists_ms_ = 0;
+    double init_ms_ = 0, tree_ms_ = 0, lists_ms_ = 0, tlists_ms_ = 0, device_ms_ = 0;
+    std::vector<std::pair<std::string, double>> dev_phases_; // setup_device phases (ms)
     StageTimes last_;
     int64_t n_coarse_total_ = 0, n_fine_total_ = 0;
     double leaf_evals_ = 0, upward_evals_ = 0;

@@ -219,6 +219,8 @@ struct Walker
     Plan& P;
     const std::function<bool(double)>& cutoff;
     const double eta = std::sqrt(3.0);
+    // (source, target) global box ids of the far and near pairs, in discovery order
+    std::vector<int32_t> fs, ft, ns, nt;
 
     // Octree::buildInteractionList (octree.hpp:272-349)
     void walk(int sl, int32_t s, int tl, int32_t t)
@@ -256,7 +258,8 @@ struct Walker
                 P.n_dropped++;
                 return;
             }
-            P.far[sg].push_back(tg);
+            fs.push_back((int32_t)sg);
+            ft.push_back((int32_t)tg);
             P.n_far_pairs++;
             P.far_target_evals += TL.last[t] - TL.first[t];
             return;
@@ -264,7 +267,8 @@ struct Walker
         const bool sleaf = SL.leaf[s], tleaf = TL.leaf[t];
         if (sleaf && tleaf)
         {
-            P.near[sg].push_back(tg);
+            ns.push_back((int32_t)sg);
+            nt.push_back((int32_t)tg);
             P.n_near_pairs++;
             P.near_point_pairs += (SL.last[s] - SL.first[s]) * (TL.last[t] - TL.first[t]);
             return;
@@ -291,16 +295,29 @@ struct Walker
 };
 } // namespace
 
+void PairLists::from_pairs(int64_t n_src_boxes, const std::vector<int32_t>& s,
+                           const std::vector<int32_t>& t)
+{
+    off.assign(n_src_boxes + 1, 0);
+    for (int32_t x : s)
+        off[x + 1]++;
+    for (int64_t i = 0; i < n_src_boxes; i++)
+        off[i + 1] += off[i];
+    tgt.resize(t.size());
+    std::vector<int64_t> at(off.begin(), off.end() - 1);
+    for (size_t i = 0; i < s.size(); i++)
+        tgt[at[s[i]]++] = t[i];
+}
+
 void Plan::build_lists(const std::function<bool(double)>& cutoff)
 {
     const int64_t nb = src.num_boxes_total();
-    far.assign(nb, {});
-    near.assign(nb, {});
     n_far_pairs = n_near_pairs = n_dropped = far_target_evals = near_point_pairs = 0;
-    if (src.n == 0 || tgt.n == 0)
-        return;
     Walker w{*this, cutoff};
-    w.walk(0, 0, 0, 0);
+    if (src.n > 0 && tgt.n > 0)
+        w.walk(0, 0, 0, 0);
+    far.from_pairs(nb, w.fs, w.ft);
+    near.from_pairs(nb, w.ns, w.nt);
 }
 
 void Plan::assign_shards(int nranks)
@@ -313,7 +330,7 @@ void Plan::assign_shards(int nranks)
     {
         bool any = false;
         for (size_t b = 0; b < src.levels[l].size() && !any; b++)
-            any = !far[src.level_off[l] + (int64_t)b].empty();
+            any = far.count(src.level_off[l] + (int64_t)b) > 0;
         if (any)
         {
             shard_level = l;
@@ -337,10 +354,10 @@ void Plan::assign_shards(int nranks)
         {
             const int64_t g = src.level_off[l] + (int64_t)b;
             const double ns = (double)(src.levels[l].last[b] - src.levels[l].first[b]);
-            for (int64_t t : near[g])
-                work[g] += ns * tsize(t);
-            for (int64_t t : far[g])
-                work[g] += 20.0 * tsize(t);
+            for (const int32_t* t = near.begin(g); t != near.end(g); t++)
+                work[g] += ns * tsize(*t);
+            for (const int32_t* t = far.begin(g); t != far.end(g); t++)
+                work[g] += 20.0 * tsize(*t);
             if (l > 0)
                 work[src.level_off[l - 1] + src.levels[l].parent[b]] += work[g];
         }
@@ -373,17 +390,28 @@ void Plan::assign_shards(int nranks)
 void Plan::build_target_lists(int rank)
 {
     const int64_t ntb = tgt.num_boxes_total();
-    std::vector<std::vector<int32_t>> far_in(ntb), near_in(ntb);
     const int64_t nsb = src.num_boxes_total();
-    for (int64_t s = 0; s < nsb; s++)
-    {
-        if (rank >= 0 && box_rank[s] != rank)
-            continue;
-        for (int64_t t : far[s])
-            far_in[t].push_back((int32_t)s);
-        for (int64_t t : near[s])
-            near_in[t].push_back((int32_t)s);
-    }
+    // transpose to per-target CSR (sources ascending), counting sort
+    auto transpose = [&](const PairLists& in, std::vector<int64_t>& off,
+                         std::vector<int32_t>& srcs) {
+        off.assign(ntb + 1, 0);
+        for (int64_t s = 0; s < nsb; s++)
+            if (rank < 0 || box_rank[s] == rank)
+                for (const int32_t* t = in.begin(s); t != in.end(s); t++)
+                    off[*t + 1]++;
+        for (int64_t i = 0; i < ntb; i++)
+            off[i + 1] += off[i];
+        srcs.resize(off[ntb]);
+        std::vector<int64_t> at(off.begin(), off.end() - 1);
+        for (int64_t s = 0; s < nsb; s++)
+            if (rank < 0 || box_rank[s] == rank)
+                for (const int32_t* t = in.begin(s); t != in.end(s); t++)
+                    srcs[at[*t]++] = (int32_t)s;
+    };
+    std::vector<int64_t> fin_off, nin_off;
+    std::vector<int32_t> fin, nin;
+    transpose(far, fin_off, fin);
+    transpose(near, nin_off, nin);
     tleaf_gid.clear();
     tleaf_far_off.assign(1, 0);
     tleaf_near_off.assign(1, 0);
@@ -404,14 +432,14 @@ void Plan::build_target_lists(int rank)
             while (al >= 0)
             {
                 const int64_t ag = tgt.level_off[al] + ab;
-                for (int32_t s : far_in[ag])
-                    tleaf_far_src.push_back(s);
+                tleaf_far_src.insert(tleaf_far_src.end(), fin.begin() + fin_off[ag],
+                                     fin.begin() + fin_off[ag + 1]);
                 ab = tgt.levels[al].parent[ab];
                 al--;
             }
             tleaf_far_off.push_back((int64_t)tleaf_far_src.size());
-            for (int32_t s : near_in[g])
-                tleaf_near_src.push_back(s);
+            tleaf_near_src.insert(tleaf_near_src.end(), nin.begin() + nin_off[g],
+                                  nin.begin() + nin_off[g + 1]);
             tleaf_near_off.push_back((int64_t)tleaf_near_src.size());
         }
     }

@@ -60,11 +60,24 @@ struct Tree
     static void child_box(const TreeLevel& L, size_t b, int j, double* cmn, double* cmx);
 };
 
+// Interaction lists in CSR form: the target boxes (global ids) of source
+// box s (global id) are tgt[off[s] .. off[s + 1]), in discovery order.
+struct PairLists
+{
+    std::vector<int64_t> off;
+    std::vector<int32_t> tgt;
+    int64_t count(int64_t s) const { return off[s + 1] - off[s]; }
+    const int32_t* begin(int64_t s) const { return tgt.data() + off[s]; }
+    const int32_t* end(int64_t s) const { return tgt.data() + off[s + 1]; }
+    // CSR from pairs listed in discovery order (stable in each source box)
+    void from_pairs(int64_t n_src_boxes, const std::vector<int32_t>& s,
+                    const std::vector<int32_t>& t);
+};
+
 struct Plan
 {
     Tree src, tgt;
-    // per source box (global id): target boxes (global ids) in discovery order
-    std::vector<std::vector<int64_t>> far, near;
+    PairLists far, near;
     // target-leaf-centric lists for the evaluation kernel
     std::vector<int64_t> tleaf_gid;       // target leaves (global target box ids)
     std::vector<int64_t> tleaf_far_off;   // CSR offsets into tleaf_far_src
@@ -84,6 +97,10 @@ struct Plan
     std::vector<int32_t> box_rank;
 
     void build_lists(const std::function<bool(double)>& cutoff);
+    // The same lists (same order) from the dual-tree walk on the GPU, without
+    // a cutoff predicate; false when the trees are too deep for its path keys
+    // (the caller then walks on the host).
+    bool build_lists_gpu();
     void assign_shards(int nranks);
     // target-leaf lists of the sources owned by `rank` (all when rank < 0)
     void build_target_lists(int rank = -1);

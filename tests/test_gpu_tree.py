@@ -49,3 +49,27 @@ def test_gpu_octree_equals_host_octree(name, pts, leaf):
             assert np.array_equal(gb, hb), (which, lvl)
     st = gpu.stats()
     assert st["init_tree_ms"] >= 0.0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,pts,leaf", _sets(), ids=lambda v: v if isinstance(v, str) else "")
+def test_gpu_interaction_lists_equal_host_lists(name, pts, leaf):
+    """The dual-tree walk on the GPU gives every source box the host walker's
+    far and near lists, in the same (discovery) order, and the same pair
+    counts."""
+    import ifgf_b200 as G
+
+    tg = W.sphere_points(5000, seed=3) * 1.5
+    gpu = G.HelmholtzIfgfOperator(5.0, leaf, 8)
+    gpu.init(pts, tg)
+    host = G.HelmholtzIfgfOperator(5.0, leaf, 8)
+    host.init_plan_only(pts, tg)
+    sg, sh = gpu.stats(), host.stats()
+    for key in ("near_pairs", "far_pairs", "near_point_pairs", "far_target_evals"):
+        assert sg[key] == sh[key], key
+    for lvl in range(host.levels(0)):
+        for box in range(host.num_boxes(lvl, 0)):
+            for far in (0, 1):
+                a = gpu.interaction_list(lvl, box, far)
+                b = host.interaction_list(lvl, box, far)
+                assert np.array_equal(a, b), (lvl, box, far)
