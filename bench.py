@@ -472,7 +472,10 @@ def run_ours(a):
     if ws == 1:
         # the reference-facing call: host arrays in, host arrays out
         def e2e_step():
-            un[:] = op.mult_batch(wn) if batch > 1 else op.mult(wn[0])
+            if batch > 1:
+                op.mult_batch(wn, out=un)
+            else:
+                op.mult(wn[0], out=un[0])
         ds = torch.cuda.default_stream()
     else:
         # per rank: pinned host densities to the GPU, its share, the

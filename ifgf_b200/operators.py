@@ -131,21 +131,33 @@ class IfgfOperator:
     def _dtype(self):
         return np.float64 if self.REAL else np.complex128
 
-    def mult(self, weights):
+    def _out(self, out, shape):
+        """The result array: a new one, or `out` when it fits (C-contiguous,
+        the operator's dtype and the result's shape) -- e.g. pinned host
+        memory, which the device-to-host copy then fills directly."""
+        if out is None:
+            return np.empty(shape, dtype=self._dtype())
+        if (not isinstance(out, np.ndarray) or out.shape != shape or out.dtype != self._dtype()
+                or not out.flags.c_contiguous):
+            raise ValueError(f"out must be a C-contiguous {self._dtype().__name__} array of "
+                             f"shape {shape}")
+        return out
+
+    def mult(self, weights, out=None):
         """IfgfOperator::mult (ifgfoperator.hpp:246-867)."""
         w = np.ascontiguousarray(np.asarray(weights, dtype=self._dtype()))
         if w.shape != (self._n_src,):
             raise ValueError(f"weights must have shape ({self._n_src},), got {w.shape}")
-        u = np.empty(self._n_tgt, dtype=self._dtype())
+        u = self._out(out, (self._n_tgt,))
         check(lib.ifgf_mult(self._h, w.ctypes.data, u.ctypes.data))
         return u
 
-    def mult_batch(self, weights):
-        """A . w for every row of a (batch, N) array."""
+    def mult_batch(self, weights, out=None):
+        """A . w for every row of a (batch, N) array (into `out` when given)."""
         w = np.ascontiguousarray(np.asarray(weights, dtype=self._dtype()))
         if w.ndim != 2 or w.shape[1] != self._n_src:
             raise ValueError("weights must have shape (batch, N)")
-        u = np.empty((w.shape[0], self._n_tgt), dtype=self._dtype())
+        u = self._out(out, (w.shape[0], self._n_tgt))
         check(lib.ifgf_mult_batch(self._h, w.ctypes.data, u.ctypes.data, w.shape[0]))
         return u
 

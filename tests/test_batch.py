@@ -91,3 +91,24 @@ def test_batch_planes_follow_a_reinitialised_tree():
     ug, uf = g.mult_batch(w), fresh.mult_batch(w)
     for b in range(5):
         assert rel2(ug[b], uf[b]) <= 1e-14, b
+
+
+@pytest.mark.gpu
+def test_results_into_caller_arrays():
+    # out= writes into the caller's (here pinned) arrays, as a new array would
+    import torch
+
+    n = 4000
+    pts = W.sphere_points(n, seed=0)
+    g = make_gpu_op("helmholtz", leaf=50, order=8)
+    g.init(pts, pts)
+    g.set_precision("mixed")
+    w = np.stack([densities_for("helmholtz", n, seed=b) for b in range(6)])
+    pinned = torch.empty((6, n), dtype=torch.complex128).pin_memory().numpy()
+    assert g.mult_batch(w, out=pinned) is pinned
+    assert np.array_equal(pinned, g.mult_batch(w))
+    one = np.empty(n, dtype=np.complex128)
+    assert g.mult(w[0], out=one) is one
+    assert np.array_equal(one, g.mult(w[0]))
+    with pytest.raises(ValueError):
+        g.mult_batch(w, out=np.empty((6, n), dtype=np.complex64))
