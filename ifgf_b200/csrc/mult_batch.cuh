@@ -314,7 +314,7 @@ __global__ void __launch_bounds__(EVAL_THREADS) near_batch_kernel(EvalArgs a, Ba
 // once per plane); each plane's Chebyshev sum uses its own coefficient block.
 // Adds the near sums and writes the caller's result planes (the first nrhs).
 template <int KIND, int N0, int N1, int N2, bool MK>
-__global__ void __launch_bounds__(EVAL_THREADS, 4) far_batch_kernel(EvalArgs a, BatchPtrs bp)
+__global__ void __launch_bounds__(FAR_THREADS, 2) far_batch_kernel(EvalArgs a, BatchPtrs bp)
 {
     constexpr int NB = BATCH_NB;
     __shared__ KParams kps[MK ? NB : 1];
@@ -322,20 +322,20 @@ __global__ void __launch_bounds__(EVAL_THREADS, 4) far_batch_kernel(EvalArgs a, 
     if constexpr (MK)
         if (threadIdx.x < NB)
             kps[threadIdx.x] = bp.kp_plane[pb + threadIdx.x]; // read after the chunk barriers
-    __shared__ double fcx[EVAL_THREADS], fcy[EVAL_THREADS], fcz[EVAL_THREADS], fH[EVAL_THREADS];
-    __shared__ long long ffm[EVAL_THREADS];
-    __shared__ int flev[EVAL_THREADS];
+    __shared__ double fcx[FAR_THREADS], fcy[FAR_THREADS], fcz[FAR_THREADS], fH[FAR_THREADS];
+    __shared__ long long ffm[FAR_THREADS];
+    __shared__ int flev[FAR_THREADS];
     __shared__ LookupF lfs[MAX_LEVELS];
-    __shared__ double rr[NB][EVAL_THREADS], ri[NB][EVAL_THREADS];
+    __shared__ double rr[NB][FAR_THREADS], ri[NB][FAR_THREADS];
     for (int l = threadIdx.x; l < a.L; l += blockDim.x)
         make_lookupf(a.lv[l], lfs[l]); // read after the first chunk's barriers
     const int tl = blockIdx.x;
     const int tf = a.tl_first[tl], tlast = a.tl_last[tl];
     const long long fb0 = a.far_off[tl], fb1 = a.far_off[tl + 1];
-    for (int base = tf; base < tlast; base += EVAL_THREADS)
+    for (int base = tf; base < tlast; base += FAR_THREADS)
     {
-        const int cnt = min(EVAL_THREADS, tlast - base);
-        const int S = EVAL_THREADS / cnt;
+        const int cnt = min(FAR_THREADS, tlast - base);
+        const int S = FAR_THREADS / cnt;
         const int ti = threadIdx.x % cnt, si = threadIdx.x / cnt;
         const bool active = si < S;
         const int t = base + ti;
@@ -344,9 +344,9 @@ __global__ void __launch_bounds__(EVAL_THREADS, 4) far_batch_kernel(EvalArgs a, 
 #pragma unroll
         for (int r = 0; r < NB; r++)
             accr[r] = acci[r] = 0.0;
-        for (long long e0 = fb0; e0 < fb1; e0 += EVAL_THREADS)
+        for (long long e0 = fb0; e0 < fb1; e0 += FAR_THREADS)
         {
-            const int fcnt = (int)min((long long)EVAL_THREADS, fb1 - e0);
+            const int fcnt = (int)min((long long)FAR_THREADS, fb1 - e0);
             __syncthreads();
             if (threadIdx.x < fcnt)
             {
@@ -610,7 +610,7 @@ static int run_mult_batch(const MultPtrs& m, const BatchPtrs& bp, const void* d_
             if (hk)
                 hk->begin(PROF_EVAL);
             far_batch_kernel<KIND, N0, N1, N2, MK>
-                <<<dim3(m.n_tleaf, bp.groups), EVAL_THREADS, 0, st>>>(ea, bp);
+                <<<dim3(m.n_tleaf, bp.groups), FAR_THREADS, 0, st>>>(ea, bp);
             IFGF_CHECK_LAUNCH();
             if (hk)
                 hk->end();
