@@ -512,7 +512,7 @@ def run_ours(a):
     traffic = None
     if precision == "mixed" and batch > 1:
         traffic = {"upward": 19.1 * entries,
-                   "target_eval": 62.0 * stats["far_target_evals"]}.get(dom)
+                   "target_eval": 55.5 * stats["far_target_evals"]}.get(dom)
     roof = {"kernel": dom, "bound": "fp64" if precision == "fp64" else "fp32",
             "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
             "traffic": traffic,
