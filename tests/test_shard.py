@@ -120,3 +120,28 @@ def test_shards_sum_to_the_matvec_on_one_gpu(name, nranks):
     o = make_oracle_op(name, leaf=50, order=8)
     init_op(o, name, pts, pts)
     assert rel2(sum(parts), o.mult(w)) <= 1e-12
+
+
+@pytest.mark.gpu
+def test_sharded_mixed_batches_sum_to_the_batch():
+    # the path of bench.py --gpus N: every rank runs the batched mixed
+    # pipeline (two plane groups here) over its subtrees
+    from .helpers import make_gpu_op
+
+    n = 20000
+    pts = W.sphere_points(n, seed=0)
+    w = np.stack([densities_for("helmholtz", n, seed=s) for s in range(5)])
+    full = make_gpu_op("helmholtz", leaf=50, order=8)
+    full.init(pts, pts)
+    full.set_precision("mixed")
+    uf = full.mult_batch(w)
+    total = np.zeros_like(uf)
+    for r in range(3):
+        g = make_gpu_op("helmholtz", leaf=50, order=8)
+        g.set_shard(r, 3)
+        g.init(pts, pts)
+        g.set_precision("mixed")
+        total += g.mult_batch(w)
+        assert g.stats()["missing_cone_lookups"] == 0
+    for b in range(5):
+        assert rel2(total[b], uf[b]) <= 1e-6, b
