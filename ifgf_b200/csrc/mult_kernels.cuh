@@ -804,7 +804,8 @@ template <int N0, int N1, bool SHARED = false> struct CoefRows
     }
 };
 
-template <int N0, int N1, int N2> struct ChebF
+// SHARED: c points into shared memory (plain loads); else read-only global.
+template <int N0, int N1, int N2, bool SHARED = false> struct ChebF
 {
     __device__ static __forceinline__ cplx<float> eval(const float2* __restrict__ c, const float* x,
                                                        const int*)
@@ -835,7 +836,7 @@ template <int N0, int N1, int N2> struct ChebF
             for (int j = 0; j < N1; j += CoefRows<N0, N1>::ROWS)
             {
                 float2 v[CoefRows<N0, N1>::ROWS * N0];
-                CoefRows<N0, N1>::load(c + N0 * (j + N1 * k), v);
+                CoefRows<N0, N1, SHARED>::load(c + N0 * (j + N1 * k), v);
 #pragma unroll
                 for (int jj = 0; jj < CoefRows<N0, N1>::ROWS; jj++)
                 {
@@ -857,7 +858,7 @@ template <int N0, int N1, int N2> struct ChebF
     }
 };
 
-template <> struct ChebF<0, 0, 0>
+template <> struct ChebF<0, 0, 0, false>
 {
     __device__ static __forceinline__ cplx<float> eval(const float2* __restrict__ c, const float* x,
                                                        const int* n)
