@@ -2111,6 +2111,8 @@ inline int node_chunks(int P_hi)
     return (P_hi + per - 1) / per;
 }
 
+#include "far_staged.cuh"
+
 template <int KIND, int N0, int N1, int N2, bool MIXED>
 static int run_mult(const MultPtrs& m, const void* d_w, void* d_u, bool real, cudaStream_t st,
                     LaunchHooks* hk)
