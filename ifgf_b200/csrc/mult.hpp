@@ -39,14 +39,17 @@ struct SrcArgs
 // Each (slot, octant) row is sorted by child element, so that the threads of
 // a warp gather the same cone's coefficients; `node` is the parent node the
 // entry belongs to.
-struct UpGeo64
+// 16-byte aligned, so that an entry loads as whole 16-byte vectors (a
+// warp reading consecutive entries touches each sector once, not once per
+// field)
+struct __align__(16) UpGeo64
 {
     double loc[3];
     double tr, ti;
     int fe;
     int node;
 };
-struct UpGeo32
+struct __align__(16) UpGeo32
 {
     float loc[3];
     float tr, ti;
@@ -54,6 +57,7 @@ struct UpGeo32
     int node;
     int pad;
 };
+static_assert(sizeof(UpGeo64) == 48 && sizeof(UpGeo32) == 32, "table entry sizes");
 
 // Per-level device lists of one operator.
 struct LevelLists
