@@ -522,6 +522,17 @@ def run_ours(a):
             "launches_per_step": kernels[dom]["launches"] / max(prof["mults"], 1) * batch,
             "ms_per_matvec": per_mult_ms,
             "model": "survey flop model: transcendental = 1 flop, FMA = 2; per matvec"}
+    # the same kernel against the measured HBM copy rate: how far it is from
+    # being memory-bound
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            hbm = float(json.load(f)["hbm_gbs"])
+    except (OSError, KeyError, ValueError):
+        hbm = None
+    if traffic is not None and hbm:
+        bw = traffic / (per_mult_ms * 1e-3) / 1e9
+        roof["hbm"] = {"achieved": bw, "peak": hbm, "unit": "GB/s", "frac": bw / hbm,
+                       "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"}
     breakdown = {k: v["ms"] / max(prof["mults"], 1) for k, v in kernels.items()}
     breakdown["serialised_total"] = sum(breakdown.values())
     per_level = {k: [round(x / max(prof["mults"], 1), 3) for x in v["level_ms"]]
