@@ -151,13 +151,16 @@ __global__ void __launch_bounds__(FAR_THREADS, 2) far_batch_kernel(EvalArgs a, B
                     hkey[tab ^ 1][q] = -1;
                 if (threadIdx.x == 0)
                     nslot[tab ^ 1] = 0;
-                for (int q = threadIdx.x; q < ns * NB * CPP; q += blockDim.x)
+                // one warp per slot, lanes over the slot's 16-byte chunks
+                for (int k = threadIdx.x >> 5; k < ns; k += FAR_THREADS / 32)
                 {
-                    const int k = q / (NB * CPP), rem = q - k * (NB * CPP);
-                    const int r = rem / CPP, ch = rem - r * CPP;
-                    cp_async16(far_sh + (size_t)k * SS + r * P_LO + 2 * ch,
-                               bp.fcoef + (size_t)(pb + r) * bp.fc_plane + (size_t)sgf[k] * P_LO +
-                                   2 * ch);
+                    const float2* src0 = bp.fcoef + (size_t)pb * bp.fc_plane + (size_t)sgf[k] * P_LO;
+                    float2* dst0 = far_sh + (size_t)k * SS;
+#pragma unroll
+                    for (int r = 0; r < NB; r++)
+                        for (int ch = threadIdx.x & 31; ch < CPP; ch += 32)
+                            cp_async16(dst0 + r * P_LO + 2 * ch,
+                                       src0 + (size_t)r * bp.fc_plane + 2 * ch);
                 }
                 cp_async_wait_all();
                 __syncthreads(); // blocks staged
