@@ -137,7 +137,8 @@ def dist_init():
         import torch.distributed as dist
 
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        # short, so that ranks waiting on a failed one end with an error
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180))
     return ws, rank, local
 
 
@@ -246,7 +247,9 @@ def cpu_sample_ms(op, sample, w, threads):
 # arms
 # ---------------------------------------------------------------------------
 def run_reference(a):
-    ws, rank, _ = dist_init()
+    # CPU only: rank 0 runs the sample, the other ranks exit without work
+    # (no process group: the arm has no collective)
+    rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     pts = W.ellipsoid_points(a.n, seed=0)
