@@ -131,3 +131,28 @@ def test_multi_wavenumber_rejects_other_cone_grids():
     w = np.stack([W.densities(n, seed=1)] * 2)
     with pytest.raises(Exception, match="cone grids"):
         op.mult_wavenumbers([20.5, 60.0], w)
+
+
+@pytest.mark.gpu
+def test_multi_wavenumber_device_entry_point():
+    # device buffers on a torch stream give the host-buffer call's result
+    import torch
+
+    import ifgf_b200 as G
+
+    n = 8000
+    pts = W.sphere_points(n, seed=0)
+    ks = cq_wavenumbers()[:6]
+    w = np.stack([W.densities(n, seed=30 + l) for l in range(len(ks))])
+    op = G.ModifiedHelmholtzIfgfOperator(ks[0], 100, 8)
+    op.init(pts, pts)
+    op.set_precision("mixed")
+    uh = op.mult_wavenumbers(ks, w)
+    dw = torch.from_numpy(w).cuda()
+    du = torch.empty_like(dw)
+    op.mult_wavenumbers_device(ks, dw.data_ptr(), du.data_ptr(),
+                               torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    ud = du.cpu().numpy()
+    for l in range(len(ks)):
+        assert rel2(ud[l], uh[l]) <= 1e-14, l
