@@ -145,3 +145,96 @@ def test_sharded_mixed_batches_sum_to_the_batch():
         assert g.stats()["missing_cone_lookups"] == 0
     for b in range(5):
         assert rel2(total[b], uf[b]) <= 1e-6, b
+
+
+def test_plane_shares_partition_every_batch():
+    from ifgf_b200.distributed import plane_range
+
+    for world in range(1, 6):
+        for n in range(0, 23):
+            shares = [plane_range(n, r, world) for r in range(world)]
+            assert shares[0][0] == 0 and shares[-1][1] == n
+            for (a, b), (c, d) in zip(shares, shares[1:]):
+                assert b == c  # contiguous, in rank order
+            sizes = [b - a for a, b in shares]
+            assert max(sizes) - min(sizes) <= 1
+
+
+def _gloo_planes(rank, world, port, n, out_dir):
+    import torch
+    import torch.distributed as dist
+
+    from ifgf_b200.distributed import PlaneParallel
+
+    class Stub(PlaneParallel):
+        # stands in for the GPU matvec: row p of the result is (1 + 2i) w_p + p
+        def _apply_batch(self, w_rows, u_rows):
+            lo, _ = self.share(n)
+            rows = torch.arange(lo, lo + w_rows.shape[0], dtype=torch.float64)[:, None]
+            u_rows[:] = (1 + 2j) * w_rows + rows
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        w = torch.from_numpy(np.stack([densities_for("helmholtz", 50, seed=s) for s in range(n)]))
+        u = torch.zeros_like(w)
+        pp = Stub(op=None)
+        pp.mult_batch_device(w, u)
+        pp.gather(u)
+        np.save(os.path.join(out_dir, f"p{rank}.npy"), u.numpy())
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world,n", [(2, 7), (3, 5)])
+def test_gloo_plane_parallel_gathers_every_share(tmp_path, world, n):
+    import torch.multiprocessing as mp
+
+    port = _free_port()
+    mp.start_processes(_gloo_planes, args=(world, port, n, str(tmp_path)), nprocs=world,
+                       join=True, start_method="spawn")
+    w = np.stack([densities_for("helmholtz", 50, seed=s) for s in range(n)])
+    want = (1 + 2j) * w + np.arange(n)[:, None]
+    for r in range(world):
+        assert np.allclose(np.load(tmp_path / f"p{r}.npy"), want, rtol=0, atol=1e-12), r
+
+
+@pytest.mark.gpu
+def test_plane_parallel_and_sharded_batches_on_one_gpu():
+    # one-rank NCCL group: both modes give the plain batched matvec
+    import torch
+    import torch.distributed as dist
+
+    from ifgf_b200.distributed import PlaneParallel, ShardedOperator
+
+    from .helpers import make_gpu_op
+
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{_free_port()}", rank=0,
+                            world_size=1)
+    try:
+        n = 6000
+        pts = W.sphere_points(n, seed=0)
+        w = np.stack([densities_for("helmholtz", n, seed=s) for s in range(5)])
+        full = make_gpu_op("helmholtz", leaf=50, order=8)
+        full.init(pts, pts)
+        full.set_precision("mixed")
+        uf = full.mult_batch(w)
+        dw = torch.from_numpy(w).cuda()
+        du = torch.zeros_like(dw)
+        pp = PlaneParallel(full)
+        pp.mult_batch_device(dw, du)
+        pp.gather(du)
+        torch.cuda.synchronize()
+        up = du.cpu().numpy()
+        sh = ShardedOperator(make_gpu_op("helmholtz", leaf=50, order=8), pts, pts)
+        sh.op.set_precision("mixed")
+        ds = torch.zeros_like(dw)
+        sh.mult_batch_device(dw, ds)
+        torch.cuda.synchronize()
+        us = ds.cpu().numpy()
+        for b in range(5):
+            assert rel2(up[b], uf[b]) <= 1e-14, b
+            assert rel2(us[b], uf[b]) <= 1e-14, b
+    finally:
+        dist.destroy_process_group()
