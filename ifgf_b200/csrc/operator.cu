@@ -136,6 +136,10 @@ struct DeviceState
     DevBuf<double> io_w, io_u; // staging for host-buffer mult
     std::vector<cudaEvent_t> prof_ev;
     cudaStream_t side = nullptr; // near-field stream
+    // pipelined host-buffer batches: compute, upload and download streams,
+    // and two events per group of right-hand sides
+    cudaStream_t io_cs = nullptr, io_up = nullptr, io_down = nullptr;
+    std::vector<cudaEvent_t> io_ev;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     int n_tleaf = 0;
     size_t c2f_smem = 0;
@@ -149,6 +153,11 @@ struct DeviceState
             cudaEventDestroy(ev_join);
         if (side)
             cudaStreamDestroy(side);
+        for (auto& e : io_ev)
+            cudaEventDestroy(e);
+        for (cudaStream_t st : {io_cs, io_up, io_down})
+            if (st)
+                cudaStreamDestroy(st);
     }
 };
 
@@ -1724,9 +1733,68 @@ void Operator::mult_host(const void* w, void* u, int64_t batch)
             D.io_w.alloc(nw);
         if (D.io_u.n < nu)
             D.io_u.alloc(nu);
-        IFGF_CUDA(cudaMemcpy(D.io_w.p, w, nw * sizeof(double), cudaMemcpyHostToDevice));
-        mult_batch_device(D.io_w.p, D.io_u.p, batch, nullptr);
-        IFGF_CUDA(cudaMemcpy(u, D.io_u.p, nu * sizeof(double), cudaMemcpyDeviceToHost));
+        auto pinned = [](const void* p) {
+            cudaPointerAttributes at;
+            if (cudaPointerGetAttributes(&at, p) != cudaSuccess)
+            {
+                cudaGetLastError();
+                return false;
+            }
+            return at.type == cudaMemoryTypeHost;
+        };
+        if (batch > BATCH_NB && pinned(w) && pinned(u))
+        {
+            // pinned host buffers: groups of BATCH_NB right-hand sides, the
+            // next group's upload and the previous group's download overlap
+            // this group's matvec
+            for (cudaStream_t* st : {&D.io_cs, &D.io_up, &D.io_down})
+                if (!*st)
+                    IFGF_CUDA(cudaStreamCreateWithFlags(st, cudaStreamNonBlocking));
+            // a lone last right-hand side joins the group before it: every
+            // group then runs the batched kernels, with planes grouped as in
+            // a single call (same results)
+            const int64_t ng = batch / BATCH_NB + (batch % BATCH_NB > 1 ? 1 : 0);
+            auto group = [&](int64_t g, int64_t& b0, int64_t& cnt) {
+                b0 = g * BATCH_NB;
+                cnt = g + 1 < ng ? BATCH_NB : batch - b0;
+            };
+            while ((int64_t)D.io_ev.size() < 2 * ng)
+            {
+                cudaEvent_t e;
+                IFGF_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+                D.io_ev.push_back(e);
+            }
+            const size_t pw = per * (size_t)n_src(), pu = per * (size_t)n_tgt();
+            for (int64_t g = 0; g < ng; g++)
+            {
+                int64_t b0, cnt;
+                group(g, b0, cnt);
+                IFGF_CUDA(cudaMemcpyAsync(D.io_w.p + b0 * pw, (const double*)w + b0 * pw,
+                                          cnt * pw * sizeof(double), cudaMemcpyHostToDevice,
+                                          D.io_up));
+                IFGF_CUDA(cudaEventRecord(D.io_ev[2 * g], D.io_up));
+            }
+            for (int64_t g = 0; g < ng; g++)
+            {
+                int64_t b0, cnt;
+                group(g, b0, cnt);
+                IFGF_CUDA(cudaStreamWaitEvent(D.io_cs, D.io_ev[2 * g], 0));
+                mult_batch_device(D.io_w.p + b0 * pw, D.io_u.p + b0 * pu, cnt, D.io_cs);
+                IFGF_CUDA(cudaEventRecord(D.io_ev[2 * g + 1], D.io_cs));
+                IFGF_CUDA(cudaStreamWaitEvent(D.io_down, D.io_ev[2 * g + 1], 0));
+                IFGF_CUDA(cudaMemcpyAsync((double*)u + b0 * pu, D.io_u.p + b0 * pu,
+                                          cnt * pu * sizeof(double), cudaMemcpyDeviceToHost,
+                                          D.io_down));
+            }
+            IFGF_CUDA(cudaStreamSynchronize(D.io_down));
+            IFGF_CUDA(cudaStreamSynchronize(D.io_cs));
+        }
+        else
+        {
+            IFGF_CUDA(cudaMemcpy(D.io_w.p, w, nw * sizeof(double), cudaMemcpyHostToDevice));
+            mult_batch_device(D.io_w.p, D.io_u.p, batch, nullptr);
+            IFGF_CUDA(cudaMemcpy(u, D.io_u.p, nu * sizeof(double), cudaMemcpyDeviceToHost));
+        }
         IFGF_CUDA(cudaMemcpy(&missing_, D.err.p, sizeof(unsigned long long),
                              cudaMemcpyDeviceToHost));
         return;

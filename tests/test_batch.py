@@ -112,3 +112,23 @@ def test_results_into_caller_arrays():
     assert np.array_equal(one, g.mult(w[0]))
     with pytest.raises(ValueError):
         g.mult_batch(w, out=np.empty((6, n), dtype=np.complex64))
+
+
+@pytest.mark.gpu
+def test_pinned_host_batches_are_pipelined_and_equal():
+    # pinned input and output: groups of four overlap their copies with the
+    # matvecs of the neighbouring groups; the result is the same
+    import torch
+
+    n = 5000
+    pts = W.sphere_points(n, seed=0)
+    g = make_gpu_op("helmholtz", leaf=50, order=8)
+    g.init(pts, pts)
+    g.set_precision("mixed")
+    w = np.stack([densities_for("helmholtz", n, seed=40 + b) for b in range(9)])
+    ref = g.mult_batch(w)
+    wp = torch.from_numpy(w).pin_memory().numpy()
+    up = torch.empty((9, n), dtype=torch.complex128).pin_memory().numpy()
+    for _ in range(2):
+        g.mult_batch(wp, out=up)
+        assert np.array_equal(up, ref)
