@@ -326,8 +326,9 @@ static int run_mult_batch(const MultPtrs& m, const BatchPtrs& bp, const void* d_
         {
             const LevelLists& LL = m.lists[l];
             if (LL.n_up > 0 && (LL.fe_pad <= 0 || upward_staged_smem<N0, N1, N2>(
-                                                      m.P_hi, upward_staged_rch<N0, N1, N2>(
-                                                                  LL.fe_pad)) >
+                                                      m.P_hi,
+                                                      upward_staged_rch<N0, N1, N2>(LL.fe_pad),
+                                                      LL.fe_pad) >
                                                       UP_STAGED_SMEM_MAX))
                 return -1;
         }
@@ -444,7 +445,7 @@ static int run_mult_batch(const MultPtrs& m, const BatchPtrs& bp, const void* d_
                 for (int d = 0; d < 3; d++)
                     ua.lo[d] = m.lo[d];
                 ua.kp = m.kp;
-                const size_t sm = upward_staged_smem<N0, N1, N2>(m.P_hi, ua.rch);
+                const size_t sm = upward_staged_smem<N0, N1, N2>(m.P_hi, ua.rch, LL.fe_pad);
                 auto kern = upward_staged_kernel<KIND, N0, N1, N2, MK>;
                 if (sm > 48 * 1024)
                     IFGF_CHECK(cudaFuncSetAttribute(

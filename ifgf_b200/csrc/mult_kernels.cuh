@@ -1366,13 +1366,16 @@ __device__ __forceinline__ void cp_async_wait_all()
     asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
 }
 
-// Shared memory of the staged upward kernel staging rch runs at a time.
+// Shared memory of the staged upward kernel staging rch runs at a time:
+// the parent's accumulators, rch coefficient blocks, and per child the fine
+// cone and first group of each of its fe_pad + 1 run-list entries plus the
+// row's run and group counts.
 template <int N0, int N1, int N2>
-size_t upward_staged_smem(int P_hi, int rch)
+size_t upward_staged_smem(int P_hi, int rch, int fe_pad)
 {
     constexpr int P_LO = N0 * N1 * N2;
     return ((size_t)((P_hi + 1) & ~1) + (size_t)rch * up_block_stride(P_LO)) * sizeof(float2) +
-           (size_t)rch * sizeof(int);
+           ((size_t)16 * (fe_pad + 1) + 16) * sizeof(int);
 }
 
 // Runs staged at a time: all of a row's runs when they fit in about 16 KB
@@ -1393,7 +1396,10 @@ constexpr int UPS_THREADS = 64;
 // memory.  Per child, every run of the (slot, octant) geometry row needs one
 // child fine cone; its block (P_lo coefficients) is copied once into shared
 // memory with cp.async (one warp per block), rch runs at a time, after which
-// the Chebyshev sums of those runs' groups read only shared memory.
+// the Chebyshev sums of those runs' groups read only shared memory.  The
+// fine cones of all eight children's runs are looked up together when the
+// block starts (one pass of independent loads), so a chunk's copies start
+// without a chain of dependent global loads.
 // Compile-time orders only (P_lo even, so that a block is a whole number of
 // 16-byte chunks).
 // MK: every plane (blockIdx.y) has its own wavenumber; the centre-shift
@@ -1409,54 +1415,69 @@ __global__ void __launch_bounds__(UPS_THREADS, 10) upward_staged_kernel(UpArgs a
     extern __shared__ __align__(16) float2 up_sh[];
     float2* acc = up_sh;
     float2* blk = up_sh + ((a.P_hi + 1) & ~1);
-    int* blk_gf = reinterpret_cast<int*>(blk + (size_t)a.rch * BS);
+    const int FL = a.fe_pad + 1;
+    int* run_gf = reinterpret_cast<int*>(blk + (size_t)a.rch * BS); // [8][FL] child fine cone
+    int* run_g = run_gf + 8 * FL;                                   // [8][FL] first group
+    int* row_n = run_g + 8 * FL; // [8] runs of the row, [8] groups of the row
     const int c = a.idx[blockIdx.x];
     const int slot = a.slot[blockIdx.x];
     const int box = a.cc_box[c], el = a.cc_el[c];
     const float2* fcf = reinterpret_cast<const float2*>(a.fcoef) + blockIdx.y * a.fc_plane;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int ngroups = a.P_pad / R;
     for (int n = threadIdx.x; n < a.P_hi; n += blockDim.x)
         acc[n] = make_float2(0.f, 0.f);
+    if (threadIdx.x < 8)
+    {
+        row_n[threadIdx.x] = a.fe_pad;
+        row_n[8 + threadIdx.x] = ngroups;
+    }
+    __syncthreads();
     const LevelGeom& C = a.GC;
     const long long nf = (long long)C.nf[0] * C.nf[1] * C.nf[2];
-    const int ngroups = a.P_pad / R;
+    for (int i = threadIdx.x; i < 8 * FL; i += blockDim.x)
+    {
+        const int o = i / FL, r = i - o * FL;
+        const int cb = a.T.box_child[8 * box + o];
+        const int2 f = a.fe_list[((size_t)slot * 8 + o) * FL + r];
+        run_gf[i] = cb >= 0 && f.x >= 0 ? a.fmap[C.fmap_off + (long long)(cb - C.box_off) * nf + f.x]
+                                        : -1;
+        run_g[i] = f.y;
+        if (f.x < 0 && f.y >= 0)
+        {
+            // the sentinel after the row's last run: (-1, groups of the row)
+            row_n[o] = r;
+            row_n[8 + o] = f.y;
+        }
+    }
+    __syncthreads();
     for (int o = 0; o < 8; o++)
     {
         const int cb = a.T.box_child[8 * box + o];
         if (cb < 0)
             continue;
         const int* fm = a.fmap + C.fmap_off + (long long)(cb - C.box_off) * nf;
-        const int2* fl = a.fe_list + ((size_t)slot * 8 + o) * (a.fe_pad + 1);
+        const int* rgf = run_gf + o * FL;
         const UpGeo32* row = a.geo32 + ((size_t)slot * 8 + o) * a.P_pad;
-        for (int r0 = 0; r0 < a.fe_pad; r0 += a.rch)
+        const int nrun = row_n[o];
+        for (int r0 = 0; r0 < nrun; r0 += a.rch)
         {
-            const int2 first = fl[r0];
-            if (first.x < 0)
-                break; // past the row's last run
-            const int r1 = min(r0 + a.rch, a.fe_pad);
-            // the next run's first group, or the row's end from its sentinel
-            const int2 next = fl[r1];
-            const int g_end = next.y >= 0 ? next.y : ngroups;
+            const int r1 = min(r0 + a.rch, nrun);
+            // the next run's first group, or the row's end
+            const int g_end = r1 < nrun ? run_g[o * FL + r1] : row_n[8 + o];
             __syncthreads(); // the previous runs' blocks are no longer read
             for (int r = r0 + warp; r < r1; r += UPS_THREADS / 32)
             {
-                int gf = -1;
-                if (lane == 0)
-                {
-                    const int fe = fl[r].x;
-                    gf = fe >= 0 ? fm[fe] : -1;
-                    blk_gf[r - r0] = gf;
-                }
-                gf = __shfl_sync(0xffffffffu, gf, 0);
+                const int gf = rgf[r];
                 if (gf < 0)
                     continue;
                 const float2* src = fcf + (size_t)gf * P_LO;
                 float2* dst = blk + (size_t)(r - r0) * BS;
-                for (int ch = lane; ch < CH; ch += 32)
+                for (int ch = threadIdx.x & 31; ch < CH; ch += 32)
                     cp_async16(dst + 2 * ch, src + 2 * ch);
             }
             // the first group's table entries load while the blocks arrive
-            const int g0 = first.y + threadIdx.x;
+            const int g0 = run_g[o * FL + r0] + threadIdx.x;
             UpGeo32 e[R];
             if (g0 < g_end)
             {
@@ -1477,7 +1498,7 @@ __global__ void __launch_bounds__(UPS_THREADS, 10) upward_staged_kernel(UpArgs a
                 if (e[0].fe < 0)
                     continue;
                 const int rl = e[0].pad - r0;
-                if (blk_gf[rl] < 0)
+                if (rgf[r0 + rl] < 0)
                 {
                     // tabulated element inactive in this child: absolute coordinates
                     const double xc[3] = {a.T.box_c[3 * box], a.T.box_c[3 * box + 1],
@@ -2256,7 +2277,7 @@ static int run_mult(const MultPtrs& m, const void* d_w, void* d_u, bool real, cu
             if constexpr (MIXED && N0 > 0 && (N0 * N1 * N2) % 2 == 0)
             {
                 ua.rch = upward_staged_rch<N0, N1, N2>(LL.fe_pad);
-                const size_t sm = upward_staged_smem<N0, N1, N2>(m.P_hi, ua.rch);
+                const size_t sm = upward_staged_smem<N0, N1, N2>(m.P_hi, ua.rch, LL.fe_pad);
                 if (LL.fe_pad > 0 && sm <= UP_STAGED_SMEM_MAX)
                 {
                     auto kern = upward_staged_kernel<KIND, N0, N1, N2>;
