@@ -104,22 +104,33 @@ __global__ void __launch_bounds__(FAR_THREADS, 2) far_batch_kernel(EvalArgs a, B
                 flev[threadIdx.x] = lev;
             }
             __syncthreads();
-            // sub-chunks of S boxes: at most one pair per thread; every
-            // thread runs every sub-chunk (barriers inside)
-            for (int c0 = 0; c0 < fcnt; c0 += S)
-            {
-                const int i = c0 + si;
-                int gf = -1, h = -1;
-                float loc[3] = {0.f, 0.f, 0.f};
-                double d2 = 0.0;
+            // the cone of this thread's pair in sub-chunk box i (gf < 0: none)
+            auto lookup = [&](int i, int& g, float (&l)[3], double& dd) {
+                g = -1;
+                l[0] = l[1] = l[2] = 0.f;
+                dd = 0.0;
                 if (active && i < fcnt)
                 {
                     const int lev = flev[i];
                     const double p[3] = {y0 - fcx[i], y1 - fcy[i], y2 - fcz[i]};
-                    gf = fine_lookup_fast(lfs[lev], a.lv[lev], a.fmap + ffm[i], p, fH[i], loc,
-                                          a.err);
-                    d2 = p[0] * p[0] + p[1] * p[1] + p[2] * p[2];
+                    g = fine_lookup_fast(lfs[lev], a.lv[lev], a.fmap + ffm[i], p, fH[i], l, a.err);
+                    dd = p[0] * p[0] + p[1] * p[1] + p[2] * p[2];
                 }
+            };
+            int gf_next;
+            float loc_next[3];
+            double d2_next;
+            lookup(si, gf_next, loc_next, d2_next);
+            // sub-chunks of S boxes: at most one pair per thread; every
+            // thread runs every sub-chunk (barriers inside).  The next
+            // sub-chunk's lookup (a dependent global load) is issued before
+            // this one's copies are waited for.
+            for (int c0 = 0; c0 < fcnt; c0 += S)
+            {
+                const int gf = gf_next;
+                const float loc[3] = {loc_next[0], loc_next[1], loc_next[2]};
+                const double d2 = d2_next;
+                int h = -1;
                 if (gf >= 0)
                 {
                     // insert the cone, bounded linear probing; the first
@@ -162,6 +173,7 @@ __global__ void __launch_bounds__(FAR_THREADS, 2) far_batch_kernel(EvalArgs a, B
                             cp_async16(dst0 + r * P_LO + 2 * ch,
                                        src0 + (size_t)r * bp.fc_plane + 2 * ch);
                 }
+                lookup(c0 + S + si, gf_next, loc_next, d2_next);
                 cp_async_wait_all();
                 __syncthreads(); // blocks staged
                 if (gf >= 0)
