@@ -19,7 +19,7 @@
 //   * the reference's own accuracy study (test/test_ifgf.cpp:143-165),
 //     restated as an asserted error bound.
 //
-// Deliberate deviations from the reference (all documented in DESIGN.md):
+// Deliberate deviations from the reference (the CUDA path makes the same ones):
 //   * the unsynchronised sibling accumulation into parentData
 //     (ifgfoperator.hpp:330-340 with :1181-1182) is serialised per parent;
 //   * interpolation buffers are zero-initialised (the reference leaves fine
