@@ -82,3 +82,4 @@ def test_reference_names_present():
     for name in ("MofifiedHelmholtzIfgfOperator", "GradHelmholtzIfgfOperator", "LaplaceIfgfOperator"):
         assert hasattr(pyifgf, name)
     assert G.MofifiedHelmholtzIfgfOperator is G.ModifiedHelmholtzIfgfOperator
+    assert pyifgf.ModifiedHelmholtzIfgfOperator is pyifgf.MofifiedHelmholtzIfgfOperator
