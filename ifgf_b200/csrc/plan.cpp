@@ -4,6 +4,8 @@
 #include <algorithm>
 #include <cmath>
 #include <numeric>
+#include <system_error>
+#include <thread>
 
 #include "common.hpp"
 
@@ -412,37 +414,95 @@ void Plan::build_target_lists(int rank)
     std::vector<int32_t> fin, nin;
     transpose(far, fin_off, fin);
     transpose(near, nin_off, nin);
+    // A target leaf's far list is the concatenation of its own far sources
+    // and those of every ancestor, leaf first.  Count them per box, parents
+    // before children (cum = own + parent's cum), so the CSR is sized exactly
+    // before it is filled.
+    const int L = tgt.num_levels();
+    std::vector<int64_t> cum((size_t)ntb, 0);
     tleaf_gid.clear();
-    tleaf_far_off.assign(1, 0);
-    tleaf_near_off.assign(1, 0);
-    tleaf_far_src.clear();
-    tleaf_near_src.clear();
-    for (int l = 0; l < tgt.num_levels(); l++)
+    for (int l = 0; l < L; l++)
     {
-        const TreeLevel& L = tgt.levels[l];
-        for (size_t b = 0; b < L.size(); b++)
+        const TreeLevel& TL = tgt.levels[l];
+        const int64_t o = tgt.level_off[l];
+        for (size_t b = 0; b < TL.size(); b++)
         {
-            if (!L.leaf[b])
-                continue;
-            const int64_t g = tgt.level_off[l] + (int64_t)b;
-            tleaf_gid.push_back(g);
-            // far interactions of this leaf and of all its ancestors
-            int al = l;
-            int32_t ab = (int32_t)b;
+            const int64_t g = o + (int64_t)b;
+            cum[g] = fin_off[g + 1] - fin_off[g] +
+                     (l > 0 ? cum[tgt.level_off[l - 1] + TL.parent[b]] : 0);
+            if (TL.leaf[b])
+                tleaf_gid.push_back(g);
+        }
+    }
+    const int64_t nl = (int64_t)tleaf_gid.size();
+    tleaf_far_off.assign((size_t)nl + 1, 0);
+    tleaf_near_off.assign((size_t)nl + 1, 0);
+    for (int64_t i = 0; i < nl; i++)
+    {
+        const int64_t g = tleaf_gid[i];
+        tleaf_far_off[i + 1] = tleaf_far_off[i] + cum[g];
+        tleaf_near_off[i + 1] = tleaf_near_off[i] + (nin_off[g + 1] - nin_off[g]);
+    }
+    tleaf_far_src.resize((size_t)tleaf_far_off[nl]);
+    tleaf_near_src.resize((size_t)tleaf_near_off[nl]);
+    // global target box id -> (level, index in level)
+    std::vector<int32_t> box_level((size_t)ntb);
+    for (int l = 0; l < L; l++)
+        std::fill(box_level.begin() + tgt.level_off[l], box_level.begin() + tgt.level_off[l + 1], l);
+    // Fill leaves [lo, hi): every leaf writes its own slice, so threads
+    // given disjoint leaf ranges need no synchronisation.
+    auto fill = [&](int64_t lo, int64_t hi) {
+        for (int64_t i = lo; i < hi; i++)
+        {
+            const int64_t g = tleaf_gid[i];
+            int32_t* out = tleaf_far_src.data() + tleaf_far_off[i];
+            int al = box_level[g];
+            int32_t ab = (int32_t)(g - tgt.level_off[al]);
             while (al >= 0)
             {
                 const int64_t ag = tgt.level_off[al] + ab;
-                tleaf_far_src.insert(tleaf_far_src.end(), fin.begin() + fin_off[ag],
-                                     fin.begin() + fin_off[ag + 1]);
+                out = std::copy(fin.begin() + fin_off[ag], fin.begin() + fin_off[ag + 1], out);
                 ab = tgt.levels[al].parent[ab];
                 al--;
             }
-            tleaf_far_off.push_back((int64_t)tleaf_far_src.size());
-            tleaf_near_src.insert(tleaf_near_src.end(), nin.begin() + nin_off[g],
-                                  nin.begin() + nin_off[g + 1]);
-            tleaf_near_off.push_back((int64_t)tleaf_near_src.size());
+            std::copy(nin.begin() + nin_off[g], nin.begin() + nin_off[g + 1],
+                      tleaf_near_src.begin() + tleaf_near_off[i]);
+        }
+    };
+    // Leaf ranges of about equal far-entry counts; small plans stay on the
+    // calling thread.
+    const int64_t total = tleaf_far_off[nl] + tleaf_near_off[nl];
+    const int nt = (int)std::min<int64_t>(
+        std::max(1u, std::min(16u, std::thread::hardware_concurrency())), 1 + total / (1 << 20));
+    if (nt <= 1)
+    {
+        fill(0, nl);
+        return;
+    }
+    std::vector<int64_t> cut((size_t)nt + 1, nl);
+    cut[0] = 0;
+    for (int t = 1; t < nt; t++)
+    {
+        const int64_t want = tleaf_far_off[nl] * t / nt;
+        cut[t] = std::lower_bound(tleaf_far_off.begin(), tleaf_far_off.end(), want) -
+                 tleaf_far_off.begin();
+        cut[t] = std::max(cut[t - 1], std::min(cut[t], nl));
+    }
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nt; t++)
+    {
+        try
+        {
+            pool.emplace_back(fill, cut[t], cut[t + 1]);
+        }
+        catch (const std::system_error&) // no thread to be had: fill here
+        {
+            fill(cut[t], cut[t + 1]);
         }
     }
+    fill(cut[0], cut[1]);
+    for (auto& th : pool)
+        th.join();
 }
 
 } // namespace ifgf
