@@ -2186,6 +2186,8 @@ std::string Operator::stats_json() const
 {
     std::ostringstream o;
     o.precision(10);
+    int64_t tl_work[4] = {0, 0, 0, 0};
+    plan_.target_list_work(tl_work);
     o << "{\"kind\":" << kind_ << ",\"precision\":" << precision_ << ",\"n_src\":" << n_src()
       << ",\"n_tgt\":" << n_tgt() << ",\"order_high\":[" << hi_[0] << "," << hi_[1] << ","
       << hi_[2] << "],\"order_low\":[" << lo_[0] << "," << lo_[1] << "," << lo_[2] << "]"
@@ -2205,6 +2207,10 @@ std::string Operator::stats_json() const
       << ",\"dropped_pairs\":" << plan_.n_dropped
       << ",\"near_point_pairs\":" << plan_.near_point_pairs
       << ",\"far_target_evals\":" << plan_.far_target_evals
+      << ",\"far_point_pairs\":" << tl_work[3]
+      << ",\"target_leaf_far_evals\":" << tl_work[0]
+      << ",\"target_leaf_far_point_pairs\":" << tl_work[1]
+      << ",\"target_leaf_near_point_pairs\":" << tl_work[2]
       << ",\"leaf_factor_evals\":" << leaf_evals_ << ",\"upward_node_evals\":" << upward_evals_
       << ",\"coarse_cones_total\":" << n_coarse_total_ << ",\"fine_cones_total\":" << n_fine_total_
       << ",\"upward_geometry_bytes\":" << upgeo_bytes_ << ",\"upward_runs_max\":[";

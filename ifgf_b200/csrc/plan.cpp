@@ -505,4 +505,35 @@ void Plan::build_target_lists(int rank)
         th.join();
 }
 
+void Plan::target_list_work(int64_t out[4]) const
+{
+    // points per box, by global box id
+    auto points = [](const Tree& T) {
+        std::vector<int64_t> n((size_t)T.num_boxes_total());
+        for (int l = 0; l < T.num_levels(); l++)
+            for (size_t b = 0; b < T.levels[l].size(); b++)
+                n[T.level_off[l] + (int64_t)b] = T.levels[l].last[b] - T.levels[l].first[b];
+        return n;
+    };
+    const std::vector<int64_t> ps = points(src), pt = points(tgt);
+    int64_t fe = 0, fp = 0, np = 0, wp = 0;
+    for (size_t i = 0; i < tleaf_gid.size(); i++)
+    {
+        const int64_t nt = pt[tleaf_gid[i]];
+        fe += nt * (tleaf_far_off[i + 1] - tleaf_far_off[i]);
+        for (int64_t j = tleaf_far_off[i]; j < tleaf_far_off[i + 1]; j++)
+            fp += nt * ps[tleaf_far_src[j]];
+        for (int64_t j = tleaf_near_off[i]; j < tleaf_near_off[i + 1]; j++)
+            np += nt * ps[tleaf_near_src[j]];
+    }
+    const int64_t nsb = src.num_boxes_total();
+    for (int64_t s = 0; s < nsb && !far.off.empty(); s++)
+        for (const int32_t* t = far.begin(s); t != far.end(s); t++)
+            wp += ps[s] * pt[*t];
+    out[0] = fe;
+    out[1] = fp;
+    out[2] = np;
+    out[3] = wp;
+}
+
 } // namespace ifgf

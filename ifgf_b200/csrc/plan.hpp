@@ -104,6 +104,16 @@ struct Plan
     void assign_shards(int nranks);
     // target-leaf lists of the sources owned by `rank` (all when rank < 0)
     void build_target_lists(int rank = -1);
+    // Point-level work the target-leaf lists describe, for checking them
+    // against the walk's lists: out[0] = sum over target leaves of (leaf
+    // points x far-list length), out[1] = of (leaf points x points of each
+    // far source box), out[2] = of (leaf points x points of each near source
+    // leaf), and out[3] = sum over the far pairs (s, t) of the walk of
+    // (points of s x points of t).  Without sharding out[0] equals
+    // far_target_evals, out[1] equals out[3] and out[2] equals
+    // near_point_pairs, since the leaves under a far pair's target box
+    // partition its points; sharded, the ranks' out[0..2] add up to them.
+    void target_list_work(int64_t out[4]) const;
 };
 
 // Morton key of a point normalised to the root box: 42 bits per dimension,

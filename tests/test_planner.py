@@ -106,3 +106,34 @@ def test_morton_order_matches_comparator():
     mn, mx = bb[0, :3], bb[0, 3:]
     for i in range(len(perm) - 1):
         assert O.morton_less(mn, mx, p[:, perm[i]], p[:, perm[i + 1]])
+
+
+@pytest.mark.parametrize("case", ["same", "distinct", "leaf_7"])
+def test_target_leaf_lists_cover_every_pair(case):
+    """The per-target-leaf CSR (a leaf's far list = its own far sources and
+    every ancestor's) describes exactly the walk's work: each far pair (s, t)
+    reaches the points of t through the leaves that partition t, each near
+    pair once; weighting every entry by its source box's points checks the
+    entries themselves, not only the list lengths.  Sharded, the ranks' lists
+    add up to the same totals."""
+    n = 60000
+    src = W.ellipsoid_points(n, seed=0)
+    tgt = src if case != "distinct" else W.sphere_points(n // 2, seed=3)
+    leaf = 7 if case == "leaf_7" else 100
+    g = G.HelmholtzIfgfOperator(20.0, leaf, 6)
+    g.init_plan_only(src, tgt)
+    st = g.stats()
+    assert st["target_leaf_far_evals"] == st["far_target_evals"] > 0
+    assert st["target_leaf_far_point_pairs"] == st["far_point_pairs"] > 0
+    assert st["target_leaf_near_point_pairs"] == st["near_point_pairs"] > 0
+    far = farp = near = 0
+    for rank in range(3):
+        s = G.HelmholtzIfgfOperator(20.0, leaf, 6)
+        s.set_shard(rank, 3)
+        s.init_plan_only(src, tgt)
+        ss = s.stats()
+        far += ss["target_leaf_far_evals"]
+        farp += ss["target_leaf_far_point_pairs"]
+        near += ss["target_leaf_near_point_pairs"]
+    assert (far, farp, near) == (st["far_target_evals"], st["far_point_pairs"],
+                                 st["near_point_pairs"])
