@@ -92,7 +92,7 @@ int ifgf_set_precision(ifgf_operator* op, int mode);
 int ifgf_set_shard(ifgf_operator* op, int rank, int nranks);
 
 /* After init: the shard level and this rank's boxes on it (level-local box
- * indices, *n of them, at most cap written). */
+ * indices, *n of them, at most cap written).  No reference counterpart. */
 int ifgf_shard_boxes(const ifgf_operator* op, int* level, long* boxes, long cap, long* n);
 
 /* Far-interaction drop predicate of IfgfOperator::init
@@ -110,7 +110,9 @@ int ifgf_init(ifgf_operator* op, const double* srcs, long n_src, const double* t
 
 /* Host half of ifgf_init: builds the octrees and interaction lists only,
  * touching no GPU (the tree and list accessors below work after it; mult
- * does not).  For tests and tooling on machines without a GPU. */
+ * does not).  For tests and tooling on machines without a GPU.  Replaces the
+ * first steps of IfgfOperator::init, Octree::build of both point sets and
+ * buildInteractionList (ifgfoperator.hpp:69-72). */
 int ifgf_init_plan_only(ifgf_operator* op, const double* srcs, long n_src, const double* tgts,
                         long n_tgt, ifgf_cutoff_fn cutoff, void* user);
 
@@ -126,7 +128,8 @@ int ifgf_mult(ifgf_operator* op, const void* w, void* u);
  * interpolants); FP64 runs them one by one.  No reference counterpart. */
 int ifgf_mult_batch(ifgf_operator* op, const void* w, void* u, long batch);
 
-/* ifgf_mult_batch on device buffers enqueued on `stream`. */
+/* ifgf_mult_batch on device buffers enqueued on `stream`.  No reference
+ * counterpart. */
 int ifgf_mult_batch_device(ifgf_operator* op, const void* d_w, void* d_u, long batch,
                            void* stream);
 
@@ -144,7 +147,7 @@ int ifgf_mult_batch_device(ifgf_operator* op, const void* d_w, void* d_u, long b
 int ifgf_mult_wavenumbers(ifgf_operator* op, const double* k, long n_k, const void* w, void* u);
 
 /* ifgf_mult_wavenumbers on device buffers enqueued on `stream` (k stays a
- * host array). */
+ * host array).  No reference counterpart. */
 int ifgf_mult_wavenumbers_device(ifgf_operator* op, const double* k, long n_k, const void* d_w,
                                  void* d_u, void* stream);
 
@@ -197,7 +200,8 @@ int ifgf_mult_adjoint_device(ifgf_operator* op, const void* d_w, void* d_u, void
  * w as in ifgf_mult (host buffer), out receives nt values.  The reference
  * checks its mult the same way on the host (test/test_ifgf.cpp:143-165). */
 int ifgf_direct_eval(ifgf_operator* op, const void* w, const long* tidx, long nt, void* out);
-/* ifgf_direct_eval of the k-derivative kernel (see ifgf_mult_dk). */
+/* ifgf_direct_eval of the k-derivative kernel (see ifgf_mult_dk).  No
+ * reference counterpart. */
 int ifgf_direct_eval_dk(ifgf_operator* op, const void* w, const long* tidx, long nt, void* out);
 
 /* Per-kernel CUDA-event timing of every following mult (on the stream the
@@ -215,7 +219,9 @@ int ifgf_num_targets(const ifgf_operator* op, long* n);
 int ifgf_stats_json(const ifgf_operator* op, char* buf, long cap, long* needed);
 
 /* Tree and cone tables, for parity tests against the reference's octree.
- * which: 0 = source tree, 1 = target tree. */
+ * which: 0 = source tree, 1 = target tree.  ifgf_tree_levels and
+ * ifgf_tree_num_boxes replace Octree::levels and Octree::numBoxes
+ * (octree.hpp:884, :915). */
 int ifgf_tree_levels(const ifgf_operator* op, int which, int* levels);
 int ifgf_tree_num_boxes(const ifgf_operator* op, int which, int level, long* n);
 /* perm[i] = original index of the i-th point in Morton order
@@ -234,14 +240,20 @@ int ifgf_box_list(const ifgf_operator* op, int level, long box, int far, long* o
  * insertion order; the set is the same). */
 int ifgf_box_cones(const ifgf_operator* op, int level, long box, int step, long* out, long cap,
                    long* n);
-/* cone grid of a level: n[3] elements per dimension; orders of a step */
+/* cone grid of a level: n[3] elements per dimension (the level's
+ * ConeDomain, octree.hpp:113, sized by elementsForBox,
+ * ifgfoperator.hpp:99); orders of a step (orderForBox,
+ * ifgfoperator.hpp:96) */
 int ifgf_level_grid(const ifgf_operator* op, int level, int step, long* n);
 int ifgf_orders(const ifgf_operator* op, int step, int* order);
 
-/* Destroys the handle and frees its device memory. */
+/* Destroys the handle and frees its device memory (the operator's
+ * destructor, ifgfoperator.hpp:61). */
 int ifgf_destroy(ifgf_operator* op);
 
-/* Message of the calling thread's last failed call ("" if none). */
+/* Message of the calling thread's last failed call ("" if none).  No
+ * reference counterpart: the reference reports errors through assert and
+ * C++ exceptions (pybind11 turns them into Python exceptions). */
 const char* ifgf_last_error(void);
 
 #ifdef __cplusplus
