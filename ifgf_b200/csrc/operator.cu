@@ -1016,8 +1016,8 @@ void Operator::setup_device(const double* normals)
         std::vector<long long> no(plan_.tleaf_near_off.begin(), plan_.tleaf_near_off.end());
         D.tl_far_off.upload(fo);
         D.tl_near_off.upload(no);
-        D.tl_far_src.upload(plan_.tleaf_far_src);
-        D.tl_near_src.upload(plan_.tleaf_near_src);
+        D.tl_far_src.upload(plan_.tleaf_far_src.data(), plan_.tleaf_far_src.size());
+        D.tl_near_src.upload(plan_.tleaf_near_src.data(), plan_.tleaf_near_src.size());
         D.n_tleaf = (int)ntl;
     }
 

@@ -412,8 +412,24 @@ void Plan::build_target_lists(int rank)
     };
     std::vector<int64_t> fin_off, nin_off;
     std::vector<int32_t> fin, nin;
+    // the two transposes are independent: for large lists the near one runs
+    // on a second thread when one can be had
+    std::thread near_thread;
+    if (near.tgt.size() + far.tgt.size() > ((size_t)1 << 18))
+    {
+        try
+        {
+            near_thread = std::thread([&] { transpose(near, nin_off, nin); });
+        }
+        catch (const std::system_error&)
+        {
+        }
+    }
+    if (!near_thread.joinable())
+        transpose(near, nin_off, nin);
     transpose(far, fin_off, fin);
-    transpose(near, nin_off, nin);
+    if (near_thread.joinable())
+        near_thread.join();
     // A target leaf's far list is the concatenation of its own far sources
     // and those of every ancestor, leaf first.  Count them per box, parents
     // before children (cum = own + parent's cum), so the CSR is sized exactly

@@ -9,10 +9,33 @@
 
 #include <cstdint>
 #include <functional>
+#include <memory>
+#include <new>
+#include <utility>
 #include <vector>
 
 namespace ifgf
 {
+
+// Allocator whose resize leaves trivially constructible elements
+// uninitialised: a vector sized here and then filled by several threads is
+// not first zeroed (and paged in) on one thread.
+template <typename T> struct UninitAlloc : std::allocator<T>
+{
+    using value_type = T;
+    template <typename U> struct rebind
+    {
+        using other = UninitAlloc<U>;
+    };
+    UninitAlloc() = default;
+    template <typename U> UninitAlloc(const UninitAlloc<U>&) noexcept {}
+    template <typename U> void construct(U* p) { ::new ((void*)p) U; }
+    template <typename U, typename... A> void construct(U* p, A&&... a)
+    {
+        ::new ((void*)p) U(std::forward<A>(a)...);
+    }
+};
+template <typename T> using FillVector = std::vector<T, UninitAlloc<T>>;
 
 struct TreeLevel
 {
@@ -81,9 +104,9 @@ struct Plan
     // target-leaf-centric lists for the evaluation kernel
     std::vector<int64_t> tleaf_gid;       // target leaves (global target box ids)
     std::vector<int64_t> tleaf_far_off;   // CSR offsets into tleaf_far_src
-    std::vector<int32_t> tleaf_far_src;   // source global box ids
+    FillVector<int32_t> tleaf_far_src;    // source global box ids
     std::vector<int64_t> tleaf_near_off;
-    std::vector<int32_t> tleaf_near_src;  // source leaf global box ids
+    FillVector<int32_t> tleaf_near_src;   // source leaf global box ids
     // counters (octree.hpp:265-268)
     int64_t n_far_pairs = 0, n_near_pairs = 0, n_dropped = 0;
     int64_t far_target_evals = 0, near_point_pairs = 0;
