@@ -108,7 +108,7 @@ def test_morton_order_matches_comparator():
         assert O.morton_less(mn, mx, p[:, perm[i]], p[:, perm[i + 1]])
 
 
-@pytest.mark.parametrize("case", ["same", "distinct", "leaf_7"])
+@pytest.mark.parametrize("case", ["same", "distinct", "leaf_7", "cutoff"])
 def test_target_leaf_lists_cover_every_pair(case):
     """The per-target-leaf CSR (a leaf's far list = its own far sources and
     every ancestor's) describes exactly the walk's work: each far pair (s, t)
@@ -120,9 +120,14 @@ def test_target_leaf_lists_cover_every_pair(case):
     src = W.ellipsoid_points(n, seed=0)
     tgt = src if case != "distinct" else W.sphere_points(n // 2, seed=3)
     leaf = 7 if case == "leaf_7" else 100
+    # a cutoff drops the far pairs beyond distance 1.2 from the walk, and so
+    # from the target-leaf lists
+    cut = (lambda d: d > 1.2) if case == "cutoff" else None
     g = G.HelmholtzIfgfOperator(20.0, leaf, 6)
-    g.init_plan_only(src, tgt)
+    g.init_plan_only(src, tgt, cut)
     st = g.stats()
+    if cut is not None:
+        assert st["dropped_pairs"] > 0
     assert st["target_leaf_far_evals"] == st["far_target_evals"] > 0
     assert st["target_leaf_far_point_pairs"] == st["far_point_pairs"] > 0
     assert st["target_leaf_near_point_pairs"] == st["near_point_pairs"] > 0
@@ -130,7 +135,7 @@ def test_target_leaf_lists_cover_every_pair(case):
     for rank in range(3):
         s = G.HelmholtzIfgfOperator(20.0, leaf, 6)
         s.set_shard(rank, 3)
-        s.init_plan_only(src, tgt)
+        s.init_plan_only(src, tgt, cut)
         ss = s.stats()
         far += ss["target_leaf_far_evals"]
         farp += ss["target_leaf_far_point_pairs"]
