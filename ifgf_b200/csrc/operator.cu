@@ -1083,6 +1083,8 @@ void Operator::setup_device(const double* normals)
     upgeo_bytes_ = 0;
     int64_t coarse_tot = 0, fine_tot = 0;
     leaf_evals_ = upward_evals_ = 0;
+    std::vector<int> tbox_first, tbox_last; // point range of every target box
+    plan_.target_box_ranges(tbox_first, tbox_last);
     for (int l = 0; l < L; l++)
     {
         LevelGeom& G = lv_[l];
@@ -1091,22 +1093,9 @@ void Operator::setup_device(const double* normals)
         const int64_t ncm = (int64_t)G.nbox * nce, nfm = (int64_t)G.nbox * nfe;
         IFGF_CUDA(cudaMemset(cmark.p, 0, ncm * sizeof(int)));
         phase("cone_marks");
-        // far pairs of this level
+        // far pairs of this level: source box, target point range
         std::vector<int> fs, f0, f1;
-        for (int b = 0; b < G.nbox; b++)
-        {
-            const int64_t g = G.box_off + b;
-            for (const int32_t* tp = plan_.far.begin(g); tp != plan_.far.end(g); tp++)
-            {
-                const int64_t t = *tp;
-                int lev = (int)(std::upper_bound(Tt.level_off.begin(), Tt.level_off.end(), t) -
-                                Tt.level_off.begin()) - 1;
-                int64_t tb = t - Tt.level_off[lev];
-                fs.push_back((int)g);
-                f0.push_back((int)Tt.levels[lev].first[tb]);
-                f1.push_back((int)Tt.levels[lev].last[tb]);
-            }
-        }
+        plan_.far_pairs_of_level(l, tbox_first, tbox_last, fs, f0, f1);
         phase("far_pairs_host");
         if (!fs.empty())
         {

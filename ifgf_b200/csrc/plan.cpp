@@ -552,4 +552,36 @@ void Plan::target_list_work(int64_t out[4]) const
     out[3] = wp;
 }
 
+void Plan::target_box_ranges(std::vector<int>& first, std::vector<int>& last) const
+{
+    const int64_t ntb = tgt.num_boxes_total();
+    first.resize((size_t)ntb);
+    last.resize((size_t)ntb);
+    for (int l = 0; l < tgt.num_levels(); l++)
+        for (size_t b = 0; b < tgt.levels[l].size(); b++)
+        {
+            first[tgt.level_off[l] + (int64_t)b] = (int)tgt.levels[l].first[b];
+            last[tgt.level_off[l] + (int64_t)b] = (int)tgt.levels[l].last[b];
+        }
+}
+
+void Plan::far_pairs_of_level(int level, const std::vector<int>& tfirst,
+                              const std::vector<int>& tlast, std::vector<int>& fs,
+                              std::vector<int>& f0, std::vector<int>& f1) const
+{
+    const int64_t lo = src.level_off[level], hi = src.level_off[level + 1];
+    const int64_t n = far.off.empty() ? 0 : far.off[hi] - far.off[lo];
+    fs.resize((size_t)n);
+    f0.resize((size_t)n);
+    f1.resize((size_t)n);
+    int64_t k = 0;
+    for (int64_t g = lo; g < hi && n > 0; g++)
+        for (const int32_t* tp = far.begin(g); tp != far.end(g); tp++, k++)
+        {
+            fs[k] = (int)g;
+            f0[k] = tfirst[*tp];
+            f1[k] = tlast[*tp];
+        }
+}
+
 } // namespace ifgf

@@ -137,6 +137,14 @@ struct Plan
     // near_point_pairs, since the leaves under a far pair's target box
     // partition its points; sharded, the ranks' out[0..2] add up to them.
     void target_list_work(int64_t out[4]) const;
+    // Point range [first, last) of every target box, by global box id.
+    void target_box_ranges(std::vector<int>& first, std::vector<int>& last) const;
+    // The far pairs of the source boxes of one level, in list order: the
+    // source global box id and the target box's point range (tfirst / tlast
+    // from target_box_ranges), the input of the cone-marking kernel.
+    void far_pairs_of_level(int level, const std::vector<int>& tfirst,
+                            const std::vector<int>& tlast, std::vector<int>& fs,
+                            std::vector<int>& f0, std::vector<int>& f1) const;
 };
 
 // Morton key of a point normalised to the root box: 42 bits per dimension,
