@@ -1192,7 +1192,7 @@ void Operator::setup_device(const double* normals)
             std::vector<int> el(lv_[l].n_coarse);
             IFGF_CUDA(cudaMemcpy(el.data(), D.cc_el[l].p, el.size() * sizeof(int),
                                  cudaMemcpyDeviceToHost));
-            std::stable_sort(uidx.begin(), uidx.end(), [&](int a, int b) { return el[a] < el[b]; });
+            stable_order_by_key(uidx, el);
             for (size_t i = 0; i < uidx.size(); i++)
             {
                 if (i == 0 || el[uidx[i]] != el[uidx[i - 1]])

@@ -584,4 +584,35 @@ void Plan::far_pairs_of_level(int level, const std::vector<int>& tfirst,
         }
 }
 
+void stable_order_by_key(std::vector<int>& idx, const std::vector<int>& key)
+{
+    int kmax = -1;
+    bool counting = true;
+    for (int i : idx)
+    {
+        const int k = key[i];
+        if (k < 0 || k >= (1 << 26))
+        {
+            counting = false;
+            break;
+        }
+        kmax = std::max(kmax, k);
+    }
+    if (!counting)
+    {
+        std::stable_sort(idx.begin(), idx.end(),
+                         [&](int a, int b) { return key[a] < key[b]; });
+        return;
+    }
+    std::vector<int64_t> at((size_t)kmax + 2, 0);
+    for (int i : idx)
+        at[key[i] + 1]++;
+    for (size_t k = 1; k < at.size(); k++)
+        at[k] += at[k - 1];
+    std::vector<int> out(idx.size());
+    for (int i : idx)
+        out[at[key[i]]++] = i;
+    idx.swap(out);
+}
+
 } // namespace ifgf

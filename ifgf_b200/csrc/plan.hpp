@@ -147,6 +147,11 @@ struct Plan
                             std::vector<int>& f0, std::vector<int>& f1) const;
 };
 
+// Reorders idx stably by key[idx[i]] -- the order std::stable_sort with a
+// key comparison gives -- by a counting sort when every key is in
+// [0, 2^26), else by std::stable_sort.
+void stable_order_by_key(std::vector<int>& idx, const std::vector<int>& key);
+
 // Morton key of a point normalised to the root box: 42 bits per dimension,
 // interleaved z,y,x most significant first, split in two 63-bit halves.
 void morton_key(const double* p, const double* center, const double* diam, uint64_t* hi,
