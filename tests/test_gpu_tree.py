@@ -65,8 +65,13 @@ def test_gpu_interaction_lists_equal_host_lists(name, pts, leaf):
     host = G.HelmholtzIfgfOperator(5.0, leaf, 8)
     host.init_plan_only(pts, tg)
     sg, sh = gpu.stats(), host.stats()
-    for key in ("near_pairs", "far_pairs", "near_point_pairs", "far_target_evals"):
+    for key in ("near_pairs", "far_pairs", "near_point_pairs", "far_target_evals",
+                "far_point_pairs", "target_leaf_far_evals", "target_leaf_far_point_pairs",
+                "target_leaf_near_point_pairs"):
         assert sg[key] == sh[key], key
+    assert sg["target_leaf_far_evals"] == sg["far_target_evals"]
+    assert sg["target_leaf_far_point_pairs"] == sg["far_point_pairs"]
+    assert sg["target_leaf_near_point_pairs"] == sg["near_point_pairs"]
     for lvl in range(host.levels(0)):
         for box in range(host.num_boxes(lvl, 0)):
             for far in (0, 1):
