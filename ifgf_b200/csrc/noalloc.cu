@@ -1,12 +1,13 @@
 // Fixed device scratch for ifgf_mult_device_noalloc.
 //
 // Some callers cannot allocate device memory at the moment they apply the
-// operator: code running while a stream is being captured into a CUDA graph,
-// solvers embedded in frameworks whose memory pool owns the whole device, or
-// real-time loops that must not hit cudaMalloc's implicit synchronisation.
-// For them the matvec can run with its per-call scratch (sorted densities,
-// coarse nodal values, fine coefficients) in the file-scope array below
-// instead of the buffers the operator allocated at init.
+// operator: solvers embedded in frameworks whose memory pool has reserved the
+// whole device (a cudaMalloc there fails or takes memory the pool counts on),
+// or real-time loops that must not stall on the implicit device
+// synchronisation of cudaMalloc / cudaFree.  For them the matvec can run with
+// its per-call scratch (sorted densities, coarse nodal values, fine
+// coefficients, near-field sums) in the file-scope array below instead of the
+// buffers the operator allocated at init.
 //
 // The array is NOALLOC_SCRATCH_BYTES (64 MiB) on every GPU that loads this
 // library, held until the process exits.  Every call shares it and it keeps

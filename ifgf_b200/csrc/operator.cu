@@ -910,6 +910,8 @@ void Operator::setup_device(const double* normals)
     D.dgeo32.clear();
     D.dgeo32_ptr.clear();
     D.dgeo_ready = false;
+    // the device this operator's tables live on
+    IFGF_CUDA(cudaGetDevice(&device_));
     const Tree& S = plan_.src;
     const Tree& Tt = plan_.tgt;
     const int L = S.num_levels();
@@ -2044,6 +2046,13 @@ void Operator::mult_device_external_scratch(const void* d_w, void* d_u, void* st
         throw Error(ERR_STATE, "mult called before init");
     if (!d_w || !d_u || !scratch)
         throw Error(ERR_INVALID, "null density, result or scratch buffer");
+    // the scratch is the current device's; the operator's tables must be there too
+    int cur = -1;
+    IFGF_CUDA(cudaGetDevice(&cur));
+    if (cur != device_)
+        throw Error(ERR_STATE, "the current device (" + std::to_string(cur) +
+                                   ") is not the device this operator was initialised on (" +
+                                   std::to_string(device_) + ")");
     DeviceState& D = *dev_;
     auto up = [](size_t b) { return (b + 255) / 256 * 256; };
     const size_t bw = up(D.w.n * sizeof(double2)), bc = up(D.cvals.n * sizeof(double2)),

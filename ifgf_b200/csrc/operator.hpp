@@ -141,6 +141,7 @@ class Operator
     int base_order_[3];
     int64_t base_n_[3];
     int precision_ = PREC_FP64;
+    int device_ = -1; // CUDA device of the device tables (set by init)
     bool initialized_ = false;
     bool planned_ = false;
     Plan plan_;

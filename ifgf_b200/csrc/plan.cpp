@@ -3,6 +3,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <exception>
 #include <numeric>
 #include <system_error>
 #include <thread>
@@ -389,6 +390,29 @@ void Plan::assign_shards(int nranks)
                 box_rank[src.level_off[l - 1] + src.levels[l].parent[b]];
 }
 
+namespace
+{
+// Joins the given threads when it goes out of scope, so that no joinable
+// std::thread is destroyed (which would end the process) when an exception
+// leaves the scope that started them.
+struct JoinAll
+{
+    std::thread* one;
+    int n_one;
+    std::vector<std::thread>* many = nullptr;
+    ~JoinAll()
+    {
+        for (int i = 0; i < n_one; i++)
+            if (one[i].joinable())
+                one[i].join();
+        if (many)
+            for (auto& t : *many)
+                if (t.joinable())
+                    t.join();
+    }
+};
+} // namespace
+
 void Plan::build_target_lists(int rank)
 {
     const int64_t ntb = tgt.num_boxes_total();
@@ -413,23 +437,40 @@ void Plan::build_target_lists(int rank)
     std::vector<int64_t> fin_off, nin_off;
     std::vector<int32_t> fin, nin;
     // the two transposes are independent: for large lists the near one runs
-    // on a second thread when one can be had
-    std::thread near_thread;
-    if (near.tgt.size() + far.tgt.size() > ((size_t)1 << 18))
+    // on a second thread when one can be had.  The thread is joined on every
+    // path out of this block (an exception from the far transpose included),
+    // and an exception inside it is carried back to this thread.
     {
-        try
+        std::exception_ptr near_err;
+        std::thread near_thread;
+        JoinAll guard{&near_thread, 1};
+        if (near.tgt.size() + far.tgt.size() > ((size_t)1 << 18))
         {
-            near_thread = std::thread([&] { transpose(near, nin_off, nin); });
+            try
+            {
+                near_thread = std::thread([&] {
+                    try
+                    {
+                        transpose(near, nin_off, nin);
+                    }
+                    catch (...)
+                    {
+                        near_err = std::current_exception();
+                    }
+                });
+            }
+            catch (const std::system_error&)
+            {
+            }
         }
-        catch (const std::system_error&)
-        {
-        }
+        if (!near_thread.joinable())
+            transpose(near, nin_off, nin);
+        transpose(far, fin_off, fin);
+        if (near_thread.joinable())
+            near_thread.join();
+        if (near_err)
+            std::rethrow_exception(near_err);
     }
-    if (!near_thread.joinable())
-        transpose(near, nin_off, nin);
-    transpose(far, fin_off, fin);
-    if (near_thread.joinable())
-        near_thread.join();
     // A target leaf's far list is the concatenation of its own far sources
     // and those of every ancestor, leaf first.  Count them per box, parents
     // before children (cum = own + parent's cum), so the CSR is sized exactly
@@ -504,7 +545,11 @@ void Plan::build_target_lists(int rank)
                  tleaf_far_off.begin();
         cut[t] = std::max(cut[t - 1], std::min(cut[t], nl));
     }
+    // fill() only copies into sized arrays, so the workers cannot throw; the
+    // joiner joins every started worker on every path out of this function
     std::vector<std::thread> pool;
+    pool.reserve((size_t)nt);
+    JoinAll guard{nullptr, 0, &pool};
     for (int t = 1; t < nt; t++)
     {
         try
@@ -517,8 +562,6 @@ void Plan::build_target_lists(int rank)
         }
     }
     fill(cut[0], cut[1]);
-    for (auto& th : pool)
-        th.join();
 }
 
 void Plan::target_list_work(int64_t out[4]) const
@@ -598,6 +641,10 @@ void stable_order_by_key(std::vector<int>& idx, const std::vector<int>& key)
         }
         kmax = std::max(kmax, k);
     }
+    // a counting array much longer than the list would cost more than it
+    // saves: keys spread that widely take the comparison sort
+    if (counting && (int64_t)kmax > 4 * (int64_t)idx.size() + 4096)
+        counting = false;
     if (!counting)
     {
         std::stable_sort(idx.begin(), idx.end(),

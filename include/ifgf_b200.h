@@ -157,15 +157,20 @@ int ifgf_mult_wavenumbers_device(ifgf_operator* op, const double* k, long n_k, c
 int ifgf_mult_device(ifgf_operator* op, const void* d_w, void* d_u, void* stream);
 
 /* ifgf_mult_device for callers that cannot allocate device memory while they
- * apply the operator -- e.g. code inside a stream capture, or an application
- * whose memory pool owns the whole GPU.  This call allocates and frees
+ * apply the operator: an application whose own memory pool has reserved the
+ * whole GPU (a cudaMalloc would fail or take memory the pool counts on), or
+ * a real-time loop that must not stall on the implicit device
+ * synchronisation of cudaMalloc / cudaFree.  This call allocates and frees
  * nothing: its per-call scratch lives in a fixed 64 MiB device array that the
  * library holds on every GPU that loads it, instead of the buffers init
  * allocated.  Operators whose matvec scratch exceeds 64 MiB are rejected with
- * IFGF_ERR_INVALID_ARG (use ifgf_mult_device for them).  The first call on a
- * device looks up the array's device address; make that first call before
- * any stream capture.  All calls share the one array, so calls whose GPU work
- * overlaps race and must be serialised.  No reference counterpart. */
+ * IFGF_ERR_INVALID_ARG (use ifgf_mult_device for them); a current device
+ * other than the one the operator was initialised on gives IFGF_ERR_STATE.
+ * The first call on a device looks up the array's device address; make that
+ * first call before any stream capture.  All calls share the one array and it
+ * keeps the last call's contents, so calls whose GPU work overlaps (two
+ * streams, two threads, two operators) race and must be serialised.  No
+ * reference counterpart. */
 int ifgf_mult_device_noalloc(ifgf_operator* op, const void* d_w, void* d_u, void* stream);
 
 /* u = (dA/dk) w: the matvec of the wavenumber derivative of the kernel,

@@ -1,7 +1,8 @@
 // Host-planner helpers against their direct definitions (built and run by
 // tests/test_host_helpers.py with g++; no GPU):
 //   * stable_order_by_key equals std::stable_sort with a key comparison,
-//     including unsorted inputs and keys outside the counting range;
+//     including unsorted inputs, keys outside the counting range and keys
+//     far larger than the list;
 //   * Plan::far_pairs_of_level equals a per-pair search of the target box's
 //     level and point range, for equal and distinct point sets.
 #include "plan.hpp"
@@ -29,6 +30,8 @@ static int check_stable_order()
             key[0] = -3; // a negative key: the comparison-sort path
         if (trial == 6)
             key[1] = 1 << 27; // a key beyond the counting range
+        if (trial == 7 || trial == 8)
+            key[2] = (1 << 25) + trial; // one large key over a short list: the comparison sort
         std::vector<int> idx;
         for (int i = 0; i < n + 7; i++)
             if (rng() % 3)

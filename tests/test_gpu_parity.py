@@ -94,6 +94,55 @@ def test_config1_laplace_20k():
 
 
 @pytest.mark.gpu
+def test_config2_helmholtz_200k():
+    """Plain Helmholtz e^{ikr}/(4 pi r), N=200,000 on the unit sphere,
+    k=16 pi (the sphere about 16 wavelengths across), leaf 100, p=8 (high
+    (5,8,8), low (2,5,5)), complex densities: the FP64 pipeline equals the
+    oracle to 1e-12, and its error against the FP64 direct sum at 1,000
+    sampled targets is the oracle's within 10 % (the error check of the
+    reference's test/test_ifgf.cpp:143-165, at this size)."""
+    n, k = 200_000, 16.0 * np.pi
+    pts = W.sphere_points(n, seed=0)
+    w = W.densities(n, complex_=True, seed=1)
+    g = make_gpu_op("helmholtz", leaf=100, order=8, k=k)
+    o = make_oracle_op("helmholtz", leaf=100, order=8, k=k)
+    g.init(pts, pts)
+    o.init(pts, pts)
+    ug, uo = g.mult(w), o.mult(w)
+    assert rel2(ug, uo) <= PARITY_TOL, rel2(ug, uo)
+    idx = W.sample_targets(n, 1000, seed=2)
+    d = O.direct_sum("helmholtz", k, pts, w, pts, idx)
+    eg, eo = rel2(ug[idx], d), rel2(uo[idx], d)
+    assert abs(eg - eo) <= 0.1 * eo, (eg, eo)
+    assert eg < 1e-3
+    assert g.stats()["missing_cone_lookups"] == 0
+
+
+@pytest.mark.gpu
+def test_mixed_precision_at_high_wavenumber():
+    """k = 150 on 100,000 points of the ellipsoid (1, 1, 0.5), p = 9: the
+    centre-shift factors and the phases k (d - d_parent) of the upward pass
+    are formed in FP64 and stored in FP32; at this k the phase of a
+    coarse-level transfer reaches tens of radians, so an FP32 phase would
+    lose about 1e-5 of it.  The mixed pipeline stays within the metric's
+    1e-4 of the FP64 direct sum and close to the FP64 pipeline."""
+    n, k = 100_000, 150.0
+    pts = W.ellipsoid_points(n, seed=0)
+    w = W.densities(n, complex_=True, seed=1)
+    g = make_gpu_op("helmholtz", leaf=100, order=9, k=k)
+    g.init(pts, pts)
+    u64 = g.mult(w)
+    g.set_precision("mixed")
+    u32 = g.mult(w)
+    idx = W.sample_targets(n, 1000, seed=2)
+    d = g.direct_eval(w, idx)
+    e64, e32 = rel2(u64[idx], d), rel2(u32[idx], d)
+    assert e32 <= 1e-4, (e32, e64)
+    assert rel2(u32, u64) <= 5e-5, rel2(u32, u64)
+    assert g.stats()["missing_cone_lookups"] == 0
+
+
+@pytest.mark.gpu
 def test_different_source_and_target_sets():
     src = W.sphere_points(5000, seed=0)
     tgt = W.ellipsoid_points(3000, axes=(1.3, 1.2, 0.9), seed=7)
