@@ -66,12 +66,12 @@ def test_noalloc_two_operators_interleaved(precision):
     """Operator A, then a larger operator B with other points and more fine
     coefficients, then A again: each call starts from the other operator's
     leftovers in the shared array."""
-    na, nb = 3000, 6000
+    na, nb = 3000, 4000
     pa = W.sphere_points(na, seed=0)
     pb = W.ellipsoid_points(nb, seed=3)
     opa = make_gpu_op("helmholtz", leaf=50, order=8, k=10.0)
     opa.init(pa, pa)
-    opb = make_gpu_op("helmholtz", leaf=40, order=9, k=30.0)
+    opb = make_gpu_op("helmholtz", leaf=50, order=8, k=16.0)
     opb.init(pb, pb)
     assert opb.stats()["fine_cones_total"] > opa.stats()["fine_cones_total"]
     for op in (opa, opb):
