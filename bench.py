@@ -70,6 +70,8 @@ def parse():
                     help="skip the convolution-quadrature frequency-set measurement")
     ap.add_argument("--batch", type=int, default=8,
                     help="right-hand sides per step of the mixed pipeline (1: single matvec)")
+    ap.add_argument("--upward", choices=["auto", "ffma", "tensor"], default="auto",
+                    help="kernel of the mixed upward transfer (tensor cores / FP32 FMA)")
     return ap.parse_args()
 
 
@@ -387,6 +389,7 @@ def run_ours(a):
     w = W.densities(a.n, seed=1)
     op = G.HelmholtzIfgfOperator(a.k, a.leaf, a.order)
     op.set_precision(precision)
+    op.set_upward_path(a.upward)
     if ws > 1:
         # each rank takes a share of the source subtrees; the partial target
         # vectors are summed by one NCCL all-reduce per matvec

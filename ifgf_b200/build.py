@@ -21,7 +21,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I", CSRC, "
 SOURCES = ["operator.cu", "plan.cpp", "gpu_tree.cu", "gpu_lists.cu", "capi.cpp", "noalloc.cu"] + [
     f"kernels_k{k}.cu" for k in range(8)]
 HEADERS = ["common.hpp", "plan.hpp", "operator.hpp", "device_math.cuh", "mult.hpp",
-           "mult_kernels.cuh", "mult_batch.cuh", "far_staged.cuh"]
+           "mult_kernels.cuh", "mult_batch.cuh", "far_staged.cuh", "tcgen05.cuh", "upward_tc.cuh"]
 
 
 def _newer(target, deps):

@@ -12,6 +12,7 @@
 namespace ifgf
 {
 void* noalloc_scratch(size_t* bytes); // noalloc.cu
+void bounded_wait_selftest(double limit_ms, double* waited_ms); // operator.cu
 }
 
 struct ifgf_operator
@@ -113,6 +114,18 @@ extern "C"
         if (!h)
             return null_handle();
         return guarded([&] { h->op.set_precision(mode); });
+    }
+
+    int ifgf_set_upward_path(ifgf_operator* h, int path)
+    {
+        if (!h)
+            return null_handle();
+        return guarded([&] { h->op.set_upward_path(path); });
+    }
+
+    int ifgf_bounded_wait_selftest(double limit_ms, double* waited_ms)
+    {
+        return guarded([&] { ifgf::bounded_wait_selftest(limit_ms, waited_ms); });
     }
 
     int ifgf_init(ifgf_operator* h, const double* srcs, long n_src, const double* tgts, long n_tgt,

@@ -76,7 +76,24 @@ struct LevelLists
     int fe_pad;         // longest run list of a row
     const int* c2f_idx; // coarse cones to refine when n_c2f >= 0 (sharded operators)
     int n_c2f;          // -1: all of the level's cones
+    // tensor-core upward transfer of single-plane matvecs: row tiles (first
+    // up_idx position, cones, first plane, planes) and the fraction of their
+    // 32 rows that hold cones
+    const int4* tc_tiles = nullptr;
+    int n_tc_tiles = 0;
+    float tc_fill = 0.f;
 };
+
+// Upward-transfer kernel choice (Operator::set_upward_path): AUTO takes the
+// tensor-core kernel on levels whose row tiles are at least UPTC_MIN_FILL
+// full, FFMA never, TENSOR wherever the order shape and shared memory allow.
+enum UpwardPath : int
+{
+    UP_AUTO = 0,
+    UP_FFMA = 1,
+    UP_TENSOR = 2
+};
+constexpr float UPTC_MIN_FILL = 0.4f;
 
 // Upward geometry tables of one level, built on the device in two passes:
 // upgeo_row_max measures every (slot, octant) row's padded length and number
@@ -136,6 +153,8 @@ struct MultPtrs
     size_t c2f_smem; // for FP64 buffers (half of it in mixed precision)
     KParams kp;
     bool mixed; // mixed-precision pipeline (buffers hold float2)
+    int up_path = UP_AUTO;           // UpwardPath
+    unsigned* tc_status = nullptr;   // bounded-wait status of the tensor-core kernels
 };
 
 // Stage classes for per-kernel timing.
@@ -182,6 +201,11 @@ struct BatchPtrs
     // the distance tables (UpGeo32::tr = d - d_parent, ::ti = d_parent / d)
     const KParams* kp_plane = nullptr;
     const UpGeo32* const* dgeo32 = nullptr; // per level (host array)
+    // tensor-core upward tiles for groups * BATCH_NB planes, per level (host
+    // arrays; null: FFMA kernel)
+    const int4* const* tc_tiles = nullptr;
+    const int* n_tc_tiles = nullptr;
+    const float* tc_fill = nullptr;
 };
 
 // Enqueues the mixed matvec of bp.nrhs <= bp.groups * BATCH_NB right-hand

@@ -445,14 +445,26 @@ static int run_mult_batch(const MultPtrs& m, const BatchPtrs& bp, const void* d_
                 for (int d = 0; d < 3; d++)
                     ua.lo[d] = m.lo[d];
                 ua.kp = m.kp;
-                const size_t sm = upward_staged_smem<N0, N1, N2>(m.P_hi, ua.rch, LL.fe_pad);
-                auto kern = upward_staged_kernel<KIND, N0, N1, N2, MK>;
-                if (sm > 48 * 1024)
-                    IFGF_CHECK(cudaFuncSetAttribute(
-                        kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
                 if (hk)
                     hk->begin(PROF_UPWARD, l);
-                kern<<<dim3(LL.n_up, bp.groups * BATCH_NB), UPS_THREADS, sm, st>>>(ua);
+                bool tensor = false;
+                if (!MK && bp.tc_tiles)
+                {
+                    ua.tc_tiles = bp.tc_tiles[l];
+                    ua.tc_status = m.tc_status;
+                    tensor = launch_upward_tc<KIND, N0, N1, N2>(ua, bp.n_tc_tiles[l],
+                                                                bp.tc_fill[l], m.up_path, st,
+                                                                bp.groups * BATCH_NB);
+                }
+                if (!tensor)
+                {
+                    const size_t sm = upward_staged_smem<N0, N1, N2>(m.P_hi, ua.rch, LL.fe_pad);
+                    auto kern = upward_staged_kernel<KIND, N0, N1, N2, MK>;
+                    if (sm > 48 * 1024)
+                        IFGF_CHECK(cudaFuncSetAttribute(
+                            kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+                    kern<<<dim3(LL.n_up, bp.groups * BATCH_NB), UPS_THREADS, sm, st>>>(ua);
+                }
                 IFGF_CHECK_LAUNCH();
                 if (hk)
                     hk->end();

@@ -239,6 +239,10 @@ struct UpArgs
     // staged kernel with MK: wavenumber of plane blockIdx.y, and geo32 holds
     // distance tables (tr = d - d_parent, ti = d_parent / d)
     const KParams* kp_plane = nullptr;
+    // tensor-core kernel: row tiles (first up_idx position, cones, first
+    // plane, planes) and the status word its bounded waits report into
+    const int4* tc_tiles = nullptr;
+    unsigned* tc_status = nullptr;
 };
 
 // One CTA per coarse cone of a box with children (CTAs ordered by cone
@@ -1563,6 +1567,11 @@ __global__ void __launch_bounds__(UPS_THREADS, 10) upward_staged_kernel(UpArgs a
         cv[(size_t)c * a.P_hi + n] = acc[n];
 }
 
+} // namespace ifgf
+#include "upward_tc.cuh"
+namespace ifgf
+{
+
 template <int KIND, int N0, int N1, int N2>
 __global__ void __launch_bounds__(UP_THREADS) upward_mixed_kernel(UpArgs a)
 {
@@ -2274,7 +2283,15 @@ static int run_mult(const MultPtrs& m, const void* d_w, void* d_u, bool real, cu
             if (hk)
                 hk->begin(PROF_UPWARD, l);
             bool staged = false;
+            if constexpr (MIXED)
+            {
+                ua.tc_tiles = LL.tc_tiles;
+                ua.tc_status = m.tc_status;
+                staged = launch_upward_tc<KIND, N0, N1, N2>(ua, LL.n_tc_tiles, LL.tc_fill,
+                                                            m.up_path, st);
+            }
             if constexpr (MIXED && N0 > 0 && (N0 * N1 * N2) % 2 == 0)
+                if (!staged)
             {
                 ua.rch = upward_staged_rch<N0, N1, N2>(LL.fe_pad);
                 const size_t sm = upward_staged_smem<N0, N1, N2>(m.P_hi, ua.rch, LL.fe_pad);

@@ -7,16 +7,18 @@
 #include <cmath>
 #include <complex>
 #include <cstring>
+#include <map>
 #include <sstream>
 
 #include "device_math.cuh"
+#include "tcgen05.cuh"
 #include "mult.hpp"
 #include "operator.hpp"
 
 namespace ifgf
 {
 
-static constexpr int ERR_INVALID = 1, ERR_CUDA = 2, ERR_STATE = 3, ERR_OOM = 4;
+static constexpr int ERR_INVALID = 1, ERR_CUDA = 2, ERR_STATE = 3, ERR_OOM = 4, ERR_TIMEOUT = 5;
 
 // Calls CALL with the compile-time kernel kind KK matching KINDVAR.
 #define IFGF_DISPATCH(KINDVAR, CALL)                                                          \
@@ -133,6 +135,17 @@ struct DeviceState
     std::vector<const UpGeo32*> dgeo32_ptr;
     bool dgeo_ready = false;
     DevBuf<unsigned long long> err;
+    // tensor-core upward transfer: per level the runs of equal slots in
+    // up_idx order (first position, cones); row tiles and their fill per
+    // plane count of a launch; the per-level views handed to a batch; the
+    // status word of the kernels' bounded waits
+    std::vector<std::vector<int2>> tc_runs;
+    std::vector<std::map<int, DevBuf<int4>>> tc_tiles;
+    std::vector<std::map<int, float>> tc_fill;
+    std::vector<const int4*> tcb_ptr;
+    std::vector<int> tcb_n;
+    std::vector<float> tcb_fill;
+    DevBuf<unsigned> tc_status;
     DevBuf<double> io_w, io_u; // staging for host-buffer mult
     std::vector<cudaEvent_t> prof_ev;
     cudaStream_t side = nullptr; // near-field stream
@@ -1062,6 +1075,10 @@ void Operator::setup_device(const double* normals)
     D.leaf_idx.resize(L);
     D.up_idx.resize(L);
     D.up_slot.resize(L);
+    D.tc_runs.assign(L, {});
+    D.tc_tiles.clear();
+    D.tc_tiles.resize(L);
+    D.tc_fill.assign(L, {});
     D.geo64.resize(L);
     D.geo32.resize(L);
     D.fe_list.resize(L);
@@ -1271,6 +1288,15 @@ void Operator::setup_device(const double* normals)
         }
         D.up_idx[l].upload(uidx);
         D.up_slot[l].upload(slot_of);
+        // runs of equal slots (first position, cones): the tensor-core
+        // kernel's tiles never mix slots
+        std::vector<int2>& runs = D.tc_runs[l];
+        runs.clear();
+        for (size_t i = 0; i < slot_of.size(); i++)
+            if (i == 0 || slot_of[i] != slot_of[i - 1])
+                runs.push_back(make_int2((int)i, 1));
+            else
+                runs.back().y++;
     }
     phase("upward_uploads");
     D.lists.assign(L, LevelLists{});
@@ -1285,6 +1311,17 @@ void Operator::setup_device(const double* normals)
                                 sharded ? D.c2f_idx[l].p : nullptr,
                                 sharded ? (int)c2f_host[l].size() : -1};
     }
+    // single-plane tiles of the tensor-core upward transfer (built here, so
+    // that a matvec never allocates them)
+    ensure_tc_tiles(1);
+    for (int l = 0; l < L; l++)
+    {
+        D.lists[l].tc_tiles = D.tc_tiles[l][1].p;
+        D.lists[l].n_tc_tiles = (int)D.tc_tiles[l][1].n;
+        D.lists[l].tc_fill = D.tc_fill[l][1];
+    }
+    D.tc_status.alloc(1);
+    D.tc_status.zero();
     n_coarse_total_ = coarse_tot;
     n_fine_total_ = fine_tot;
     D.lv.upload(lv_);
@@ -1386,6 +1423,117 @@ void Operator::fill_mult_ptrs(MultPtrs& m, bool variant) const
     m.c2f_smem = D.c2f_smem;
     m.kp = make_kparams(kr_, ki_, dx_);
     m.mixed = precision_ == PREC_MIXED;
+    m.up_path = up_path_;
+    m.tc_status = D.tc_status.p;
+}
+
+// Row tiles of the tensor-core upward transfer for launches over `planes`
+// right-hand-side planes, per level: each run of cones of one slot in
+// chunks of up to 32 / planes cones (planes <= 32) x min(planes, 32) planes.
+void Operator::ensure_tc_tiles(int planes)
+{
+    DeviceState& D = *dev_;
+    const int L = (int)lv_.size();
+    const int pq = std::min(planes, 32), cpt = 32 / pq;
+    for (int l = 0; l < L && l < (int)D.tc_runs.size(); l++)
+    {
+        if (D.tc_tiles[l].count(planes))
+            continue;
+        std::vector<int4> t;
+        int64_t rows = 0;
+        for (const int2& r : D.tc_runs[l])
+            for (int cs = 0; cs < r.y; cs += cpt)
+                for (int q0 = 0; q0 < planes; q0 += pq)
+                {
+                    const int nc = std::min(cpt, r.y - cs), nq = std::min(pq, planes - q0);
+                    t.push_back(make_int4(r.x + cs, nc, q0, nq));
+                    rows += (int64_t)nc * nq;
+                }
+        DevBuf<int4>& b = D.tc_tiles[l][planes];
+        if (!t.empty())
+            b.upload(t);
+        D.tc_fill[l][planes] = t.empty() ? 0.f : (float)((double)rows / (32.0 * (double)t.size()));
+    }
+}
+
+// The tensor-core tiles for a batch launch over bp.groups * BATCH_NB planes.
+void Operator::set_batch_tc(BatchPtrs& bp)
+{
+    DeviceState& D = *dev_;
+    const int planes = bp.groups * BATCH_NB;
+    ensure_tc_tiles(planes);
+    const int L = (int)lv_.size();
+    D.tcb_ptr.assign(L, nullptr);
+    D.tcb_n.assign(L, 0);
+    D.tcb_fill.assign(L, 0.f);
+    for (int l = 0; l < L; l++)
+    {
+        const DevBuf<int4>& b = D.tc_tiles[l][planes];
+        D.tcb_ptr[l] = b.p;
+        D.tcb_n[l] = (int)b.n;
+        D.tcb_fill[l] = D.tc_fill[l][planes];
+    }
+    bp.tc_tiles = D.tcb_ptr.data();
+    bp.n_tc_tiles = D.tcb_n.data();
+    bp.tc_fill = D.tcb_fill.data();
+}
+
+// One thread waits on an mbarrier that nothing arrives at, bounded by
+// limit_ns; out[0] = 1 when the wait gave up, out[1..2] = the nanoseconds it
+// waited (low, high word).
+static __global__ void bounded_wait_probe_kernel(unsigned long long limit_ns, unsigned* out)
+{
+    __shared__ __align__(8) unsigned long long bar;
+    if (threadIdx.x != 0)
+        return;
+    tc::mbar_init(tc::smem_u32(&bar), 1);
+    const unsigned long long t0 = tc::global_ns();
+    const bool ok = tc::mbar_wait(tc::smem_u32(&bar), 0, limit_ns);
+    const unsigned long long dt = tc::global_ns() - t0;
+    out[0] = ok ? 0u : 1u;
+    out[1] = (unsigned)(dt & 0xffffffffu);
+    out[2] = (unsigned)(dt >> 32);
+}
+
+void bounded_wait_selftest(double limit_ms, double* waited_ms)
+{
+    if (!(limit_ms > 0) || limit_ms > 10000)
+        throw Error(ERR_INVALID, "limit_ms must be in (0, 10000]");
+    DevBuf<unsigned> out;
+    out.alloc(3);
+    out.zero();
+    bounded_wait_probe_kernel<<<1, 32>>>((unsigned long long)(limit_ms * 1e6), out.p);
+    IFGF_CUDA(cudaGetLastError());
+    unsigned h[3];
+    IFGF_CUDA(cudaMemcpy(h, out.p, sizeof(h), cudaMemcpyDeviceToHost));
+    if (waited_ms)
+        *waited_ms = (double)(((unsigned long long)h[2] << 32) | h[1]) * 1e-6;
+    if (h[0])
+        throw Error(ERR_TIMEOUT, "bounded wait gave up after its limit (as designed)");
+}
+
+void Operator::set_upward_path(int path)
+{
+    if (path < UP_AUTO || path > UP_TENSOR)
+        throw Error(ERR_INVALID, "upward path must be 0 (auto), 1 (FFMA) or 2 (tensor cores)");
+    up_path_ = path;
+}
+
+// Reports a bounded device wait of a tensor-core kernel that gave up (the
+// status word is cleared, so that the next call starts clean).
+void Operator::check_device_status()
+{
+    DeviceState& D = *dev_;
+    if (!D.tc_status.p)
+        return;
+    unsigned st = 0;
+    IFGF_CUDA(cudaMemcpy(&st, D.tc_status.p, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    if (st)
+    {
+        IFGF_CUDA(cudaMemset(D.tc_status.p, 0, sizeof(unsigned)));
+        throw Error(ERR_TIMEOUT, "a tensor-core kernel's bounded wait gave up (pipeline stalled); "
+                                 "results of the last matvec are invalid");
+    }
 }
 
 
@@ -1788,6 +1936,7 @@ void Operator::mult_host(const void* w, void* u, int64_t batch)
         }
         IFGF_CUDA(cudaMemcpy(&missing_, D.err.p, sizeof(unsigned long long),
                              cudaMemcpyDeviceToHost));
+        check_device_status();
         return;
     }
     host_mult_loop(w, u, batch, -1);
@@ -1816,6 +1965,7 @@ void Operator::mult_batch_device(const void* d_w, void* d_u, int64_t batch, void
         {
             bp.nrhs = (int)std::min<int64_t>(planes, batch - done);
             bp.groups = (bp.nrhs + BATCH_NB - 1) / BATCH_NB;
+            set_batch_tc(bp);
             EventHooks log(D, st);
             int r = -1;
             IFGF_DISPATCH(kind_, r = launch_mult_batch_kernels<KK>(
@@ -1932,6 +2082,7 @@ void Operator::mult_wavenumbers_host(const double* k, int64_t nk, const void* w,
     mult_wavenumbers_device(k, nk, D.io_w.p, D.io_u.p, nullptr);
     IFGF_CUDA(cudaMemcpy(u, D.io_u.p, nu * sizeof(double), cudaMemcpyDeviceToHost));
     IFGF_CUDA(cudaMemcpy(&missing_, D.err.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+    check_device_status();
 }
 
 void Operator::mult_wavenumbers_device(const double* k, int64_t nk, const void* d_w, void* d_u,
@@ -2037,6 +2188,7 @@ void Operator::host_mult_loop(const void* w, void* u, int64_t batch, int vkind)
                              cudaMemcpyDeviceToHost));
     }
     IFGF_CUDA(cudaMemcpy(&missing_, D.err.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+    check_device_status();
 }
 
 void Operator::mult_device_external_scratch(const void* d_w, void* d_u, void* stream,

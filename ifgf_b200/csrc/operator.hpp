@@ -100,6 +100,11 @@ class Operator
     // with dk, of the k-derivative kernel
     void direct_eval(const void* w, const int64_t* tidx, int64_t nt, void* out, bool dk = false);
     void set_profiling(bool on);
+    // upward-transfer kernel: UP_AUTO, UP_FFMA or UP_TENSOR (mult.hpp)
+    void set_upward_path(int path);
+    int upward_path() const { return up_path_; }
+    // throws IFGF_ERR_TIMEOUT when a tensor-core kernel's bounded wait gave up
+    void check_device_status();
 
     int kind() const { return kind_; }
     bool is_real() const { return kind_ == K_LAPLACE; }
@@ -123,6 +128,8 @@ class Operator
     int ensure_batch_planes(int64_t want);
     BatchPtrs batch_ptrs(long long in_plane, long long out_plane) const;
     void ensure_distance_tables();
+    void ensure_tc_tiles(int planes);
+    void set_batch_tc(BatchPtrs& bp);
     void setup_device(const double* normals);
     // vkind >= 0: run that kernel with the variant geometry tables
     void launch_mult(const void* d_w, void* d_u, void* stream, bool timed, int vkind = -1);
@@ -142,6 +149,7 @@ class Operator
     int64_t base_n_[3];
     int precision_ = PREC_FP64;
     int device_ = -1; // CUDA device of the device tables (set by init)
+    int up_path_ = 0; // UpwardPath
     bool initialized_ = false;
     bool planned_ = false;
     Plan plan_;

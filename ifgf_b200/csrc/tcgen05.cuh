@@ -1,0 +1,197 @@
+// Thin wrappers over the sm_100a tensor-core, tensor-memory, mbarrier and
+// bulk-copy instructions used by the tensor-core kernels (inline PTX; no
+// library).  Every wait is bounded by the GPU's global timer so that a kernel
+// whose partner never arrives returns with an error status instead of
+// hanging.
+#pragma once
+
+#include <cstdint>
+
+namespace ifgf
+{
+namespace tc
+{
+
+__device__ __forceinline__ unsigned smem_u32(const void* p)
+{
+    return (unsigned)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// ---------------------------------------------------------------------------
+// mbarriers (shared::cta)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void mbar_init(unsigned bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+// makes initialised barriers visible to the asynchronous proxy (bulk copies,
+// tensor-core commits)
+__device__ __forceinline__ void mbar_init_fence()
+{
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive(unsigned bar)
+{
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(bar)
+                 : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned bar, unsigned bytes)
+{
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}" ::"r"(bar),
+                 "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned bar, unsigned parity)
+{
+    unsigned ok;
+    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(ok)
+                 : "r"(bar), "r"(parity)
+                 : "memory");
+    return ok != 0;
+}
+// Waits for the completion of the phase with the given parity; gives up and
+// returns false after limit_ns nanoseconds.
+__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity,
+                                          unsigned long long limit_ns)
+{
+    if (mbar_try_wait(bar, parity))
+        return true;
+    const unsigned long long t0 = global_ns();
+    for (;;)
+    {
+        for (int i = 0; i < 64; i++)
+            if (mbar_try_wait(bar, parity))
+                return true;
+        if (global_ns() - t0 > limit_ns)
+            return false;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// bulk copies global -> shared, completion counted on an mbarrier
+// (addresses 16-byte aligned, size a multiple of 16)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void bulk_g2s(unsigned dst, const void* src, unsigned bytes,
+                                         unsigned bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], "
+                 "%2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+
+// generic-proxy shared-memory writes -> visible to the tensor cores
+__device__ __forceinline__ void fence_proxy_async()
+{
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// ---------------------------------------------------------------------------
+// tensor memory
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void fence_before_sync()
+{
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void fence_after_sync()
+{
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+// one full warp; the base address is written to shared memory
+__device__ __forceinline__ void tmem_alloc(unsigned dst_smem, unsigned ncols)
+{
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(dst_smem),
+                 "r"(ncols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(unsigned taddr, unsigned ncols)
+{
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols)
+                 : "memory");
+}
+// 32 lanes (the warp's quarter) x 8 consecutive 32-bit columns
+__device__ __forceinline__ void tmem_st8(unsigned taddr, const unsigned (&r)[8])
+{
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"r"(
+                     taddr),
+                 "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]),
+                 "r"(r[7])
+                 : "memory");
+}
+__device__ __forceinline__ void tmem_ld16(unsigned taddr, unsigned (&r)[16])
+{
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+                 "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
+                   "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]),
+                   "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+                 : "r"(taddr)
+                 : "memory");
+}
+__device__ __forceinline__ void tmem_wait_st()
+{
+    asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_wait_ld()
+{
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// ---------------------------------------------------------------------------
+// tensor-core MMA, kind::tf32, A from tensor memory, B from shared memory,
+// D (FP32) in tensor memory; one thread issues
+// ---------------------------------------------------------------------------
+// Instruction descriptor: D F32 (bits 4-5 = 1), A and B TF32 (bits 7-9 and
+// 10-12 = 2), both K-major, N >> 3 at bits 17-22, M >> 4 at bits 24-28.
+__host__ __device__ constexpr unsigned idesc_tf32(int M, int N)
+{
+    return (1u << 4) | (2u << 7) | (2u << 10) | ((unsigned)(N >> 3) << 17) |
+           ((unsigned)(M >> 4) << 24);
+}
+// Shared-memory matrix descriptor of a K-major operand without swizzling:
+// 8-row x 16-byte core matrices, `lbo` bytes between the two core matrices
+// of one K step, `sbo` bytes between consecutive 8-row groups; bits 46-47 =
+// 1 (the sm_100 descriptor version).
+__device__ __forceinline__ unsigned long long smem_desc(unsigned addr, unsigned lbo, unsigned sbo)
+{
+    return (unsigned long long)((addr >> 4) & 0x3fffu) |
+           ((unsigned long long)((lbo >> 4) & 0x3fffu) << 16) |
+           ((unsigned long long)((sbo >> 4) & 0x3fffu) << 32) | (1ull << 46);
+}
+__device__ __forceinline__ void mma_tf32_ts(unsigned d_tmem, unsigned a_tmem,
+                                            unsigned long long b_desc, unsigned idesc,
+                                            unsigned accumulate)
+{
+    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                 "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, p;\n\t}" ::"r"(d_tmem),
+                 "r"(a_tmem), "l"(b_desc), "r"(idesc), "r"(accumulate)
+                 : "memory");
+}
+// arrive on `bar` once every MMA this thread issued so far has completed
+__device__ __forceinline__ void mma_commit(unsigned bar)
+{
+    asm volatile(
+        "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+        : "memory");
+}
+
+// x rounded to TF32 (10 explicit mantissa bits, nearest, ties away)
+__device__ __forceinline__ float tf32_round(float x)
+{
+    unsigned u;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(u) : "f"(x));
+    return __uint_as_float(u);
+}
+
+} // namespace tc
+} // namespace ifgf

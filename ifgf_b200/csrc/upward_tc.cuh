@@ -1,0 +1,688 @@
+// Upward transfer on the tensor cores (mixed precision, sm_100a tcgen05).
+//
+// The transfer of one level (transferInterp, ifgfoperator.hpp:1639-1705)
+// evaluates, for every active coarse cone of a parent box and every child,
+// the child's fine Chebyshev interpolant (P_LO = N0 N1 N2 complex
+// coefficients) at the cone's high-order nodes, times the centre-shift
+// factor, and sums over the children.  All boxes of a level have the same
+// shape, so the node positions relative to a child -- its fine element, the
+// local coordinates and the factor -- depend only on the parent element (the
+// slot), the octant and the node (the level's geometry table).  Within one
+// (slot, octant) row the nodes are sorted by child element into runs; every
+// parent cone of the slot evaluates run r against ITS child's coefficient
+// block of that element.  So for the cones of a slot, run r is a product
+//
+//     values[cone][entry] = sum_k coef[child(cone), element_r][k] * T_k(entry),
+//
+// with T_k(entry) = T_a(x) T_b(y) T_c(z) the tensor Chebyshev basis at the
+// entry's local coordinates -- the same basis rows for every cone.  That is
+// a GEMM with the cones (times right-hand-side planes) as M, the run's
+// entries as N and the coefficients as K.
+//
+// One CTA takes a tile of 32 rows (cone, plane) of one slot.  The four
+// lanes of a row in the 128-lane MMA are (real / imaginary part of the
+// coefficients) x (TF32 high / low part of them): A lives in tensor memory
+// (K columns per lane), the basis B = B_hi + B_lo in shared memory, and
+//     D[lane][entry] = A[lane] . B_hi[entry] + A[lane] . B_lo[entry]
+// so that summing the hi / lo lanes gives (A_hi + A_lo)(B_hi + B_lo), an
+// FP32-accurate product (the 3xTF32 idea, with the A split carried by lanes
+// instead of extra MMAs).  D accumulates in FP32 in tensor memory.
+//
+// Warp roles (14 warps):
+//   0-3   A producers: stage a run's coefficient blocks from shared memory
+//         into tensor memory, split into TF32 hi / lo (one lane each)
+//   4-7   epilogue: read D, sum the hi / lo lanes, form the complex value,
+//         multiply by the centre-shift factor and add it into the cone's
+//         node accumulators (shared memory, FP32)
+//   8-11  B producers: the basis rows of a chunk of <= 48 entries
+//   12    loader: per run, the child fine cone of every row, and bulk copies
+//         (cp.async.bulk) of the coefficient blocks into shared memory
+//   13    lane 0 issues the MMAs (tcgen05.mma kind::tf32) and commits
+// Pipelines: coefficient blocks and A in two stages (per run), B one stage,
+// D two stages (per chunk), all synchronised by mbarriers.  Every wait is
+// bounded (global timer); a wait that gives up sets bit 0 of *tc_status and
+// the CTA leaves its loops (the host reports IFGF_ERR_TIMEOUT).
+//
+// A tabulated element may be inactive in a child (the table works in
+// coordinates relative to the parent, the cone activation in absolute ones,
+// which can differ within one rounding of an element boundary); that row's
+// A lanes are zero and the epilogue evaluates its entries from absolute
+// coordinates on the CUDA cores, as the FFMA kernels do.
+#pragma once
+
+#include "tcgen05.cuh"
+
+namespace ifgf
+{
+
+constexpr int UPTC_ROWS = 32;     // rows (cone, plane) per tile
+constexpr int UPTC_NMAX = 48;     // entries per chunk (MMA N <= 48)
+constexpr int UPTC_THREADS = 448; // 14 warps
+constexpr unsigned long long UPTC_WAIT_NS = 2000000000ull; // 2 s per wait
+// tensor-memory columns: A stages at 0 / 128, D stages at 256 / 320
+constexpr int UPTC_TM_A = 0, UPTC_TM_A_STRIDE = 128, UPTC_TM_D = 256, UPTC_TM_D_STRIDE = 64;
+constexpr int UPTC_TM_COLS = 512;
+// shared memory below which two CTAs could share an SM (and then wait for
+// each other's tensor-memory columns): every launch asks for at least this
+constexpr size_t UPTC_SMEM_MIN = 120 * 1024;
+
+// mbarrier indices
+enum UpTcBar
+{
+    UTB_RAW_FULL = 0,  // [2] coefficient blocks landed (loader expect_tx + bulk copies)
+    UTB_RAW_EMPTY = 2, // [2] A producers done reading the stage (4 arrivals)
+    UTB_A_FULL = 4,    // [2] A stage written to tensor memory (4 arrivals)
+    UTB_A_EMPTY = 6,   // [2] MMAs of the run done (commit)
+    UTB_B_FULL = 8,    // B stage written (4 arrivals)
+    UTB_B_EMPTY = 9,   // MMAs of the chunk done (commit)
+    UTB_D_FULL = 10,   // [2] D stage complete (commit)
+    UTB_D_EMPTY = 12,  // [2] epilogue done with the D stage and its entry data (4 arrivals)
+    UTB_META_FULL = 14, // [2] a chunk's entry data (node, factor) written (4 arrivals)
+    UTB_COUNT = 16
+};
+
+// Row flags of a run: which rows have a staged coefficient block.
+constexpr int UPTC_NONE = -1;     // no child at this octant, or a padding row
+constexpr int UPTC_FALLBACK = -2; // element inactive in the child: CUDA-core path
+
+struct UpTcLayout
+{
+    size_t b, raw, acc, meta, rowgf, rowinfo, runs, bars, total;
+    int rs; // accumulator row stride (floats, odd)
+};
+
+template <int N0, int N1, int N2> struct UpTcShape
+{
+    static constexpr int P_LO = N0 * N1 * N2;
+    static constexpr int K = (P_LO + 7) / 8 * 8; // MMA K steps of 8
+    static constexpr int KS = K / 8;
+    static constexpr int RAW_ROW = P_LO * 8;       // bytes of one coefficient block
+    static constexpr int B_BYTES = UPTC_NMAX * K * 4; // one of B_hi / B_lo
+    static constexpr int SBO = (K / 4) * 128;      // bytes between 8-entry groups of B
+    static_assert(K <= UPTC_TM_A_STRIDE, "coefficient blocks wider than a tensor-memory stage");
+    static_assert(RAW_ROW % 16 == 0, "bulk copies move multiples of 16 bytes");
+    static_assert(UPTC_NMAX % 16 == 0 && UPTC_NMAX <= UPTC_TM_D_STRIDE, "chunk width");
+};
+
+template <int N0, int N1, int N2>
+inline __host__ __device__ UpTcLayout uptc_layout(int P_hi, int fe_pad)
+{
+    using S = UpTcShape<N0, N1, N2>;
+    auto al = [](size_t x) { return (x + 15) / 16 * 16; };
+    UpTcLayout L{};
+    L.rs = P_hi | 1;
+    size_t o = 0;
+    L.b = o;
+    o = al(o + 2 * (size_t)S::B_BYTES);
+    L.raw = o;
+    o = al(o + 2 * (size_t)UPTC_ROWS * S::RAW_ROW);
+    L.acc = o;
+    o = al(o + 2 * ((size_t)UPTC_ROWS * L.rs + 16) * sizeof(float));
+    L.meta = o; // [2][NMAX] (node, factor re, factor im, -)
+    o = al(o + 2 * (size_t)UPTC_NMAX * 16);
+    L.rowgf = o; // [2][ROWS]
+    o = al(o + 2 * (size_t)UPTC_ROWS * 4);
+    L.rowinfo = o; // cone, plane, box, child[8] per row; octant used [8]
+    o = al(o + (size_t)UPTC_ROWS * 11 * 4 + 8 * 4);
+    L.runs = o; // [8][fe_pad + 1] int2, then row_n[16]
+    o = al(o + (size_t)8 * (fe_pad + 1) * 8 + 16 * 4);
+    L.bars = o; // the mbarriers, then the tensor-memory base address
+    o = al(o + UTB_COUNT * 8 + 16);
+    L.total = o;
+    return L;
+}
+
+// Dynamic shared memory of a launch (at least UPTC_SMEM_MIN, so that one CTA
+// holds an SM and its tensor-memory allocation never waits).
+template <int N0, int N1, int N2> inline size_t uptc_smem_bytes(int P_hi, int fe_pad)
+{
+    const size_t total = uptc_layout<N0, N1, N2>(P_hi, fe_pad).total;
+    return total < UPTC_SMEM_MIN ? UPTC_SMEM_MIN : total;
+}
+
+// Basis rows of one entry for the K columns [H * K / 2, (H + 1) * K / 2):
+// TF32 high parts into bh, low parts into bl (the K-major core-matrix layout
+// of the B operand; column group k / 4 at 32-float steps).  Compile-time H
+// keeps every index a constant.
+template <int N0, int N1, int N2, int H>
+__device__ __forceinline__ void uptc_basis_half(bool live, float x0, float x1, float x2,
+                                                float* bh, float* bl)
+{
+    constexpr int P_LO = N0 * N1 * N2;
+    constexpr int KH = UpTcShape<N0, N1, N2>::K / 2;
+    float t0[N0], t1[N1], t2[N2];
+    cheb_basis<float, N0>(x0, t0);
+    cheb_basis<float, N1>(x1, t1);
+    cheb_basis<float, N2>(x2, t2);
+#pragma unroll
+    for (int k4 = 0; k4 < KH; k4 += 4)
+    {
+        float hv[4], lv[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+        {
+            const int k = H * KH + k4 + j;
+            float v = 0.f;
+            if (k < P_LO)
+                v = live ? t0[k % N0] * t1[(k / N0) % N1] * t2[k / (N0 * N1)] : 0.f;
+            hv[j] = tc::tf32_round(v);
+            lv[j] = v - hv[j];
+        }
+        const int kk = H * KH + k4;
+        *reinterpret_cast<float4*>(bh + (kk >> 2) * 32) = make_float4(hv[0], hv[1], hv[2], hv[3]);
+        *reinterpret_cast<float4*>(bl + (kk >> 2) * 32) = make_float4(lv[0], lv[1], lv[2], lv[3]);
+    }
+}
+
+template <int KIND, int N0, int N1, int N2>
+__global__ void __launch_bounds__(UPTC_THREADS, 1) upward_tc_kernel(UpArgs a)
+{
+    using S = UpTcShape<N0, N1, N2>;
+    constexpr int P_LO = S::P_LO, K = S::K, KS = S::KS;
+    constexpr int GMAX = UPTC_NMAX / UPGEO_RUN; // groups per chunk
+    extern __shared__ __align__(1024) unsigned char uptc_sm[];
+    unsigned char* sm = uptc_sm;
+    const UpTcLayout LY = uptc_layout<N0, N1, N2>(a.P_hi, a.fe_pad);
+    float* Bs = reinterpret_cast<float*>(sm + LY.b);
+    float2* raw = reinterpret_cast<float2*>(sm + LY.raw);
+    float* acc = reinterpret_cast<float*>(sm + LY.acc);
+    int4* meta = reinterpret_cast<int4*>(sm + LY.meta);
+    int* rowgf = reinterpret_cast<int*>(sm + LY.rowgf);
+    int* row_c = reinterpret_cast<int*>(sm + LY.rowinfo);
+    int* row_q = row_c + UPTC_ROWS;
+    int* row_box = row_q + UPTC_ROWS;
+    int* row_cb = row_box + UPTC_ROWS; // [ROWS][8]
+    int* used = row_cb + 8 * UPTC_ROWS;
+    int2* fl = reinterpret_cast<int2*>(sm + LY.runs);
+    const int FL = a.fe_pad + 1;
+    int* row_n = reinterpret_cast<int*>(fl + 8 * FL);
+    unsigned long long* bars = reinterpret_cast<unsigned long long*>(sm + LY.bars);
+    unsigned* tbase_sm = reinterpret_cast<unsigned*>(bars + UTB_COUNT);
+    const int RS = LY.rs;
+    const int accp = UPTC_ROWS * RS + 16; // floats between the real and imaginary accumulators
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int4 tile = a.tc_tiles[blockIdx.x]; // (first up_idx position, cones, first plane, planes)
+    const int nrows = tile.y * tile.w;
+    const int ngroups = a.P_pad / UPGEO_RUN;
+    const LevelGeom& C = a.GC;
+    const long long nf = (long long)C.nf[0] * C.nf[1] * C.nf[2];
+    const float2* fc2 = reinterpret_cast<const float2*>(a.fcoef);
+    const int slot = a.slot[tile.x];
+    const int el = a.cc_el[a.idx[tile.x]];
+
+    // ---- set-up: row tables, run lists, accumulators, barriers, TMEM ----
+    if (tid < UPTC_ROWS)
+    {
+        const int i = tid;
+        if (i < nrows)
+        {
+            const int c = a.idx[tile.x + i / tile.w];
+            const int box = a.cc_box[c];
+            row_c[i] = c;
+            row_q[i] = tile.z + i % tile.w;
+            row_box[i] = box;
+            for (int o = 0; o < 8; o++)
+                row_cb[8 * i + o] = a.T.box_child[8 * box + o];
+        }
+        else
+        {
+            row_c[i] = -1;
+            row_q[i] = 0;
+            row_box[i] = -1;
+            for (int o = 0; o < 8; o++)
+                row_cb[8 * i + o] = -1;
+        }
+    }
+    if (tid >= 64 && tid < 72)
+    {
+        row_n[tid - 64] = a.fe_pad;
+        row_n[8 + tid - 64] = ngroups;
+    }
+    for (int i = tid; i < 2 * accp; i += blockDim.x)
+        acc[i] = 0.f;
+    if (tid == 96)
+    {
+        for (int b = 0; b < UTB_COUNT; b++)
+        {
+            unsigned cnt = 1;
+            if (b == UTB_RAW_EMPTY || b == UTB_RAW_EMPTY + 1 || b == UTB_A_FULL ||
+                b == UTB_A_FULL + 1 || b == UTB_B_FULL || b == UTB_D_EMPTY ||
+                b == UTB_D_EMPTY + 1 || b == UTB_META_FULL || b == UTB_META_FULL + 1)
+                cnt = 4;
+            tc::mbar_init(tc::smem_u32(bars + b), cnt);
+        }
+        tc::mbar_init_fence();
+    }
+    if (warp == 13)
+        tc::tmem_alloc(tc::smem_u32(tbase_sm), UPTC_TM_COLS);
+    __syncthreads();
+    for (int i = tid; i < 8 * FL; i += blockDim.x)
+    {
+        const int o = i / FL, r = i - o * FL;
+        const int2 f = a.fe_list[((size_t)slot * 8 + o) * FL + r];
+        fl[i] = f;
+        if (f.x < 0 && f.y >= 0)
+        {
+            // the sentinel after the row's last run: (-1, groups of the row)
+            row_n[o] = r;
+            row_n[8 + o] = f.y;
+        }
+    }
+    if (tid < 8)
+    {
+        int u = 0;
+        for (int i = 0; i < nrows; i++)
+            u |= row_cb[8 * i + tid] >= 0;
+        used[tid] = u;
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const unsigned tbase = *tbase_sm;
+    auto bar = [&](int b) { return tc::smem_u32(bars + b); };
+    bool ok = true;
+
+    // (octant, run) -> element, first and end group
+    auto run_info = [&](int o, int r, int& ce, int& g0, int& g1) {
+        const int2 f = fl[o * FL + r];
+        ce = f.x;
+        g0 = f.y;
+        g1 = r + 1 < row_n[o] ? fl[o * FL + r + 1].y : row_n[8 + o];
+    };
+    // child fine cone of row i for octant o, element ce
+    auto row_block = [&](int i, int o, int ce) -> int {
+        const int cb = row_cb[8 * i + o];
+        if (cb < 0)
+            return UPTC_NONE;
+        const int gf = a.fmap[C.fmap_off + (long long)(cb - C.box_off) * nf + ce];
+        return gf >= 0 ? gf : UPTC_FALLBACK;
+    };
+
+    if (warp == 12)
+    {
+        // ---------------- loader ----------------
+        int R = 0;
+        for (int o = 0; o < 8 && ok; o++)
+        {
+            if (!used[o])
+                continue;
+            for (int r = 0; r < row_n[o] && ok; r++, R++)
+            {
+                int ce, g0, g1;
+                run_info(o, r, ce, g0, g1);
+                const int st = R & 1;
+                if (R >= 2 && !tc::mbar_wait(bar(UTB_RAW_EMPTY + st), ((R >> 1) - 1) & 1, UPTC_WAIT_NS))
+                {
+                    ok = false;
+                    break;
+                }
+                const int gf = row_block(lane, o, ce);
+                rowgf[st * UPTC_ROWS + lane] = gf;
+                const unsigned have = __ballot_sync(0xffffffffu, gf >= 0);
+                if (lane == 0)
+                    tc::mbar_arrive_expect_tx(bar(UTB_RAW_FULL + st),
+                                              (unsigned)__popc(have) * (unsigned)S::RAW_ROW);
+                __syncwarp();
+                if (gf >= 0)
+                    tc::bulk_g2s(tc::smem_u32(raw + ((size_t)st * UPTC_ROWS + lane) * P_LO),
+                                 fc2 + (size_t)row_q[lane] * a.fc_plane + (size_t)gf * P_LO,
+                                 (unsigned)S::RAW_ROW, bar(UTB_RAW_FULL + st));
+            }
+        }
+        // a loader that gave up leaves no copy in flight: wait (bounded) for
+        // the stages it armed
+        if (!ok)
+        {
+            if (lane == 0)
+                atomicOr(a.tc_status, 1u);
+            for (int q = (R >= 2 ? R - 2 : 0); q < R; q++)
+                tc::mbar_wait(bar(UTB_RAW_FULL + (q & 1)), (q >> 1) & 1, UPTC_WAIT_NS);
+        }
+    }
+    else if (warp < 4)
+    {
+        // ---------------- A producers ----------------
+        const int L = 32 * warp + lane;
+        const int ri = L >> 2, part = (L >> 1) & 1, split = L & 1;
+        int R = 0;
+        for (int o = 0; o < 8 && ok; o++)
+        {
+            if (!used[o])
+                continue;
+            for (int r = 0; r < row_n[o]; r++, R++)
+            {
+                const int st = R & 1;
+                if (!tc::mbar_wait(bar(UTB_RAW_FULL + st), (R >> 1) & 1, UPTC_WAIT_NS) ||
+                    (R >= 2 && !tc::mbar_wait(bar(UTB_A_EMPTY + st), ((R >> 1) - 1) & 1, UPTC_WAIT_NS)))
+                {
+                    ok = false;
+                    break;
+                }
+                tc::fence_after_sync();
+                const int gf = rowgf[st * UPTC_ROWS + ri];
+                const float2* src = raw + ((size_t)st * UPTC_ROWS + ri) * P_LO;
+                const unsigned taddr =
+                    tbase + ((unsigned)(32 * warp) << 16) + UPTC_TM_A + st * UPTC_TM_A_STRIDE;
+#pragma unroll
+                for (int kc = 0; kc < K; kc += 8)
+                {
+                    unsigned v[8];
+#pragma unroll
+                    for (int j = 0; j < 8; j++)
+                    {
+                        float x = 0.f;
+                        if (gf >= 0 && kc + j < P_LO)
+                        {
+                            const float2 c2 = src[kc + j];
+                            x = part ? c2.y : c2.x;
+                        }
+                        const float hi = tc::tf32_round(x);
+                        v[j] = __float_as_uint(split ? x - hi : hi);
+                    }
+                    tc::tmem_st8(taddr + kc, v);
+                }
+                tc::tmem_wait_st();
+                tc::fence_before_sync();
+                __syncwarp();
+                if (lane == 0)
+                {
+                    tc::mbar_arrive(bar(UTB_A_FULL + st));
+                    tc::mbar_arrive(bar(UTB_RAW_EMPTY + st));
+                }
+            }
+        }
+        if (!ok && lane == 0)
+            atomicOr(a.tc_status, 1u);
+    }
+    else if (warp >= 8 && warp < 12)
+    {
+        // ---------------- B producers ----------------
+        const int tb = tid - 256;          // 0..127
+        const int half = tb >> 6, e = tb & 63; // K half, entry
+        const UpGeo32* __restrict__ trow = nullptr;
+        int Cn = 0;
+        for (int o = 0; o < 8 && ok; o++)
+        {
+            if (!used[o])
+                continue;
+            trow = a.geo32 + ((size_t)slot * 8 + o) * a.P_pad;
+            for (int r = 0; r < row_n[o] && ok; r++)
+            {
+                int ce, g0, g1;
+                run_info(o, r, ce, g0, g1);
+                for (int cg = g0; cg < g1; cg += GMAX, Cn++)
+                {
+                    const int nent = UPGEO_RUN * min(GMAX, g1 - cg);
+                    const int N = (nent + 15) & ~15;
+                    if ((Cn >= 1 && !tc::mbar_wait(bar(UTB_B_EMPTY), (Cn - 1) & 1, UPTC_WAIT_NS)) ||
+                        (Cn >= 2 &&
+                         !tc::mbar_wait(bar(UTB_D_EMPTY + (Cn & 1)), ((Cn >> 1) - 1) & 1, UPTC_WAIT_NS)))
+                    {
+                        ok = false;
+                        break;
+                    }
+                    if (e < N)
+                    {
+                        int node = -1;
+                        float x0 = 0.f, x1 = 0.f, x2 = 0.f, fr = 0.f, fi = 0.f;
+                        if (e < nent)
+                        {
+                            const UpGeo32 g =
+                                trow[(size_t)(e % UPGEO_RUN) * ngroups + cg + e / UPGEO_RUN];
+                            node = g.node;
+                            x0 = g.loc[0];
+                            x1 = g.loc[1];
+                            x2 = g.loc[2];
+                            fr = g.tr;
+                            fi = g.ti;
+                        }
+                        float* bh = Bs + (size_t)(e >> 3) * (S::SBO / 4) + (e & 7) * 4;
+                        float* bl = bh + S::B_BYTES / 4;
+                        if (half == 0)
+                            uptc_basis_half<N0, N1, N2, 0>(node >= 0, x0, x1, x2, bh, bl);
+                        else
+                            uptc_basis_half<N0, N1, N2, 1>(node >= 0, x0, x1, x2, bh, bl);
+                        if (half == 0)
+                            meta[(Cn & 1) * UPTC_NMAX + e] =
+                                make_int4(node, __float_as_int(fr), __float_as_int(fi), 0);
+                    }
+                    tc::fence_proxy_async();
+                    __syncwarp();
+                    if (lane == 0)
+                    {
+                        tc::mbar_arrive(bar(UTB_B_FULL));
+                        tc::mbar_arrive(bar(UTB_META_FULL + (Cn & 1)));
+                    }
+                }
+            }
+        }
+        if (!ok && lane == 0)
+            atomicOr(a.tc_status, 1u);
+    }
+    else if (warp == 13)
+    {
+        // ---------------- MMA issuer ----------------
+        int R = 0, Cn = 0;
+        unsigned last_bar = 0, last_par = 0;
+        bool issued = false;
+        if (lane == 0)
+        {
+            for (int o = 0; o < 8 && ok; o++)
+            {
+                if (!used[o])
+                    continue;
+                for (int r = 0; r < row_n[o] && ok; r++, R++)
+                {
+                    int ce, g0, g1;
+                    run_info(o, r, ce, g0, g1);
+                    const int st = R & 1;
+                    if (!tc::mbar_wait(bar(UTB_A_FULL + st), (R >> 1) & 1, UPTC_WAIT_NS))
+                    {
+                        ok = false;
+                        break;
+                    }
+                    for (int cg = g0; cg < g1; cg += GMAX, Cn++)
+                    {
+                        const int nent = UPGEO_RUN * min(GMAX, g1 - cg);
+                        const int N = (nent + 15) & ~15;
+                        const int ds = Cn & 1;
+                        if (!tc::mbar_wait(bar(UTB_B_FULL), Cn & 1, UPTC_WAIT_NS) ||
+                            (Cn >= 2 &&
+                             !tc::mbar_wait(bar(UTB_D_EMPTY + ds), ((Cn >> 1) - 1) & 1, UPTC_WAIT_NS)))
+                        {
+                            ok = false;
+                            break;
+                        }
+                        tc::fence_after_sync();
+                        const unsigned idesc = tc::idesc_tf32(128, N);
+                        const unsigned dcol = tbase + UPTC_TM_D + ds * UPTC_TM_D_STRIDE;
+                        const unsigned acol = tbase + UPTC_TM_A + st * UPTC_TM_A_STRIDE;
+                        const unsigned bb = tc::smem_u32(Bs);
+#pragma unroll 1
+                        for (int pass = 0; pass < 2; pass++)
+#pragma unroll 1
+                            for (int s = 0; s < KS; s++)
+                                tc::mma_tf32_ts(dcol, acol + 8 * s,
+                                                tc::smem_desc(bb + pass * S::B_BYTES + 256 * s, 128,
+                                                              S::SBO),
+                                                idesc, (pass | s) != 0);
+                        tc::mma_commit(bar(UTB_B_EMPTY));
+                        tc::mma_commit(bar(UTB_D_FULL + ds));
+                        last_bar = bar(UTB_D_FULL + ds);
+                        last_par = (Cn >> 1) & 1;
+                        issued = true;
+                        if (cg + GMAX >= g1)
+                            tc::mma_commit(bar(UTB_A_EMPTY + st));
+                    }
+                }
+            }
+            if (!ok)
+            {
+                atomicOr(a.tc_status, 1u);
+                // leave no MMA in flight
+                if (issued)
+                    tc::mbar_wait(last_bar, last_par, UPTC_WAIT_NS);
+            }
+        }
+        __syncwarp();
+    }
+    else
+    {
+        // ---------------- epilogue (warps 4-7) ----------------
+        const int L = 32 * (warp - 4) + lane;
+        const int ri = L >> 2, part = (L >> 1) & 1, split = L & 1;
+        const bool valid = ri < nrows;
+        float* accp_row = acc + part * accp + ri * RS;
+        const float2* fcq = fc2 + (size_t)row_q[ri] * a.fc_plane;
+        int Cn = 0;
+        for (int o = 0; o < 8 && ok; o++)
+        {
+            if (!used[o])
+                continue;
+            const int cb = row_cb[8 * ri + o];
+            for (int r = 0; r < row_n[o] && ok; r++)
+            {
+                int ce, g0, g1;
+                run_info(o, r, ce, g0, g1);
+                const int flag = valid ? row_block(ri, o, ce) : UPTC_NONE;
+                for (int cg = g0; cg < g1; cg += GMAX, Cn++)
+                {
+                    const int nent = UPGEO_RUN * min(GMAX, g1 - cg);
+                    const int ds = Cn & 1;
+                    // the entry data comes straight from the B producers (its own
+                    // barrier); D from the MMA completion
+                    if (!tc::mbar_wait(bar(UTB_META_FULL + ds), (Cn >> 1) & 1, UPTC_WAIT_NS) ||
+                        !tc::mbar_wait(bar(UTB_D_FULL + ds), (Cn >> 1) & 1, UPTC_WAIT_NS))
+                    {
+                        ok = false;
+                        break;
+                    }
+                    tc::fence_after_sync();
+                    float v[UPTC_NMAX];
+                    const unsigned taddr = tbase + ((unsigned)(32 * (warp - 4)) << 16) + UPTC_TM_D +
+                                           ds * UPTC_TM_D_STRIDE;
+#pragma unroll
+                    for (int c16 = 0; c16 < UPTC_NMAX; c16 += 16)
+                    {
+                        if (c16 < nent)
+                        {
+                            unsigned u[16];
+                            tc::tmem_ld16(taddr + c16, u);
+                            tc::tmem_wait_ld();
+#pragma unroll
+                            for (int j = 0; j < 16; j++)
+                                v[c16 + j] = __uint_as_float(u[j]);
+                        }
+                    }
+                    const int4* mt = meta + ds * UPTC_NMAX;
+#pragma unroll
+                    for (int j = 0; j < UPTC_NMAX; j++)
+                    {
+                        if (j < nent)
+                        {
+                            const float tot = v[j] + __shfl_xor_sync(0xffffffffu, v[j], 1);
+                            const float oth = __shfl_xor_sync(0xffffffffu, tot, 2);
+                            const int4 m = mt[j];
+                            if (flag >= 0 && m.x >= 0 && (j & 1) == split)
+                            {
+                                const float re = part ? oth : tot, im = part ? tot : oth;
+                                const float fr = __int_as_float(m.y), fi = __int_as_float(m.z);
+                                accp_row[m.x] += part ? re * fi + im * fr : re * fr - im * fi;
+                            }
+                        }
+                    }
+                    if (flag == UPTC_FALLBACK)
+                    {
+                        // tabulated element inactive in this child: absolute coordinates
+                        const int box = row_box[ri];
+                        for (int j = split; j < nent; j += 2)
+                        {
+                            const int node = mt[j].x;
+                            if (node < 0)
+                                continue;
+                            const double xc[3] = {a.T.box_c[3 * box], a.T.box_c[3 * box + 1],
+                                                  a.T.box_c[3 * box + 2]};
+                            double y[3];
+                            node_position(a.G, el, node, a.hi_nodes, xc, a.T.box_H[box], y);
+                            const double p[3] = {y[0] - a.T.box_c[3 * cb], y[1] - a.T.box_c[3 * cb + 1],
+                                                 y[2] - a.T.box_c[3 * cb + 2]};
+                            float loc[3];
+                            const int* fm = a.fmap + C.fmap_off + (long long)(cb - C.box_off) * nf;
+                            const int gf2 = fine_lookup_mixed(C, fm, p, a.T.box_H[cb], loc, a.err);
+                            if (gf2 < 0)
+                                continue;
+                            const double e0 = y[0] - xc[0], e1 = y[1] - xc[1], e2 = y[2] - xc[2];
+                            cplx<float> val = {0.f, 0.f};
+                            cfmaf(val, ChebF<N0, N1, N2>::eval(fcq + (size_t)gf2 * P_LO, loc, a.lo),
+                                  transfer_mixed<KIND>(p[0] * p[0] + p[1] * p[1] + p[2] * p[2],
+                                                       e0 * e0 + e1 * e1 + e2 * e2, a.kp));
+                            accp_row[node] += part ? val.im : val.re;
+                        }
+                    }
+                    tc::fence_before_sync();
+                    __syncwarp();
+                    if (lane == 0)
+                        tc::mbar_arrive(bar(UTB_D_EMPTY + ds));
+                }
+            }
+        }
+        if (!ok && lane == 0)
+            atomicOr(a.tc_status, 1u);
+    }
+
+    // ---- write the accumulated node values (plane q, cone c) ----
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    float2* cv = reinterpret_cast<float2*>(a.cvals);
+    for (int i = 0; i < nrows; i++)
+    {
+        float2* out = cv + (size_t)row_q[i] * a.cv_plane + (size_t)row_c[i] * a.P_hi;
+        const float* ar = acc + i * RS;
+        for (int n = tid; n < a.P_hi; n += blockDim.x)
+            out[n] = make_float2(ar[n], ar[accp + n]);
+    }
+    if (warp == 13)
+        tc::tmem_dealloc(tbase, UPTC_TM_COLS);
+}
+
+// Order shapes with a tensor-core upward kernel: the low orders of p = 8 and
+// p = 9 (an even number of coefficients, at most 128 of them).
+template <int N0, int N1, int N2> constexpr bool uptc_shape()
+{
+    return (N0 == 2 && N1 == 5 && N2 == 5) || (N0 == 3 && N1 == 6 && N2 == 6);
+}
+
+// Launches the tensor-core upward transfer of one level over `n_tiles` row
+// tiles (a.tc_tiles) when the path, the order shape, the tile fill and the
+// shared memory allow; returns false (nothing launched) otherwise, and the
+// caller runs an FFMA kernel.
+template <int KIND, int N0, int N1, int N2>
+bool launch_upward_tc(const UpArgs& a, int n_tiles, float fill, int path, cudaStream_t st,
+                      int planes = 1)
+{
+    if constexpr (!uptc_shape<N0, N1, N2>())
+        return false;
+    else
+    {
+        if (path == UP_FFMA || !a.tc_tiles || n_tiles <= 0 || !a.tc_status || a.kp_plane ||
+            (path == UP_AUTO && fill < UPTC_MIN_FILL) || a.fe_pad <= 0)
+            return false;
+        // 16-byte aligned coefficient planes for the bulk copies
+        if (planes > 1 && (a.fc_plane % 2) != 0)
+            return false;
+        const size_t sm = uptc_smem_bytes<N0, N1, N2>(a.P_hi, a.fe_pad);
+        if (sm > 227 * 1024)
+            return false;
+        auto kern = upward_tc_kernel<KIND, N0, N1, N2>;
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)sm);
+        if (e != cudaSuccess)
+            throw Error(2, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
+        kern<<<n_tiles, UPTC_THREADS, sm, st>>>(a);
+        return true;
+    }
+}
+
+} // namespace ifgf

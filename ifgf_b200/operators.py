@@ -127,6 +127,12 @@ class IfgfOperator:
         m = {"fp64": _lib.PREC_FP64, "mixed": _lib.PREC_MIXED}.get(mode, mode)
         check(lib.ifgf_set_precision(self._h, int(m)))
 
+    def set_upward_path(self, path):
+        """Kernel of the mixed-precision upward transfer: "auto" (default;
+        tensor cores on levels with well-filled tiles), "ffma" or "tensor"."""
+        p = {"auto": 0, "ffma": 1, "tensor": 2}.get(path, path)
+        check(lib.ifgf_set_upward_path(self._h, int(p)))
+
     # -- matvec -------------------------------------------------------------
     def _dtype(self):
         return np.float64 if self.REAL else np.complex128

@@ -47,6 +47,11 @@ typedef struct ifgf_operator ifgf_operator;
 #define IFGF_PREC_FP64 0  /* FP64 throughout                                  */
 #define IFGF_PREC_MIXED 1 /* FP32 sums with FP64 phase / final accumulation   */
 
+/* ifgf_set_upward_path */
+#define IFGF_UPWARD_AUTO 0   /* tensor cores on levels with well-filled tiles */
+#define IFGF_UPWARD_FFMA 1   /* FP32 FMA kernels only                         */
+#define IFGF_UPWARD_TENSOR 2 /* tensor cores wherever the order shape allows  */
+
 /* Replaces the IfgfOperator constructor (ifgfoperator.hpp:36-59) together
  * with the plug-in constructors (helmholtz_ifgf.hpp:13-20,
  * laplace_ifgf.hpp:12-15, modified_helmholtz_ifgf.hpp:13-20,
@@ -79,6 +84,25 @@ int ifgf_set_wavenumber(ifgf_operator* op, double k_re, double k_im);
 /* Selects FP64 (default) or the mixed-precision pipeline.  No reference
  * counterpart (the reference is FP64 only). */
 int ifgf_set_precision(ifgf_operator* op, int mode);
+
+/* Selects the kernel of the mixed-precision upward transfer (the
+ * interpolation of children's fine interpolants at parent cone nodes,
+ * transferInterp, ifgfoperator.hpp:1639-1705): IFGF_UPWARD_AUTO (default)
+ * runs it on the tensor cores (tcgen05, split-TF32, FP32-accurate) on the
+ * levels whose cones fill the kernel's 32-row tiles well enough and with
+ * FP32 FMA kernels elsewhere; IFGF_UPWARD_FFMA never uses the tensor cores;
+ * IFGF_UPWARD_TENSOR uses them on every level the order shape allows (low
+ * orders (2,5,5) and (3,6,6)).  FP64 always runs the FP64 kernels.  No
+ * reference counterpart. */
+int ifgf_set_upward_path(ifgf_operator* op, int path);
+
+/* Diagnostic of the bounded waits the tensor-core kernels use: launches a
+ * one-block kernel that waits, for at most limit_ms milliseconds, on a
+ * barrier that nothing arrives at.  Returns IFGF_ERR_TIMEOUT (the wait gave
+ * up and the kernel returned normally, as designed) with the time the kernel
+ * waited in *waited_ms; any other status means the mechanism is broken.  No
+ * reference counterpart. */
+int ifgf_bounded_wait_selftest(double limit_ms, double* waited_ms);
 
 /* Multi-GPU sharding, called before ifgf_init: the operator takes share
  * `rank` of `nranks` -- a contiguous Morton range, balanced by modelled work,
