@@ -48,13 +48,17 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(unsigned bar, unsigned byt
                  "r"(bytes)
                  : "memory");
 }
-__device__ __forceinline__ bool mbar_try_wait(unsigned bar, unsigned parity)
+// Tests for the completion of the phase with the given parity; while it is
+// incomplete the thread is suspended (not spinning: no issue slots or
+// shared-memory bandwidth taken from the working warps) until it completes
+// or about suspend_ns nanoseconds have passed.
+__device__ __forceinline__ bool mbar_try_wait(unsigned bar, unsigned parity, unsigned suspend_ns)
 {
     unsigned ok;
-    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
                  "selp.u32 %0, 1, 0, p;\n\t}"
                  : "=r"(ok)
-                 : "r"(bar), "r"(parity)
+                 : "r"(bar), "r"(parity), "r"(suspend_ns)
                  : "memory");
     return ok != 0;
 }
@@ -63,14 +67,11 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned bar, unsigned parity)
 __device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity,
                                           unsigned long long limit_ns)
 {
-    if (mbar_try_wait(bar, parity))
-        return true;
     const unsigned long long t0 = global_ns();
     for (;;)
     {
-        for (int i = 0; i < 64; i++)
-            if (mbar_try_wait(bar, parity))
-                return true;
+        if (mbar_try_wait(bar, parity, 1000000u))
+            return true;
         if (global_ns() - t0 > limit_ns)
             return false;
     }
@@ -185,12 +186,13 @@ __device__ __forceinline__ void mma_commit(unsigned bar)
         : "memory");
 }
 
-// x rounded to TF32 (10 explicit mantissa bits, nearest, ties away)
+// x rounded to TF32 (10 explicit mantissa bits, nearest, ties away from
+// zero) for finite x below FLT_MAX: half a TF32 unit is added to the
+// magnitude bits and the 13 low bits dropped (sign-magnitude, so both signs
+// round alike).  The tensor core then reads the value exactly.
 __device__ __forceinline__ float tf32_round(float x)
 {
-    unsigned u;
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(u) : "f"(x));
-    return __uint_as_float(u);
+    return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xffffe000u);
 }
 
 } // namespace tc

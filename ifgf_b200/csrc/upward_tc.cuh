@@ -22,11 +22,14 @@
 // One CTA takes a tile of 32 rows (cone, plane) of one slot.  The four
 // lanes of a row in the 128-lane MMA are (real / imaginary part of the
 // coefficients) x (TF32 high / low part of them): A lives in tensor memory
-// (K columns per lane), the basis B = B_hi + B_lo in shared memory, and
-//     D[lane][entry] = A[lane] . B_hi[entry] + A[lane] . B_lo[entry]
-// so that summing the hi / lo lanes gives (A_hi + A_lo)(B_hi + B_lo), an
-// FP32-accurate product (the 3xTF32 idea, with the A split carried by lanes
-// instead of extra MMAs).  D accumulates in FP32 in tensor memory.
+// (K columns per lane), the basis in shared memory as 2 N rows -- the TF32
+// high parts B_hi of the chunk's N entries, then their low parts B_lo -- so
+// that one MMA per K step gives
+//     D[lane][e] = A[lane] . B_hi[e],  D[lane][N + e] = A[lane] . B_lo[e]
+// and summing both columns and the hi / lo lanes gives (A_hi + A_lo)(B_hi +
+// B_lo), an FP32-accurate product (the 3xTF32 idea, with the splits carried
+// by lanes and columns instead of extra MMAs).  D accumulates in FP32 in
+// tensor memory.
 //
 // Warp roles (14 warps):
 //   0-3   A producers: stage a run's coefficient blocks from shared memory
@@ -59,8 +62,9 @@ constexpr int UPTC_ROWS = 32;     // rows (cone, plane) per tile
 constexpr int UPTC_NMAX = 48;     // entries per chunk (MMA N <= 48)
 constexpr int UPTC_THREADS = 448; // 14 warps
 constexpr unsigned long long UPTC_WAIT_NS = 2000000000ull; // 2 s per wait
-// tensor-memory columns: A stages at 0 / 128, D stages at 256 / 320
-constexpr int UPTC_TM_A = 0, UPTC_TM_A_STRIDE = 128, UPTC_TM_D = 256, UPTC_TM_D_STRIDE = 64;
+// tensor-memory columns: A stages at 0 / 128, D stages (2 x 48 columns:
+// high- and low-part basis) at 256 / 352
+constexpr int UPTC_TM_A = 0, UPTC_TM_A_STRIDE = 128, UPTC_TM_D = 256, UPTC_TM_D_STRIDE = 96;
 constexpr int UPTC_TM_COLS = 512;
 // shared memory below which two CTAs could share an SM (and then wait for
 // each other's tensor-memory columns): every launch asks for at least this
@@ -97,11 +101,11 @@ template <int N0, int N1, int N2> struct UpTcShape
     static constexpr int K = (P_LO + 7) / 8 * 8; // MMA K steps of 8
     static constexpr int KS = K / 8;
     static constexpr int RAW_ROW = P_LO * 8;       // bytes of one coefficient block
-    static constexpr int B_BYTES = UPTC_NMAX * K * 4; // one of B_hi / B_lo
-    static constexpr int SBO = (K / 4) * 128;      // bytes between 8-entry groups of B
+    static constexpr int B_BYTES = 2 * UPTC_NMAX * K * 4; // B_hi and B_lo rows of a chunk
+    static constexpr int SBO = (K / 4) * 128;      // bytes between 8-row groups of B
     static_assert(K <= UPTC_TM_A_STRIDE, "coefficient blocks wider than a tensor-memory stage");
     static_assert(RAW_ROW % 16 == 0, "bulk copies move multiples of 16 bytes");
-    static_assert(UPTC_NMAX % 16 == 0 && UPTC_NMAX <= UPTC_TM_D_STRIDE, "chunk width");
+    static_assert(UPTC_NMAX % 16 == 0 && 2 * UPTC_NMAX <= UPTC_TM_D_STRIDE, "chunk width");
 };
 
 template <int N0, int N1, int N2>
@@ -113,7 +117,7 @@ inline __host__ __device__ UpTcLayout uptc_layout(int P_hi, int fe_pad)
     L.rs = P_hi | 1;
     size_t o = 0;
     L.b = o;
-    o = al(o + 2 * (size_t)S::B_BYTES);
+    o = al(o + (size_t)S::B_BYTES);
     L.raw = o;
     o = al(o + 2 * (size_t)UPTC_ROWS * S::RAW_ROW);
     L.acc = o;
@@ -140,7 +144,7 @@ template <int N0, int N1, int N2> inline size_t uptc_smem_bytes(int P_hi, int fe
     return total < UPTC_SMEM_MIN ? UPTC_SMEM_MIN : total;
 }
 
-// Basis rows of one entry for the K columns [H * K / 2, (H + 1) * K / 2):
+// Basis row of one entry for the K columns [H * K / 2, (H + 1) * K / 2):
 // TF32 high parts into bh, low parts into bl (the K-major core-matrix layout
 // of the B operand; column group k / 4 at 32-float steps).  Compile-time H
 // keeps every index a constant.
@@ -174,8 +178,37 @@ __device__ __forceinline__ void uptc_basis_half(bool live, float x0, float x1, f
     }
 }
 
+// The upward contribution of one table entry (parent node `node` of cone
+// element `el` of box `box`, child `cb`) evaluated from absolute coordinates
+// on the CUDA cores, as the FFMA kernels do: for a tabulated element that is
+// inactive in the child.  Out of line: it runs rarely and its code would
+// otherwise crowd the instruction cache of the pipelined roles.
 template <int KIND, int N0, int N1, int N2>
-__global__ void __launch_bounds__(UPTC_THREADS, 1) upward_tc_kernel(UpArgs a)
+__device__ __noinline__ cplx<float> uptc_fallback(const UpArgs& a, int box, int el, int node,
+                                                  int cb, const float2* fcq)
+{
+    const LevelGeom& C = a.GC;
+    const long long nf = (long long)C.nf[0] * C.nf[1] * C.nf[2];
+    const double xc[3] = {a.T.box_c[3 * box], a.T.box_c[3 * box + 1], a.T.box_c[3 * box + 2]};
+    double y[3];
+    node_position(a.G, el, node, a.hi_nodes, xc, a.T.box_H[box], y);
+    const double p[3] = {y[0] - a.T.box_c[3 * cb], y[1] - a.T.box_c[3 * cb + 1],
+                         y[2] - a.T.box_c[3 * cb + 2]};
+    float loc[3];
+    const int* fm = a.fmap + C.fmap_off + (long long)(cb - C.box_off) * nf;
+    const int gf2 = fine_lookup_mixed(C, fm, p, a.T.box_H[cb], loc, a.err);
+    cplx<float> val = {0.f, 0.f};
+    if (gf2 < 0)
+        return val;
+    const double e0 = y[0] - xc[0], e1 = y[1] - xc[1], e2 = y[2] - xc[2];
+    cfmaf(val, ChebF<N0, N1, N2>::eval(fcq + (size_t)gf2 * (N0 * N1 * N2), loc, a.lo),
+          transfer_mixed<KIND>(p[0] * p[0] + p[1] * p[1] + p[2] * p[2],
+                               e0 * e0 + e1 * e1 + e2 * e2, a.kp));
+    return val;
+}
+
+template <int KIND, int N0, int N1, int N2>
+__global__ void __launch_bounds__(UPTC_THREADS, 1) upward_tc_kernel(const __grid_constant__ UpArgs a)
 {
     using S = UpTcShape<N0, N1, N2>;
     constexpr int P_LO = S::P_LO, K = S::K, KS = S::KS;
@@ -364,7 +397,7 @@ __global__ void __launch_bounds__(UPTC_THREADS, 1) upward_tc_kernel(UpArgs a)
                 const float2* src = raw + ((size_t)st * UPTC_ROWS + ri) * P_LO;
                 const unsigned taddr =
                     tbase + ((unsigned)(32 * warp) << 16) + UPTC_TM_A + st * UPTC_TM_A_STRIDE;
-#pragma unroll
+#pragma unroll 1
                 for (int kc = 0; kc < K; kc += 8)
                 {
                     unsigned v[8];
@@ -398,63 +431,79 @@ __global__ void __launch_bounds__(UPTC_THREADS, 1) upward_tc_kernel(UpArgs a)
     else if (warp >= 8 && warp < 12)
     {
         // ---------------- B producers ----------------
-        const int tb = tid - 256;          // 0..127
-        const int half = tb >> 6, e = tb & 63; // K half, entry
-        const UpGeo32* __restrict__ trow = nullptr;
-        int Cn = 0;
-        for (int o = 0; o < 8 && ok; o++)
-        {
-            if (!used[o])
-                continue;
-            trow = a.geo32 + ((size_t)slot * 8 + o) * a.P_pad;
-            for (int r = 0; r < row_n[o] && ok; r++)
+        const int tb = tid - 256;              // 0..127
+        const int half = tb >> 6, e = tb & 63; // K half, entry of the chunk
+        // the (octant, run, chunk) walk, one chunk ahead: the next chunk's
+        // table entry is loaded before this chunk's buffer is free
+        int o = 0, r = 0, cg = 0, g1 = 0, ce = 0, g0 = 0;
+        auto next_chunk = [&](int& po, int& pr, int& pcg, int& pg1) -> bool {
+            // advance (po, pr, pcg) to the next chunk; false at the end
+            if (pcg >= 0)
             {
-                int ce, g0, g1;
-                run_info(o, r, ce, g0, g1);
-                for (int cg = g0; cg < g1; cg += GMAX, Cn++)
-                {
-                    const int nent = UPGEO_RUN * min(GMAX, g1 - cg);
-                    const int N = (nent + 15) & ~15;
-                    if ((Cn >= 1 && !tc::mbar_wait(bar(UTB_B_EMPTY), (Cn - 1) & 1, UPTC_WAIT_NS)) ||
-                        (Cn >= 2 &&
-                         !tc::mbar_wait(bar(UTB_D_EMPTY + (Cn & 1)), ((Cn >> 1) - 1) & 1, UPTC_WAIT_NS)))
-                    {
-                        ok = false;
-                        break;
-                    }
-                    if (e < N)
-                    {
-                        int node = -1;
-                        float x0 = 0.f, x1 = 0.f, x2 = 0.f, fr = 0.f, fi = 0.f;
-                        if (e < nent)
-                        {
-                            const UpGeo32 g =
-                                trow[(size_t)(e % UPGEO_RUN) * ngroups + cg + e / UPGEO_RUN];
-                            node = g.node;
-                            x0 = g.loc[0];
-                            x1 = g.loc[1];
-                            x2 = g.loc[2];
-                            fr = g.tr;
-                            fi = g.ti;
-                        }
-                        float* bh = Bs + (size_t)(e >> 3) * (S::SBO / 4) + (e & 7) * 4;
-                        float* bl = bh + S::B_BYTES / 4;
-                        if (half == 0)
-                            uptc_basis_half<N0, N1, N2, 0>(node >= 0, x0, x1, x2, bh, bl);
-                        else
-                            uptc_basis_half<N0, N1, N2, 1>(node >= 0, x0, x1, x2, bh, bl);
-                        if (half == 0)
-                            meta[(Cn & 1) * UPTC_NMAX + e] =
-                                make_int4(node, __float_as_int(fr), __float_as_int(fi), 0);
-                    }
-                    tc::fence_proxy_async();
-                    __syncwarp();
-                    if (lane == 0)
-                    {
-                        tc::mbar_arrive(bar(UTB_B_FULL));
-                        tc::mbar_arrive(bar(UTB_META_FULL + (Cn & 1)));
-                    }
-                }
+                pcg += GMAX;
+                if (pcg < pg1)
+                    return true;
+                pr++;
+            }
+            for (; po < 8; po++, pr = 0)
+            {
+                if (!used[po] || pr >= row_n[po])
+                    continue;
+                run_info(po, pr, ce, g0, pg1);
+                pcg = g0;
+                return true;
+            }
+            return false;
+        };
+        cg = -1;
+        bool have = next_chunk(o, r, cg, g1);
+        UpGeo32 gnext;
+        auto load_entry = [&](int po, int pcg, int pg1, UpGeo32& g) {
+            const int nent = UPGEO_RUN * min(GMAX, pg1 - pcg);
+            g.node = -1;
+            if (e < nent)
+                g = a.geo32[((size_t)slot * 8 + po) * a.P_pad + (size_t)(e % UPGEO_RUN) * ngroups +
+                            pcg + e / UPGEO_RUN];
+        };
+        if (have)
+            load_entry(o, cg, g1, gnext);
+        for (int Cn = 0; have && ok; Cn++)
+        {
+            const UpGeo32 g = gnext;
+            const int co = o, ccg = cg, cg1 = g1;
+            have = next_chunk(o, r, cg, g1);
+            if (have)
+                load_entry(o, cg, g1, gnext);
+            const int nent = UPGEO_RUN * min(GMAX, cg1 - ccg);
+            const int N = (nent + 15) & ~15;
+            (void)co;
+            if ((Cn >= 1 && !tc::mbar_wait(bar(UTB_B_EMPTY), (Cn - 1) & 1, UPTC_WAIT_NS)) ||
+                (Cn >= 2 &&
+                 !tc::mbar_wait(bar(UTB_D_EMPTY + (Cn & 1)), ((Cn >> 1) - 1) & 1, UPTC_WAIT_NS)))
+            {
+                ok = false;
+                break;
+            }
+            if (e < N)
+            {
+                const int node = e < nent ? g.node : -1;
+                // high part at row e, low part at row N + e
+                float* bh = Bs + (size_t)(e >> 3) * (S::SBO / 4) + (e & 7) * 4;
+                float* bl = Bs + (size_t)((N + e) >> 3) * (S::SBO / 4) + ((N + e) & 7) * 4;
+                if (half == 0)
+                    uptc_basis_half<N0, N1, N2, 0>(node >= 0, g.loc[0], g.loc[1], g.loc[2], bh, bl);
+                else
+                    uptc_basis_half<N0, N1, N2, 1>(node >= 0, g.loc[0], g.loc[1], g.loc[2], bh, bl);
+                if (half == 0)
+                    meta[(Cn & 1) * UPTC_NMAX + e] =
+                        make_int4(node, __float_as_int(g.tr), __float_as_int(g.ti), 0);
+            }
+            tc::fence_proxy_async();
+            __syncwarp();
+            if (lane == 0)
+            {
+                tc::mbar_arrive(bar(UTB_B_FULL));
+                tc::mbar_arrive(bar(UTB_META_FULL + (Cn & 1)));
             }
         }
         if (!ok && lane == 0)
@@ -495,18 +544,16 @@ __global__ void __launch_bounds__(UPTC_THREADS, 1) upward_tc_kernel(UpArgs a)
                             break;
                         }
                         tc::fence_after_sync();
-                        const unsigned idesc = tc::idesc_tf32(128, N);
+                        // rows [0, N): B_hi, [N, 2N): B_lo of the chunk's entries
+                        const unsigned idesc = tc::idesc_tf32(128, 2 * N);
                         const unsigned dcol = tbase + UPTC_TM_D + ds * UPTC_TM_D_STRIDE;
                         const unsigned acol = tbase + UPTC_TM_A + st * UPTC_TM_A_STRIDE;
                         const unsigned bb = tc::smem_u32(Bs);
 #pragma unroll 1
-                        for (int pass = 0; pass < 2; pass++)
-#pragma unroll 1
-                            for (int s = 0; s < KS; s++)
-                                tc::mma_tf32_ts(dcol, acol + 8 * s,
-                                                tc::smem_desc(bb + pass * S::B_BYTES + 256 * s, 128,
-                                                              S::SBO),
-                                                idesc, (pass | s) != 0);
+                        for (int s = 0; s < KS; s++)
+                            tc::mma_tf32_ts(dcol, acol + 8 * s,
+                                            tc::smem_desc(bb + 256 * s, 128, S::SBO), idesc,
+                                            s != 0);
                         tc::mma_commit(bar(UTB_B_EMPTY));
                         tc::mma_commit(bar(UTB_D_FULL + ds));
                         last_bar = bar(UTB_D_FULL + ds);
@@ -535,96 +582,115 @@ __global__ void __launch_bounds__(UPTC_THREADS, 1) upward_tc_kernel(UpArgs a)
         const bool valid = ri < nrows;
         float* accp_row = acc + part * accp + ri * RS;
         const float2* fcq = fc2 + (size_t)row_q[ri] * a.fc_plane;
+        const unsigned tq = tbase + ((unsigned)(32 * (warp - 4)) << 16) + UPTC_TM_D;
         int Cn = 0;
-        for (int o = 0; o < 8 && ok; o++)
+        // row flag of the next run, looked up one run ahead
+        int po = 0, pr = 0, pce = 0, pg0 = 0, pg1 = 0;
+        auto next_run = [&](int& qo, int& qr) -> bool {
+            for (; qo < 8; qo++, qr = 0)
+                if (used[qo] && qr < row_n[qo])
+                    return true;
+            return false;
+        };
+        bool more = next_run(po, pr);
+        int flag_next = UPTC_NONE;
+        if (more)
         {
-            if (!used[o])
-                continue;
-            const int cb = row_cb[8 * ri + o];
-            for (int r = 0; r < row_n[o] && ok; r++)
+            run_info(po, pr, pce, pg0, pg1);
+            flag_next = valid ? row_block(ri, po, pce) : UPTC_NONE;
+        }
+        while (more && ok)
+        {
+            const int o = po, g0 = pg0, g1 = pg1, flag = flag_next;
+            pr++;
+            more = next_run(po, pr);
+            if (more)
             {
-                int ce, g0, g1;
-                run_info(o, r, ce, g0, g1);
-                const int flag = valid ? row_block(ri, o, ce) : UPTC_NONE;
-                for (int cg = g0; cg < g1; cg += GMAX, Cn++)
+                run_info(po, pr, pce, pg0, pg1);
+                flag_next = valid ? row_block(ri, po, pce) : UPTC_NONE;
+            }
+            const int cb = row_cb[8 * ri + o];
+            for (int cg = g0; cg < g1; cg += GMAX, Cn++)
+            {
+                const int nent = UPGEO_RUN * min(GMAX, g1 - cg);
+                const int N = (nent + 15) & ~15;
+                const int ds = Cn & 1;
+                // the entry data comes straight from the B producers (its own
+                // barrier); D from the MMA completion
+                if (!tc::mbar_wait(bar(UTB_META_FULL + ds), (Cn >> 1) & 1, UPTC_WAIT_NS) ||
+                    !tc::mbar_wait(bar(UTB_D_FULL + ds), (Cn >> 1) & 1, UPTC_WAIT_NS))
                 {
-                    const int nent = UPGEO_RUN * min(GMAX, g1 - cg);
-                    const int ds = Cn & 1;
-                    // the entry data comes straight from the B producers (its own
-                    // barrier); D from the MMA completion
-                    if (!tc::mbar_wait(bar(UTB_META_FULL + ds), (Cn >> 1) & 1, UPTC_WAIT_NS) ||
-                        !tc::mbar_wait(bar(UTB_D_FULL + ds), (Cn >> 1) & 1, UPTC_WAIT_NS))
-                    {
-                        ok = false;
-                        break;
-                    }
-                    tc::fence_after_sync();
-                    float v[UPTC_NMAX];
-                    const unsigned taddr = tbase + ((unsigned)(32 * (warp - 4)) << 16) + UPTC_TM_D +
-                                           ds * UPTC_TM_D_STRIDE;
-#pragma unroll
-                    for (int c16 = 0; c16 < UPTC_NMAX; c16 += 16)
-                    {
-                        if (c16 < nent)
-                        {
-                            unsigned u[16];
-                            tc::tmem_ld16(taddr + c16, u);
-                            tc::tmem_wait_ld();
-#pragma unroll
-                            for (int j = 0; j < 16; j++)
-                                v[c16 + j] = __uint_as_float(u[j]);
-                        }
-                    }
-                    const int4* mt = meta + ds * UPTC_NMAX;
-#pragma unroll
-                    for (int j = 0; j < UPTC_NMAX; j++)
-                    {
-                        if (j < nent)
-                        {
-                            const float tot = v[j] + __shfl_xor_sync(0xffffffffu, v[j], 1);
-                            const float oth = __shfl_xor_sync(0xffffffffu, tot, 2);
-                            const int4 m = mt[j];
-                            if (flag >= 0 && m.x >= 0 && (j & 1) == split)
-                            {
-                                const float re = part ? oth : tot, im = part ? tot : oth;
-                                const float fr = __int_as_float(m.y), fi = __int_as_float(m.z);
-                                accp_row[m.x] += part ? re * fi + im * fr : re * fr - im * fi;
-                            }
-                        }
-                    }
-                    if (flag == UPTC_FALLBACK)
-                    {
-                        // tabulated element inactive in this child: absolute coordinates
-                        const int box = row_box[ri];
-                        for (int j = split; j < nent; j += 2)
-                        {
-                            const int node = mt[j].x;
-                            if (node < 0)
-                                continue;
-                            const double xc[3] = {a.T.box_c[3 * box], a.T.box_c[3 * box + 1],
-                                                  a.T.box_c[3 * box + 2]};
-                            double y[3];
-                            node_position(a.G, el, node, a.hi_nodes, xc, a.T.box_H[box], y);
-                            const double p[3] = {y[0] - a.T.box_c[3 * cb], y[1] - a.T.box_c[3 * cb + 1],
-                                                 y[2] - a.T.box_c[3 * cb + 2]};
-                            float loc[3];
-                            const int* fm = a.fmap + C.fmap_off + (long long)(cb - C.box_off) * nf;
-                            const int gf2 = fine_lookup_mixed(C, fm, p, a.T.box_H[cb], loc, a.err);
-                            if (gf2 < 0)
-                                continue;
-                            const double e0 = y[0] - xc[0], e1 = y[1] - xc[1], e2 = y[2] - xc[2];
-                            cplx<float> val = {0.f, 0.f};
-                            cfmaf(val, ChebF<N0, N1, N2>::eval(fcq + (size_t)gf2 * P_LO, loc, a.lo),
-                                  transfer_mixed<KIND>(p[0] * p[0] + p[1] * p[1] + p[2] * p[2],
-                                                       e0 * e0 + e1 * e1 + e2 * e2, a.kp));
-                            accp_row[node] += part ? val.im : val.re;
-                        }
-                    }
-                    tc::fence_before_sync();
-                    __syncwarp();
-                    if (lane == 0)
-                        tc::mbar_arrive(bar(UTB_D_EMPTY + ds));
+                    ok = false;
+                    break;
                 }
+                tc::fence_after_sync();
+                const int4* mt = meta + ds * UPTC_NMAX;
+                const unsigned taddr = tq + ds * UPTC_TM_D_STRIDE;
+#pragma unroll 1
+                for (int c16 = 0; c16 < nent; c16 += 16)
+                {
+                    unsigned uh[16], ul[16];
+                    tc::tmem_ld16(taddr + c16, uh);     // A . B_hi
+                    tc::tmem_ld16(taddr + N + c16, ul); // A . B_lo
+                    tc::tmem_wait_ld();
+                    // contributions of the block's 16 entries; this thread adds
+                    // those of its parity (8), all loads before all stores: the
+                    // entries of a chunk have distinct nodes, so the
+                    // read-modify-writes are independent and overlap
+                    // stage by stage over the 16 entries, so that the shuffles of
+                    // different entries overlap: v = (B_hi + B_lo) columns, sum of
+                    // the TF32 hi / lo lanes, exchange of the real / imaginary lanes
+                    float v[16], w[16];
+#pragma unroll
+                    for (int j = 0; j < 16; j++)
+                        v[j] = __uint_as_float(uh[j]) + __uint_as_float(ul[j]);
+#pragma unroll
+                    for (int j = 0; j < 16; j++)
+                        w[j] = __shfl_xor_sync(0xffffffffu, v[j], 1);
+#pragma unroll
+                    for (int j = 0; j < 16; j++)
+                        v[j] += w[j];
+#pragma unroll
+                    for (int j = 0; j < 16; j++)
+                        w[j] = __shfl_xor_sync(0xffffffffu, v[j], 2);
+                    // this thread's entries: those of its split parity
+                    float cv[8];
+                    int nd[8];
+#pragma unroll
+                    for (int i = 0; i < 8; i++)
+                    {
+                        const float tot = split ? v[2 * i + 1] : v[2 * i];
+                        const float oth = split ? w[2 * i + 1] : w[2 * i];
+                        const int jj = c16 + 2 * i + split;
+                        const int4 m = mt[min(jj, UPTC_NMAX - 1)];
+                        const float re = part ? oth : tot, im = part ? tot : oth;
+                        const float fr = __int_as_float(m.y), fi = __int_as_float(m.z);
+                        cv[i] = part ? re * fi + im * fr : re * fr - im * fi;
+                        nd[i] = (flag >= 0 && jj < nent) ? m.x : -1;
+                    }
+                    float old[8];
+#pragma unroll
+                    for (int i = 0; i < 8; i++)
+                        old[i] = nd[i] >= 0 ? accp_row[nd[i]] : 0.f;
+#pragma unroll
+                    for (int i = 0; i < 8; i++)
+                        if (nd[i] >= 0)
+                            accp_row[nd[i]] = old[i] + cv[i];
+                }
+                if (flag == UPTC_FALLBACK)
+                    for (int j = split; j < nent; j += 2)
+                    {
+                        const int node = mt[j].x;
+                        if (node < 0)
+                            continue;
+                        const cplx<float> val =
+                            uptc_fallback<KIND, N0, N1, N2>(a, row_box[ri], el, node, cb, fcq);
+                        accp_row[node] += part ? val.im : val.re;
+                    }
+                tc::fence_before_sync();
+                __syncwarp();
+                if (lane == 0)
+                    tc::mbar_arrive(bar(UTB_D_EMPTY + ds));
             }
         }
         if (!ok && lane == 0)
