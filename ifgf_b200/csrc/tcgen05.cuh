@@ -178,6 +178,14 @@ __device__ __forceinline__ void mma_tf32_ts(unsigned d_tmem, unsigned a_tmem,
                  "r"(a_tmem), "l"(b_desc), "r"(idesc), "r"(accumulate)
                  : "memory");
 }
+// true in exactly one lane of the (converged) calling warp
+__device__ __forceinline__ bool elect_one()
+{
+    unsigned pred = 0;
+    asm volatile("{\n\t.reg .pred P;\n\telect.sync _|P, 0xffffffff;\n\tselp.u32 %0, 1, 0, P;\n\t}"
+                 : "=r"(pred));
+    return pred != 0;
+}
 // arrive on `bar` once every MMA this thread issued so far has completed
 __device__ __forceinline__ void mma_commit(unsigned bar)
 {

@@ -397,21 +397,27 @@ __global__ void __launch_bounds__(UPTC_THREADS, 1) upward_tc_kernel(const __grid
                 const float2* src = raw + ((size_t)st * UPTC_ROWS + ri) * P_LO;
                 const unsigned taddr =
                     tbase + ((unsigned)(32 * warp) << 16) + UPTC_TM_A + st * UPTC_TM_A_STRIDE;
-#pragma unroll 1
+                // 16-byte loads of two coefficients (the block is 16-byte aligned and
+                // P_LO even); this lane keeps its part (real / imaginary) and its
+                // TF32 piece (high / low)
+                const float4* src4 = reinterpret_cast<const float4*>(src);
+#pragma unroll 2
                 for (int kc = 0; kc < K; kc += 8)
                 {
                     unsigned v[8];
 #pragma unroll
-                    for (int j = 0; j < 8; j++)
+                    for (int j = 0; j < 8; j += 2)
                     {
-                        float x = 0.f;
+                        float x0 = 0.f, x1 = 0.f;
                         if (gf >= 0 && kc + j < P_LO)
                         {
-                            const float2 c2 = src[kc + j];
-                            x = part ? c2.y : c2.x;
+                            const float4 c4 = src4[(kc + j) >> 1];
+                            x0 = part ? c4.y : c4.x;
+                            x1 = part ? c4.w : c4.z;
                         }
-                        const float hi = tc::tf32_round(x);
-                        v[j] = __float_as_uint(split ? x - hi : hi);
+                        const float h0 = tc::tf32_round(x0), h1 = tc::tf32_round(x1);
+                        v[j] = __float_as_uint(split ? x0 - h0 : h0);
+                        v[j + 1] = __float_as_uint(split ? x1 - h1 : h1);
                     }
                     tc::tmem_st8(taddr + kc, v);
                 }
@@ -512,67 +518,71 @@ __global__ void __launch_bounds__(UPTC_THREADS, 1) upward_tc_kernel(const __grid
     else if (warp == 13)
     {
         // ---------------- MMA issuer ----------------
+        // The whole warp walks the sequence and waits (converged); one
+        // elected lane issues each chunk's fully unrolled K loop.  Issued
+        // from a diverged single thread, every MMA took ~3x as long.
         int R = 0, Cn = 0;
         unsigned last_bar = 0, last_par = 0;
         bool issued = false;
-        if (lane == 0)
+        const unsigned bb = tc::smem_u32(Bs);
+        for (int o = 0; o < 8 && ok; o++)
         {
-            for (int o = 0; o < 8 && ok; o++)
+            if (!used[o])
+                continue;
+            for (int r = 0; r < row_n[o] && ok; r++, R++)
             {
-                if (!used[o])
-                    continue;
-                for (int r = 0; r < row_n[o] && ok; r++, R++)
+                int ce, g0, g1;
+                run_info(o, r, ce, g0, g1);
+                const int st = R & 1;
+                if (!tc::mbar_wait(bar(UTB_A_FULL + st), (R >> 1) & 1, UPTC_WAIT_NS))
                 {
-                    int ce, g0, g1;
-                    run_info(o, r, ce, g0, g1);
-                    const int st = R & 1;
-                    if (!tc::mbar_wait(bar(UTB_A_FULL + st), (R >> 1) & 1, UPTC_WAIT_NS))
+                    ok = false;
+                    break;
+                }
+                for (int cg = g0; cg < g1; cg += GMAX, Cn++)
+                {
+                    const int nent = UPGEO_RUN * min(GMAX, g1 - cg);
+                    const int N = (nent + 15) & ~15;
+                    const int ds = Cn & 1;
+                    if (!tc::mbar_wait(bar(UTB_B_FULL), Cn & 1, UPTC_WAIT_NS) ||
+                        (Cn >= 2 &&
+                         !tc::mbar_wait(bar(UTB_D_EMPTY + ds), ((Cn >> 1) - 1) & 1, UPTC_WAIT_NS)))
                     {
                         ok = false;
                         break;
                     }
-                    for (int cg = g0; cg < g1; cg += GMAX, Cn++)
+                    tc::fence_after_sync();
+                    // rows [0, N): B_hi, [N, 2N): B_lo of the chunk's entries
+                    const unsigned idesc = tc::idesc_tf32(128, 2 * N);
+                    const unsigned dcol = tbase + UPTC_TM_D + ds * UPTC_TM_D_STRIDE;
+                    const unsigned acol = tbase + UPTC_TM_A + st * UPTC_TM_A_STRIDE;
+                    const bool last = cg + GMAX >= g1;
+                    if (tc::elect_one())
                     {
-                        const int nent = UPGEO_RUN * min(GMAX, g1 - cg);
-                        const int N = (nent + 15) & ~15;
-                        const int ds = Cn & 1;
-                        if (!tc::mbar_wait(bar(UTB_B_FULL), Cn & 1, UPTC_WAIT_NS) ||
-                            (Cn >= 2 &&
-                             !tc::mbar_wait(bar(UTB_D_EMPTY + ds), ((Cn >> 1) - 1) & 1, UPTC_WAIT_NS)))
-                        {
-                            ok = false;
-                            break;
-                        }
-                        tc::fence_after_sync();
-                        // rows [0, N): B_hi, [N, 2N): B_lo of the chunk's entries
-                        const unsigned idesc = tc::idesc_tf32(128, 2 * N);
-                        const unsigned dcol = tbase + UPTC_TM_D + ds * UPTC_TM_D_STRIDE;
-                        const unsigned acol = tbase + UPTC_TM_A + st * UPTC_TM_A_STRIDE;
-                        const unsigned bb = tc::smem_u32(Bs);
-#pragma unroll 1
+#pragma unroll
                         for (int s = 0; s < KS; s++)
                             tc::mma_tf32_ts(dcol, acol + 8 * s,
-                                            tc::smem_desc(bb + 256 * s, 128, S::SBO), idesc,
-                                            s != 0);
+                                            tc::smem_desc(bb + 256 * s, 128, S::SBO), idesc, s != 0);
                         tc::mma_commit(bar(UTB_B_EMPTY));
                         tc::mma_commit(bar(UTB_D_FULL + ds));
-                        last_bar = bar(UTB_D_FULL + ds);
-                        last_par = (Cn >> 1) & 1;
-                        issued = true;
-                        if (cg + GMAX >= g1)
+                        if (last)
                             tc::mma_commit(bar(UTB_A_EMPTY + st));
                     }
+                    __syncwarp();
+                    last_bar = bar(UTB_D_FULL + ds);
+                    last_par = (Cn >> 1) & 1;
+                    issued = true;
                 }
             }
-            if (!ok)
-            {
-                atomicOr(a.tc_status, 1u);
-                // leave no MMA in flight
-                if (issued)
-                    tc::mbar_wait(last_bar, last_par, UPTC_WAIT_NS);
-            }
         }
-        __syncwarp();
+        if (!ok)
+        {
+            if (lane == 0)
+                atomicOr(a.tc_status, 1u);
+            // leave no MMA in flight
+            if (issued)
+                tc::mbar_wait(last_bar, last_par, UPTC_WAIT_NS);
+        }
     }
     else
     {
