@@ -90,6 +90,13 @@ __device__ __forceinline__ void bulk_g2s(unsigned dst, const void* src, unsigned
                  : "memory");
 }
 
+// asks for `bytes` (a multiple of 16, 16-byte aligned) of global memory to be
+// brought into L2 (no completion to wait for)
+__device__ __forceinline__ void prefetch_l2(const void* src, unsigned bytes)
+{
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+}
+
 // generic-proxy shared-memory writes -> visible to the tensor cores
 __device__ __forceinline__ void fence_proxy_async()
 {
@@ -136,6 +143,23 @@ __device__ __forceinline__ void tmem_ld16(unsigned taddr, unsigned (&r)[16])
                  : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
                    "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]),
                    "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+                 : "r"(taddr)
+                 : "memory");
+}
+// 16 lanes (base lane in the address: 0 or 16 of the warp's quarter) x 8
+// columns: thread t holds columns 2 (t % 4), 2 (t % 4) + 1 of lane t / 4 (r[0],
+// r[1]) and of lane t / 4 + 8 (r[2], r[3])
+__device__ __forceinline__ void tmem_st16x256(unsigned taddr, unsigned r0, unsigned r1, unsigned r2,
+                                              unsigned r3)
+{
+    asm volatile("tcgen05.st.sync.aligned.16x256b.x1.b32 [%0], {%1,%2,%3,%4};" ::"r"(taddr), "r"(r0),
+                 "r"(r1), "r"(r2), "r"(r3)
+                 : "memory");
+}
+__device__ __forceinline__ void tmem_ld16x256(unsigned taddr, unsigned (&r)[4])
+{
+    asm volatile("tcgen05.ld.sync.aligned.16x256b.x1.b32 {%0,%1,%2,%3}, [%4];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
                  : "r"(taddr)
                  : "memory");
 }

@@ -21,7 +21,10 @@
 //
 // One CTA takes a tile of 32 rows (cone, plane) of one slot.  The four
 // lanes of a row in the 128-lane MMA are (real / imaginary part of the
-// coefficients) x (TF32 high / low part of them): A lives in tensor memory
+// coefficients) x (TF32 high / low part of them) -- row 8 q + i of quarter q
+// at lanes 32 q + 16 s + 8 p + i (part p, piece s), so that the 16-lane x
+// 256-bit tensor-memory accesses hand one thread both parts of a row, and
+// two of them both pieces, without shuffles.  A lives in tensor memory
 // (K columns per lane), the basis in shared memory as 2 N rows -- the TF32
 // high parts B_hi of the chunk's N entries, then their low parts B_lo -- so
 // that one MMA per K step gives
@@ -32,17 +35,18 @@
 // tensor memory.
 //
 // Warp roles (14 warps):
-//   0-3   A producers: stage a run's coefficient blocks from shared memory
-//         into tensor memory, split into TF32 hi / lo (one lane each)
+//   0-3   A producers: load a run's coefficient blocks (global memory, made
+//         L2-resident by the loader) into tensor memory, split into TF32
+//         high / low pieces
 //   4-7   epilogue: read D, sum the hi / lo lanes, form the complex value,
 //         multiply by the centre-shift factor and add it into the cone's
 //         node accumulators (shared memory, FP32)
 //   8-11  B producers: the basis rows of a chunk of <= 48 entries
-//   12    loader: per run, the child fine cone of every row, and bulk copies
-//         (cp.async.bulk) of the coefficient blocks into shared memory
+//   12    loader: per run, the child fine cone of every row (looked up up
+//         to four runs ahead) and an L2 prefetch of its coefficient block
 //   13    lane 0 issues the MMAs (tcgen05.mma kind::tf32) and commits
-// Pipelines: coefficient blocks and A in two stages (per run), B one stage,
-// D two stages (per chunk), all synchronised by mbarriers.  Every wait is
+// Pipelines: look-ups in four stages, A in two (per run), B and D in two
+// (per chunk), all synchronised by mbarriers.  Every wait is
 // bounded (global timer); a wait that gives up sets bit 0 of *tc_status and
 // the CTA leaves its loops (the host reports IFGF_ERR_TIMEOUT).
 //
@@ -73,17 +77,18 @@ constexpr size_t UPTC_SMEM_MIN = 120 * 1024;
 // mbarrier indices
 enum UpTcBar
 {
-    UTB_RAW_FULL = 0,  // [2] coefficient blocks landed (loader expect_tx + bulk copies)
-    UTB_RAW_EMPTY = 2, // [2] A producers done reading the stage (4 arrivals)
-    UTB_A_FULL = 4,    // [2] A stage written to tensor memory (4 arrivals)
-    UTB_A_EMPTY = 6,   // [2] MMAs of the run done (commit)
-    UTB_B_FULL = 8,    // B stage written (4 arrivals)
-    UTB_B_EMPTY = 9,   // MMAs of the chunk done (commit)
-    UTB_D_FULL = 10,   // [2] D stage complete (commit)
-    UTB_D_EMPTY = 12,  // [2] epilogue done with the D stage and its entry data (4 arrivals)
-    UTB_META_FULL = 14, // [2] a chunk's entry data (node, factor) written (4 arrivals)
-    UTB_COUNT = 16
+    UTB_ROW_FULL = 0,   // [4] a run's fine cones looked up (loader)
+    UTB_ROW_EMPTY = 4,  // [4] A producers done with them (4 arrivals)
+    UTB_A_FULL = 8,     // [2] A stage written to tensor memory (4 arrivals)
+    UTB_A_EMPTY = 10,   // [2] MMAs of the run done (commit)
+    UTB_B_FULL = 12,    // [2] B stage written (4 arrivals)
+    UTB_B_EMPTY = 14,   // [2] MMAs of the chunk done (commit)
+    UTB_D_FULL = 16,    // [2] D stage complete (commit)
+    UTB_D_EMPTY = 18,   // [2] epilogue done with the D stage and its entry data (4 arrivals)
+    UTB_META_FULL = 20, // [2] a chunk's entry data (node, factor) written (4 arrivals)
+    UTB_COUNT = 22
 };
+constexpr int UPTC_ROW_STAGES = 4; // look-up stages the loader runs ahead of the A producers
 
 // Row flags of a run: which rows have a staged coefficient block.
 constexpr int UPTC_NONE = -1;     // no child at this octant, or a padding row
@@ -91,7 +96,7 @@ constexpr int UPTC_FALLBACK = -2; // element inactive in the child: CUDA-core pa
 
 struct UpTcLayout
 {
-    size_t b, raw, acc, meta, rowgf, rowinfo, runs, bars, total;
+    size_t b, acc, meta, rowgf, rowinfo, runs, bars, total;
     int rs; // accumulator row stride (floats, odd)
 };
 
@@ -100,11 +105,11 @@ template <int N0, int N1, int N2> struct UpTcShape
     static constexpr int P_LO = N0 * N1 * N2;
     static constexpr int K = (P_LO + 7) / 8 * 8; // MMA K steps of 8
     static constexpr int KS = K / 8;
-    static constexpr int RAW_ROW = P_LO * 8;       // bytes of one coefficient block
+    static constexpr int RAW_ROW = P_LO * 8;       // bytes of one coefficient block (L2 prefetch)
     static constexpr int B_BYTES = 2 * UPTC_NMAX * K * 4; // B_hi and B_lo rows of a chunk
     static constexpr int SBO = (K / 4) * 128;      // bytes between 8-row groups of B
     static_assert(K <= UPTC_TM_A_STRIDE, "coefficient blocks wider than a tensor-memory stage");
-    static_assert(RAW_ROW % 16 == 0, "bulk copies move multiples of 16 bytes");
+    static_assert(RAW_ROW % 16 == 0, "bulk prefetches move multiples of 16 bytes");
     static_assert(UPTC_NMAX % 16 == 0 && 2 * UPTC_NMAX <= UPTC_TM_D_STRIDE, "chunk width");
 };
 
@@ -116,16 +121,14 @@ inline __host__ __device__ UpTcLayout uptc_layout(int P_hi, int fe_pad)
     UpTcLayout L{};
     L.rs = P_hi | 1;
     size_t o = 0;
-    L.b = o;
-    o = al(o + (size_t)S::B_BYTES);
-    L.raw = o;
-    o = al(o + 2 * (size_t)UPTC_ROWS * S::RAW_ROW);
+    L.b = o; // two stages
+    o = al(o + 2 * (size_t)S::B_BYTES);
     L.acc = o;
     o = al(o + 2 * ((size_t)UPTC_ROWS * L.rs + 16) * sizeof(float));
     L.meta = o; // [2][NMAX] (node, factor re, factor im, -)
     o = al(o + 2 * (size_t)UPTC_NMAX * 16);
-    L.rowgf = o; // [2][ROWS]
-    o = al(o + 2 * (size_t)UPTC_ROWS * 4);
+    L.rowgf = o; // [UPTC_ROW_STAGES][ROWS]
+    o = al(o + UPTC_ROW_STAGES * (size_t)UPTC_ROWS * 4);
     L.rowinfo = o; // cone, plane, box, child[8] per row; octant used [8]
     o = al(o + (size_t)UPTC_ROWS * 11 * 4 + 8 * 4);
     L.runs = o; // [8][fe_pad + 1] int2, then row_n[16]
@@ -217,7 +220,6 @@ __global__ void __launch_bounds__(UPTC_THREADS, 1) upward_tc_kernel(const __grid
     unsigned char* sm = uptc_sm;
     const UpTcLayout LY = uptc_layout<N0, N1, N2>(a.P_hi, a.fe_pad);
     float* Bs = reinterpret_cast<float*>(sm + LY.b);
-    float2* raw = reinterpret_cast<float2*>(sm + LY.raw);
     float* acc = reinterpret_cast<float*>(sm + LY.acc);
     int4* meta = reinterpret_cast<int4*>(sm + LY.meta);
     int* rowgf = reinterpret_cast<int*>(sm + LY.rowgf);
@@ -279,9 +281,10 @@ __global__ void __launch_bounds__(UPTC_THREADS, 1) upward_tc_kernel(const __grid
         for (int b = 0; b < UTB_COUNT; b++)
         {
             unsigned cnt = 1;
-            if (b == UTB_RAW_EMPTY || b == UTB_RAW_EMPTY + 1 || b == UTB_A_FULL ||
-                b == UTB_A_FULL + 1 || b == UTB_B_FULL || b == UTB_D_EMPTY ||
-                b == UTB_D_EMPTY + 1 || b == UTB_META_FULL || b == UTB_META_FULL + 1)
+            if ((b >= UTB_ROW_EMPTY && b < UTB_ROW_EMPTY + UPTC_ROW_STAGES) ||
+                b == UTB_A_FULL || b == UTB_A_FULL + 1 || b == UTB_B_FULL || b == UTB_B_FULL + 1 ||
+                b == UTB_D_EMPTY || b == UTB_D_EMPTY + 1 || b == UTB_META_FULL ||
+                b == UTB_META_FULL + 1)
                 cnt = 4;
             tc::mbar_init(tc::smem_u32(bars + b), cnt);
         }
@@ -335,49 +338,82 @@ __global__ void __launch_bounds__(UPTC_THREADS, 1) upward_tc_kernel(const __grid
     if (warp == 12)
     {
         // ---------------- loader ----------------
-        int R = 0;
-        for (int o = 0; o < 8 && ok; o++)
+        // The fine-cone lookups (a dependent, often uncached global load per
+        // row) run two runs ahead of the copies that need them.
+        auto next_run = [&](int& qo, int& qr) -> bool {
+            for (; qo < 8; qo++, qr = 0)
+                if (used[qo] && qr < row_n[qo])
+                    return true;
+            return false;
+        };
+        int lo_[3] = {0, 0, 0}, lr_[3] = {0, 0, 0}, lgf[3] = {UPTC_NONE, UPTC_NONE, UPTC_NONE};
+        bool lv[3] = {false, false, false};
         {
-            if (!used[o])
-                continue;
-            for (int r = 0; r < row_n[o] && ok; r++, R++)
+            int qo = 0, qr = 0;
+            for (int i = 0; i < 3; i++)
             {
-                int ce, g0, g1;
-                run_info(o, r, ce, g0, g1);
-                const int st = R & 1;
-                if (R >= 2 && !tc::mbar_wait(bar(UTB_RAW_EMPTY + st), ((R >> 1) - 1) & 1, UPTC_WAIT_NS))
-                {
-                    ok = false;
+                lv[i] = next_run(qo, qr);
+                if (!lv[i])
                     break;
-                }
-                const int gf = row_block(lane, o, ce);
-                rowgf[st * UPTC_ROWS + lane] = gf;
-                const unsigned have = __ballot_sync(0xffffffffu, gf >= 0);
-                if (lane == 0)
-                    tc::mbar_arrive_expect_tx(bar(UTB_RAW_FULL + st),
-                                              (unsigned)__popc(have) * (unsigned)S::RAW_ROW);
-                __syncwarp();
-                if (gf >= 0)
-                    tc::bulk_g2s(tc::smem_u32(raw + ((size_t)st * UPTC_ROWS + lane) * P_LO),
-                                 fc2 + (size_t)row_q[lane] * a.fc_plane + (size_t)gf * P_LO,
-                                 (unsigned)S::RAW_ROW, bar(UTB_RAW_FULL + st));
+                lo_[i] = qo;
+                lr_[i] = qr;
+                int ce, g0, g1;
+                run_info(qo, qr, ce, g0, g1);
+                lgf[i] = row_block(lane, qo, ce);
+                qr++;
             }
         }
-        // a loader that gave up leaves no copy in flight: wait (bounded) for
-        // the stages it armed
-        if (!ok)
+        int R = 0;
+        while (lv[0] && ok)
         {
+            const int gf = lgf[0];
+            // shift the look-ahead window and start the lookup of the run after it
+            int qo = lo_[2], qr = lr_[2] + 1;
+            const bool have_last = lv[2];
+            lo_[0] = lo_[1];
+            lr_[0] = lr_[1];
+            lgf[0] = lgf[1];
+            lv[0] = lv[1];
+            lo_[1] = lo_[2];
+            lr_[1] = lr_[2];
+            lgf[1] = lgf[2];
+            lv[1] = lv[2];
+            lv[2] = have_last && next_run(qo, qr);
+            if (lv[2])
+            {
+                lo_[2] = qo;
+                lr_[2] = qr;
+                int ce, g0, g1;
+                run_info(qo, qr, ce, g0, g1);
+                lgf[2] = row_block(lane, qo, ce);
+            }
+            const int st = R % UPTC_ROW_STAGES, ph = R / UPTC_ROW_STAGES;
+            if (R >= UPTC_ROW_STAGES && !tc::mbar_wait(bar(UTB_ROW_EMPTY + st), (ph - 1) & 1, UPTC_WAIT_NS))
+            {
+                ok = false;
+                break;
+            }
+            if (gf >= 0)
+                tc::prefetch_l2(fc2 + (size_t)row_q[lane] * a.fc_plane + (size_t)gf * P_LO,
+                                (unsigned)S::RAW_ROW);
+            rowgf[st * UPTC_ROWS + lane] = gf;
+            __syncwarp();
             if (lane == 0)
-                atomicOr(a.tc_status, 1u);
-            for (int q = (R >= 2 ? R - 2 : 0); q < R; q++)
-                tc::mbar_wait(bar(UTB_RAW_FULL + (q & 1)), (q >> 1) & 1, UPTC_WAIT_NS);
+                tc::mbar_arrive(bar(UTB_ROW_FULL + st));
+            R++;
         }
+        if (!ok && lane == 0)
+            atomicOr(a.tc_status, 1u);
     }
     else if (warp < 4)
     {
         // ---------------- A producers ----------------
-        const int L = 32 * warp + lane;
-        const int ri = L >> 2, part = (L >> 1) & 1, split = L & 1;
+        // warp q writes rows 8 q .. 8 q + 7: thread t takes row 8 q + t / 4 and,
+        // per group of 8 coefficients, the pair 2 (t % 4), 2 (t % 4) + 1 -- one
+        // 16-byte load gives both parts of both, stored to the high-piece lanes
+        // (16 s = 0) and the low-piece lanes (16 s = 16) of the row
+        const int ri = 8 * warp + (lane >> 2), t0 = lane & 3;
+        const unsigned lane_base = tbase + ((unsigned)(32 * warp) << 16);
         int R = 0;
         for (int o = 0; o < 8 && ok; o++)
         {
@@ -386,49 +422,47 @@ __global__ void __launch_bounds__(UPTC_THREADS, 1) upward_tc_kernel(const __grid
             for (int r = 0; r < row_n[o]; r++, R++)
             {
                 const int st = R & 1;
-                if (!tc::mbar_wait(bar(UTB_RAW_FULL + st), (R >> 1) & 1, UPTC_WAIT_NS) ||
+                const int rs = R % UPTC_ROW_STAGES;
+                if (!tc::mbar_wait(bar(UTB_ROW_FULL + rs), (R / UPTC_ROW_STAGES) & 1, UPTC_WAIT_NS) ||
                     (R >= 2 && !tc::mbar_wait(bar(UTB_A_EMPTY + st), ((R >> 1) - 1) & 1, UPTC_WAIT_NS)))
                 {
                     ok = false;
                     break;
                 }
                 tc::fence_after_sync();
-                const int gf = rowgf[st * UPTC_ROWS + ri];
-                const float2* src = raw + ((size_t)st * UPTC_ROWS + ri) * P_LO;
-                const unsigned taddr =
-                    tbase + ((unsigned)(32 * warp) << 16) + UPTC_TM_A + st * UPTC_TM_A_STRIDE;
-                // 16-byte loads of two coefficients (the block is 16-byte aligned and
-                // P_LO even); this lane keeps its part (real / imaginary) and its
-                // TF32 piece (high / low)
-                const float4* src4 = reinterpret_cast<const float4*>(src);
-#pragma unroll 2
-                for (int kc = 0; kc < K; kc += 8)
-                {
-                    unsigned v[8];
+                const int gf = rowgf[rs * UPTC_ROWS + ri];
+                __syncwarp();
+                if (lane == 0)
+                    tc::mbar_arrive(bar(UTB_ROW_EMPTY + rs));
+                const float4* src4 = reinterpret_cast<const float4*>(
+                    fc2 + (size_t)row_q[ri] * a.fc_plane + (size_t)(gf >= 0 ? gf : 0) * P_LO);
+                const unsigned col = UPTC_TM_A + st * UPTC_TM_A_STRIDE;
+                // all of this thread's coefficient pairs in flight at once
+                float4 c4[K / 8];
 #pragma unroll
-                    for (int j = 0; j < 8; j += 2)
-                    {
-                        float x0 = 0.f, x1 = 0.f;
-                        if (gf >= 0 && kc + j < P_LO)
-                        {
-                            const float4 c4 = src4[(kc + j) >> 1];
-                            x0 = part ? c4.y : c4.x;
-                            x1 = part ? c4.w : c4.z;
-                        }
-                        const float h0 = tc::tf32_round(x0), h1 = tc::tf32_round(x1);
-                        v[j] = __float_as_uint(split ? x0 - h0 : h0);
-                        v[j + 1] = __float_as_uint(split ? x1 - h1 : h1);
-                    }
-                    tc::tmem_st8(taddr + kc, v);
+                for (int g = 0; g < K / 8; g++)
+                {
+                    const int k = 8 * g + 2 * t0; // the coefficient pair of this thread
+                    c4[g] = (gf >= 0 && k < P_LO) ? __ldg(src4 + (k >> 1))
+                                                  : make_float4(0.f, 0.f, 0.f, 0.f);
+                }
+#pragma unroll
+                for (int g = 0; g < K / 8; g++)
+                {
+                    const float h0 = tc::tf32_round(c4[g].x), h1 = tc::tf32_round(c4[g].z);
+                    const float h2 = tc::tf32_round(c4[g].y), h3 = tc::tf32_round(c4[g].w);
+                    // (real k, real k + 1) -> lane of part 0, (imag k, imag k + 1) -> part 1
+                    tc::tmem_st16x256(lane_base + col + 8 * g, __float_as_uint(h0),
+                                      __float_as_uint(h1), __float_as_uint(h2), __float_as_uint(h3));
+                    tc::tmem_st16x256(lane_base + (16u << 16) + col + 8 * g,
+                                      __float_as_uint(c4[g].x - h0), __float_as_uint(c4[g].z - h1),
+                                      __float_as_uint(c4[g].y - h2), __float_as_uint(c4[g].w - h3));
                 }
                 tc::tmem_wait_st();
                 tc::fence_before_sync();
                 __syncwarp();
                 if (lane == 0)
-                {
                     tc::mbar_arrive(bar(UTB_A_FULL + st));
-                    tc::mbar_arrive(bar(UTB_RAW_EMPTY + st));
-                }
             }
         }
         if (!ok && lane == 0)
@@ -483,19 +517,21 @@ __global__ void __launch_bounds__(UPTC_THREADS, 1) upward_tc_kernel(const __grid
             const int nent = UPGEO_RUN * min(GMAX, cg1 - ccg);
             const int N = (nent + 15) & ~15;
             (void)co;
-            if ((Cn >= 1 && !tc::mbar_wait(bar(UTB_B_EMPTY), (Cn - 1) & 1, UPTC_WAIT_NS)) ||
-                (Cn >= 2 &&
-                 !tc::mbar_wait(bar(UTB_D_EMPTY + (Cn & 1)), ((Cn >> 1) - 1) & 1, UPTC_WAIT_NS)))
+            const int bs = Cn & 1; // B stage; also the stage of the entry data
+            if (Cn >= 2 &&
+                (!tc::mbar_wait(bar(UTB_B_EMPTY + bs), ((Cn >> 1) - 1) & 1, UPTC_WAIT_NS) ||
+                 !tc::mbar_wait(bar(UTB_D_EMPTY + bs), ((Cn >> 1) - 1) & 1, UPTC_WAIT_NS)))
             {
                 ok = false;
                 break;
             }
+            float* Bst = Bs + (size_t)bs * (S::B_BYTES / 4);
             if (e < N)
             {
                 const int node = e < nent ? g.node : -1;
                 // high part at row e, low part at row N + e
-                float* bh = Bs + (size_t)(e >> 3) * (S::SBO / 4) + (e & 7) * 4;
-                float* bl = Bs + (size_t)((N + e) >> 3) * (S::SBO / 4) + ((N + e) & 7) * 4;
+                float* bh = Bst + (size_t)(e >> 3) * (S::SBO / 4) + (e & 7) * 4;
+                float* bl = Bst + (size_t)((N + e) >> 3) * (S::SBO / 4) + ((N + e) & 7) * 4;
                 if (half == 0)
                     uptc_basis_half<N0, N1, N2, 0>(node >= 0, g.loc[0], g.loc[1], g.loc[2], bh, bl);
                 else
@@ -508,8 +544,8 @@ __global__ void __launch_bounds__(UPTC_THREADS, 1) upward_tc_kernel(const __grid
             __syncwarp();
             if (lane == 0)
             {
-                tc::mbar_arrive(bar(UTB_B_FULL));
-                tc::mbar_arrive(bar(UTB_META_FULL + (Cn & 1)));
+                tc::mbar_arrive(bar(UTB_B_FULL + bs));
+                tc::mbar_arrive(bar(UTB_META_FULL + bs));
             }
         }
         if (!ok && lane == 0)
@@ -544,7 +580,7 @@ __global__ void __launch_bounds__(UPTC_THREADS, 1) upward_tc_kernel(const __grid
                     const int nent = UPGEO_RUN * min(GMAX, g1 - cg);
                     const int N = (nent + 15) & ~15;
                     const int ds = Cn & 1;
-                    if (!tc::mbar_wait(bar(UTB_B_FULL), Cn & 1, UPTC_WAIT_NS) ||
+                    if (!tc::mbar_wait(bar(UTB_B_FULL + ds), (Cn >> 1) & 1, UPTC_WAIT_NS) ||
                         (Cn >= 2 &&
                          !tc::mbar_wait(bar(UTB_D_EMPTY + ds), ((Cn >> 1) - 1) & 1, UPTC_WAIT_NS)))
                     {
@@ -562,8 +598,9 @@ __global__ void __launch_bounds__(UPTC_THREADS, 1) upward_tc_kernel(const __grid
 #pragma unroll
                         for (int s = 0; s < KS; s++)
                             tc::mma_tf32_ts(dcol, acol + 8 * s,
-                                            tc::smem_desc(bb + 256 * s, 128, S::SBO), idesc, s != 0);
-                        tc::mma_commit(bar(UTB_B_EMPTY));
+                                            tc::smem_desc(bb + ds * S::B_BYTES + 256 * s, 128, S::SBO),
+                                            idesc, s != 0);
+                        tc::mma_commit(bar(UTB_B_EMPTY + ds));
                         tc::mma_commit(bar(UTB_D_FULL + ds));
                         if (last)
                             tc::mma_commit(bar(UTB_A_EMPTY + st));
@@ -587,12 +624,17 @@ __global__ void __launch_bounds__(UPTC_THREADS, 1) upward_tc_kernel(const __grid
     else
     {
         // ---------------- epilogue (warps 4-7) ----------------
-        const int L = 32 * (warp - 4) + lane;
-        const int ri = L >> 2, part = (L >> 1) & 1, split = L & 1;
+        // warp 4 + q reads rows 8 q .. 8 q + 7: thread t takes row 8 q + t / 4
+        // and, per group of 8 entries, entries 2 (t % 4) and 2 (t % 4) + 1, for
+        // which four 16x256b loads (TF32 piece s of A x high / low rows of B)
+        // give both parts; their sum is the full value, with no shuffles
+        const int q = warp - 4;
+        const int ri = 8 * q + (lane >> 2), t0 = lane & 3;
         const bool valid = ri < nrows;
-        float* accp_row = acc + part * accp + ri * RS;
+        float* acc_re = acc + ri * RS;
+        float* acc_im = acc_re + accp;
         const float2* fcq = fc2 + (size_t)row_q[ri] * a.fc_plane;
-        const unsigned tq = tbase + ((unsigned)(32 * (warp - 4)) << 16) + UPTC_TM_D;
+        const unsigned lane_base = tbase + ((unsigned)(32 * q) << 16);
         int Cn = 0;
         // row flag of the next run, looked up one run ahead
         int po = 0, pr = 0, pce = 0, pg0 = 0, pg1 = 0;
@@ -635,67 +677,72 @@ __global__ void __launch_bounds__(UPTC_THREADS, 1) upward_tc_kernel(const __grid
                 }
                 tc::fence_after_sync();
                 const int4* mt = meta + ds * UPTC_NMAX;
-                const unsigned taddr = tq + ds * UPTC_TM_D_STRIDE;
+                const unsigned dcol = UPTC_TM_D + ds * UPTC_TM_D_STRIDE;
+                // 16 entries at a time (two groups of 8; the chunk is padded to a
+                // multiple of 16 columns, so both groups' loads are in range):
+                // eight tensor-memory loads, one wait; then this thread's four
+                // entries -- distinct nodes, so all accumulator loads are issued
+                // before any store
+                auto load_group = [&](int g, unsigned (&x)[4][4]) {
+                    tc::tmem_ld16x256(lane_base + dcol + g, x[0]);                  // A_hi . B_hi
+                    tc::tmem_ld16x256(lane_base + dcol + N + g, x[1]);              // A_hi . B_lo
+                    tc::tmem_ld16x256(lane_base + (16u << 16) + dcol + g, x[2]);     // A_lo . B_hi
+                    tc::tmem_ld16x256(lane_base + (16u << 16) + dcol + N + g, x[3]); // A_lo . B_lo
+                };
 #pragma unroll 1
-                for (int c16 = 0; c16 < nent; c16 += 16)
+                for (int g = 0; g < nent; g += 16)
                 {
-                    unsigned uh[16], ul[16];
-                    tc::tmem_ld16(taddr + c16, uh);     // A . B_hi
-                    tc::tmem_ld16(taddr + N + c16, ul); // A . B_lo
-                    tc::tmem_wait_ld();
-                    // contributions of the block's 16 entries; this thread adds
-                    // those of its parity (8), all loads before all stores: the
-                    // entries of a chunk have distinct nodes, so the
-                    // read-modify-writes are independent and overlap
-                    // stage by stage over the 16 entries, so that the shuffles of
-                    // different entries overlap: v = (B_hi + B_lo) columns, sum of
-                    // the TF32 hi / lo lanes, exchange of the real / imaginary lanes
-                    float v[16], w[16];
+                    unsigned u[2][4][4];
+                    load_group(g, u[0]);
+                    load_group(g + 8, u[1]);
+                    int nd[4];
+                    float fr[4], fi[4];
 #pragma unroll
-                    for (int j = 0; j < 16; j++)
-                        v[j] = __uint_as_float(uh[j]) + __uint_as_float(ul[j]);
-#pragma unroll
-                    for (int j = 0; j < 16; j++)
-                        w[j] = __shfl_xor_sync(0xffffffffu, v[j], 1);
-#pragma unroll
-                    for (int j = 0; j < 16; j++)
-                        v[j] += w[j];
-#pragma unroll
-                    for (int j = 0; j < 16; j++)
-                        w[j] = __shfl_xor_sync(0xffffffffu, v[j], 2);
-                    // this thread's entries: those of its split parity
-                    float cv[8];
-                    int nd[8];
-#pragma unroll
-                    for (int i = 0; i < 8; i++)
+                    for (int j = 0; j < 4; j++)
                     {
-                        const float tot = split ? v[2 * i + 1] : v[2 * i];
-                        const float oth = split ? w[2 * i + 1] : w[2 * i];
-                        const int jj = c16 + 2 * i + split;
-                        const int4 m = mt[min(jj, UPTC_NMAX - 1)];
-                        const float re = part ? oth : tot, im = part ? tot : oth;
-                        const float fr = __int_as_float(m.y), fi = __int_as_float(m.z);
-                        cv[i] = part ? re * fi + im * fr : re * fr - im * fi;
-                        nd[i] = (flag >= 0 && jj < nent) ? m.x : -1;
+                        // entries g + 2 t0 + {0, 1} and g + 8 + 2 t0 + {0, 1}
+                        const int e = g + 8 * (j >> 1) + 2 * t0 + (j & 1);
+                        const int4 m = mt[min(e, UPTC_NMAX - 1)];
+                        nd[j] = (flag >= 0 && e < nent) ? m.x : -1;
+                        fr[j] = __int_as_float(m.y);
+                        fi[j] = __int_as_float(m.z);
                     }
-                    float old[8];
+                    float ar[4], ai[4];
 #pragma unroll
-                    for (int i = 0; i < 8; i++)
-                        old[i] = nd[i] >= 0 ? accp_row[nd[i]] : 0.f;
+                    for (int j = 0; j < 4; j++)
+                    {
+                        ar[j] = nd[j] >= 0 ? acc_re[nd[j]] : 0.f;
+                        ai[j] = nd[j] >= 0 ? acc_im[nd[j]] : 0.f;
+                    }
+                    tc::tmem_wait_ld();
 #pragma unroll
-                    for (int i = 0; i < 8; i++)
-                        if (nd[i] >= 0)
-                            accp_row[nd[i]] = old[i] + cv[i];
+                    for (int j = 0; j < 4; j++)
+                    {
+                        const unsigned(&x)[4][4] = u[j >> 1];
+                        const int h = j & 1;
+                        // (re, im) of the entry: the four TF32 products summed
+                        const float re = (__uint_as_float(x[0][h]) + __uint_as_float(x[1][h])) +
+                                         (__uint_as_float(x[2][h]) + __uint_as_float(x[3][h]));
+                        const float im =
+                            (__uint_as_float(x[0][2 + h]) + __uint_as_float(x[1][2 + h])) +
+                            (__uint_as_float(x[2][2 + h]) + __uint_as_float(x[3][2 + h]));
+                        if (nd[j] >= 0)
+                        {
+                            acc_re[nd[j]] = ar[j] + (re * fr[j] - im * fi[j]);
+                            acc_im[nd[j]] = ai[j] + (re * fi[j] + im * fr[j]);
+                        }
+                    }
                 }
                 if (flag == UPTC_FALLBACK)
-                    for (int j = split; j < nent; j += 2)
+                    for (int e = t0; e < nent; e += 4)
                     {
-                        const int node = mt[j].x;
+                        const int node = mt[e].x;
                         if (node < 0)
                             continue;
                         const cplx<float> val =
                             uptc_fallback<KIND, N0, N1, N2>(a, row_box[ri], el, node, cb, fcq);
-                        accp_row[node] += part ? val.im : val.re;
+                        acc_re[node] += val.re;
+                        acc_im[node] += val.im;
                     }
                 tc::fence_before_sync();
                 __syncwarp();
