@@ -90,11 +90,16 @@ __device__ __forceinline__ void bulk_g2s(unsigned dst, const void* src, unsigned
                  : "memory");
 }
 
-// asks for `bytes` (a multiple of 16, 16-byte aligned) of global memory to be
-// brought into L2 (no completion to wait for)
+// asks for the 128-byte lines covering [src, src + bytes) to be brought into
+// L2 (one plain prefetch per line: no completion to wait for, and unlike a
+// bulk prefetch no trip through the copy engine)
 __device__ __forceinline__ void prefetch_l2(const void* src, unsigned bytes)
 {
-    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+    const char* p = static_cast<const char*>(src);
+    const char* end = p + bytes;
+    for (p = reinterpret_cast<const char*>(reinterpret_cast<unsigned long long>(p) & ~127ull);
+         p < end; p += 128)
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(p) : "memory");
 }
 
 // generic-proxy shared-memory writes -> visible to the tensor cores

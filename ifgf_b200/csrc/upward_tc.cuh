@@ -93,6 +93,7 @@ constexpr int UPTC_ROW_STAGES = 4; // look-up stages the loader runs ahead of th
 // Row flags of a run: which rows have a staged coefficient block.
 constexpr int UPTC_NONE = -1;     // no child at this octant, or a padding row
 constexpr int UPTC_FALLBACK = -2; // element inactive in the child: CUDA-core path
+constexpr int UPTC_END = -3;      // loader look-up slot past the tile's last run
 
 struct UpTcLayout
 {
@@ -339,59 +340,43 @@ __global__ void __launch_bounds__(UPTC_THREADS, 1) upward_tc_kernel(const __grid
     {
         // ---------------- loader ----------------
         // The fine-cone lookups (a dependent, often uncached global load per
-        // row) run two runs ahead of the copies that need them.
+        // row) run four runs ahead of their use: the loop is unrolled four
+        // times so that look-up slot i (a register) is read only by step i,
+        // four runs after its load was issued.
         auto next_run = [&](int& qo, int& qr) -> bool {
             for (; qo < 8; qo++, qr = 0)
                 if (used[qo] && qr < row_n[qo])
                     return true;
             return false;
         };
-        int lo_[3] = {0, 0, 0}, lr_[3] = {0, 0, 0}, lgf[3] = {UPTC_NONE, UPTC_NONE, UPTC_NONE};
-        bool lv[3] = {false, false, false};
-        {
-            int qo = 0, qr = 0;
-            for (int i = 0; i < 3; i++)
+        int io = 0, ir = 0; // the next run to look up
+        auto issue = [&](int& slot_gf) {
+            slot_gf = UPTC_END;
+            if (next_run(io, ir))
             {
-                lv[i] = next_run(qo, qr);
-                if (!lv[i])
-                    break;
-                lo_[i] = qo;
-                lr_[i] = qr;
                 int ce, g0, g1;
-                run_info(qo, qr, ce, g0, g1);
-                lgf[i] = row_block(lane, qo, ce);
-                qr++;
+                run_info(io, ir, ce, g0, g1);
+                slot_gf = row_block(lane, io, ce);
+                ir++;
             }
-        }
+        };
+        int lgf0, lgf1, lgf2, lgf3;
+        issue(lgf0);
+        issue(lgf1);
+        issue(lgf2);
+        issue(lgf3);
         int R = 0;
-        while (lv[0] && ok)
-        {
-            const int gf = lgf[0];
-            // shift the look-ahead window and start the lookup of the run after it
-            int qo = lo_[2], qr = lr_[2] + 1;
-            const bool have_last = lv[2];
-            lo_[0] = lo_[1];
-            lr_[0] = lr_[1];
-            lgf[0] = lgf[1];
-            lv[0] = lv[1];
-            lo_[1] = lo_[2];
-            lr_[1] = lr_[2];
-            lgf[1] = lgf[2];
-            lv[1] = lv[2];
-            lv[2] = have_last && next_run(qo, qr);
-            if (lv[2])
-            {
-                lo_[2] = qo;
-                lr_[2] = qr;
-                int ce, g0, g1;
-                run_info(qo, qr, ce, g0, g1);
-                lgf[2] = row_block(lane, qo, ce);
-            }
+        auto step = [&](int& slot_gf) -> bool {
+            const int gf = slot_gf;
+            if (gf == UPTC_END)
+                return false;
+            issue(slot_gf);
             const int st = R % UPTC_ROW_STAGES, ph = R / UPTC_ROW_STAGES;
-            if (R >= UPTC_ROW_STAGES && !tc::mbar_wait(bar(UTB_ROW_EMPTY + st), (ph - 1) & 1, UPTC_WAIT_NS))
+            if (R >= UPTC_ROW_STAGES &&
+                !tc::mbar_wait(bar(UTB_ROW_EMPTY + st), (ph - 1) & 1, UPTC_WAIT_NS))
             {
                 ok = false;
-                break;
+                return false;
             }
             if (gf >= 0)
                 tc::prefetch_l2(fc2 + (size_t)row_q[lane] * a.fc_plane + (size_t)gf * P_LO,
@@ -401,6 +386,10 @@ __global__ void __launch_bounds__(UPTC_THREADS, 1) upward_tc_kernel(const __grid
             if (lane == 0)
                 tc::mbar_arrive(bar(UTB_ROW_FULL + st));
             R++;
+            return true;
+        };
+        while (step(lgf0) && step(lgf1) && step(lgf2) && step(lgf3))
+        {
         }
         if (!ok && lane == 0)
             atomicOr(a.tc_status, 1u);
