@@ -572,6 +572,7 @@ def run_ours(a):
         "e2e": {"value": e2e_ms, "unit": UNIT, "h2d_bytes_per_step": int(wb.nbytes),
                 "d2h_bytes_per_step": int(wb.nbytes), "note": "ms per matvec"},
         "roofline": roof, "clocks": clk,
+        "upward_tuner": stats.get("upward_tuner"),
         "work": {k: stats[k] for k in ("near_point_pairs", "far_target_evals",
                                        "leaf_factor_evals", "upward_node_evals",
                                        "coarse_cones_total", "fine_cones_total",

@@ -155,7 +155,12 @@ struct MultPtrs
     bool mixed; // mixed-precision pipeline (buffers hold float2)
     int up_path = UP_AUTO;           // UpwardPath
     unsigned* tc_status = nullptr;   // bounded-wait status of the tensor-core kernels
+    // the upward-kernel autotuner's per-level choice for single-plane
+    // matvecs (host array of L: 1 tensor cores, 0 FFMA, -1 none yet)
+    const signed char* up_choice = nullptr;
 };
+
+
 
 // Stage classes for per-kernel timing.
 enum ProfClass
@@ -206,6 +211,7 @@ struct BatchPtrs
     const int4* const* tc_tiles = nullptr;
     const int* n_tc_tiles = nullptr;
     const float* tc_fill = nullptr;
+    const signed char* up_choice = nullptr; // autotuner's choice for these planes (per level)
 };
 
 // Enqueues the mixed matvec of bp.nrhs <= bp.groups * BATCH_NB right-hand
@@ -216,6 +222,19 @@ struct BatchPtrs
 template <int KIND>
 int launch_mult_batch_kernels(const MultPtrs& m, const BatchPtrs& bp, const void* d_w, void* d_u,
                               bool real, cudaStream_t st, LaunchHooks* hooks);
+
+// Upward-kernel autotuner: for every level whose shape has both kernels,
+// the FFMA and the tensor-core upward transfer of one launch over `planes`
+// right-hand-side planes (bp null: the single-plane buffers of m) are timed
+// on the operator's own tables and buffers (each kernel once to warm up,
+// then the better of two timed launches); choice[l] = 1 where the tensor
+// cores were faster by more than 3 %, 0 elsewhere, -1 on levels without
+// both kernels; ms_ffma / ms_tc receive the times (0 where not timed).
+// The buffers' contents are left unspecified (the next matvec rewrites
+// them).  Returns the number of levels timed.
+template <int KIND>
+int tune_upward_kernels(const MultPtrs& m, const BatchPtrs* bp, int planes, cudaStream_t st,
+                        signed char* choice, double* ms_ffma, double* ms_tc);
 
 // Only the density permutation into m.w (for direct sums).
 template <int KIND>

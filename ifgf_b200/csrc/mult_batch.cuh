@@ -452,9 +452,9 @@ static int run_mult_batch(const MultPtrs& m, const BatchPtrs& bp, const void* d_
                 {
                     ua.tc_tiles = bp.tc_tiles[l];
                     ua.tc_status = m.tc_status;
-                    tensor = launch_upward_tc<KIND, N0, N1, N2>(ua, bp.n_tc_tiles[l],
-                                                                bp.tc_fill[l], m.up_path, st,
-                                                                bp.groups * BATCH_NB);
+                    tensor = launch_upward_tc<KIND, N0, N1, N2>(
+                        ua, bp.n_tc_tiles[l], bp.tc_fill[l], m.up_path, st, bp.groups * BATCH_NB,
+                        bp.up_choice ? bp.up_choice[l] : -1);
                 }
                 if (!tensor)
                 {
@@ -519,6 +519,120 @@ static int run_mult_batch(const MultPtrs& m, const BatchPtrs& bp, const void* d_
         }
         return launches;
     }
+}
+
+// The upward-kernel autotuner of one order shape (see tune_upward_kernels).
+template <int KIND, int N0, int N1, int N2>
+static int tune_upward_shape(const MultPtrs& m, const BatchPtrs* bp, int planes, cudaStream_t st,
+                             signed char* choice, double* ms_ffma, double* ms_tc)
+{
+    for (int l = 0; l < m.L; l++)
+    {
+        choice[l] = -1;
+        ms_ffma[l] = ms_tc[l] = 0;
+    }
+    if constexpr (!uptc_shape<N0, N1, N2>())
+        return 0;
+    else
+    {
+        cudaEvent_t e0, e1;
+        IFGF_CHECK(cudaEventCreate(&e0));
+        IFGF_CHECK(cudaEventCreate(&e1));
+        struct Ev
+        {
+            cudaEvent_t a, b;
+            ~Ev()
+            {
+                cudaEventDestroy(a);
+                cudaEventDestroy(b);
+            }
+        } ev{e0, e1};
+        auto timed = [&](auto&& launch) {
+            float best = 1e30f;
+            for (int rep = 0; rep < 3; rep++)
+            {
+                IFGF_CHECK(cudaEventRecord(e0, st));
+                launch();
+                IFGF_CHECK_LAUNCH();
+                IFGF_CHECK(cudaEventRecord(e1, st));
+                IFGF_CHECK(cudaEventSynchronize(e1));
+                float ms = 0;
+                IFGF_CHECK(cudaEventElapsedTime(&ms, e0, e1));
+                if (rep > 0 && ms < best) // the first launch warms up
+                    best = ms;
+            }
+            return (double)best;
+        };
+        int tuned = 0;
+        for (int l = 0; l + 1 < m.L; l++)
+        {
+            const LevelLists& LL = m.lists[l];
+            const int4* tiles = bp ? bp->tc_tiles[l] : LL.tc_tiles;
+            const int nt = bp ? bp->n_tc_tiles[l] : LL.n_tc_tiles;
+            if (LL.n_up <= 0 || LL.fe_pad <= 0 || !tiles || nt <= 0)
+                continue;
+            UpArgs ua;
+            ua.G = m.lv_host[l];
+            ua.GC = m.lv_host[l + 1];
+            ua.T = m.T;
+            ua.cc_box = LL.cc_box;
+            ua.cc_el = LL.cc_el;
+            ua.idx = LL.up_idx;
+            ua.slot = LL.up_slot;
+            ua.geo64 = LL.geo64;
+            ua.geo32 = LL.geo32;
+            ua.P_pad = LL.up_pad;
+            ua.fe_list = LL.fe_list;
+            ua.fe_pad = LL.fe_pad;
+            ua.rch = upward_staged_rch<N0, N1, N2>(LL.fe_pad);
+            ua.cv_plane = bp ? bp->cv_plane : 0;
+            ua.fc_plane = bp ? bp->fc_plane : 0;
+            ua.hi_nodes = m.hi_nodes;
+            ua.fmap = m.fmap;
+            ua.fcoef = bp ? reinterpret_cast<const double2*>(bp->fcoef) : m.fcoef;
+            ua.cvals = bp ? reinterpret_cast<double2*>(bp->cvals) : m.cvals;
+            ua.err = m.err;
+            ua.P_hi = m.P_hi;
+            ua.P_lo = m.P_lo;
+            for (int d = 0; d < 3; d++)
+                ua.lo[d] = m.lo[d];
+            ua.kp = m.kp;
+            ua.tc_tiles = tiles;
+            ua.tc_status = m.tc_status;
+            const size_t sm = upward_staged_smem<N0, N1, N2>(m.P_hi, ua.rch, LL.fe_pad);
+            if (sm > UP_STAGED_SMEM_MAX ||
+                uptc_smem_bytes<N0, N1, N2>(m.P_hi, LL.fe_pad) > 227 * 1024)
+                continue;
+            auto kern = upward_staged_kernel<KIND, N0, N1, N2, false>;
+            if (sm > 48 * 1024)
+                IFGF_CHECK(
+                    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+            ms_ffma[l] = timed([&] { kern<<<dim3(LL.n_up, planes), UPS_THREADS, sm, st>>>(ua); });
+            ms_tc[l] = timed([&] {
+                launch_upward_tc<KIND, N0, N1, N2>(ua, nt, 1.f, UP_TENSOR, st, planes, 1);
+            });
+            choice[l] = ms_tc[l] < 0.97 * ms_ffma[l] ? 1 : 0;
+            tuned++;
+        }
+        return tuned;
+    }
+}
+
+template <int KIND>
+int tune_upward_kernels(const MultPtrs& m, const BatchPtrs* bp, int planes, cudaStream_t st,
+                        signed char* choice, double* ms_ffma, double* ms_tc)
+{
+    const int* lo = m.lo;
+    if (lo[0] == 2 && lo[1] == 5 && lo[2] == 5)
+        return tune_upward_shape<KIND, 2, 5, 5>(m, bp, planes, st, choice, ms_ffma, ms_tc);
+    if (lo[0] == 3 && lo[1] == 6 && lo[2] == 6)
+        return tune_upward_shape<KIND, 3, 6, 6>(m, bp, planes, st, choice, ms_ffma, ms_tc);
+    for (int l = 0; l < m.L; l++)
+    {
+        choice[l] = -1;
+        ms_ffma[l] = ms_tc[l] = 0;
+    }
+    return 0;
 }
 
 template <int KIND>

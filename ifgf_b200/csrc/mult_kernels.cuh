@@ -2288,7 +2288,8 @@ static int run_mult(const MultPtrs& m, const void* d_w, void* d_u, bool real, cu
                 ua.tc_tiles = LL.tc_tiles;
                 ua.tc_status = m.tc_status;
                 staged = launch_upward_tc<KIND, N0, N1, N2>(ua, LL.n_tc_tiles, LL.tc_fill,
-                                                            m.up_path, st);
+                                                            m.up_path, st, 1,
+                                                            m.up_choice ? m.up_choice[l] : -1);
             }
             if constexpr (MIXED && N0 > 0 && (N0 * N1 * N2) % 2 == 0)
                 if (!staged)
@@ -2451,6 +2452,8 @@ void launch_order_probe(const ProbeArgs& a, int n_samples, int max_nodes, cudaSt
                                         LaunchHooks*);                                         \
     template int launch_mult_batch_kernels<K>(const MultPtrs&, const BatchPtrs&, const void*,  \
                                               void*, bool, cudaStream_t, LaunchHooks*);        \
+    template int tune_upward_kernels<K>(const MultPtrs&, const BatchPtrs*, int, cudaStream_t,   \
+                                        signed char*, double*, double*);                       \
     template void launch_direct_kernel<K>(const MultPtrs&, const int*, int, double2*, cudaStream_t); \
     template void permute_only<K>(const MultPtrs&, const void*, bool, cudaStream_t);         \
     template void launch_order_probe<K>(const ProbeArgs&, int, int, cudaStream_t);             \

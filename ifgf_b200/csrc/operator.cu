@@ -146,6 +146,10 @@ struct DeviceState
     std::vector<int> tcb_n;
     std::vector<float> tcb_fill;
     DevBuf<unsigned> tc_status;
+    // upward-kernel autotuner: per plane count of a launch, the per-level
+    // choice (1 tensor cores, 0 FFMA, -1 not both) and the timed milliseconds
+    std::map<int, std::vector<signed char>> up_choice;
+    std::map<int, std::vector<double>> up_ms_ffma, up_ms_tc;
     DevBuf<double> io_w, io_u; // staging for host-buffer mult
     std::vector<cudaEvent_t> prof_ev;
     cudaStream_t side = nullptr; // near-field stream
@@ -1079,6 +1083,9 @@ void Operator::setup_device(const double* normals)
     D.tc_tiles.clear();
     D.tc_tiles.resize(L);
     D.tc_fill.assign(L, {});
+    D.up_choice.clear();
+    D.up_ms_ffma.clear();
+    D.up_ms_tc.clear();
     D.geo64.resize(L);
     D.geo32.resize(L);
     D.fe_list.resize(L);
@@ -1425,6 +1432,31 @@ void Operator::fill_mult_ptrs(MultPtrs& m, bool variant) const
     m.mixed = precision_ == PREC_MIXED;
     m.up_path = up_path_;
     m.tc_status = D.tc_status.p;
+    auto it = D.up_choice.find(1);
+    m.up_choice = it != D.up_choice.end() ? it->second.data() : nullptr;
+}
+
+// Runs the upward-kernel autotuner for launches over `planes` planes once
+// (AUTO path, mixed precision): times the FFMA and the tensor-core kernel of
+// every level on this operator's tables and buffers (bp: the batch planes;
+// null: the single-plane buffers) and keeps the per-level choice.  It
+// synchronises `st` once; the buffers it ran on are rewritten by the matvec
+// that follows.
+void Operator::ensure_upward_tuned(int planes, const BatchPtrs* bp, void* stream)
+{
+    DeviceState& D = *dev_;
+    if (up_path_ != UP_AUTO || precision_ != PREC_MIXED || D.up_choice.count(planes))
+        return;
+    const int L = (int)lv_.size();
+    std::vector<signed char> ch(L, -1);
+    std::vector<double> mf(L, 0.0), mt(L, 0.0);
+    MultPtrs m;
+    fill_mult_ptrs(m);
+    IFGF_DISPATCH(kind_, tune_upward_kernels<KK>(m, bp, planes, (cudaStream_t)stream, ch.data(),
+                                                 mf.data(), mt.data()));
+    D.up_choice[planes] = std::move(ch);
+    D.up_ms_ffma[planes] = std::move(mf);
+    D.up_ms_tc[planes] = std::move(mt);
 }
 
 // Row tiles of the tensor-core upward transfer for launches over `planes`
@@ -1456,8 +1488,9 @@ void Operator::ensure_tc_tiles(int planes)
     }
 }
 
-// The tensor-core tiles for a batch launch over bp.groups * BATCH_NB planes.
-void Operator::set_batch_tc(BatchPtrs& bp)
+// The tensor-core tiles for a batch launch over bp.groups * BATCH_NB planes,
+// and (single-wavenumber batches) the autotuner's choice for them.
+void Operator::set_batch_tc(BatchPtrs& bp, void* stream)
 {
     DeviceState& D = *dev_;
     const int planes = bp.groups * BATCH_NB;
@@ -1476,6 +1509,14 @@ void Operator::set_batch_tc(BatchPtrs& bp)
     bp.tc_tiles = D.tcb_ptr.data();
     bp.n_tc_tiles = D.tcb_n.data();
     bp.tc_fill = D.tcb_fill.data();
+    bp.up_choice = nullptr;
+    if (!bp.kp_plane)
+    {
+        ensure_upward_tuned(planes, &bp, stream);
+        auto it = D.up_choice.find(planes);
+        if (it != D.up_choice.end())
+            bp.up_choice = it->second.data();
+    }
 }
 
 // One thread waits on an mbarrier that nothing arrives at, bounded by
@@ -1792,6 +1833,8 @@ void Operator::launch_mult(const void* d_w, void* d_u, void* stream, bool timed,
     DeviceState& D = *dev_;
     if (vkind >= 0)
         ensure_variant_tables(vkind);
+    if (vkind < 0 && precision_ == PREC_MIXED)
+        ensure_upward_tuned(1, nullptr, stream);
     MultPtrs m;
     fill_mult_ptrs(m, vkind >= 0);
     EventHooks log(D, st);
@@ -1965,7 +2008,7 @@ void Operator::mult_batch_device(const void* d_w, void* d_u, int64_t batch, void
         {
             bp.nrhs = (int)std::min<int64_t>(planes, batch - done);
             bp.groups = (bp.nrhs + BATCH_NB - 1) / BATCH_NB;
-            set_batch_tc(bp);
+            set_batch_tc(bp, st);
             EventHooks log(D, st);
             int r = -1;
             IFGF_DISPATCH(kind_, r = launch_mult_batch_kernels<KK>(
@@ -2378,6 +2421,27 @@ std::string Operator::stats_json() const
       << ",\"init_device_ms\":" << device_ms_ << ",\"init_device_phases_ms\":{";
     for (size_t i = 0; i < dev_phases_.size(); i++)
         o << (i ? "," : "") << "\"" << dev_phases_[i].first << "\":" << dev_phases_[i].second;
+    o << "},\"upward_path\":" << up_path_ << ",\"upward_tuner\":{";
+    {
+        bool first = true;
+        for (const auto& kv : dev_->up_choice)
+        {
+            auto arr = [&](const char* name, auto const& v) {
+                o << "\"" << name << "\":[";
+                for (size_t i = 0; i < v.size(); i++)
+                    o << (i ? "," : "") << (double)v[i];
+                o << "]";
+            };
+            o << (first ? "" : ",") << "\"" << kv.first << "\":{";
+            arr("tensor", kv.second);
+            o << ",";
+            arr("ms_ffma", dev_->up_ms_ffma.at(kv.first));
+            o << ",";
+            arr("ms_tensor", dev_->up_ms_tc.at(kv.first));
+            o << "}";
+            first = false;
+        }
+    }
     o << "},\"launches_per_mult\":" << launches_per_mult_
       << ",\"batch_planes\":" << dev_->b_planes
       << ",\"last_mult_ms\":{\"permute\":" << last_.permute << ",\"leaf_sample\":" << last_.coarse

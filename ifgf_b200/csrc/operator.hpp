@@ -129,7 +129,8 @@ class Operator
     BatchPtrs batch_ptrs(long long in_plane, long long out_plane) const;
     void ensure_distance_tables();
     void ensure_tc_tiles(int planes);
-    void set_batch_tc(BatchPtrs& bp);
+    void set_batch_tc(BatchPtrs& bp, void* stream);
+    void ensure_upward_tuned(int planes, const BatchPtrs* bp, void* stream);
     void setup_device(const double* normals);
     // vkind >= 0: run that kernel with the variant geometry tables
     void launch_mult(const void* d_w, void* d_u, void* stream, bool timed, int vkind = -1);

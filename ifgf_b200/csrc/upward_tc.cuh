@@ -770,16 +770,21 @@ template <int N0, int N1, int N2> constexpr bool uptc_shape()
 // tiles (a.tc_tiles) when the path, the order shape, the tile fill and the
 // shared memory allow; returns false (nothing launched) otherwise, and the
 // caller runs an FFMA kernel.
+// choice: the autotuner's decision for this level and plane count (1 tensor
+// cores, 0 FFMA), or -1 when there is none (AUTO then falls back to the tile
+// fill).
 template <int KIND, int N0, int N1, int N2>
 bool launch_upward_tc(const UpArgs& a, int n_tiles, float fill, int path, cudaStream_t st,
-                      int planes = 1)
+                      int planes = 1, int choice = -1)
 {
     if constexpr (!uptc_shape<N0, N1, N2>())
         return false;
     else
     {
         if (path == UP_FFMA || !a.tc_tiles || n_tiles <= 0 || !a.tc_status || a.kp_plane ||
-            (path == UP_AUTO && fill < UPTC_MIN_FILL) || a.fe_pad <= 0)
+            a.fe_pad <= 0)
+            return false;
+        if (path == UP_AUTO && (choice == 0 || (choice < 0 && fill < UPTC_MIN_FILL)))
             return false;
         // 16-byte aligned coefficient planes for the bulk copies
         if (planes > 1 && (a.fc_plane % 2) != 0)

@@ -121,3 +121,29 @@ def test_bounded_wait_gives_up_with_timeout_status():
     o.init(pts, pts)
     w = W.densities(n, complex_=False, seed=1)
     assert rel2(g.mult(w), o.mult(w)) <= 1e-12
+
+
+@pytest.mark.gpu
+def test_autotuner_records_a_choice_per_level_and_plane_count():
+    """The AUTO path times both upward kernels once per plane count on the
+    operator's own tables and keeps the faster per level; the choice and the
+    times are reported in the stats, and results match the FFMA path."""
+    n = 30000
+    pts = W.ellipsoid_points(n, seed=0)
+    g = make_gpu_op("helmholtz", leaf=60, order=9, k=60.0)
+    g.init(pts, pts)
+    g.set_precision("mixed")
+    w = W.densities(n, seed=1)
+    wb = np.stack([W.densities(n, seed=20 + b) for b in range(8)])
+    u1, ub = g.mult(w), g.mult_batch(wb)
+    tuner = g.stats()["upward_tuner"]
+    assert "1" in tuner and "8" in tuner, tuner.keys()
+    for planes, rec in tuner.items():
+        timed = [i for i, c in enumerate(rec["tensor"]) if c >= 0]
+        assert timed, planes
+        for i in timed:
+            assert rec["ms_ffma"][i] > 0 and rec["ms_tensor"][i] > 0
+            assert rec["tensor"][i] == (1 if rec["ms_tensor"][i] < 0.97 * rec["ms_ffma"][i] else 0)
+    g.set_upward_path("ffma")
+    assert rel2(u1, g.mult(w)) <= TC_VS_FFMA
+    assert rel2(ub, g.mult_batch(wb)) <= TC_VS_FFMA
