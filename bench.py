@@ -52,6 +52,12 @@ TOL = 1e-4
 # seconds of whole oracle matvecs the reference arm times at most (about a
 # minute each on 16 host cores at the headline size)
 REF_BUDGET_S = 100.0
+# DRAM bytes per unit and right-hand side of the dominant kernels (see the
+# roofline section): upward FFMA / tensor-core kernels per padded
+# geometry-table entry, far field per (target, far box) pair
+UPWARD_FFMA_DRAM_B = 18.9
+UPWARD_TC_DRAM_B = 18.9
+FAR_DRAM_B = 53.0
 
 
 def parse():
@@ -510,38 +516,71 @@ def run_ours(a):
     e2e_ms = max_over_ranks(ws, f0.elapsed_time(f1) / a.steps) / batch
 
     # ---- roofline of the dominant kernel (per matvec) ----
+    # Peaks: MEASURED_PEAKS.json (driver-measured on this pool's B200s): the
+    # sustained bf16 tensor rate for a kernel timed inside a long step, the
+    # HBM copy rate.  The flop figure is the algorithmic model (per unit:
+    # transcendental = 1, FMA = 2), so `frac` is algorithmic work over the
+    # measured peak of the pipe the kernel runs its contraction on.
     flops = model(stats)
     kernels = {k: v for k, v in prof.items() if isinstance(v, dict)}
     dom = max(kernels, key=lambda k: kernels[k]["ms"])
     per_mult_ms = kernels[dom]["ms"] / max(prof["mults"], 1)
-    peak = measured_peak_tflops(torch.float64 if precision == "fp64" else torch.float32)
-    achieved = flops[dom] / (per_mult_ms * 1e-3) / 1e12
-    # DRAM bytes per work unit of the two largest kernels, from one ncu
-    # capture each (dram__bytes_read.sum + dram__bytes_write.sum) on the
-    # N=200k case of this workload, scaled here by the units of one matvec:
-    # upward -- per padded geometry-table entry and right-hand side; far
-    # field -- per (target, far box) pair and right-hand side (mixed, batched)
-    entries = sum(u["padded_entries"] for u in stats["upward_levels"])
-    traffic = None
-    if precision == "mixed" and batch > 1:
-        traffic = {"upward": 19.1 * entries,
-                   "target_eval": 55.5 * stats["far_target_evals"]}.get(dom)
-    roof = {"kernel": dom, "bound": "fp64" if precision == "fp64" else "fp32",
-            "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-            "traffic": traffic,
-            "traffic_note": "DRAM bytes per matvec of the kernel, ncu per-unit figure scaled",
-            "peak_source": "measured: cuBLAS GEMM via torch.matmul 8192^3 in this run "
-                           "(MEASURED_PEAKS.json holds only HBM and bf16 figures)",
-            "launches_per_step": kernels[dom]["launches"] / max(prof["mults"], 1) * batch,
-            "ms_per_matvec": per_mult_ms,
-            "model": "survey flop model: transcendental = 1 flop, FMA = 2; per matvec"}
-    # the same kernel against the measured HBM copy rate: how far it is from
-    # being memory-bound
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
-            hbm = float(json.load(f)["hbm_gbs"])
-    except (OSError, KeyError, ValueError):
-        hbm = None
+            peaks = json.load(f)
+    except (OSError, ValueError):
+        peaks = {}
+    hbm = peaks.get("hbm_gbs")
+    bf16 = peaks.get("bf16_tflops_sustained")
+    achieved = flops[dom] / (per_mult_ms * 1e-3) / 1e12
+    # levels whose upward transfer ran on the tensor cores (the autotuner's
+    # choice for this step's plane count)
+    planes_per_pass = min(batch, max(stats.get("batch_planes", 4), 1)) if batch > 1 else 1
+    tuner = (stats.get("upward_tuner") or {}).get(str(planes_per_pass), {})
+    tc_levels = [i for i, c in enumerate(tuner.get("tensor", [])) if c == 1]
+    levels = stats["upward_levels"]
+    # DRAM bytes per padded geometry-table entry and right-hand side, per
+    # upward kernel, and per (target, far box) pair and right-hand side of
+    # the far field: one ncu capture of dram__bytes_read.sum +
+    # dram__bytes_write.sum of this bench command (a one-pass metric set),
+    # summed over its launches and divided by the units they processed
+    # (profiles/launches_bench_1e6_mixed_batched.md)
+    bytes_per_unit = {"upward_ffma": UPWARD_FFMA_DRAM_B, "upward_tensor": UPWARD_TC_DRAM_B,
+                      "target_eval": FAR_DRAM_B}
+    traffic = None
+    if precision == "mixed" and batch > 1:
+        if dom == "upward":
+            traffic = sum(u["padded_entries"] * (bytes_per_unit["upward_tensor"] if i in tc_levels
+                                                 else bytes_per_unit["upward_ffma"])
+                          for i, u in enumerate(levels))
+        elif dom == "target_eval":
+            traffic = bytes_per_unit["target_eval"] * stats["far_target_evals"]
+    if precision == "mixed" and dom == "upward" and tc_levels and bf16:
+        roof = {"kernel": dom, "bound": "tensor", "achieved": achieved, "peak": bf16,
+                "unit": "TFLOP/s", "frac": achieved / bf16,
+                "peak_source": "MEASURED_PEAKS.json bf16_tflops_sustained (of measured)",
+                "tensor_levels": tc_levels,
+                "tensor_note": "upward transfer on the tensor cores (tcgen05 kind::tf32, split "
+                               "TF32 pieces) on the listed levels, FP32 FMA elsewhere; per padded "
+                               "entry and plane the tensor cores execute 4 lanes x 2 basis pieces "
+                               "x 112 x 2 = 1792 flops for the model's 933"}
+    else:
+        sgemm = measured_peak_tflops(torch.float64 if precision == "fp64" else torch.float32)
+        roof = {"kernel": dom, "bound": "fp64" if precision == "fp64" else "fp32",
+                "achieved": achieved, "peak": sgemm, "unit": "TFLOP/s", "frac": achieved / sgemm,
+                "peak_source": "builder's in-run cuBLAS GEMM via torch.matmul 8192^3 "
+                               "(MEASURED_PEAKS.json has no FP32/FP64 figure)"}
+    roof.update({
+        "traffic": traffic,
+        "traffic_note": "DRAM bytes per matvec of the kernel: ncu per-unit figures of this "
+                        "command, scaled by the units of one matvec",
+        "launches_per_step": kernels[dom]["launches"] / max(prof["mults"], 1) * batch,
+        "ms_per_matvec": per_mult_ms,
+        "ms_note": "per-kernel times come from a pass with CUDA events around every launch "
+                   "(serialised on one stream); the timed step overlaps the near field",
+        "model": "survey flop model: transcendental = 1 flop, FMA = 2; per matvec; the FFMA "
+                 "upward kernel executes 600 flops per unit (basis-vector FMAs) for the "
+                 "model's 933"})
     if traffic is not None and hbm:
         bw = traffic / (per_mult_ms * 1e-3) / 1e9
         roof["hbm"] = {"achieved": bw, "peak": hbm, "unit": "GB/s", "frac": bw / hbm,
