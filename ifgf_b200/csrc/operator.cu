@@ -131,6 +131,7 @@ struct DeviceState
     // multi-wavenumber batches: per-plane wavenumbers and the per-level
     // distance tables (built on first use after an init)
     DevBuf<KParams> kp_plane;
+    std::vector<KParams> kp_host; // what kp_plane holds
     std::vector<DevBuf<UpGeo32>> dgeo32;
     std::vector<const UpGeo32*> dgeo32_ptr;
     bool dgeo_ready = false;
@@ -2177,10 +2178,22 @@ void Operator::mult_wavenumbers_device(const double* k, int64_t nk, const void* 
         const int64_t q = std::min(p, nk - 1);
         kps[(size_t)p] = make_kparams(k[2 * q], k[2 * q + 1], dx_);
     }
-    if (D.kp_plane.n < kps.size())
-        D.kp_plane.alloc(kps.size());
-    IFGF_CUDA(cudaMemcpyAsync(D.kp_plane.p, kps.data(), kps.size() * sizeof(KParams),
-                              cudaMemcpyHostToDevice, st));
+    // uploaded only when they change: a repeated call (the same frequency
+    // set) then enqueues kernels only, so that it can be captured into a
+    // CUDA graph after a first call
+    bool same_k = D.kp_host.size() == kps.size();
+    for (size_t i = 0; same_k && i < kps.size(); i++)
+        same_k = D.kp_host[i].kr == kps[i].kr && D.kp_host[i].ki == kps[i].ki &&
+                 D.kp_host[i].dx == kps[i].dx;
+    if (!same_k)
+    {
+        if (D.kp_plane.n < kps.size())
+            D.kp_plane.alloc(kps.size());
+        IFGF_CUDA(cudaMemcpyAsync(D.kp_plane.p, kps.data(), kps.size() * sizeof(KParams),
+                                  cudaMemcpyHostToDevice, st));
+        IFGF_CUDA(cudaStreamSynchronize(st)); // kps is a temporary
+        D.kp_host = kps;
+    }
     BatchPtrs bp = batch_ptrs(in_plane, out_plane);
     bp.dgeo32 = D.dgeo32_ptr.data();
     MultPtrs m;
