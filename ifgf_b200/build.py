@@ -18,9 +18,11 @@ NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I", CSRC, "-I", INCLUDE]
 
-SOURCES = ["operator.cu", "plan.cpp", "gpu_tree.cu", "gpu_lists.cu", "capi.cpp", "noalloc.cu"] + [
+SOURCES = ["operator.cu", "plan.cpp", "gpu_tree.cu", "gpu_lists.cu", "gpu_target_lists.cu",
+           "capi.cpp", "noalloc.cu"] + [
     f"kernels_k{k}.cu" for k in range(8)]
-HEADERS = ["common.hpp", "plan.hpp", "operator.hpp", "device_math.cuh", "mult.hpp",
+HEADERS = ["common.hpp", "devbuf.hpp", "gpu_target_lists.hpp", "plan.hpp", "operator.hpp",
+           "device_math.cuh", "mult.hpp",
            "mult_kernels.cuh", "mult_batch.cuh", "far_staged.cuh", "tcgen05.cuh", "upward_tc.cuh"]
 
 

@@ -20,6 +20,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <memory>
 #include <numeric>
 #include <string>
 #include <vector>
@@ -74,6 +75,14 @@ template <typename T> struct LBuf
             cudaFree(p);
         p = q;
         n = count;
+    }
+    // hands the allocation over to the caller
+    T* release()
+    {
+        T* q = p;
+        p = nullptr;
+        n = 0;
+        return q;
     }
     void swap(LBuf& o)
     {
@@ -232,11 +241,19 @@ __global__ void iota_kernel(int* v, long long n)
 
 unsigned grid_for(long long n) { return (unsigned)((n + 255) / 256); }
 
-// (source, target) pairs ordered by (source, k0, k1), as CSR on the host
-void sort_to_csr(const PairBuf& pb, long long n, int64_t n_src_boxes, PairLists& out)
+template <typename T> std::shared_ptr<T> device_owned(T* p)
+{
+    return std::shared_ptr<T>(p, [](T* q) { cudaFree(q); });
+}
+
+// (source, target) pairs ordered by (source, k0, k1), as CSR on the host and
+// as (source, target) arrays left on the device
+void sort_to_csr(const PairBuf& pb, long long n, int64_t n_src_boxes, PairLists& out,
+                 DevicePairs& dev)
 {
     out.off.assign(n_src_boxes + 1, 0);
     out.tgt.clear();
+    dev = DevicePairs{};
     if (n == 0)
         return;
     LBuf<int> ia, ib;
@@ -272,6 +289,9 @@ void sort_to_csr(const PairBuf& pb, long long n, int64_t n_src_boxes, PairLists&
         out.off[s_sorted[i] + 1]++;
     for (int64_t b = 0; b < n_src_boxes; b++)
         out.off[b + 1] += out.off[b];
+    dev.src = device_owned(sb.release());
+    dev.tgt = device_owned(sa.release());
+    dev.n = n;
 }
 
 } // namespace
@@ -434,9 +454,34 @@ bool Plan::build_lists_gpu()
     n_near_pairs = (int64_t)ctr[C_NEAR];
     far_target_evals = (int64_t)ctr[C_FAR_EVALS];
     near_point_pairs = (int64_t)ctr[C_NEAR_PAIRS];
-    sort_to_csr(fl.buf(), n_far_pairs, nsb, far);
-    sort_to_csr(nl.buf(), n_near_pairs, nsb, near);
+    sort_to_csr(fl.buf(), n_far_pairs, nsb, far, far_dev);
+    sort_to_csr(nl.buf(), n_near_pairs, nsb, near, near_dev);
     return true;
+}
+
+void Plan::ensure_device_pairs()
+{
+    auto up = [&](const PairLists& L, DevicePairs& dev) {
+        const int64_t n = L.off.empty() ? 0 : L.off.back();
+        if (dev.n == n && (n == 0 || dev.src))
+            return;
+        dev = DevicePairs{};
+        if (n == 0)
+            return;
+        std::vector<int32_t> s((size_t)n);
+        for (size_t b = 0; b + 1 < L.off.size(); b++)
+            std::fill(s.begin() + L.off[b], s.begin() + L.off[b + 1], (int32_t)b);
+        LBuf<int32_t> ds, dt;
+        ds.alloc(n);
+        dt.alloc(n);
+        LIST_CUDA(cudaMemcpy(ds.p, s.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice));
+        LIST_CUDA(cudaMemcpy(dt.p, L.tgt.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice));
+        dev.src = device_owned(ds.release());
+        dev.tgt = device_owned(dt.release());
+        dev.n = n;
+    };
+    up(far, far_dev);
+    up(near, near_dev);
 }
 
 } // namespace ifgf

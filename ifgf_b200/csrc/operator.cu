@@ -10,15 +10,15 @@
 #include <map>
 #include <sstream>
 
+#include "devbuf.hpp"
 #include "device_math.cuh"
+#include "gpu_target_lists.hpp"
 #include "tcgen05.cuh"
 #include "mult.hpp"
 #include "operator.hpp"
 
 namespace ifgf
 {
-
-static constexpr int ERR_INVALID = 1, ERR_CUDA = 2, ERR_STATE = 3, ERR_OOM = 4, ERR_TIMEOUT = 5;
 
 // Calls CALL with the compile-time kernel kind KK matching KINDVAR.
 #define IFGF_DISPATCH(KINDVAR, CALL)                                                          \
@@ -33,63 +33,6 @@ static constexpr int ERR_INVALID = 1, ERR_CUDA = 2, ERR_STATE = 3, ERR_OOM = 4, 
     case K_HELMHOLTZ_DK: { constexpr int KK = K_HELMHOLTZ_DK; CALL; } break;                  \
     case K_COMBINEDFIELD_DK: { constexpr int KK = K_COMBINEDFIELD_DK; CALL; } break;          \
     }
-
-#define IFGF_CUDA(x)                                                                          \
-    do                                                                                         \
-    {                                                                                          \
-        cudaError_t e_ = (x);                                                                  \
-        if (e_ != cudaSuccess)                                                                 \
-            throw Error(ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_));           \
-    } while (0)
-
-template <typename T> struct DevBuf
-{
-    T* p = nullptr;
-    size_t n = 0;
-    DevBuf() = default;
-    DevBuf(const DevBuf&) = delete;
-    DevBuf& operator=(const DevBuf&) = delete;
-    DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n)
-    {
-        o.p = nullptr;
-        o.n = 0;
-    }
-    ~DevBuf() { release(); }
-    void alloc(size_t count)
-    {
-        release();
-        if (count == 0)
-            return;
-        cudaError_t e = cudaMalloc((void**)&p, count * sizeof(T));
-        if (e != cudaSuccess)
-        {
-            cudaGetLastError();
-            p = nullptr;
-            throw Error(ERR_OOM, "cudaMalloc(" + std::to_string(count * sizeof(T)) +
-                                     " bytes) failed: " + cudaGetErrorString(e));
-        }
-        n = count;
-    }
-    void upload(const T* h, size_t count)
-    {
-        alloc(count);
-        if (count)
-            IFGF_CUDA(cudaMemcpy(p, h, count * sizeof(T), cudaMemcpyHostToDevice));
-    }
-    void upload(const std::vector<T>& v) { upload(v.data(), v.size()); }
-    void zero()
-    {
-        if (n)
-            IFGF_CUDA(cudaMemset(p, 0, n * sizeof(T)));
-    }
-    void release()
-    {
-        if (p)
-            cudaFree(p);
-        p = nullptr;
-        n = 0;
-    }
-};
 
 struct DeviceState
 {
@@ -199,19 +142,21 @@ struct AdjointState
 // One CTA per far pair (source box, target range): mark the fine and coarse
 // cones that contain the far targets (octree.hpp:574-590).
 __global__ void mark_far_kernel(LevelGeom G, TreeArgs T, const int* __restrict__ fp_src,
-                                const int* __restrict__ fp_t0, const int* __restrict__ fp_t1,
-                                const double* __restrict__ tx, const double* __restrict__ ty,
-                                const double* __restrict__ tz, int* fmark, int* cmark)
+                                const int* __restrict__ fp_tgt, const int* __restrict__ tbox_first,
+                                const int* __restrict__ tbox_last, const double* __restrict__ tx,
+                                const double* __restrict__ ty, const double* __restrict__ tz,
+                                int* fmark, int* cmark)
 {
     const int pr = blockIdx.x;
     const int sb = fp_src[pr];
+    const int tb = fp_tgt[pr];
     const int lb = sb - G.box_off;
     const double xc0 = T.box_c[3 * sb], xc1 = T.box_c[3 * sb + 1], xc2 = T.box_c[3 * sb + 2];
     const double H = T.box_H[sb];
     const long long nf = (long long)G.nf[0] * G.nf[1] * G.nf[2];
     const long long nc = (long long)G.nc[0] * G.nc[1] * G.nc[2];
-    const int t1 = fp_t1[pr];
-    for (int t = fp_t0[pr] + threadIdx.x; t < t1; t += blockDim.x)
+    const int t1 = tbox_last[tb];
+    for (int t = tbox_first[tb] + threadIdx.x; t < t1; t += blockDim.x)
     {
         double s[3];
         cart_to_interp(tx[t] - xc0, ty[t] - xc1, tz[t] - xc2, H, s);
@@ -836,7 +781,12 @@ void Operator::init(const double* srcs, int64_t ns, const double* tgts, int64_t 
                     .count();
     const auto tt2 = std::chrono::steady_clock::now();
     plan_.assign_shards(shard_n_);
-    plan_.build_target_lists(shard_n_ > 1 ? shard_rank_ : -1);
+    // the target-leaf lists: on the host for a plan-only init, else built on
+    // the GPU by setup_device
+    if (plan_only)
+        plan_.build_target_lists(shard_n_ > 1 ? shard_rank_ : -1);
+    else
+        plan_.collect_target_leaves();
     tlists_ms_ = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tt2)
                      .count();
     if (tol_ > 0) // ifgfoperator.hpp:80-85
@@ -1032,16 +982,12 @@ void Operator::setup_device(const double* normals)
         }
         D.tl_first.upload(f);
         D.tl_last.upload(l);
-        std::vector<long long> fo(plan_.tleaf_far_off.begin(), plan_.tleaf_far_off.end());
-        std::vector<long long> no(plan_.tleaf_near_off.begin(), plan_.tleaf_near_off.end());
-        D.tl_far_off.upload(fo);
-        D.tl_near_off.upload(no);
-        D.tl_far_src.upload(plan_.tleaf_far_src.data(), plan_.tleaf_far_src.size());
-        D.tl_near_src.upload(plan_.tleaf_near_src.data(), plan_.tleaf_near_src.size());
         D.n_tleaf = (int)ntl;
     }
-
-    phase("boxes_points_lists_upload");
+    phase("boxes_points_upload");
+    build_target_lists_gpu(plan_, shard_n_ > 1 ? shard_rank_ : -1, D.tl_far_off, D.tl_far_src,
+                           D.tl_near_off, D.tl_near_src);
+    phase("target_leaf_lists");
     // ---- active cones (octree.hpp:351-816) on the GPU ----
     int64_t fmap_total = 0;
     for (auto& G : lv_)
@@ -1110,8 +1056,16 @@ void Operator::setup_device(const double* normals)
     upgeo_bytes_ = 0;
     int64_t coarse_tot = 0, fine_tot = 0;
     leaf_evals_ = upward_evals_ = 0;
-    std::vector<int> tbox_first, tbox_last; // point range of every target box
-    plan_.target_box_ranges(tbox_first, tbox_last);
+    // point range of every target box, by global id, for the far pairs of
+    // the cone-marking kernel (read from the device pair lists)
+    DevBuf<int> tbox_first, tbox_last;
+    {
+        std::vector<int> tf, tl;
+        plan_.target_box_ranges(tf, tl);
+        tbox_first.upload(tf);
+        tbox_last.upload(tl);
+    }
+    plan_.ensure_device_pairs();
     for (int l = 0; l < L; l++)
     {
         LevelGeom& G = lv_[l];
@@ -1120,18 +1074,15 @@ void Operator::setup_device(const double* normals)
         const int64_t ncm = (int64_t)G.nbox * nce, nfm = (int64_t)G.nbox * nfe;
         IFGF_CUDA(cudaMemset(cmark.p, 0, ncm * sizeof(int)));
         phase("cone_marks");
-        // far pairs of this level: source box, target point range
-        std::vector<int> fs, f0, f1;
-        plan_.far_pairs_of_level(l, tbox_first, tbox_last, fs, f0, f1);
-        phase("far_pairs_host");
-        if (!fs.empty())
+        // far pairs of this level's source boxes: a contiguous range of the
+        // source-major device pair list
+        const int64_t p0 = plan_.far.off.empty() ? 0 : plan_.far.off[S.level_off[l]];
+        const int64_t p1 = plan_.far.off.empty() ? 0 : plan_.far.off[S.level_off[l + 1]];
+        if (p1 > p0)
         {
-            DevBuf<int> dfs, df0, df1;
-            dfs.upload(fs);
-            df0.upload(f0);
-            df1.upload(f1);
-            mark_far_kernel<<<(unsigned)fs.size(), 128>>>(G, TA, dfs.p, df0.p, df1.p, D.tx.p,
-                                                           D.ty.p, D.tz.p, D.fmap.p, cmark.p);
+            mark_far_kernel<<<(unsigned)(p1 - p0), 128>>>(
+                G, TA, plan_.far_dev.src.get() + p0, plan_.far_dev.tgt.get() + p0, tbox_first.p,
+                tbox_last.p, D.tx.p, D.ty.p, D.tz.p, D.fmap.p, cmark.p);
             IFGF_CUDA(cudaGetLastError());
             IFGF_CUDA(cudaDeviceSynchronize());
         }
@@ -2392,8 +2343,16 @@ std::string Operator::stats_json() const
 {
     std::ostringstream o;
     o.precision(10);
+    // work the target-leaf lists describe, from the device tables of an
+    // initialised operator (the host tables of a plan-only one)
     int64_t tl_work[4] = {0, 0, 0, 0};
-    plan_.target_list_work(tl_work);
+    uint64_t tl_sum = 0;
+    if (initialized_)
+        plan_.target_list_work(dev_->tl_far_off.download(), dev_->tl_far_src.download(),
+                               dev_->tl_near_off.download(), dev_->tl_near_src.download(),
+                               tl_work, &tl_sum);
+    else
+        plan_.target_list_work(tl_work, &tl_sum);
     o << "{\"kind\":" << kind_ << ",\"precision\":" << precision_ << ",\"n_src\":" << n_src()
       << ",\"n_tgt\":" << n_tgt() << ",\"order_high\":[" << hi_[0] << "," << hi_[1] << ","
       << hi_[2] << "],\"order_low\":[" << lo_[0] << "," << lo_[1] << "," << lo_[2] << "]"
@@ -2417,6 +2376,7 @@ std::string Operator::stats_json() const
       << ",\"target_leaf_far_evals\":" << tl_work[0]
       << ",\"target_leaf_far_point_pairs\":" << tl_work[1]
       << ",\"target_leaf_near_point_pairs\":" << tl_work[2]
+      << ",\"target_leaf_lists_checksum\":" << tl_sum
       << ",\"leaf_factor_evals\":" << leaf_evals_ << ",\"upward_node_evals\":" << upward_evals_
       << ",\"coarse_cones_total\":" << n_coarse_total_ << ",\"fine_cones_total\":" << n_fine_total_
       << ",\"upward_geometry_bytes\":" << upgeo_bytes_ << ",\"upward_runs_max\":[";

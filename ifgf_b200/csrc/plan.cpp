@@ -316,6 +316,7 @@ void Plan::build_lists(const std::function<bool(double)>& cutoff)
 {
     const int64_t nb = src.num_boxes_total();
     n_far_pairs = n_near_pairs = n_dropped = far_target_evals = near_point_pairs = 0;
+    far_dev = near_dev = DevicePairs{}; // device copies of earlier lists
     Walker w{*this, cutoff};
     if (src.n > 0 && tgt.n > 0)
         w.walk(0, 0, 0, 0);
@@ -477,7 +478,7 @@ void Plan::build_target_lists(int rank)
     // before it is filled.
     const int L = tgt.num_levels();
     std::vector<int64_t> cum((size_t)ntb, 0);
-    tleaf_gid.clear();
+    collect_target_leaves();
     for (int l = 0; l < L; l++)
     {
         const TreeLevel& TL = tgt.levels[l];
@@ -487,8 +488,6 @@ void Plan::build_target_lists(int rank)
             const int64_t g = o + (int64_t)b;
             cum[g] = fin_off[g + 1] - fin_off[g] +
                      (l > 0 ? cum[tgt.level_off[l - 1] + TL.parent[b]] : 0);
-            if (TL.leaf[b])
-                tleaf_gid.push_back(g);
         }
     }
     const int64_t nl = (int64_t)tleaf_gid.size();
@@ -564,9 +563,30 @@ void Plan::build_target_lists(int rank)
     fill(cut[0], cut[1]);
 }
 
-void Plan::target_list_work(int64_t out[4]) const
+void Plan::collect_target_leaves()
 {
-    // points per box, by global box id
+    tleaf_gid.clear();
+    for (int l = 0; l < tgt.num_levels(); l++)
+        for (size_t b = 0; b < tgt.levels[l].size(); b++)
+            if (tgt.levels[l].leaf[b])
+                tleaf_gid.push_back(tgt.level_off[l] + (int64_t)b);
+}
+
+std::vector<int> Plan::target_parents() const
+{
+    std::vector<int> par((size_t)tgt.num_boxes_total(), -1);
+    for (int l = 1; l < tgt.num_levels(); l++)
+        for (size_t b = 0; b < tgt.levels[l].size(); b++)
+            par[tgt.level_off[l] + (int64_t)b] =
+                (int)(tgt.level_off[l - 1] + tgt.levels[l].parent[b]);
+    return par;
+}
+
+void Plan::target_list_work(const std::vector<long long>& far_off, const std::vector<int>& far_src,
+                            const std::vector<long long>& near_off,
+                            const std::vector<int>& near_src, int64_t out[4],
+                            uint64_t* checksum) const
+{
     auto points = [](const Tree& T) {
         std::vector<int64_t> n((size_t)T.num_boxes_total());
         for (int l = 0; l < T.num_levels(); l++)
@@ -575,16 +595,25 @@ void Plan::target_list_work(int64_t out[4]) const
         return n;
     };
     const std::vector<int64_t> ps = points(src), pt = points(tgt);
-    int64_t fe = 0, fp = 0, np = 0, wp = 0;
+    int64_t fe = 0, fp = 0, np = 0;
+    uint64_t h = 0;
     for (size_t i = 0; i < tleaf_gid.size(); i++)
     {
         const int64_t nt = pt[tleaf_gid[i]];
-        fe += nt * (tleaf_far_off[i + 1] - tleaf_far_off[i]);
-        for (int64_t j = tleaf_far_off[i]; j < tleaf_far_off[i + 1]; j++)
-            fp += nt * ps[tleaf_far_src[j]];
-        for (int64_t j = tleaf_near_off[i]; j < tleaf_near_off[i + 1]; j++)
-            np += nt * ps[tleaf_near_src[j]];
+        fe += nt * (far_off[i + 1] - far_off[i]);
+        for (long long j = far_off[i]; j < far_off[i + 1]; j++)
+        {
+            fp += nt * ps[far_src[j]];
+            h = h * 1000003ull + (uint64_t)(far_src[j] + 1) * (uint64_t)(j + 1);
+        }
+        for (long long j = near_off[i]; j < near_off[i + 1]; j++)
+        {
+            np += nt * ps[near_src[j]];
+            h = h * 998244353ull + (uint64_t)(near_src[j] + 1) * (uint64_t)(j + 7);
+        }
+        h ^= (uint64_t)far_off[i + 1] * 31ull + (uint64_t)near_off[i + 1];
     }
+    int64_t wp = 0;
     const int64_t nsb = src.num_boxes_total();
     for (int64_t s = 0; s < nsb && !far.off.empty(); s++)
         for (const int32_t* t = far.begin(s); t != far.end(s); t++)
@@ -593,6 +622,17 @@ void Plan::target_list_work(int64_t out[4]) const
     out[1] = fp;
     out[2] = np;
     out[3] = wp;
+    if (checksum)
+        *checksum = h;
+}
+
+void Plan::target_list_work(int64_t out[4], uint64_t* checksum) const
+{
+    const std::vector<long long> fo(tleaf_far_off.begin(), tleaf_far_off.end()),
+        no(tleaf_near_off.begin(), tleaf_near_off.end());
+    const std::vector<int> fs(tleaf_far_src.begin(), tleaf_far_src.end()),
+        ns(tleaf_near_src.begin(), tleaf_near_src.end());
+    target_list_work(fo, fs, no, ns, out, checksum);
 }
 
 void Plan::target_box_ranges(std::vector<int>& first, std::vector<int>& last) const
@@ -605,25 +645,6 @@ void Plan::target_box_ranges(std::vector<int>& first, std::vector<int>& last) co
         {
             first[tgt.level_off[l] + (int64_t)b] = (int)tgt.levels[l].first[b];
             last[tgt.level_off[l] + (int64_t)b] = (int)tgt.levels[l].last[b];
-        }
-}
-
-void Plan::far_pairs_of_level(int level, const std::vector<int>& tfirst,
-                              const std::vector<int>& tlast, std::vector<int>& fs,
-                              std::vector<int>& f0, std::vector<int>& f1) const
-{
-    const int64_t lo = src.level_off[level], hi = src.level_off[level + 1];
-    const int64_t n = far.off.empty() ? 0 : far.off[hi] - far.off[lo];
-    fs.resize((size_t)n);
-    f0.resize((size_t)n);
-    f1.resize((size_t)n);
-    int64_t k = 0;
-    for (int64_t g = lo; g < hi && n > 0; g++)
-        for (const int32_t* tp = far.begin(g); tp != far.end(g); tp++, k++)
-        {
-            fs[k] = (int)g;
-            f0[k] = tfirst[*tp];
-            f1[k] = tlast[*tp];
         }
 }
 

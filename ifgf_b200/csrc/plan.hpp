@@ -97,10 +97,23 @@ struct PairLists
                     const std::vector<int32_t>& t);
 };
 
+// Device copy of a source-major pair list: pair i's source and target
+// global box ids, sources ascending and each source's targets in discovery
+// order (the order of PairLists).  The buffers are freed with the last
+// copy of the Plan.
+struct DevicePairs
+{
+    std::shared_ptr<int32_t> src, tgt;
+    int64_t n = 0;
+};
+
 struct Plan
 {
     Tree src, tgt;
     PairLists far, near;
+    // the same lists on the device: left there by the GPU walk, uploaded by
+    // ensure_device_pairs after a host walk
+    DevicePairs far_dev, near_dev;
     // target-leaf-centric lists for the evaluation kernel
     std::vector<int64_t> tleaf_gid;       // target leaves (global target box ids)
     std::vector<int64_t> tleaf_far_off;   // CSR offsets into tleaf_far_src
@@ -125,7 +138,13 @@ struct Plan
     // (the caller then walks on the host).
     bool build_lists_gpu();
     void assign_shards(int nranks);
-    // target-leaf lists of the sources owned by `rank` (all when rank < 0)
+    // Device copies of far and near (no-op where the GPU walk left them).
+    void ensure_device_pairs();
+    // tleaf_gid: the target leaves, by global box id
+    void collect_target_leaves();
+    // target-leaf lists of the sources owned by `rank` (all when rank < 0),
+    // on the host (a plan-only init; the device tables are built from the
+    // device pair lists by build_target_lists_gpu)
     void build_target_lists(int rank = -1);
     // Point-level work the target-leaf lists describe, for checking them
     // against the walk's lists: out[0] = sum over target leaves of (leaf
@@ -136,15 +155,18 @@ struct Plan
     // far_target_evals, out[1] equals out[3] and out[2] equals
     // near_point_pairs, since the leaves under a far pair's target box
     // partition its points; sharded, the ranks' out[0..2] add up to them.
-    void target_list_work(int64_t out[4]) const;
+    void target_list_work(int64_t out[4], uint64_t* checksum = nullptr) const;
+    // the same from target-leaf lists given as arrays (the device tables
+    // read back); checksum: a position-weighted sum of both lists, equal
+    // for equal lists in equal order
+    void target_list_work(const std::vector<long long>& far_off, const std::vector<int>& far_src,
+                          const std::vector<long long>& near_off,
+                          const std::vector<int>& near_src, int64_t out[4],
+                          uint64_t* checksum) const;
     // Point range [first, last) of every target box, by global box id.
     void target_box_ranges(std::vector<int>& first, std::vector<int>& last) const;
-    // The far pairs of the source boxes of one level, in list order: the
-    // source global box id and the target box's point range (tfirst / tlast
-    // from target_box_ranges), the input of the cone-marking kernel.
-    void far_pairs_of_level(int level, const std::vector<int>& tfirst,
-                            const std::vector<int>& tlast, std::vector<int>& fs,
-                            std::vector<int>& f0, std::vector<int>& f1) const;
+    // Global id of the parent of every target box (-1 for the root).
+    std::vector<int> target_parents() const;
 };
 
 // Reorders idx stably by key[idx[i]] -- the order std::stable_sort with a

@@ -3,8 +3,12 @@
 //   * stable_order_by_key equals std::stable_sort with a key comparison,
 //     including unsorted inputs, keys outside the counting range and keys
 //     far larger than the list;
-//   * Plan::far_pairs_of_level equals a per-pair search of the target box's
-//     level and point range, for equal and distinct point sets.
+//   * Plan::target_parents equals the per-level parent indices, and the
+//     target-leaf lists of Plan::build_target_lists equal their definition
+//     (per target leaf: the far sources of the leaf and of each ancestor,
+//     leaf first, each group with sources ascending; then its near source
+//     leaves ascending), for equal and distinct point sets; the array form
+//     of target_list_work gives the host form's sums and checksum.
 #include "plan.hpp"
 
 #include <algorithm>
@@ -64,7 +68,7 @@ static std::vector<double> surface(int64_t n, double az, double scale, std::mt19
     return p;
 }
 
-static int check_far_pairs(bool distinct)
+static int check_target_lists(bool distinct)
 {
     std::mt19937_64 rng(7);
     const int64_t n = 40000;
@@ -76,37 +80,64 @@ static int check_far_pairs(bool distinct)
     else
         P.tgt = P.src;
     P.build_lists(nullptr);
-    std::vector<int> tf, tl;
-    P.target_box_ranges(tf, tl);
+    P.build_target_lists(-1);
     const Tree& T = P.tgt;
     int bad = 0;
-    int64_t total = 0;
-    for (int l = 0; l < P.src.num_levels(); l++)
-    {
-        std::vector<int> fs, f0, f1;
-        for (int64_t g = P.src.level_off[l]; g < P.src.level_off[l + 1]; g++)
-            for (const int32_t* tp = P.far.begin(g); tp != P.far.end(g); tp++)
-            {
-                const int lev = (int)(std::upper_bound(T.level_off.begin(), T.level_off.end(),
-                                                       (int64_t)*tp) -
-                                      T.level_off.begin()) - 1;
-                const int64_t b = *tp - T.level_off[lev];
-                fs.push_back((int)g);
-                f0.push_back((int)T.levels[lev].first[b]);
-                f1.push_back((int)T.levels[lev].last[b]);
-            }
-        std::vector<int> a, b, c;
-        P.far_pairs_of_level(l, tf, tl, a, b, c);
-        if (a != fs || b != f0 || c != f1)
+    const std::vector<int> par = P.target_parents();
+    for (int l = 0; l < T.num_levels(); l++)
+        for (size_t b = 0; b < T.levels[l].size(); b++)
         {
-            std::printf("far_pairs_of_level differs at level %d (distinct %d)\n", l, (int)distinct);
-            bad++;
+            const int want = l == 0 ? -1 : (int)(T.level_off[l - 1] + T.levels[l].parent[b]);
+            if (par[T.level_off[l] + (int64_t)b] != want)
+                bad++;
         }
-        total += (int64_t)fs.size();
-    }
-    if (total == 0)
+    if (bad)
+        std::printf("target_parents differs at %d boxes (distinct %d)\n", bad, (int)distinct);
+    // per target box, its far and near sources ascending (the transposes)
+    const int64_t ntb = T.num_boxes_total();
+    std::vector<std::vector<int>> fin((size_t)ntb), nin((size_t)ntb);
+    for (int64_t s = 0; s < P.src.num_boxes_total(); s++)
     {
-        std::printf("no far pairs (distinct %d): the case tests nothing\n", (int)distinct);
+        for (const int32_t* t = P.far.begin(s); t != P.far.end(s); t++)
+            fin[*t].push_back((int)s);
+        for (const int32_t* t = P.near.begin(s); t != P.near.end(s); t++)
+            nin[*t].push_back((int)s);
+    }
+    std::vector<long long> fo{0}, no{0};
+    std::vector<int> fs, ns;
+    for (size_t i = 0; i < P.tleaf_gid.size(); i++)
+    {
+        for (int a = (int)P.tleaf_gid[i]; a >= 0; a = par[a])
+            fs.insert(fs.end(), fin[a].begin(), fin[a].end());
+        ns.insert(ns.end(), nin[P.tleaf_gid[i]].begin(), nin[P.tleaf_gid[i]].end());
+        fo.push_back((long long)fs.size());
+        no.push_back((long long)ns.size());
+    }
+    const bool same = fo.size() == P.tleaf_far_off.size() &&
+                      std::equal(fo.begin(), fo.end(), P.tleaf_far_off.begin()) &&
+                      std::equal(no.begin(), no.end(), P.tleaf_near_off.begin()) &&
+                      fs.size() == P.tleaf_far_src.size() &&
+                      std::equal(fs.begin(), fs.end(), P.tleaf_far_src.begin()) &&
+                      ns.size() == P.tleaf_near_src.size() &&
+                      std::equal(ns.begin(), ns.end(), P.tleaf_near_src.begin());
+    if (!same)
+    {
+        std::printf("target-leaf lists differ from their definition (distinct %d)\n",
+                    (int)distinct);
+        bad++;
+    }
+    int64_t w0[4], w1[4];
+    uint64_t h0 = 0, h1 = 1;
+    P.target_list_work(w0, &h0);
+    P.target_list_work(fo, fs, no, ns, w1, &h1);
+    if (!std::equal(w0, w0 + 4, w1) || h0 != h1)
+    {
+        std::printf("target_list_work forms differ (distinct %d)\n", (int)distinct);
+        bad++;
+    }
+    if (fs.empty() || ns.empty())
+    {
+        std::printf("empty lists (distinct %d): the case tests nothing\n", (int)distinct);
         bad++;
     }
     return bad;
@@ -114,7 +145,7 @@ static int check_far_pairs(bool distinct)
 
 int main()
 {
-    const int bad = check_stable_order() + check_far_pairs(false) + check_far_pairs(true);
+    const int bad = check_stable_order() + check_target_lists(false) + check_target_lists(true);
     std::printf(bad ? "FAILED\n" : "OK\n");
     return bad ? 1 : 0;
 }

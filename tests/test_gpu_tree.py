@@ -78,3 +78,66 @@ def test_gpu_interaction_lists_equal_host_lists(name, pts, leaf):
                 a = gpu.interaction_list(lvl, box, far)
                 b = host.interaction_list(lvl, box, far)
                 assert np.array_equal(a, b), (lvl, box, far)
+
+
+_TL_KEYS = ("target_leaf_far_evals", "target_leaf_far_point_pairs",
+            "target_leaf_near_point_pairs", "target_leaf_lists_checksum", "target_leaves")
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,pts,leaf", _sets(), ids=lambda v: v if isinstance(v, str) else "")
+def test_gpu_target_leaf_lists_equal_host_lists(name, pts, leaf):
+    """The target-leaf lists built on the GPU (stable radix sort by target,
+    ancestor concatenation, one warp per leaf) equal the host build entry for
+    entry: the same work sums and the same position-weighted checksum."""
+    import ifgf_b200 as G
+
+    for tg in (None, W.sphere_points(5000, seed=3) * 1.5):
+        t = pts if tg is None else tg
+        gpu = G.HelmholtzIfgfOperator(5.0, leaf, 8)
+        gpu.init(pts, t)
+        host = G.HelmholtzIfgfOperator(5.0, leaf, 8)
+        host.init_plan_only(pts, t)
+        sg, sh = gpu.stats(), host.stats()
+        for key in _TL_KEYS[:4]:
+            assert sg[key] == sh[key], (key, tg is None)
+        assert sg["target_leaf_far_evals"] == sg["far_target_evals"]
+        assert sg["target_leaf_near_point_pairs"] == sg["near_point_pairs"]
+
+
+@pytest.mark.gpu
+def test_gpu_target_leaf_lists_sharded_and_host_walk():
+    """Per-rank lists of a sharded operator (another rank's source boxes
+    dropped) and lists from pairs uploaded after a host walk (a cutoff
+    predicate) equal the host build."""
+    import ifgf_b200 as G
+
+    pts = W.ellipsoid_points(60000, seed=0)
+    tot = None
+    sums = [0, 0, 0]
+    for rank in range(3):
+        gpu = G.HelmholtzIfgfOperator(20.0, 60, 8)
+        gpu.set_shard(rank, 3)
+        gpu.init(pts, pts)
+        host = G.HelmholtzIfgfOperator(20.0, 60, 8)
+        host.set_shard(rank, 3)
+        host.init_plan_only(pts, pts)
+        sg, sh = gpu.stats(), host.stats()
+        for key in _TL_KEYS[:4]:
+            assert sg[key] == sh[key], (key, rank)
+        for i, key in enumerate(_TL_KEYS[:3]):
+            sums[i] += sg[key]
+        tot = sg
+    assert sums == [tot["far_target_evals"], tot["far_point_pairs"], tot["near_point_pairs"]]
+
+    def cut(d):
+        return d > 0.3
+
+    gpu = G.HelmholtzIfgfOperator(20.0, 60, 8)
+    gpu.init(pts, pts, cutOff=cut)
+    host = G.HelmholtzIfgfOperator(20.0, 60, 8)
+    host.init_plan_only(pts, pts, cutOff=cut)
+    sg, sh = gpu.stats(), host.stats()
+    assert sg["dropped_pairs"] > 0
+    for key in _TL_KEYS[:4]:
+        assert sg[key] == sh[key], key
