@@ -6,22 +6,37 @@
 // the evaluation helpers.
 #pragma once
 
-// Far field of a plane group (blockIdx.y; NP planes): the cone lookup and the centred
-// factor of a (target, far box) pair are computed once (with MK the factor
-// once per plane); each plane's Chebyshev sum uses its own coefficient block.
-// Adds the near sums and writes the caller's result planes (the first nrhs).
+// Far field of a plane group (blockIdx.y; NP planes) for one target leaf per
+// CTA (evaluateFromInterp, ifgfoperator.hpp:1736-1891, for every far source
+// box of the leaf and of its ancestors).  Adds the near sums and writes the
+// caller's result planes (the first nrhs).
+//
 // Thread (ti, si) owns target ti and far boxes si, si + S, ... (S = threads /
-// targets).  Coefficient blocks are staged in shared memory: for every S
-// consecutive far boxes (one pair per thread) the CTA collects the distinct
-// fine cones of its pairs in a small hash table, copies up to far_slots() of
-// their 4-plane blocks with cp.async and evaluates from shared memory.  The
-// lanes of a warp are targets of one leaf at one box, which fall into a few
-// cones: from global memory every such load touches one sector per cone, from
-// shared memory the few blocks are served together (slots start 16 bytes
-// apart modulo 128, in different banks).  Pairs whose cone found no slot read
-// global memory.  The evaluation order, and so the result, is that of the
-// unstaged loop.
+// targets): it looks up the fine cone of its (target, box) pair once for all
+// NP planes, computes the centred factor and adds the pair's NP values to
+// its FP64 sums.  For every S consecutive far boxes (one pair per thread):
+//   1. the distinct cones of the pairs go into a small hash table; the first
+//      far_slots() of them get a shared-memory slot for their NP-plane
+//      coefficient blocks (cp.async copies);
+//   2. the pairs are written as records (local coordinates, slot) in slot
+//      order, each slot's group padded to 8 positions;
+//   3. an evaluating thread takes positions 2q and 2q + 1 -- two pairs of
+//      one cone -- for half of the planes, so every 16-byte coefficient load
+//      feeds both pairs' FMAs, and the 4 lanes of a quad read one block (an
+//      LDS.128 is then served in its minimum of one wavefront per
+//      half-warp); the plane halves keep all threads busy;
+//   4. the owner of each pair reads the pair's values back, applies the
+//      factor and adds them, in box order.
+// Evaluated in owner order, one pair per thread, the lanes of a warp read the
+// few cones of their targets from unrelated slots: the shared loads split
+// into about three wavefronts each, and with one pair per load the L1 data
+// pipe, not the FMA pipe, bounds the kernel.  Pairs whose cone found no slot
+// are sorted last, one per evaluating thread, and read global memory.
+constexpr int FARB_THREADS = 256; // threads of one CTA (one pair each per group)
+constexpr int FARB_CTAS = 2;      // resident CTAs per SM (registers: 128 per thread)
 constexpr int FAR_HASH = 128;
+constexpr int FAR_BOXES = 128; // far boxes whose geometry is loaded at once
+constexpr int FAR_PAD = 8;     // positions per quad of evaluating lanes
 template <int P_LO, int NP> __host__ __device__ constexpr int far_slot_stride()
 {
     int s = NP * P_LO; // float2 per slot: NP planes, then pad to 16 B mod 128
@@ -29,55 +44,158 @@ template <int P_LO, int NP> __host__ __device__ constexpr int far_slot_stride()
         s++;
     return s;
 }
+// record positions of one group of boxes: one pair per thread, plus the
+// padding of each slot's group (at most FAR_PAD - 1 each)
+__host__ __device__ constexpr int far_positions(int nslot)
+{
+    return (FARB_THREADS + (FAR_PAD - 1) * nslot + 7) / 8 * 8;
+}
+// static shared memory of far_batch_kernel, for the slot budget
+template <int NP> __host__ __device__ constexpr int far_static_bytes(int nslot)
+{
+    return 3 * 2 * FAR_HASH * 4 + 2 * nslot * 4 + 16 + far_positions(nslot) * (16 + 8 * NP) +
+           NP * (int)sizeof(KParams) + FAR_BOXES * (4 * 8 + 8 + 4) +
+           MAX_LEVELS * (int)sizeof(LookupF);
+}
+// slots: as many as fit beside the static arrays with FARB_CTAS CTAs per SM
+// (233472 bytes of shared memory per SM, 1 KB reserved per CTA, 512 bytes
+// margin), at most 96 / NP (well inside the FAR_HASH entries) and 32 (one
+// warp scans the slot counts)
 template <int P_LO, int NP> __host__ __device__ constexpr int far_slots()
 {
-    const int fit = 86016 / (far_slot_stride<P_LO, NP>() * 8); // about 84 KB: 2 CTAs per SM
-    const int cap = 96 / NP; // within the hash table (FAR_HASH entries)
-    return fit < cap ? fit : cap;
+    int n = 96 / NP < 32 ? 96 / NP : 32;
+    while (n > 1 && n * far_slot_stride<P_LO, NP>() * 8 + far_static_bytes<NP>(n) >
+                        233472 / FARB_CTAS - 1024 - 512)
+        n--;
+    return n;
 }
 template <int N0, int N1, int N2, int NP> constexpr size_t far_batch_smem()
 {
     constexpr size_t slots =
         (size_t)far_slots<N0 * N1 * N2, NP>() * far_slot_stride<N0 * N1 * N2, NP>() * 8;
-    constexpr size_t red = 2 * NP * FAR_THREADS * sizeof(double); // final reduction
+    constexpr size_t red = 2 * NP * FARB_THREADS * sizeof(double); // final reduction
     return slots > red ? slots : red;
 }
+// record of a pair in slot order: local coordinates (float bits) and the slot,
+// or ~(global fine cone) for a pair read from global memory
+struct __align__(16) FarRec
+{
+    int l0, l1, l2, code;
+};
+
+// Two points of one cone block in shared memory: the tensor-product
+// Chebyshev sums of ChebF, sharing every coefficient load.
+template <int N0, int N1, int N2> struct ChebF2
+{
+    __device__ static __forceinline__ void basis(const float* x, float (&t0)[N0], float (&t1)[N1],
+                                                 float (&t2)[N2])
+    {
+        t0[0] = t1[0] = t2[0] = 1.f;
+        if (N0 > 1)
+            t0[1] = x[0];
+        if (N1 > 1)
+            t1[1] = x[1];
+        if (N2 > 1)
+            t2[1] = x[2];
+#pragma unroll
+        for (int i = 2; i < N0; i++)
+            t0[i] = fmaf(2.f * x[0], t0[i - 1], -t0[i - 2]);
+#pragma unroll
+        for (int i = 2; i < N1; i++)
+            t1[i] = fmaf(2.f * x[1], t1[i - 1], -t1[i - 2]);
+#pragma unroll
+        for (int i = 2; i < N2; i++)
+            t2[i] = fmaf(2.f * x[2], t2[i - 1], -t2[i - 2]);
+    }
+    __device__ static __forceinline__ void eval(const float2* __restrict__ c, const float* xa,
+                                                const float* xb, cplx<float>& va, cplx<float>& vb)
+    {
+        float a0[N0], a1[N1], a2[N2], b0[N0], b1[N1], b2[N2];
+        basis(xa, a0, a1, a2);
+        basis(xb, b0, b1, b2);
+        float aar = 0, aai = 0, bar = 0, bai = 0;
+#pragma unroll
+        for (int k = 0; k < N2; k++)
+        {
+            float abr = 0, abi = 0, bbr = 0, bbi = 0;
+#pragma unroll
+            for (int j = 0; j < N1; j += CoefRows<N0, N1>::ROWS)
+            {
+                float2 v[CoefRows<N0, N1>::ROWS * N0];
+                CoefRows<N0, N1, true>::load(c + N0 * (j + N1 * k), v);
+#pragma unroll
+                for (int jj = 0; jj < CoefRows<N0, N1>::ROWS; jj++)
+                {
+                    float acr = 0, aci = 0, bcr = 0, bci = 0;
+#pragma unroll
+                    for (int i = 0; i < N0; i++)
+                    {
+                        acr = fmaf(v[jj * N0 + i].x, a0[i], acr);
+                        aci = fmaf(v[jj * N0 + i].y, a0[i], aci);
+                        bcr = fmaf(v[jj * N0 + i].x, b0[i], bcr);
+                        bci = fmaf(v[jj * N0 + i].y, b0[i], bci);
+                    }
+                    abr = fmaf(acr, a1[j + jj], abr);
+                    abi = fmaf(aci, a1[j + jj], abi);
+                    bbr = fmaf(bcr, b1[j + jj], bbr);
+                    bbi = fmaf(bci, b1[j + jj], bbi);
+                }
+            }
+            aar = fmaf(abr, a2[k], aar);
+            aai = fmaf(abi, a2[k], aai);
+            bar = fmaf(bbr, b2[k], bar);
+            bai = fmaf(bbi, b2[k], bai);
+        }
+        va = {aar, aai};
+        vb = {bar, bai};
+    }
+};
 
 template <int KIND, int N0, int N1, int N2, bool MK, int NP>
-__global__ void __launch_bounds__(FAR_THREADS, 2) far_batch_kernel(EvalArgs a, BatchPtrs bp)
+__global__ void __launch_bounds__(FARB_THREADS, FARB_CTAS)
+    far_batch_kernel(EvalArgs a, BatchPtrs bp)
 {
     constexpr int NB = NP;
     constexpr int P_LO = N0 * N1 * N2;
     constexpr int SS = far_slot_stride<P_LO, NP>();
     constexpr int NSLOT = far_slots<P_LO, NP>();
+    constexpr int NPOS = far_positions(NSLOT);
     constexpr int CPP = P_LO / 2; // 16-byte chunks of one plane's block
     static_assert(P_LO % 2 == 0, "blocks must be whole 16-byte chunks");
     static_assert(NSLOT > 0, "one slot must fit");
+    static_assert(NSLOT <= 32, "one warp scans the slot counts");
     extern __shared__ __align__(16) float2 far_sh[]; // slots; the final reduction reuses it
-    __shared__ int hkey[2][FAR_HASH], hslot[2][FAR_HASH], sgf[NSLOT], nslot[2];
+    __shared__ int hkey[2][FAR_HASH], hslot[2][FAR_HASH], hcnt[2][FAR_HASH];
+    __shared__ int sgf[NSLOT], sent[NSLOT], nslot[2], novf[2];
+    __shared__ FarRec frec[NPOS];
+    __shared__ float2 fres[NB][NPOS];
     __shared__ KParams kps[MK ? NB : 1];
     const int pb = blockIdx.y * NB;
     if constexpr (MK)
         if (threadIdx.x < NB)
             kps[threadIdx.x] = bp.kp_plane[pb + threadIdx.x]; // read after the chunk barriers
     for (int q = threadIdx.x; q < 2 * FAR_HASH; q += blockDim.x)
+    {
         hkey[q / FAR_HASH][q % FAR_HASH] = -1;
+        hcnt[q / FAR_HASH][q % FAR_HASH] = 0;
+    }
     if (threadIdx.x < 2)
-        nslot[threadIdx.x] = 0;
-    __shared__ double fcx[FAR_THREADS], fcy[FAR_THREADS], fcz[FAR_THREADS], fH[FAR_THREADS];
-    __shared__ long long ffm[FAR_THREADS];
-    __shared__ int flev[FAR_THREADS];
+        nslot[threadIdx.x] = novf[threadIdx.x] = 0;
+    const int lane = threadIdx.x & 31;
+    __shared__ double fcx[FAR_BOXES], fcy[FAR_BOXES], fcz[FAR_BOXES], fH[FAR_BOXES];
+    __shared__ long long ffm[FAR_BOXES];
+    __shared__ int flev[FAR_BOXES];
     __shared__ LookupF lfs[MAX_LEVELS];
     for (int l = threadIdx.x; l < a.L; l += blockDim.x)
         make_lookupf(a.lv[l], lfs[l]); // read after the first chunk's barriers
     const int tl = blockIdx.x;
     const int tf = a.tl_first[tl], tlast = a.tl_last[tl];
     const long long fb0 = a.far_off[tl], fb1 = a.far_off[tl + 1];
-    int tab = 0; // hash table of the current sub-chunk (CTA-uniform)
-    for (int base = tf; base < tlast; base += FAR_THREADS)
+    int tab = 0; // hash table of the current group of boxes (CTA-uniform)
+    for (int base = tf; base < tlast; base += FARB_THREADS)
     {
-        const int cnt = min(FAR_THREADS, tlast - base);
-        const int S = FAR_THREADS / cnt;
+        const int cnt = min(FARB_THREADS, tlast - base);
+        const int S = FARB_THREADS / cnt;
         const int ti = threadIdx.x % cnt, si = threadIdx.x / cnt;
         const bool active = si < S;
         const int t = base + ti;
@@ -86,9 +204,9 @@ __global__ void __launch_bounds__(FAR_THREADS, 2) far_batch_kernel(EvalArgs a, B
 #pragma unroll
         for (int r = 0; r < NB; r++)
             accr[r] = acci[r] = 0.0;
-        for (long long e0 = fb0; e0 < fb1; e0 += FAR_THREADS)
+        for (long long e0 = fb0; e0 < fb1; e0 += FAR_BOXES)
         {
-            const int fcnt = (int)min((long long)FAR_THREADS, fb1 - e0);
+            const int fcnt = (int)min((long long)FAR_BOXES, fb1 - e0);
             __syncthreads();
             if (threadIdx.x < fcnt)
             {
@@ -104,7 +222,7 @@ __global__ void __launch_bounds__(FAR_THREADS, 2) far_batch_kernel(EvalArgs a, B
                 flev[threadIdx.x] = lev;
             }
             __syncthreads();
-            // the cone of this thread's pair in sub-chunk box i (gf < 0: none)
+            // the cone of this thread's pair in box i of the chunk (g < 0: none)
             auto lookup = [&](int i, int& g, float (&l)[3], double& dd) {
                 g = -1;
                 l[0] = l[1] = l[2] = 0.f;
@@ -121,20 +239,21 @@ __global__ void __launch_bounds__(FAR_THREADS, 2) far_batch_kernel(EvalArgs a, B
             float loc_next[3];
             double d2_next;
             lookup(si, gf_next, loc_next, d2_next);
-            // sub-chunks of S boxes: at most one pair per thread; every
-            // thread runs every sub-chunk (barriers inside).  The next
-            // sub-chunk's lookup (a dependent global load) is issued before
-            // this one's copies are waited for.
+            // groups of S boxes: at most one pair per thread; every thread
+            // runs every group (barriers inside).  The next group's lookup (a
+            // dependent global load) is issued before this one's copies are
+            // waited for.
             for (int c0 = 0; c0 < fcnt; c0 += S)
             {
                 const int gf = gf_next;
                 const float loc[3] = {loc_next[0], loc_next[1], loc_next[2]};
                 const double d2 = d2_next;
-                int h = -1;
+                int h = -1, rank = 0;
                 if (gf >= 0)
                 {
                     // insert the cone, bounded linear probing; the first
-                    // inserter takes a slot while slots last
+                    // inserter takes a slot while slots last.  rank: this
+                    // pair's place among the pairs of its cone.
                     int hh = (int)(((unsigned)gf * 2654435761u) >> 25) & (FAR_HASH - 1);
                     for (int q = 0; q < FAR_HASH; q++, hh = (hh + 1) & (FAR_HASH - 1))
                     {
@@ -143,7 +262,10 @@ __global__ void __launch_bounds__(FAR_THREADS, 2) far_batch_kernel(EvalArgs a, B
                         {
                             const int k = atomicAdd(&nslot[tab], 1);
                             if (k < NSLOT)
+                            {
                                 sgf[k] = gf;
+                                sent[k] = hh;
+                            }
                             hslot[tab][hh] = k < NSLOT ? k : -1;
                             h = hh;
                             break;
@@ -154,31 +276,111 @@ __global__ void __launch_bounds__(FAR_THREADS, 2) far_batch_kernel(EvalArgs a, B
                             break;
                         }
                     }
+                    if (h >= 0)
+                        rank = atomicAdd(&hcnt[tab][h], 1);
                 }
-                __syncthreads(); // table and slot list complete
+                __syncthreads(); // table, slot list and counts complete
                 const int ns = min(nslot[tab], NSLOT);
+                // group starts: every warp scans the padded slot counts
+                const int ck = lane < ns ? hcnt[tab][sent[lane]] : 0;
+                const int pk = (ck + FAR_PAD - 1) & ~(FAR_PAD - 1);
+                int incl = pk;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1)
+                {
+                    const int v = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= o)
+                        incl += v;
+                }
+                const int slotted = __shfl_sync(0xffffffffu, incl, 31); // padded
+                const int k = h >= 0 ? hslot[tab][h] : -1;
+                const int src = k >= 0 ? k : 0;
+                const int kbase = __shfl_sync(0xffffffffu, incl - pk, src);
+                const int kcnt = __shfl_sync(0xffffffffu, ck, src);
+                const int kend = __shfl_sync(0xffffffffu, incl, src);
+                int pos = -1;
+                if (gf >= 0)
+                {
+                    pos = k >= 0 ? kbase + rank : slotted + atomicAdd(&novf[tab], 1);
+                    frec[pos] = FarRec{__float_as_int(loc[0]), __float_as_int(loc[1]),
+                                       __float_as_int(loc[2]), k >= 0 ? k : ~gf};
+                    // the last pair of a slot fills its group's padding
+                    // (coordinates 0: evaluated, never read)
+                    if (k >= 0 && rank == kcnt - 1)
+                        for (int p = kbase + kcnt; p < kend; p++)
+                            frec[p] = FarRec{0, 0, 0, k};
+                }
                 // the other table was last read before this barrier: clear it
                 for (int q = threadIdx.x; q < FAR_HASH; q += blockDim.x)
-                    hkey[tab ^ 1][q] = -1;
-                if (threadIdx.x == 0)
-                    nslot[tab ^ 1] = 0;
-                // one warp per slot, lanes over the slot's 16-byte chunks
-                for (int k = threadIdx.x >> 5; k < ns; k += FAR_THREADS / 32)
                 {
-                    const float2* src0 = bp.fcoef + (size_t)pb * bp.fc_plane + (size_t)sgf[k] * P_LO;
-                    float2* dst0 = far_sh + (size_t)k * SS;
+                    hkey[tab ^ 1][q] = -1;
+                    hcnt[tab ^ 1][q] = 0;
+                }
+                if (threadIdx.x == 0)
+                    nslot[tab ^ 1] = novf[tab ^ 1] = 0;
+                // one warp per slot, lanes over the slot's 16-byte chunks
+                for (int ks = threadIdx.x >> 5; ks < ns; ks += FARB_THREADS / 32)
+                {
+                    const float2* src0 = bp.fcoef + (size_t)pb * bp.fc_plane + (size_t)sgf[ks] * P_LO;
+                    float2* dst0 = far_sh + (size_t)ks * SS;
 #pragma unroll
                     for (int r = 0; r < NB; r++)
-                        for (int ch = threadIdx.x & 31; ch < CPP; ch += 32)
+                        for (int ch = lane; ch < CPP; ch += 32)
                             cp_async16(dst0 + r * P_LO + 2 * ch,
                                        src0 + (size_t)r * bp.fc_plane + 2 * ch);
                 }
                 lookup(c0 + S + si, gf_next, loc_next, d2_next);
                 cp_async_wait_all();
-                __syncthreads(); // blocks staged
+                __syncthreads(); // blocks staged, records written
+                // evaluate: work item = (two pairs of one slot, half of the
+                // planes), then (one pair read from global memory, half of
+                // the planes); consecutive threads take consecutive pairs
+                constexpr int NH = NB > 1 ? 2 : 1, RH = NB / NH;
+                static_assert(NB % NH == 0, "plane halves");
+                const int n_two = slotted / 2, n_one = novf[tab];
+                const int n_item = NH * (n_two + n_one);
+                for (int w = threadIdx.x; w < n_item; w += FARB_THREADS)
+                {
+                    if (w < NH * n_two)
+                    {
+                        const int q = w % n_two, r0 = (w / n_two) * RH;
+                        const FarRec ra = frec[2 * q], rb = frec[2 * q + 1];
+                        const float la[3] = {__int_as_float(ra.l0), __int_as_float(ra.l1),
+                                             __int_as_float(ra.l2)};
+                        const float lb[3] = {__int_as_float(rb.l0), __int_as_float(rb.l1),
+                                             __int_as_float(rb.l2)};
+#pragma unroll
+                        for (int rr = 0; rr < RH; rr++)
+                        {
+                            cplx<float> va, vb;
+                            ChebF2<N0, N1, N2>::eval(far_sh + (size_t)ra.code * SS +
+                                                         (r0 + rr) * P_LO,
+                                                     la, lb, va, vb);
+                            fres[r0 + rr][2 * q] = make_float2(va.re, va.im);
+                            fres[r0 + rr][2 * q + 1] = make_float2(vb.re, vb.im);
+                        }
+                    }
+                    else
+                    {
+                        const int w1 = w - NH * n_two;
+                        const int p = slotted + w1 % n_one, r0 = (w1 / n_one) * RH;
+                        const FarRec rc = frec[p];
+                        const float l3[3] = {__int_as_float(rc.l0), __int_as_float(rc.l1),
+                                             __int_as_float(rc.l2)};
+#pragma unroll
+                        for (int rr = 0; rr < RH; rr++)
+                        {
+                            const cplx<float> v = ChebF<N0, N1, N2>::eval(
+                                bp.fcoef + (size_t)(pb + r0 + rr) * bp.fc_plane +
+                                    (size_t)(~rc.code) * P_LO,
+                                l3, a.lo);
+                            fres[r0 + rr][p] = make_float2(v.re, v.im);
+                        }
+                    }
+                }
+                __syncthreads(); // values of every pair written
                 if (gf >= 0)
                 {
-                    const int k = h >= 0 ? hslot[tab][h] : -1;
                     cplx<float> cf;
                     if constexpr (!MK)
                         cf = cf_mixed<KIND>(d2, a.kp);
@@ -187,16 +389,9 @@ __global__ void __launch_bounds__(FAR_THREADS, 2) far_batch_kernel(EvalArgs a, B
                     {
                         if constexpr (MK)
                             cf = cf_mixed<KIND>(d2, kps[r]);
-                        const cplx<float> v =
-                            k >= 0 ? ChebF<N0, N1, N2, true>::eval(far_sh + (size_t)k * SS +
-                                                                       r * P_LO,
-                                                                   loc, a.lo)
-                                   : ChebF<N0, N1, N2>::eval(bp.fcoef +
-                                                                 (size_t)(pb + r) * bp.fc_plane +
-                                                                 (size_t)gf * P_LO,
-                                                             loc, a.lo);
-                        accr[r] += (double)(v.re * cf.re - v.im * cf.im);
-                        acci[r] += (double)(v.re * cf.im + v.im * cf.re);
+                        const float2 v = fres[r][pos];
+                        accr[r] += (double)(v.x * cf.re - v.y * cf.im);
+                        acci[r] += (double)(v.x * cf.im + v.y * cf.re);
                     }
                 }
                 tab ^= 1;
@@ -204,12 +399,12 @@ __global__ void __launch_bounds__(FAR_THREADS, 2) far_batch_kernel(EvalArgs a, B
         }
         __syncthreads(); // the slots are no longer read: reduce through them
         double* rr = reinterpret_cast<double*>(far_sh);
-        double* ri = rr + NB * FAR_THREADS;
+        double* ri = rr + NB * FARB_THREADS;
 #pragma unroll
         for (int r = 0; r < NB; r++)
         {
-            rr[r * FAR_THREADS + threadIdx.x] = accr[r];
-            ri[r * FAR_THREADS + threadIdx.x] = acci[r];
+            rr[r * FARB_THREADS + threadIdx.x] = accr[r];
+            ri[r * FARB_THREADS + threadIdx.x] = acci[r];
         }
         __syncthreads();
         if (active && si == 0)
@@ -220,8 +415,8 @@ __global__ void __launch_bounds__(FAR_THREADS, 2) far_batch_kernel(EvalArgs a, B
                 double sr = 0, sim = 0;
                 for (int s = 0; s < S; s++)
                 {
-                    sr += rr[r * FAR_THREADS + ti + s * cnt];
-                    sim += ri[r * FAR_THREADS + ti + s * cnt];
+                    sr += rr[r * FARB_THREADS + ti + s * cnt];
+                    sim += ri[r * FARB_THREADS + ti + s * cnt];
                 }
                 const double2 nr = bp.unear[(size_t)(pb + r) * bp.n_tgt + t];
                 sr += nr.x;
@@ -238,4 +433,3 @@ __global__ void __launch_bounds__(FAR_THREADS, 2) far_batch_kernel(EvalArgs a, B
         }
     }
 }
-

@@ -511,7 +511,7 @@ static int run_mult_batch(const MultPtrs& m, const BatchPtrs& bp, const void* d_
             auto fk = far_batch_kernel<KIND, N0, N1, N2, MK, BATCH_NB>;
             IFGF_CHECK(cudaFuncSetAttribute(fk, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             (int)fsm));
-            fk<<<dim3(m.n_tleaf, bp.groups), FAR_THREADS, fsm, st>>>(ea, bp);
+            fk<<<dim3(m.n_tleaf, bp.groups), FARB_THREADS, fsm, st>>>(ea, bp);
             IFGF_CHECK_LAUNCH();
             if (hk)
                 hk->end();
