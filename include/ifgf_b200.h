@@ -48,7 +48,7 @@ typedef struct ifgf_operator ifgf_operator;
 #define IFGF_PREC_MIXED 1 /* FP32 sums with FP64 phase / final accumulation   */
 
 /* ifgf_set_upward_path */
-#define IFGF_UPWARD_AUTO 0   /* tensor cores on levels with well-filled tiles */
+#define IFGF_UPWARD_AUTO 0   /* per level, the faster of the two (timed)      */
 #define IFGF_UPWARD_FFMA 1   /* FP32 FMA kernels only                         */
 #define IFGF_UPWARD_TENSOR 2 /* tensor cores wherever the order shape allows  */
 
@@ -88,9 +88,12 @@ int ifgf_set_precision(ifgf_operator* op, int mode);
 /* Selects the kernel of the mixed-precision upward transfer (the
  * interpolation of children's fine interpolants at parent cone nodes,
  * transferInterp, ifgfoperator.hpp:1639-1705): IFGF_UPWARD_AUTO (default)
- * runs it on the tensor cores (tcgen05, split-TF32, FP32-accurate) on the
- * levels whose cones fill the kernel's 32-row tiles well enough and with
- * FP32 FMA kernels elsewhere; IFGF_UPWARD_FFMA never uses the tensor cores;
+ * times the tensor-core kernel (tcgen05, split-TF32, FP32-accurate) and the
+ * FP32 FMA kernel once per level and right-hand-side count on the operator's
+ * own tables (the first mixed matvec of that count) and keeps the faster per
+ * level (the choice and the times are in ifgf_stats_json, "upward_tuner");
+ * levels it has not timed use the tensor cores when their cones fill the
+ * kernel's 32-row tiles well enough; IFGF_UPWARD_FFMA never uses the tensor cores;
  * IFGF_UPWARD_TENSOR uses them on every level the order shape allows (low
  * orders (2,5,5) and (3,6,6)).  FP64 always runs the FP64 kernels.  No
  * reference counterpart. */
