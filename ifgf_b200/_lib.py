@@ -48,6 +48,7 @@ def _load():
         "ifgf_set_dx": [H, C.c_int],
         "ifgf_set_precision": [H, C.c_int],
         "ifgf_set_upward_path": [H, C.c_int],
+        "ifgf_set_far_plan": [H, C.c_int],
         "ifgf_bounded_wait_selftest": [C.c_double, _dp],
         "ifgf_set_shard": [H, C.c_int, C.c_int],
         "ifgf_set_wavenumber": [H, C.c_double, C.c_double],
@@ -95,7 +96,7 @@ lib = _load()
 # Every symbol declared in include/ifgf_b200.h.
 EXPORTED = [
     "ifgf_create", "ifgf_set_dx", "ifgf_set_precision", "ifgf_set_shard", "ifgf_shard_boxes",
-    "ifgf_set_upward_path", "ifgf_bounded_wait_selftest",
+    "ifgf_set_upward_path", "ifgf_set_far_plan", "ifgf_bounded_wait_selftest",
     "ifgf_set_wavenumber",
     "ifgf_init", "ifgf_init_plan_only",
     "ifgf_box_list", "ifgf_mult",

@@ -123,6 +123,13 @@ extern "C"
         return guarded([&] { h->op.set_upward_path(path); });
     }
 
+    int ifgf_set_far_plan(ifgf_operator* h, int enable)
+    {
+        if (!h)
+            return null_handle();
+        return guarded([&] { h->op.set_far_plan(enable != 0); });
+    }
+
     int ifgf_bounded_wait_selftest(double limit_ms, double* waited_ms)
     {
         return guarded([&] { ifgf::bounded_wait_selftest(limit_ms, waited_ms); });

@@ -898,4 +898,79 @@ __device__ __forceinline__ void cart_to_interp_f(float p0, float p1, float p2, f
     s[0] = H * rsqrtf(a + p2 * p2);
 }
 
+
+// FP32 cone-lookup parameters of one level, made once per CTA in shared
+// memory so that the far-field lookups read no level data from global memory.
+struct LookupF
+{
+    float lo[3], hi[3], hinv[3], top[3]; // domain, 1 / fine width, nf - 1
+    int nf[3];
+};
+
+__device__ __forceinline__ void make_lookupf(const LevelGeom& G, LookupF& L)
+{
+#pragma unroll
+    for (int d = 0; d < 3; d++)
+    {
+        L.lo[d] = (float)G.dmin[d];
+        L.hi[d] = (float)G.dmax[d];
+        L.hinv[d] = (float)G.hfi[d];
+        L.top[d] = (float)(G.nf[d] - 1);
+        L.nf[d] = G.nf[d];
+    }
+}
+
+// fine_lookup_mixed with the level's FP32 parameters at hand: with
+// t = (s - lo) / h the element index is q = floor(t) (clamped) and the local
+// coordinate 2 (t - q) - 1, the same quantities as (s - centre) / (h / 2).
+// The FP64 fallback (outside the FP32 domain or an inactive cone) is that of
+// fine_lookup_mixed.
+__device__ __forceinline__ int fine_lookup_fast(const LookupF& L, const LevelGeom& G,
+                                                const int* __restrict__ fm, const double* p,
+                                                double H, float* loc, unsigned long long* err)
+{
+    float sf[3];
+    cart_to_interp_f((float)p[0], (float)p[1], (float)p[2], (float)H, sf);
+    bool inside = true;
+    int id = 0, stride = 1;
+    float fr[3];
+#pragma unroll
+    for (int j = 0; j < 3; j++)
+    {
+        inside = inside && sf[j] >= L.lo[j] && sf[j] <= L.hi[j];
+        const float t = (sf[j] - L.lo[j]) * L.hinv[j];
+        const float q = fminf(fmaxf(floorf(t), 0.f), L.top[j]);
+        fr[j] = t - q;
+        id += __float2int_rz(q) * stride;
+        stride *= L.nf[j];
+    }
+    if (inside)
+    {
+        const int gf = fm[id];
+        if (gf >= 0)
+        {
+#pragma unroll
+            for (int d = 0; d < 3; d++)
+                loc[d] = fmaf(2.f, fr[d], -1.f);
+            return gf;
+        }
+    }
+    double s[3], ld[3];
+    cart_to_interp(p[0], p[1], p[2], H, s);
+    const int fe = element_for_point(s, G.dmin, G.dmax, G.hfi, G.nf);
+    if (fe < 0)
+        return -1;
+    const int gf = fm[fe];
+    if (gf < 0)
+    {
+        atomicAdd(err, 1ull);
+        return -1;
+    }
+    to_local(fe, s, G.dmin, G.hf, G.hfi, G.nf, ld);
+    loc[0] = (float)ld[0];
+    loc[1] = (float)ld[1];
+    loc[2] = (float)ld[2];
+    return gf;
+}
+
 } // namespace ifgf

@@ -433,3 +433,181 @@ __global__ void __launch_bounds__(FARB_THREADS, FARB_CTAS)
         }
     }
 }
+
+// The far field of far_batch_kernel from the far-field plan built at init
+// (FarChunk / FarGroup / FarPlanRec): the cone lookups, the slot assignment
+// and the cone-ordered, padded records of every group are read instead of
+// computed, so a group is: copy its records and slot blocks (cp.async), the
+// owners' box distances meanwhile, one barrier, the sums (two pairs of one
+// slot per work item, as in far_batch_kernel), one barrier, the owners'
+// factors and FP64 sums in box order, overlapping the next group's copies.  One CTA per chunk of up to 256
+// targets of a leaf and per group of NP planes.
+constexpr int FAR_PLAN_POS = (FARB_THREADS + (FAR_PAD - 1) * FAR_PLAN_SLOTS + 7) / 8 * 8;
+template <int P_LO, int NP> __host__ __device__ constexpr size_t far_plan_smem()
+{
+    const size_t slots = (size_t)FAR_PLAN_SLOTS * far_slot_stride<P_LO, NP>() * 8;
+    const size_t red = 2 * NP * FARB_THREADS * sizeof(double); // final reduction
+    return slots > red ? slots : red;
+}
+
+template <int KIND, int N0, int N1, int N2, bool MK, int NP>
+__global__ void __launch_bounds__(FARB_THREADS, FARB_CTAS)
+    far_plan_kernel(EvalArgs a, BatchPtrs bp)
+{
+    constexpr int NB = NP;
+    constexpr int P_LO = N0 * N1 * N2;
+    constexpr int SS = far_slot_stride<P_LO, NP>();
+    constexpr int CPP = P_LO / 2; // 16-byte chunks of one plane's block
+    constexpr int NH = NB > 1 ? 2 : 1, RH = NB / NH;
+    static_assert(NB % NH == 0, "plane halves");
+    static_assert(FARB_THREADS == 256, "the plan's owner index is a thread of 256");
+    extern __shared__ __align__(16) float2 far_sh[]; // slots; the final reduction reuses it
+    __shared__ FarPlanRec frec[FAR_PLAN_POS];
+    __shared__ float2 fres[NB][FARB_THREADS + 1]; // column FARB_THREADS: padding
+    __shared__ KParams kps[MK ? NB : 1];
+    const int pb = blockIdx.y * NB;
+    if constexpr (MK)
+        if (threadIdx.x < NB)
+            kps[threadIdx.x] = bp.kp_plane[pb + threadIdx.x]; // read after the first barrier
+    const int lane = threadIdx.x & 31;
+    const FarChunk C = bp.fp_chunk[blockIdx.x];
+    const int cnt = C.cnt;
+    const int S = FARB_THREADS / cnt;
+    const int ti = threadIdx.x % cnt, si = threadIdx.x / cnt;
+    const bool active = si < S;
+    const int t = C.t0 + ti;
+    const double y0 = a.tx[t], y1 = a.ty[t], y2 = a.tz[t];
+    double accr[NB], acci[NB];
+#pragma unroll
+    for (int r = 0; r < NB; r++)
+        accr[r] = acci[r] = 0.0;
+    for (long long g = C.g0; g < C.g1; g++)
+    {
+        const FarGroup G = bp.fp_group[g];
+        for (int i = threadIdx.x; i < G.npos; i += FARB_THREADS)
+            cp_async16(&frec[i], bp.fp_rec + G.rec + i);
+        // one warp per slot, lanes over the slot's 16-byte chunks
+        for (int ks = threadIdx.x >> 5; ks < G.nslot; ks += FARB_THREADS / 32)
+        {
+            const int cone = bp.fp_slot[G.slot + ks];
+            const float2* src0 = bp.fcoef + (size_t)pb * bp.fc_plane + (size_t)cone * P_LO;
+            float2* dst0 = far_sh + (size_t)ks * SS;
+#pragma unroll
+            for (int r = 0; r < NB; r++)
+                for (int ch = lane; ch < CPP; ch += 32)
+                    cp_async16(dst0 + r * P_LO + 2 * ch, src0 + (size_t)r * bp.fc_plane + 2 * ch);
+        }
+        // this thread's pair: its box's distance, and a zero value in case
+        // the pair has no record (no cone)
+        const bool mine = active && si < G.nbox;
+        double d2 = 0.0;
+        if (mine)
+        {
+            const int sb = a.far_src[G.box0 + si];
+            const double p0 = y0 - a.T.box_c[3 * sb], p1 = y1 - a.T.box_c[3 * sb + 1],
+                         p2 = y2 - a.T.box_c[3 * sb + 2];
+            d2 = p0 * p0 + p1 * p1 + p2 * p2;
+        }
+#pragma unroll
+        for (int r = 0; r < NB; r++)
+            fres[r][threadIdx.x] = make_float2(0.f, 0.f);
+        cp_async_wait_all();
+        __syncthreads(); // records and blocks staged
+        const int n_two = G.nslotted / 2, n_one = G.npos - G.nslotted;
+        const int n_item = NH * (n_two + n_one);
+        for (int w = threadIdx.x; w < n_item; w += FARB_THREADS)
+        {
+            if (w < NH * n_two)
+            {
+                const int q = w % n_two, r0 = (w / n_two) * RH;
+                const FarPlanRec ra = frec[2 * q], rb = frec[2 * q + 1];
+                const float la[3] = {__int_as_float(ra.l0), __int_as_float(ra.l1),
+                                     __int_as_float(ra.l2)};
+                const float lb[3] = {__int_as_float(rb.l0), __int_as_float(rb.l1),
+                                     __int_as_float(rb.l2)};
+                const int k = (ra.w >> 9) & 31;
+                const int oa = min(ra.w & 511, FARB_THREADS), ob = min(rb.w & 511, FARB_THREADS);
+#pragma unroll
+                for (int rr = 0; rr < RH; rr++)
+                {
+                    cplx<float> va, vb;
+                    ChebF2<N0, N1, N2>::eval(far_sh + (size_t)k * SS + (r0 + rr) * P_LO, la, lb,
+                                             va, vb);
+                    fres[r0 + rr][oa] = make_float2(va.re, va.im);
+                    fres[r0 + rr][ob] = make_float2(vb.re, vb.im);
+                }
+            }
+            else
+            {
+                const int w1 = w - NH * n_two;
+                const int j = w1 % n_one, r0 = (w1 / n_one) * RH;
+                const FarPlanRec rc = frec[G.nslotted + j];
+                const float l3[3] = {__int_as_float(rc.l0), __int_as_float(rc.l1),
+                                     __int_as_float(rc.l2)};
+                const int cone = bp.fp_slot[G.slot + G.nslot + j];
+                const int o = min(rc.w & 511, FARB_THREADS);
+#pragma unroll
+                for (int rr = 0; rr < RH; rr++)
+                {
+                    const cplx<float> v = ChebF<N0, N1, N2>::eval(
+                        bp.fcoef + (size_t)(pb + r0 + rr) * bp.fc_plane + (size_t)cone * P_LO, l3,
+                        a.lo);
+                    fres[r0 + rr][o] = make_float2(v.re, v.im);
+                }
+            }
+        }
+        __syncthreads(); // values of every pair written
+        if (mine)
+        {
+            cplx<float> cf;
+            if constexpr (!MK)
+                cf = cf_mixed<KIND>(d2, a.kp);
+#pragma unroll
+            for (int r = 0; r < NB; r++)
+            {
+                if constexpr (MK)
+                    cf = cf_mixed<KIND>(d2, kps[r]);
+                const float2 v = fres[r][threadIdx.x];
+                accr[r] += (double)(v.x * cf.re - v.y * cf.im);
+                acci[r] += (double)(v.x * cf.im + v.y * cf.re);
+            }
+        }
+        // no barrier: records and slots are not read after the last one, so
+        // the next group's copies overlap these sums, and each thread zeroes
+        // only its own value column
+    }
+    __syncthreads();
+    double* rr = reinterpret_cast<double*>(far_sh);
+    double* ri = rr + NB * FARB_THREADS;
+#pragma unroll
+    for (int r = 0; r < NB; r++)
+    {
+        rr[r * FARB_THREADS + threadIdx.x] = accr[r];
+        ri[r * FARB_THREADS + threadIdx.x] = acci[r];
+    }
+    __syncthreads();
+    if (active && si == 0)
+    {
+        const long long o = a.tgt_perm[t];
+        for (int r = 0; r < NB && pb + r < bp.nrhs; r++)
+        {
+            double sr = 0, sim = 0;
+            for (int s = 0; s < S; s++)
+            {
+                sr += rr[r * FARB_THREADS + ti + s * cnt];
+                sim += ri[r * FARB_THREADS + ti + s * cnt];
+            }
+            const double2 nr = bp.unear[(size_t)(pb + r) * bp.n_tgt + t];
+            sr += nr.x;
+            sim += nr.y;
+            double* out = a.out + (size_t)(pb + r) * bp.out_plane;
+            if (a.real_out)
+                out[o] = sr;
+            else
+            {
+                out[2 * o] = sr;
+                out[2 * o + 1] = sim;
+            }
+        }
+    }
+}

@@ -190,6 +190,38 @@ int launch_mult_kernels(const MultPtrs& m, const void* d_w, void* d_u, bool real
 // `groups` groups of BATCH_NB planes; plane p (group p / BATCH_NB) lives at
 // offset p * plane of each buffer.
 constexpr int BATCH_NB = 4;
+// Far-field plan of the batched mixed matvec (built once per init, used by
+// every batched or multi-wavenumber matvec): the (target, far box) pairs of
+// each target-leaf chunk in groups of S consecutive far boxes (one pair per
+// thread of a 256-thread CTA, thread = target + (box - first box) x targets),
+// each group's distinct fine cones in slots (the 24 with the smallest ids)
+// and its pairs as records in slot order, every slot's run padded to 8.
+struct FarChunk // up to 256 targets of one target leaf
+{
+    long long g0, g1; // its groups
+    int t0, cnt;      // first target (sorted order) and number of targets
+};
+struct FarGroup
+{
+    long long rec;  // first record
+    long long box0; // index of its first far box in the target-leaf far list
+    int slot;       // first slot cone id (then the cone ids of its overflow records)
+    unsigned short npos, nslotted; // records: all, in slots (padded)
+    unsigned short nbox;           // boxes in the group
+    unsigned char nslot;           // slots
+    unsigned char pad_;
+};
+// local coordinates (float bits) and w = owner thread | slot << 9 (slot 31:
+// read from global memory, cone id in the group's overflow list; owner 511:
+// padding)
+struct __align__(16) FarPlanRec
+{
+    int l0, l1, l2, w;
+};
+constexpr int FAR_PLAN_SLOTS = 24;
+constexpr int FAR_PLAN_OVF = 31;
+constexpr int FAR_PLAN_PAD_OWNER = 511;
+
 struct BatchPtrs
 {
     float2* w;      // planes of n_src permuted densities
@@ -212,6 +244,12 @@ struct BatchPtrs
     const int* n_tc_tiles = nullptr;
     const float* tc_fill = nullptr;
     const signed char* up_choice = nullptr; // autotuner's choice for these planes (per level)
+    // far-field plan (null: the far kernel finds cones and slots itself)
+    const FarChunk* fp_chunk = nullptr;
+    int fp_nchunk = 0;
+    const FarGroup* fp_group = nullptr;
+    const FarPlanRec* fp_rec = nullptr;
+    const int* fp_slot = nullptr;
 };
 
 // Enqueues the mixed matvec of bp.nrhs <= bp.groups * BATCH_NB right-hand

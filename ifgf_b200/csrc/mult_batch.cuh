@@ -507,11 +507,22 @@ static int run_mult_batch(const MultPtrs& m, const BatchPtrs& bp, const void* d_
                 IFGF_CHECK(cudaStreamWaitEvent(st, m.ev_join, 0));
             if (hk)
                 hk->begin(PROF_EVAL);
-            constexpr size_t fsm = far_batch_smem<N0, N1, N2, BATCH_NB>();
-            auto fk = far_batch_kernel<KIND, N0, N1, N2, MK, BATCH_NB>;
-            IFGF_CHECK(cudaFuncSetAttribute(fk, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            (int)fsm));
-            fk<<<dim3(m.n_tleaf, bp.groups), FARB_THREADS, fsm, st>>>(ea, bp);
+            if (bp.fp_chunk)
+            {
+                constexpr size_t fsm = far_plan_smem<N0 * N1 * N2, BATCH_NB>();
+                auto fk = far_plan_kernel<KIND, N0, N1, N2, MK, BATCH_NB>;
+                IFGF_CHECK(cudaFuncSetAttribute(fk, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                (int)fsm));
+                fk<<<dim3(bp.fp_nchunk, bp.groups), FARB_THREADS, fsm, st>>>(ea, bp);
+            }
+            else
+            {
+                constexpr size_t fsm = far_batch_smem<N0, N1, N2, BATCH_NB>();
+                auto fk = far_batch_kernel<KIND, N0, N1, N2, MK, BATCH_NB>;
+                IFGF_CHECK(cudaFuncSetAttribute(fk, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                (int)fsm));
+                fk<<<dim3(m.n_tleaf, bp.groups), FARB_THREADS, fsm, st>>>(ea, bp);
+            }
             IFGF_CHECK_LAUNCH();
             if (hk)
                 hk->end();

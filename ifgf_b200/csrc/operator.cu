@@ -63,6 +63,14 @@ struct DeviceState
     std::vector<double> A_host; // host copy of A
     DevBuf<int> tl_first, tl_last, tl_far_src, tl_near_src;
     DevBuf<long long> tl_far_off, tl_near_off;
+    // far-field plan of the batched mixed matvec (built on first use)
+    DevBuf<FarChunk> fp_chunk;
+    DevBuf<FarGroup> fp_group;
+    DevBuf<FarPlanRec> fp_rec;
+    DevBuf<int> fp_slot;
+    int fp_nchunk = 0;
+    bool fp_ready = false;
+    double fp_ms = 0;
     DevBuf<double2> w, cvals, fcoef, unear;
     // planes of the batched mixed matvec, allocated on first use for
     // b_planes planes of the plane sizes recorded beside them
@@ -166,6 +174,213 @@ __global__ void mark_far_kernel(LevelGeom G, TreeArgs T, const int* __restrict__
             fmark[G.fmap_off + lb * nf + fe] = 1;
         if (ce >= 0)
             cmark[lb * nc + ce] = 1;
+    }
+}
+
+// Far-field plan (FarChunk / FarGroup / FarPlanRec, mult.hpp): one CTA per
+// chunk of up to 256 targets of a target leaf, thread (ti, si) = target ti,
+// far box si of each group of S = 256 / targets consecutive boxes of the
+// leaf's far list (evaluateFromInterp's pairs, ifgfoperator.hpp:1736-1891).
+// Per group: the fine cone and local coordinates of every pair (the lookup
+// of the far kernels), the distinct cones in a hash table of twice the pairs
+// (never full, so every cone is in it), slots for the FAR_PLAN_SLOTS
+// smallest cone ids, and the records in slot order, each slot's run padded
+// to 8 positions; pairs of the other cones go last, with their cone ids
+// after the group's slot list.  Every count depends only on the set of cones
+// of the group, not on the order of the atomics, so the two passes agree:
+// FILL = false counts the groups, records and slot-list entries of every
+// chunk; FILL = true writes them at the offsets the counts gave and reports
+// its own totals, which the host compares.
+struct FarBuildArgs
+{
+    const LevelGeom* lv;
+    int L;
+    const double* box_c;
+    const double* box_H;
+    const int* box_level;
+    const double *tx, *ty, *tz;
+    const int* fmap;
+    const long long* far_off;
+    const int* far_src;
+    const int* c_leaf;
+    const int* c_t0;
+    const int* c_cnt;
+    unsigned long long* err;
+    long long *n_group, *n_rec, *n_slot;             // counting pass
+    const long long *g_off, *rec_off, *slot_off;     // filling pass
+    FarGroup* group;
+    FarPlanRec* rec;
+    int* slot;
+};
+
+template <bool FILL>
+__global__ void __launch_bounds__(256) far_plan_build_kernel(FarBuildArgs b)
+{
+    constexpr int T = 256, NS = FAR_PLAN_SLOTS, H = 2 * T, NBOX = 128;
+    __shared__ int hkey[H], hcnt[H], hrank[H];
+    __shared__ int klist[T], kent[T]; // distinct cones, their table entries
+    __shared__ int sgf[NS], scnt[NS];
+    __shared__ int ndist, novf;
+    __shared__ double fcx[NBOX], fcy[NBOX], fcz[NBOX], fH[NBOX];
+    __shared__ long long ffm[NBOX];
+    __shared__ int flev[NBOX];
+    __shared__ LookupF lfs[MAX_LEVELS];
+    const int c = blockIdx.x;
+    const int tl = b.c_leaf[c], t0 = b.c_t0[c], cnt = b.c_cnt[c];
+    const int S = T / cnt, ti = threadIdx.x % cnt, si = threadIdx.x / cnt;
+    const bool active = si < S;
+    const int lane = threadIdx.x & 31;
+    for (int l = threadIdx.x; l < b.L; l += T)
+        make_lookupf(b.lv[l], lfs[l]);
+    for (int e = threadIdx.x; e < H; e += T)
+    {
+        hkey[e] = -1;
+        hcnt[e] = 0;
+    }
+    if (threadIdx.x == 0)
+        ndist = novf = 0;
+    const double y0 = b.tx[t0 + ti], y1 = b.ty[t0 + ti], y2 = b.tz[t0 + ti];
+    const long long fb0 = b.far_off[tl], fb1 = b.far_off[tl + 1];
+    long long gi = FILL ? b.g_off[c] : 0, ri = FILL ? b.rec_off[c] : 0,
+              sl = FILL ? b.slot_off[c] : 0;
+    for (long long e0 = fb0; e0 < fb1; e0 += NBOX)
+    {
+        const int fcnt = (int)min((long long)NBOX, fb1 - e0);
+        __syncthreads();
+        if (threadIdx.x < fcnt)
+        {
+            const int sb = b.far_src[e0 + threadIdx.x];
+            const int lev = b.box_level[sb];
+            const LevelGeom& G = b.lv[lev];
+            const long long nft = (long long)G.nf[0] * G.nf[1] * G.nf[2];
+            fcx[threadIdx.x] = b.box_c[3 * sb];
+            fcy[threadIdx.x] = b.box_c[3 * sb + 1];
+            fcz[threadIdx.x] = b.box_c[3 * sb + 2];
+            fH[threadIdx.x] = b.box_H[sb];
+            ffm[threadIdx.x] = G.fmap_off + (long long)(sb - G.box_off) * nft;
+            flev[threadIdx.x] = lev;
+        }
+        __syncthreads();
+        for (int c0 = 0; c0 < fcnt; c0 += S)
+        {
+            const int i = c0 + si;
+            int gf = -1;
+            float loc[3] = {0.f, 0.f, 0.f};
+            if (active && i < fcnt)
+            {
+                const int lev = flev[i];
+                const double p[3] = {y0 - fcx[i], y1 - fcy[i], y2 - fcz[i]};
+                gf = fine_lookup_fast(lfs[lev], b.lv[lev], b.fmap + ffm[i], p, fH[i], loc, b.err);
+            }
+            int h = -1, rank = 0;
+            if (gf >= 0)
+            {
+                int hh = (int)(((unsigned)gf * 2654435761u) >> 23) & (H - 1);
+                for (int q = 0; q < H; q++, hh = (hh + 1) & (H - 1))
+                {
+                    const int prev = atomicCAS(&hkey[hh], -1, gf);
+                    if (prev == -1)
+                    {
+                        const int id = atomicAdd(&ndist, 1);
+                        klist[id] = gf;
+                        kent[id] = hh;
+                    }
+                    if (prev == -1 || prev == gf)
+                    {
+                        h = hh;
+                        break;
+                    }
+                }
+                rank = atomicAdd(&hcnt[h], 1); // the table has room for every pair
+            }
+            __syncthreads(); // table, cone list and counts complete
+            const int nd = ndist;
+            if (threadIdx.x < nd)
+            {
+                const int key = klist[threadIdx.x];
+                int r = 0;
+                for (int u = 0; u < nd; u++)
+                    r += klist[u] < key ? 1 : 0;
+                hrank[kent[threadIdx.x]] = r;
+                if (r < NS)
+                {
+                    sgf[r] = key;
+                    scnt[r] = hcnt[kent[threadIdx.x]];
+                }
+            }
+            __syncthreads(); // slot order complete
+            const int ns = min(nd, NS);
+            const int ck = lane < ns ? scnt[lane] : 0;
+            const int pk = (ck + 7) & ~7;
+            int incl = pk;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1)
+            {
+                const int v = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o)
+                    incl += v;
+            }
+            const int slotted = __shfl_sync(0xffffffffu, incl, 31);
+            const int k = h >= 0 ? hrank[h] : -1;
+            const bool in_slot = k >= 0 && k < NS;
+            const int src = in_slot ? k : 0;
+            const int kbase = __shfl_sync(0xffffffffu, incl - pk, src);
+            const int kcnt = __shfl_sync(0xffffffffu, ck, src);
+            const int kend = __shfl_sync(0xffffffffu, incl, src);
+            int pos = -1;
+            if (gf >= 0)
+                pos = in_slot ? kbase + rank : slotted + atomicAdd(&novf, 1);
+            __syncthreads(); // overflow count complete
+            const int nov = novf;
+            if (FILL)
+            {
+                if (gf >= 0)
+                {
+                    b.rec[ri + pos] =
+                        FarPlanRec{__float_as_int(loc[0]), __float_as_int(loc[1]),
+                                   __float_as_int(loc[2]),
+                                   (int)threadIdx.x | ((in_slot ? k : FAR_PLAN_OVF) << 9)};
+                    if (in_slot && rank == kcnt - 1)
+                        for (int q = kbase + kcnt; q < kend; q++)
+                            b.rec[ri + q] = FarPlanRec{0, 0, 0, FAR_PLAN_PAD_OWNER | (k << 9)};
+                    if (!in_slot)
+                        b.slot[sl + ns + (pos - slotted)] = gf;
+                }
+                if (threadIdx.x < ns)
+                    b.slot[sl + threadIdx.x] = sgf[threadIdx.x];
+                if (threadIdx.x == 0)
+                {
+                    FarGroup G;
+                    G.rec = ri;
+                    G.box0 = e0 + c0;
+                    G.slot = (int)sl;
+                    G.npos = (unsigned short)(slotted + nov);
+                    G.nslotted = (unsigned short)slotted;
+                    G.nbox = (unsigned short)min(S, fcnt - c0);
+                    G.nslot = (unsigned char)ns;
+                    G.pad_ = 0;
+                    b.group[gi] = G;
+                }
+            }
+            gi++;
+            ri += slotted + nov;
+            sl += ns + nov;
+            __syncthreads(); // the table is read no more: clear it
+            for (int e = threadIdx.x; e < H; e += T)
+            {
+                hkey[e] = -1;
+                hcnt[e] = 0;
+            }
+            if (threadIdx.x == 0)
+                ndist = novf = 0;
+            __syncthreads();
+        }
+    }
+    if (threadIdx.x == 0) // FILL: the end offsets, which the host checks
+    {
+        b.n_group[c] = gi;
+        b.n_rec[c] = ri;
+        b.n_slot[c] = sl;
     }
 }
 
@@ -987,6 +1202,13 @@ void Operator::setup_device(const double* normals)
     phase("boxes_points_upload");
     build_target_lists_gpu(plan_, shard_n_ > 1 ? shard_rank_ : -1, D.tl_far_off, D.tl_far_src,
                            D.tl_near_off, D.tl_near_src);
+    // the far-field plan of earlier tables is stale: rebuilt on first use
+    D.fp_chunk.release();
+    D.fp_group.release();
+    D.fp_rec.release();
+    D.fp_slot.release();
+    D.fp_nchunk = 0;
+    D.fp_ready = false;
     phase("target_leaf_lists");
     // ---- active cones (octree.hpp:351-816) on the GPU ----
     int64_t fmap_total = 0;
@@ -1442,6 +1664,142 @@ void Operator::ensure_tc_tiles(int planes)
 
 // The tensor-core tiles for a batch launch over bp.groups * BATCH_NB planes,
 // and (single-wavenumber batches) the autotuner's choice for them.
+void Operator::set_far_plan(bool on)
+{
+    far_plan_on_ = on;
+    if (!on && dev_)
+    {
+        DeviceState& D = *dev_;
+        D.fp_chunk.release();
+        D.fp_group.release();
+        D.fp_rec.release();
+        D.fp_slot.release();
+        D.fp_nchunk = 0;
+        D.fp_ready = false;
+    }
+}
+
+void Operator::ensure_far_plan()
+{
+    DeviceState& D = *dev_;
+    if (D.fp_ready || !far_plan_on_ || D.n_tleaf == 0)
+        return;
+    const auto t0 = std::chrono::steady_clock::now();
+    IFGF_CUDA(cudaSetDevice(device_));
+    // chunks of up to 256 targets of every target leaf
+    const std::vector<int> tf = D.tl_first.download(), tlast = D.tl_last.download();
+    std::vector<int> c_leaf, c_t0, c_cnt;
+    for (int i = 0; i < D.n_tleaf; i++)
+        for (int t = tf[i]; t < tlast[i]; t += 256)
+        {
+            c_leaf.push_back(i);
+            c_t0.push_back(t);
+            c_cnt.push_back(std::min(256, tlast[i] - t));
+        }
+    const int nc = (int)c_leaf.size();
+    if (nc == 0)
+        return;
+    DevBuf<int> d_leaf, d_t0, d_cnt;
+    d_leaf.upload(c_leaf);
+    d_t0.upload(c_t0);
+    d_cnt.upload(c_cnt);
+    DevBuf<long long> n_group, n_rec, n_slot;
+    n_group.alloc(nc);
+    n_rec.alloc(nc);
+    n_slot.alloc(nc);
+    FarBuildArgs b{};
+    b.lv = D.lv.p;
+    b.L = (int)lv_.size();
+    b.box_c = D.box_c.p;
+    b.box_H = D.box_H.p;
+    b.box_level = D.box_level.p;
+    b.tx = D.tx.p;
+    b.ty = D.ty.p;
+    b.tz = D.tz.p;
+    b.fmap = D.fmap.p;
+    b.far_off = D.tl_far_off.p;
+    b.far_src = D.tl_far_src.p;
+    b.c_leaf = d_leaf.p;
+    b.c_t0 = d_t0.p;
+    b.c_cnt = d_cnt.p;
+    b.err = D.err.p;
+    b.n_group = n_group.p;
+    b.n_rec = n_rec.p;
+    b.n_slot = n_slot.p;
+    far_plan_build_kernel<false><<<nc, 256>>>(b);
+    IFGF_CUDA(cudaGetLastError());
+    IFGF_CUDA(cudaDeviceSynchronize());
+    const std::vector<long long> hg = n_group.download(), hr = n_rec.download(),
+                                 hs = n_slot.download();
+    std::vector<long long> g_off(nc), r_off(nc), s_off(nc);
+    long long tg = 0, tr = 0, ts = 0;
+    std::vector<FarChunk> chunks(nc);
+    for (int c = 0; c < nc; c++)
+    {
+        g_off[c] = tg;
+        r_off[c] = tr;
+        s_off[c] = ts;
+        chunks[c] = FarChunk{tg, tg + hg[c], c_t0[c], c_cnt[c]};
+        tg += hg[c];
+        tr += hr[c];
+        ts += hs[c];
+    }
+    if (ts > (1ll << 31) - 1)
+        throw Error(ERR_OOM, "far-field plan: slot list exceeds 2^31 entries");
+    D.fp_group.alloc(std::max(tg, 1ll));
+    D.fp_rec.alloc(std::max(tr, 1ll));
+    D.fp_slot.alloc(std::max(ts, 1ll));
+    D.fp_chunk.upload(chunks);
+    DevBuf<long long> dg, dr, ds;
+    dg.upload(g_off);
+    dr.upload(r_off);
+    ds.upload(s_off);
+    b.g_off = dg.p;
+    b.rec_off = dr.p;
+    b.slot_off = ds.p;
+    b.group = D.fp_group.p;
+    b.rec = D.fp_rec.p;
+    b.slot = D.fp_slot.p;
+    far_plan_build_kernel<true><<<nc, 256>>>(b);
+    IFGF_CUDA(cudaGetLastError());
+    IFGF_CUDA(cudaDeviceSynchronize());
+    {
+        // every chunk must end where the next one starts
+        const std::vector<long long> eg = n_group.download(), er = n_rec.download(),
+                                     es = n_slot.download();
+        for (int c = 0; c < nc; c++)
+            if (eg[c] != g_off[c] + hg[c] || er[c] != r_off[c] + hr[c] || es[c] != s_off[c] + hs[c])
+            {
+                D.fp_chunk.release();
+                D.fp_group.release();
+                D.fp_rec.release();
+                D.fp_slot.release();
+                throw Error(ERR_STATE, "far-field plan: the filling pass disagrees with the "
+                                       "counting pass");
+            }
+    }
+    D.fp_nchunk = nc;
+    D.fp_ready = true;
+    D.fp_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0)
+                  .count();
+}
+
+void Operator::set_batch_far(BatchPtrs& bp)
+{
+    DeviceState& D = *dev_;
+    ensure_far_plan();
+    if (!D.fp_ready)
+    {
+        bp.fp_chunk = nullptr;
+        return;
+    }
+    bp.fp_chunk = D.fp_chunk.p;
+    bp.fp_nchunk = D.fp_nchunk;
+    bp.fp_group = D.fp_group.p;
+    bp.fp_rec = D.fp_rec.p;
+    bp.fp_slot = D.fp_slot.p;
+}
+
 void Operator::set_batch_tc(BatchPtrs& bp, void* stream)
 {
     DeviceState& D = *dev_;
@@ -1953,6 +2311,7 @@ void Operator::mult_batch_device(const void* d_w, void* d_u, int64_t batch, void
     {
         const int planes = ensure_batch_planes(batch);
         BatchPtrs bp = batch_ptrs(in_plane, out_plane);
+        set_batch_far(bp);
         MultPtrs m;
         fill_mult_ptrs(m);
         cudaStream_t st = (cudaStream_t)stream;
@@ -2147,6 +2506,7 @@ void Operator::mult_wavenumbers_device(const double* k, int64_t nk, const void* 
     }
     BatchPtrs bp = batch_ptrs(in_plane, out_plane);
     bp.dgeo32 = D.dgeo32_ptr.data();
+    set_batch_far(bp);
     MultPtrs m;
     fill_mult_ptrs(m);
     int64_t done = 0;
@@ -2394,7 +2754,14 @@ std::string Operator::stats_json() const
       << ",\"init_device_ms\":" << device_ms_ << ",\"init_device_phases_ms\":{";
     for (size_t i = 0; i < dev_phases_.size(); i++)
         o << (i ? "," : "") << "\"" << dev_phases_[i].first << "\":" << dev_phases_[i].second;
-    o << "},\"upward_path\":" << up_path_ << ",\"upward_tuner\":{";
+    o << "},\"far_plan\":{\"on\":" << (far_plan_on_ ? 1 : 0) << ",\"built\":"
+      << (dev_->fp_ready ? 1 : 0) << ",\"chunks\":" << dev_->fp_nchunk
+      << ",\"groups\":" << dev_->fp_group.n << ",\"records\":" << dev_->fp_rec.n
+      << ",\"slot_entries\":" << dev_->fp_slot.n << ",\"bytes\":"
+      << (dev_->fp_group.n * sizeof(FarGroup) + dev_->fp_rec.n * sizeof(FarPlanRec) +
+          dev_->fp_slot.n * sizeof(int) + dev_->fp_chunk.n * sizeof(FarChunk))
+      << ",\"build_ms\":" << dev_->fp_ms << "}";
+    o << ",\"upward_path\":" << up_path_ << ",\"upward_tuner\":{";
     {
         bool first = true;
         for (const auto& kv : dev_->up_choice)

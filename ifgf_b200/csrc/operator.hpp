@@ -102,6 +102,8 @@ class Operator
     void set_profiling(bool on);
     // upward-transfer kernel: UP_AUTO, UP_FFMA or UP_TENSOR (mult.hpp)
     void set_upward_path(int path);
+    void set_far_plan(bool on);
+    bool far_plan() const { return far_plan_on_; }
     int upward_path() const { return up_path_; }
     // throws IFGF_ERR_TIMEOUT when a tensor-core kernel's bounded wait gave up
     void check_device_status();
@@ -130,6 +132,11 @@ class Operator
     void ensure_distance_tables();
     void ensure_tc_tiles(int planes);
     void set_batch_tc(BatchPtrs& bp, void* stream);
+    // far-field plan of the batched mixed matvec: built on first use (once
+    // per init), handed to the far kernel through bp; off: the far kernel
+    // finds its cones itself (no plan memory)
+    void ensure_far_plan();
+    void set_batch_far(BatchPtrs& bp);
     void ensure_upward_tuned(int planes, const BatchPtrs* bp, void* stream);
     void setup_device(const double* normals);
     // vkind >= 0: run that kernel with the variant geometry tables
@@ -151,6 +158,7 @@ class Operator
     int precision_ = PREC_FP64;
     int device_ = -1; // CUDA device of the device tables (set by init)
     int up_path_ = 0; // UpwardPath
+    bool far_plan_on_ = true;
     bool initialized_ = false;
     bool planned_ = false;
     Plan plan_;

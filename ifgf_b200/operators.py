@@ -129,9 +129,16 @@ class IfgfOperator:
 
     def set_upward_path(self, path):
         """Kernel of the mixed-precision upward transfer: "auto" (default;
-        tensor cores on levels with well-filled tiles), "ffma" or "tensor"."""
+        per level the faster of the two, timed on this operator), "ffma" or
+        "tensor"."""
         p = {"auto": 0, "ffma": 1, "tensor": 2}.get(path, path)
         check(lib.ifgf_set_upward_path(self._h, int(p)))
+
+    def set_far_plan(self, enable):
+        """Far-field plan of the batched mixed matvecs: the far pairs' cone
+        lookups done once and stored sorted by cone (default on; off frees
+        its memory and looks the cones up in every matvec)."""
+        check(lib.ifgf_set_far_plan(self._h, 1 if enable else 0))
 
     # -- matvec -------------------------------------------------------------
     def _dtype(self):

@@ -99,6 +99,18 @@ int ifgf_set_precision(ifgf_operator* op, int mode);
  * reference counterpart. */
 int ifgf_set_upward_path(ifgf_operator* op, int path);
 
+/* Far-field plan of the batched and multi-wavenumber mixed matvecs
+ * (enable = 1, the default): on their first call the (target, far box) pairs
+ * of every target leaf are looked up once -- fine cone, local coordinates --
+ * and stored grouped and sorted by cone (a 16-byte record per pair plus
+ * padding, about 19 bytes per pair in all: 7.2 GB at N = 1e6, k = 100, p = 9;
+ * the size is in ifgf_stats_json, "far_plan"),
+ * so that every later matvec skips the lookups (evaluateFromInterp,
+ * ifgfoperator.hpp:1736-1891, done as a lookup pass at setup and a sum pass
+ * per matvec).  enable = 0 frees the plan and the far kernel looks the cones
+ * up in every matvec (same results).  No reference counterpart. */
+int ifgf_set_far_plan(ifgf_operator* op, int enable);
+
 /* Diagnostic of the bounded waits the tensor-core kernels use: launches a
  * one-block kernel that waits, for at most limit_ms milliseconds, on a
  * barrier that nothing arrives at.  Returns IFGF_ERR_TIMEOUT (the wait gave
