@@ -442,16 +442,17 @@ __global__ void __launch_bounds__(FARB_THREADS, FARB_CTAS)
 // slot per work item, as in far_batch_kernel), one barrier, the owners'
 // factors and FP64 sums in box order, overlapping the next group's copies.  One CTA per chunk of up to 256
 // targets of a leaf and per group of NP planes.
-constexpr int FAR_PLAN_POS = (FARB_THREADS + (FAR_PAD - 1) * FAR_PLAN_SLOTS + 7) / 8 * 8;
-template <int P_LO, int NP> __host__ __device__ constexpr size_t far_plan_smem()
+static_assert(FAR_PLAN_THREADS == FARB_THREADS && FAR_PLAN_PAD == FAR_PAD,
+              "the plan's layout is the far kernels'");
+template <int P_LO, int NP, int NSL> __host__ __device__ constexpr size_t far_plan_smem()
 {
-    const size_t slots = (size_t)FAR_PLAN_SLOTS * far_slot_stride<P_LO, NP>() * 8;
+    const size_t slots = (size_t)NSL * far_slot_stride<P_LO, NP>() * 8;
     const size_t red = 2 * NP * FARB_THREADS * sizeof(double); // final reduction
     return slots > red ? slots : red;
 }
 
-template <int KIND, int N0, int N1, int N2, bool MK, int NP>
-__global__ void __launch_bounds__(FARB_THREADS, FARB_CTAS)
+template <int KIND, int N0, int N1, int N2, bool MK, int NP, int NSL>
+__global__ void __launch_bounds__(FARB_THREADS, far_plan_ctas(NSL, N0 * N1 * N2, NP))
     far_plan_kernel(EvalArgs a, BatchPtrs bp)
 {
     constexpr int NB = NP;
@@ -462,7 +463,7 @@ __global__ void __launch_bounds__(FARB_THREADS, FARB_CTAS)
     static_assert(NB % NH == 0, "plane halves");
     static_assert(FARB_THREADS == 256, "the plan's owner index is a thread of 256");
     extern __shared__ __align__(16) float2 far_sh[]; // slots; the final reduction reuses it
-    __shared__ FarPlanRec frec[FAR_PLAN_POS];
+    __shared__ FarPlanRec frec[far_plan_pos(NSL)];
     __shared__ float2 fres[NB][FARB_THREADS + 1]; // column FARB_THREADS: padding
     __shared__ KParams kps[MK ? NB : 1];
     const int pb = blockIdx.y * NB;

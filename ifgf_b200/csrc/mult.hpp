@@ -218,7 +218,36 @@ struct __align__(16) FarPlanRec
 {
     int l0, l1, l2, w;
 };
+// slots per group of a plan: FAR_PLAN_SLOTS, or FAR_PLAN_SLOTS_FEW where
+// the fewer slots let more far CTAs reside per SM and at most 10 % of the
+// records then read global memory
 constexpr int FAR_PLAN_SLOTS = 24;
+constexpr int FAR_PLAN_SLOTS_FEW = 16;
+constexpr int FAR_PLAN_THREADS = 256, FAR_PLAN_PAD = 8;
+// record positions of a group with nsl slots (each slot's run padded)
+__host__ __device__ constexpr int far_plan_pos(int nsl)
+{
+    return (FAR_PLAN_THREADS + (FAR_PLAN_PAD - 1) * nsl + 7) / 8 * 8;
+}
+// float2 per shared-memory slot of np planes of p_lo coefficients, padded
+// to start 16 bytes apart modulo 128
+__host__ __device__ constexpr int far_slot_stride_rt(int p_lo, int np)
+{
+    int s = np * p_lo;
+    while ((s * 8) % 128 != 16 && (s * 8) % 128 != 80)
+        s++;
+    return s;
+}
+// resident CTAs per SM of the plan's far kernel with nsl slots: as many as
+// its shared memory allows (slots, records, values, factors, 1 KB reserved
+// per CTA), at most three (80 registers a thread; two get 128)
+__host__ __device__ constexpr int far_plan_ctas(int nsl, int p_lo, int np)
+{
+    const int bytes = nsl * far_slot_stride_rt(p_lo, np) * 8 + far_plan_pos(nsl) * 16 +
+                      np * (FAR_PLAN_THREADS + 1) * 8 + np * (int)sizeof(KParams) + 1024 + 512;
+    const int n = 233472 / bytes;
+    return n < 1 ? 1 : (n > 3 ? 3 : n);
+}
 constexpr int FAR_PLAN_OVF = 31;
 constexpr int FAR_PLAN_PAD_OWNER = 511;
 
@@ -247,6 +276,7 @@ struct BatchPtrs
     // far-field plan (null: the far kernel finds cones and slots itself)
     const FarChunk* fp_chunk = nullptr;
     int fp_nchunk = 0;
+    int fp_nslot = 0; // slots per group the plan was built for
     const FarGroup* fp_group = nullptr;
     const FarPlanRec* fp_rec = nullptr;
     const int* fp_slot = nullptr;

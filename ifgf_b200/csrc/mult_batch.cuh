@@ -509,11 +509,19 @@ static int run_mult_batch(const MultPtrs& m, const BatchPtrs& bp, const void* d_
                 hk->begin(PROF_EVAL);
             if (bp.fp_chunk)
             {
-                constexpr size_t fsm = far_plan_smem<N0 * N1 * N2, BATCH_NB>();
-                auto fk = far_plan_kernel<KIND, N0, N1, N2, MK, BATCH_NB>;
-                IFGF_CHECK(cudaFuncSetAttribute(fk, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                (int)fsm));
-                fk<<<dim3(bp.fp_nchunk, bp.groups), FARB_THREADS, fsm, st>>>(ea, bp);
+                auto launch_plan = [&](auto nsl) {
+                    constexpr int NSL = decltype(nsl)::value;
+                    constexpr size_t fsm = far_plan_smem<N0 * N1 * N2, BATCH_NB, NSL>();
+                    auto fk = far_plan_kernel<KIND, N0, N1, N2, MK, BATCH_NB, NSL>;
+                    IFGF_CHECK(cudaFuncSetAttribute(
+                        fk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsm));
+                    fk<<<dim3(bp.fp_nchunk, bp.groups), FARB_THREADS, fsm, st>>>(ea, bp);
+                    return cudaSuccess;
+                };
+                if (bp.fp_nslot <= FAR_PLAN_SLOTS_FEW)
+                    IFGF_CHECK(launch_plan(std::integral_constant<int, FAR_PLAN_SLOTS_FEW>{}));
+                else
+                    IFGF_CHECK(launch_plan(std::integral_constant<int, FAR_PLAN_SLOTS>{}));
             }
             else
             {

@@ -69,6 +69,8 @@ struct DeviceState
     DevBuf<FarPlanRec> fp_rec;
     DevBuf<int> fp_slot;
     int fp_nchunk = 0;
+    int fp_nslot = 0;
+    double fp_ovf_few = 0; // share of the records beyond FAR_PLAN_SLOTS_FEW slots
     bool fp_ready = false;
     double fp_ms = 0;
     DevBuf<double2> w, cvals, fcoef, unear;
@@ -183,14 +185,15 @@ __global__ void mark_far_kernel(LevelGeom G, TreeArgs T, const int* __restrict__
 // leaf's far list (evaluateFromInterp's pairs, ifgfoperator.hpp:1736-1891).
 // Per group: the fine cone and local coordinates of every pair (the lookup
 // of the far kernels), the distinct cones in a hash table of twice the pairs
-// (never full, so every cone is in it), slots for the FAR_PLAN_SLOTS
-// smallest cone ids, and the records in slot order, each slot's run padded
+// (never full, so every cone is in it), slots for the nslot smallest cone
+// ids, and the records in slot order, each slot's run padded
 // to 8 positions; pairs of the other cones go last, with their cone ids
 // after the group's slot list.  Every count depends only on the set of cones
 // of the group, not on the order of the atomics, so the two passes agree:
 // FILL = false counts the groups, records and slot-list entries of every
-// chunk; FILL = true writes them at the offsets the counts gave and reports
-// its own totals, which the host compares.
+// chunk (and the pairs beyond the slots, which read global memory); FILL =
+// true writes them at the offsets the counts gave and reports its own
+// totals, which the host compares.
 struct FarBuildArgs
 {
     const LevelGeom* lv;
@@ -206,7 +209,8 @@ struct FarBuildArgs
     const int* c_t0;
     const int* c_cnt;
     unsigned long long* err;
-    long long *n_group, *n_rec, *n_slot;             // counting pass
+    int nslot; // slots per group, <= FAR_PLAN_SLOTS
+    long long *n_group, *n_rec, *n_slot, *n_ovf;             // counting pass
     const long long *g_off, *rec_off, *slot_off;     // filling pass
     FarGroup* group;
     FarPlanRec* rec;
@@ -216,10 +220,11 @@ struct FarBuildArgs
 template <bool FILL>
 __global__ void __launch_bounds__(256) far_plan_build_kernel(FarBuildArgs b)
 {
-    constexpr int T = 256, NS = FAR_PLAN_SLOTS, H = 2 * T, NBOX = 128;
+    constexpr int T = 256, H = 2 * T, NBOX = 128;
+    const int NS = b.nslot;
     __shared__ int hkey[H], hcnt[H], hrank[H];
     __shared__ int klist[T], kent[T]; // distinct cones, their table entries
-    __shared__ int sgf[NS], scnt[NS];
+    __shared__ int sgf[FAR_PLAN_SLOTS], scnt[FAR_PLAN_SLOTS];
     __shared__ int ndist, novf;
     __shared__ double fcx[NBOX], fcy[NBOX], fcz[NBOX], fH[NBOX];
     __shared__ long long ffm[NBOX];
@@ -243,6 +248,7 @@ __global__ void __launch_bounds__(256) far_plan_build_kernel(FarBuildArgs b)
     const long long fb0 = b.far_off[tl], fb1 = b.far_off[tl + 1];
     long long gi = FILL ? b.g_off[c] : 0, ri = FILL ? b.rec_off[c] : 0,
               sl = FILL ? b.slot_off[c] : 0;
+    long long ovf = 0; // pairs beyond the slots
     for (long long e0 = fb0; e0 < fb1; e0 += NBOX)
     {
         const int fcnt = (int)min((long long)NBOX, fb1 - e0);
@@ -365,6 +371,7 @@ __global__ void __launch_bounds__(256) far_plan_build_kernel(FarBuildArgs b)
             gi++;
             ri += slotted + nov;
             sl += ns + nov;
+            ovf += nov;
             __syncthreads(); // the table is read no more: clear it
             for (int e = threadIdx.x; e < H; e += T)
             {
@@ -381,6 +388,7 @@ __global__ void __launch_bounds__(256) far_plan_build_kernel(FarBuildArgs b)
         b.n_group[c] = gi;
         b.n_rec[c] = ri;
         b.n_slot[c] = sl;
+        b.n_ovf[c] = ovf;
     }
 }
 
@@ -1703,10 +1711,11 @@ void Operator::ensure_far_plan()
     d_leaf.upload(c_leaf);
     d_t0.upload(c_t0);
     d_cnt.upload(c_cnt);
-    DevBuf<long long> n_group, n_rec, n_slot;
+    DevBuf<long long> n_group, n_rec, n_slot, n_ovf;
     n_group.alloc(nc);
     n_rec.alloc(nc);
     n_slot.alloc(nc);
+    n_ovf.alloc(nc);
     FarBuildArgs b{};
     b.lv = D.lv.p;
     b.L = (int)lv_.size();
@@ -1726,9 +1735,33 @@ void Operator::ensure_far_plan()
     b.n_group = n_group.p;
     b.n_rec = n_rec.p;
     b.n_slot = n_slot.p;
-    far_plan_build_kernel<false><<<nc, 256>>>(b);
-    IFGF_CUDA(cudaGetLastError());
-    IFGF_CUDA(cudaDeviceSynchronize());
+    b.n_ovf = n_ovf.p;
+    // the smaller slot count where it lets more far CTAs reside per SM and at
+    // most 10 % of the records would overflow it and read global memory
+    // (measured at p = 9: 16 slots and three CTAs 4.5 % faster at N = 1e6,
+    // k = 100, with 4.6 % overflowing; 10 % slower at N = 2e5 with 15.7 %)
+    auto count = [&](int nslot) {
+        b.nslot = nslot;
+        far_plan_build_kernel<false><<<nc, 256>>>(b);
+        IFGF_CUDA(cudaGetLastError());
+        IFGF_CUDA(cudaDeviceSynchronize());
+    };
+    count(FAR_PLAN_SLOTS_FEW);
+    {
+        const std::vector<long long> ho = n_ovf.download(), hr0 = n_rec.download();
+        long long o = 0, r = 0;
+        for (int c = 0; c < nc; c++)
+        {
+            o += ho[c];
+            r += hr0[c];
+        }
+        D.fp_ovf_few = r > 0 ? (double)o / (double)r : 0.0;
+        const int p_lo = lo_[0] * lo_[1] * lo_[2];
+        const bool more_ctas = far_plan_ctas(FAR_PLAN_SLOTS_FEW, p_lo, BATCH_NB) >
+                               far_plan_ctas(FAR_PLAN_SLOTS, p_lo, BATCH_NB);
+        if (!more_ctas || o * 10 > r)
+            count(FAR_PLAN_SLOTS);
+    }
     const std::vector<long long> hg = n_group.download(), hr = n_rec.download(),
                                  hs = n_slot.download();
     std::vector<long long> g_off(nc), r_off(nc), s_off(nc);
@@ -1779,6 +1812,7 @@ void Operator::ensure_far_plan()
             }
     }
     D.fp_nchunk = nc;
+    D.fp_nslot = b.nslot;
     D.fp_ready = true;
     D.fp_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0)
                   .count();
@@ -1795,6 +1829,7 @@ void Operator::set_batch_far(BatchPtrs& bp)
     }
     bp.fp_chunk = D.fp_chunk.p;
     bp.fp_nchunk = D.fp_nchunk;
+    bp.fp_nslot = D.fp_nslot;
     bp.fp_group = D.fp_group.p;
     bp.fp_rec = D.fp_rec.p;
     bp.fp_slot = D.fp_slot.p;
@@ -2760,7 +2795,7 @@ std::string Operator::stats_json() const
       << ",\"slot_entries\":" << dev_->fp_slot.n << ",\"bytes\":"
       << (dev_->fp_group.n * sizeof(FarGroup) + dev_->fp_rec.n * sizeof(FarPlanRec) +
           dev_->fp_slot.n * sizeof(int) + dev_->fp_chunk.n * sizeof(FarChunk))
-      << ",\"build_ms\":" << dev_->fp_ms << "}";
+      << ",\"slots_per_group\":" << dev_->fp_nslot << ",\"overflow_share_at_few_slots\":" << dev_->fp_ovf_few << ",\"build_ms\":" << dev_->fp_ms << "}";
     o << ",\"upward_path\":" << up_path_ << ",\"upward_tuner\":{";
     {
         bool first = true;
