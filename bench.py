@@ -54,10 +54,13 @@ TOL = 1e-4
 REF_BUDGET_S = 100.0
 # DRAM bytes per unit and right-hand side of the dominant kernels (see the
 # roofline section): upward FFMA / tensor-core kernels per padded
-# geometry-table entry, far field per (target, far box) pair
-UPWARD_FFMA_DRAM_B = 18.9
-UPWARD_TC_DRAM_B = 18.9
-FAR_DRAM_B = 53.0
+# geometry-table entry over the levels each runs at this workload, far field
+# per (target, far box) pair; from the full-size launch list with
+# dram__bytes_read.sum + dram__bytes_write.sum
+# (profiles/launches_bench_1e6_mixed_batched.md)
+UPWARD_FFMA_DRAM_B = 26.4
+UPWARD_TC_DRAM_B = 18.0
+FAR_DRAM_B = 26.6
 
 
 def parse():
@@ -568,8 +571,8 @@ def run_ours(a):
     # DRAM bytes per padded geometry-table entry and right-hand side, per
     # upward kernel, and per (target, far box) pair and right-hand side of
     # the far field: one ncu capture of dram__bytes_read.sum +
-    # dram__bytes_write.sum of this bench command (a one-pass metric set),
-    # summed over its launches and divided by the units they processed
+    # dram__bytes_write.sum of this bench command at full size, summed over
+    # the launches of each kernel and divided by the units they processed
     # (profiles/launches_bench_1e6_mixed_batched.md)
     bytes_per_unit = {"upward_ffma": UPWARD_FFMA_DRAM_B, "upward_tensor": UPWARD_TC_DRAM_B,
                       "target_eval": FAR_DRAM_B}
