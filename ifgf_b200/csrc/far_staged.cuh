@@ -515,48 +515,65 @@ __global__ void __launch_bounds__(FARB_THREADS, far_plan_ctas(NSL, N0 * N1 * N2,
         cp_async_wait_all();
         __syncthreads(); // records and blocks staged
         const int n_two = G.nslotted / 2, n_one = G.npos - G.nslotted;
-        const int n_item = NH * (n_two + n_one);
-        for (int w = threadIdx.x; w < n_item; w += FARB_THREADS)
-        {
-            if (w < NH * n_two)
+        // work item = (two pairs of one slot, or one pair from global
+        // memory) x NHX of the planes: a group whose items would spill into
+        // a second round of the threads takes smaller ones if the rounds
+        // then cost less (rounds x planes per item, with 10 % for the bases
+        // and records each item repeats)
+        auto items = [&](auto nh) {
+            constexpr int NHX = decltype(nh)::value, RHX = NB / NHX;
+            const int n_item = NHX * (n_two + n_one);
+            for (int w = threadIdx.x; w < n_item; w += FARB_THREADS)
             {
-                const int q = w % n_two, r0 = (w / n_two) * RH;
-                const FarPlanRec ra = frec[2 * q], rb = frec[2 * q + 1];
-                const float la[3] = {__int_as_float(ra.l0), __int_as_float(ra.l1),
-                                     __int_as_float(ra.l2)};
-                const float lb[3] = {__int_as_float(rb.l0), __int_as_float(rb.l1),
-                                     __int_as_float(rb.l2)};
-                const int k = (ra.w >> 9) & 31;
-                const int oa = min(ra.w & 511, FARB_THREADS), ob = min(rb.w & 511, FARB_THREADS);
-#pragma unroll
-                for (int rr = 0; rr < RH; rr++)
+                if (w < NHX * n_two)
                 {
-                    cplx<float> va, vb;
-                    ChebF2<N0, N1, N2>::eval(far_sh + (size_t)k * SS + (r0 + rr) * P_LO, la, lb,
-                                             va, vb);
-                    fres[r0 + rr][oa] = make_float2(va.re, va.im);
-                    fres[r0 + rr][ob] = make_float2(vb.re, vb.im);
+                    const int q = w % n_two, r0 = (w / n_two) * RHX;
+                    const FarPlanRec ra = frec[2 * q], rb = frec[2 * q + 1];
+                    const float la[3] = {__int_as_float(ra.l0), __int_as_float(ra.l1),
+                                         __int_as_float(ra.l2)};
+                    const float lb[3] = {__int_as_float(rb.l0), __int_as_float(rb.l1),
+                                         __int_as_float(rb.l2)};
+                    const int k = (ra.w >> 9) & 31;
+                    const int oa = min(ra.w & 511, FARB_THREADS),
+                              ob = min(rb.w & 511, FARB_THREADS);
+#pragma unroll
+                    for (int rr = 0; rr < RHX; rr++)
+                    {
+                        cplx<float> va, vb;
+                        ChebF2<N0, N1, N2>::eval(far_sh + (size_t)k * SS + (r0 + rr) * P_LO, la,
+                                                 lb, va, vb);
+                        fres[r0 + rr][oa] = make_float2(va.re, va.im);
+                        fres[r0 + rr][ob] = make_float2(vb.re, vb.im);
+                    }
+                }
+                else
+                {
+                    const int w1 = w - NHX * n_two;
+                    const int j = w1 % n_one, r0 = (w1 / n_one) * RHX;
+                    const FarPlanRec rc = frec[G.nslotted + j];
+                    const float l3[3] = {__int_as_float(rc.l0), __int_as_float(rc.l1),
+                                         __int_as_float(rc.l2)};
+                    const int cone = bp.fp_slot[G.slot + G.nslot + j];
+                    const int o = min(rc.w & 511, FARB_THREADS);
+#pragma unroll
+                    for (int rr = 0; rr < RHX; rr++)
+                    {
+                        const cplx<float> v = ChebF<N0, N1, N2>::eval(
+                            bp.fcoef + (size_t)(pb + r0 + rr) * bp.fc_plane +
+                                (size_t)cone * P_LO,
+                            l3, a.lo);
+                        fres[r0 + rr][o] = make_float2(v.re, v.im);
+                    }
                 }
             }
-            else
-            {
-                const int w1 = w - NH * n_two;
-                const int j = w1 % n_one, r0 = (w1 / n_one) * RH;
-                const FarPlanRec rc = frec[G.nslotted + j];
-                const float l3[3] = {__int_as_float(rc.l0), __int_as_float(rc.l1),
-                                     __int_as_float(rc.l2)};
-                const int cone = bp.fp_slot[G.slot + G.nslot + j];
-                const int o = min(rc.w & 511, FARB_THREADS);
-#pragma unroll
-                for (int rr = 0; rr < RH; rr++)
-                {
-                    const cplx<float> v = ChebF<N0, N1, N2>::eval(
-                        bp.fcoef + (size_t)(pb + r0 + rr) * bp.fc_plane + (size_t)cone * P_LO, l3,
-                        a.lo);
-                    fres[r0 + rr][o] = make_float2(v.re, v.im);
-                }
-            }
-        }
+        };
+        const int n = n_two + n_one;
+        const int rounds_h = (NH * n + FARB_THREADS - 1) / FARB_THREADS;
+        const int rounds_q = (NB * n + FARB_THREADS - 1) / FARB_THREADS;
+        if (NB > NH && 11 * rounds_q * (NB / NB) < 10 * rounds_h * (NB / NH))
+            items(std::integral_constant<int, NB>{});
+        else
+            items(std::integral_constant<int, NH>{});
         __syncthreads(); // values of every pair written
         if (mine)
         {
