@@ -63,6 +63,7 @@ __global__ void __launch_bounds__(NODE_THREADS) leaf_sample_batch_kernel(LeafArg
     const double xc[3] = {a.T.box_c[3 * box], a.T.box_c[3 * box + 1], a.T.box_c[3 * box + 2]};
     const double H = a.T.box_H[box];
     float b[NPT][3], dc[NPT];
+    bool live[NPT];
     cplx<float> acc[NPT][NB];
 #pragma unroll
     for (int q = 0; q < NPT; q++)
@@ -73,6 +74,7 @@ __global__ void __launch_bounds__(NODE_THREADS) leaf_sample_batch_kernel(LeafArg
             acc[q][r] = {0.f, 0.f};
         b[q][0] = b[q][1] = b[q][2] = 0.f;
         dc[q] = 1.f;
+        live[q] = n < a.P_hi;
         if (n < a.P_hi)
         {
             double y[3];
@@ -117,38 +119,43 @@ __global__ void __launch_bounds__(NODE_THREADS) leaf_sample_batch_kernel(LeafArg
             }
         }
         __syncthreads();
-#pragma unroll
-        for (int q = 0; q < NPT; q++)
+        // sources outer, nodes inner: each source's data is read from shared
+        // memory once for all of the thread's nodes (every node's sum still
+        // runs over the sources in order)
+        for (int i = 0; i < cnt; i++)
         {
-            if (node0 + threadIdx.x + q * blockDim.x >= a.P_hi)
-                continue;
-            for (int i = 0; i < cnt; i++)
+            const float av[3] = {ax[i], ay[i], az[i]};
+            const float aai = aa[i];
+            const float nv[3] = {P::needs_normals ? n0[i] : 0.f, P::needs_normals ? n1[i] : 0.f,
+                                 P::needs_normals ? n2[i] : 0.f};
+            float2 wr[NB];
+#pragma unroll
+            for (int r = 0; r < NB; r++)
+                wr[r] = wv[r * nt + i];
+#pragma unroll
+            for (int q = 0; q < NPT; q++)
             {
-                const float av[3] = {ax[i], ay[i], az[i]};
-                const float nv[3] = {P::needs_normals ? n0[i] : 0.f, P::needs_normals ? n1[i] : 0.f,
-                                     P::needs_normals ? n2[i] : 0.f};
+                if (!live[q])
+                    continue;
                 if constexpr (MK)
                 {
 #pragma unroll
                     for (int r = 0; r < NB; r++)
                     {
                         const cplx<float> v =
-                            P::factored(av, aa[i], b[q], nv, {1.f, 0.f}, dc[q], kps[r]);
-                        const float2 wr = wv[r * nt + i];
-                        acc[q][r].re = fmaf(wr.x, v.re, fmaf(-wr.y, v.im, acc[q][r].re));
-                        acc[q][r].im = fmaf(wr.x, v.im, fmaf(wr.y, v.re, acc[q][r].im));
+                            P::factored(av, aai, b[q], nv, {1.f, 0.f}, dc[q], kps[r]);
+                        acc[q][r].re = fmaf(wr[r].x, v.re, fmaf(-wr[r].y, v.im, acc[q][r].re));
+                        acc[q][r].im = fmaf(wr[r].x, v.im, fmaf(wr[r].y, v.re, acc[q][r].im));
                     }
                 }
                 else
                 {
-                    const cplx<float> v =
-                        P::factored(av, aa[i], b[q], nv, {1.f, 0.f}, dc[q], a.kp);
+                    const cplx<float> v = P::factored(av, aai, b[q], nv, {1.f, 0.f}, dc[q], a.kp);
 #pragma unroll
                     for (int r = 0; r < NB; r++)
                     {
-                        const float2 wr = wv[r * nt + i];
-                        acc[q][r].re = fmaf(wr.x, v.re, fmaf(-wr.y, v.im, acc[q][r].re));
-                        acc[q][r].im = fmaf(wr.x, v.im, fmaf(wr.y, v.re, acc[q][r].im));
+                        acc[q][r].re = fmaf(wr[r].x, v.re, fmaf(-wr[r].y, v.im, acc[q][r].re));
+                        acc[q][r].im = fmaf(wr[r].x, v.im, fmaf(wr[r].y, v.re, acc[q][r].im));
                     }
                 }
             }
