@@ -104,3 +104,25 @@ def test_far_plan_rebuilt_after_reinit():
         wb = np.stack([W.densities(n, seed=5 + b) for b in range(3)])
         u = _on_off(g, lambda: g.mult_batch(wb))
         assert np.array_equal(u[True], u[False]), seed
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("order", [9, 10])
+def test_far_plan_higher_orders(order):
+    """Orders 9 and 10 (low-order cones (3,6,6) and (4,7,7): larger slots,
+    other slot counts and CTAs per SM): the plan equals the no-plan kernel
+    bit for bit, and the batched mixed matvec stays within the mixed
+    tolerance of the FP64 pipeline."""
+    import ifgf_b200 as G
+
+    n = 15000
+    pts = W.ellipsoid_points(n, seed=1)
+    g = G.HelmholtzIfgfOperator(40.0, 60, order)
+    g.init(pts, pts)
+    wb = np.stack([W.densities(n, seed=30 + b) for b in range(4)])
+    u64 = np.stack([g.mult(w) for w in wb])
+    g.set_precision("mixed")
+    u = _on_off(g, lambda: g.mult_batch(wb))
+    assert np.array_equal(u[True], u[False]), order
+    assert rel2(u[True], u64) <= 2e-5, rel2(u[True], u64)
+    assert g.stats()["far_plan"]["slots_per_group"] in (16, 24)
