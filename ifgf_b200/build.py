@@ -19,7 +19,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I", CSRC, "-I", INCLUDE]
 
 SOURCES = ["operator.cu", "plan.cpp", "gpu_tree.cu", "gpu_lists.cu", "gpu_target_lists.cu",
-           "capi.cpp", "noalloc.cu"] + [
+           "capi.cpp", "noalloc.cu", "upward_images.cu"] + [
     f"kernels_k{k}.cu" for k in range(8)]
 HEADERS = ["common.hpp", "devbuf.hpp", "gpu_target_lists.hpp", "plan.hpp", "operator.hpp",
            "device_math.cuh", "mult.hpp",

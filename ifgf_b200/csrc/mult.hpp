@@ -82,6 +82,10 @@ struct LevelLists
     const int4* tc_tiles = nullptr;
     int n_tc_tiles = 0;
     float tc_fill = 0.f;
+    // basis images of the tensor-core upward transfer (null: none), with the
+    // byte offset of every (slot, octant)
+    const unsigned char* tc_img = nullptr;
+    const long long* tc_img_off = nullptr;
 };
 
 // Upward-transfer kernel choice (Operator::set_upward_path): AUTO takes the
@@ -281,6 +285,25 @@ struct BatchPtrs
     const FarPlanRec* fp_rec = nullptr;
     const int* fp_slot = nullptr;
 };
+
+// Basis images of the tensor-core upward transfer of one level, for the low
+// order shape lo (a shape with a tensor-core kernel): for every (slot,
+// octant) row of the geometry tables and every chunk of <= 48 entries of its
+// runs (the walk of the kernel), the chunk's entry data (node, centre-shift
+// factor) and its B operand -- the TF32 high and low parts of the basis rows
+// in the kernel's shared-memory layout -- so that the kernel copies them
+// instead of computing them in every tile of the slot.
+// upward_tc_image_sizes writes the bytes of every row (nslots x 8 entries);
+// upward_tc_image_fill writes the images at the given byte offsets.
+// Both synchronise the device.  False: no tensor-core kernel for lo.
+// Levels get images when their slots average at least UPTC_IMG_MIN_CONES
+// cones (row tiles reusing each image), up to UPTC_IMG_BUDGET bytes in all.
+constexpr double UPTC_IMG_MIN_CONES = 24.0;
+constexpr long long UPTC_IMG_BUDGET = 8ll << 30;
+bool upward_tc_image_sizes(const int* lo, const int2* fe_list, int fe_pad, int up_pad, int nslots,
+                           long long* d_sizes);
+bool upward_tc_image_fill(const int* lo, const int2* fe_list, int fe_pad, const UpGeo32* geo32,
+                          int up_pad, int nslots, const long long* d_off, unsigned char* img);
 
 // Enqueues the mixed matvec of bp.nrhs <= bp.groups * BATCH_NB right-hand
 // sides, one launch per stage and level for all of them; planes of a group

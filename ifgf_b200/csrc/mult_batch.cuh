@@ -458,6 +458,8 @@ static int run_mult_batch(const MultPtrs& m, const BatchPtrs& bp, const void* d_
                 if (!MK && bp.tc_tiles)
                 {
                     ua.tc_tiles = bp.tc_tiles[l];
+                    ua.tc_img = LL.tc_img;
+                    ua.tc_img_off = LL.tc_img_off;
                     ua.tc_status = m.tc_status;
                     tensor = launch_upward_tc<KIND, N0, N1, N2>(
                         ua, bp.n_tc_tiles[l], bp.tc_fill[l], m.up_path, st, bp.groups * BATCH_NB,
@@ -624,6 +626,8 @@ static int tune_upward_shape(const MultPtrs& m, const BatchPtrs* bp, int planes,
                 ua.lo[d] = m.lo[d];
             ua.kp = m.kp;
             ua.tc_tiles = tiles;
+            ua.tc_img = LL.tc_img;
+            ua.tc_img_off = LL.tc_img_off;
             ua.tc_status = m.tc_status;
             const size_t sm = upward_staged_smem<N0, N1, N2>(m.P_hi, ua.rch, LL.fe_pad);
             if (sm > UP_STAGED_SMEM_MAX ||

@@ -243,6 +243,10 @@ struct UpArgs
     // plane, planes) and the status word its bounded waits report into
     const int4* tc_tiles = nullptr;
     unsigned* tc_status = nullptr;
+    // tensor-core kernel: the level's basis images (null: the kernel builds
+    // the basis rows itself), with the byte offset of every (slot, octant)
+    const unsigned char* tc_img = nullptr;
+    const long long* tc_img_off = nullptr;
 };
 
 // One CTA per coarse cone of a box with children (CTAs ordered by cone
@@ -2213,6 +2217,8 @@ static int run_mult(const MultPtrs& m, const void* d_w, void* d_u, bool real, cu
             if constexpr (MIXED)
             {
                 ua.tc_tiles = LL.tc_tiles;
+                ua.tc_img = LL.tc_img;
+                ua.tc_img_off = LL.tc_img_off;
                 ua.tc_status = m.tc_status;
                 staged = launch_upward_tc<KIND, N0, N1, N2>(ua, LL.n_tc_tiles, LL.tc_fill,
                                                             m.up_path, st, 1,

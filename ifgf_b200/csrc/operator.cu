@@ -95,6 +95,11 @@ struct DeviceState
     // status word of the kernels' bounded waits
     std::vector<std::vector<int2>> tc_runs;
     std::vector<std::map<int, DevBuf<int4>>> tc_tiles;
+    // basis images of the tensor-core upward transfer, per level (built on
+    // first use of the mixed pipeline; empty where not worth their memory)
+    std::vector<DevBuf<unsigned char>> tc_img;
+    std::vector<DevBuf<long long>> tc_img_off;
+    bool tc_img_ready = false;
     std::vector<std::map<int, float>> tc_fill;
     std::vector<const int4*> tcb_ptr;
     std::vector<int> tcb_n;
@@ -612,6 +617,8 @@ void Operator::set_wavenumber(double k_re, double k_im)
     }
     IFGF_CUDA(cudaDeviceSynchronize());
     D.vkind = -1; // variant (k-derivative) tables are rebuilt on next use
+    // the basis images hold the old centre-shift factors: rebuilt on next use
+    drop_tc_images();
 }
 
 // Whether wavenumber k_re + i k_im gives every level the cone grids and
@@ -1257,6 +1264,9 @@ void Operator::setup_device(const double* normals)
     D.up_idx.resize(L);
     D.up_slot.resize(L);
     D.tc_runs.assign(L, {});
+    D.tc_img.clear();
+    D.tc_img_off.clear();
+    D.tc_img_ready = false;
     D.tc_tiles.clear();
     D.tc_tiles.resize(L);
     D.tc_fill.assign(L, {});
@@ -1624,6 +1634,74 @@ void Operator::fill_mult_ptrs(MultPtrs& m, bool variant) const
 // null: the single-plane buffers) and keeps the per-level choice.  It
 // synchronises `st` once; the buffers it ran on are rewritten by the matvec
 // that follows.
+void Operator::drop_tc_images()
+{
+    DeviceState& D = *dev_;
+    for (auto& b : D.tc_img)
+        b.release();
+    for (auto& b : D.tc_img_off)
+        b.release();
+    for (auto& LL : D.lists)
+    {
+        LL.tc_img = nullptr;
+        LL.tc_img_off = nullptr;
+    }
+    D.tc_img_ready = false;
+}
+
+void Operator::ensure_tc_images()
+{
+    DeviceState& D = *dev_;
+    if (D.tc_img_ready)
+        return;
+    D.tc_img_ready = true;
+    const int L = (int)lv_.size();
+    D.tc_img.resize(L);
+    D.tc_img_off.resize(L);
+    // levels whose slots have many cones (so many row tiles reuse every
+    // image), most cones per slot first, within a memory budget
+    std::vector<std::pair<double, int>> cand;
+    for (int l = 0; l + 1 < L; l++)
+    {
+        const LevelLists& LL = D.lists[l];
+        const int ns = (int)D.slot_el[l].n;
+        if (LL.n_up <= 0 || ns == 0 || LL.up_pad <= 0 || LL.fe_pad <= 0)
+            continue;
+        const double cps = (double)LL.n_up / ns;
+        if (cps >= UPTC_IMG_MIN_CONES)
+            cand.push_back({cps, l});
+    }
+    std::sort(cand.begin(), cand.end(), [](auto& x, auto& y) { return x.first > y.first; });
+    long long used = 0;
+    for (const auto& c : cand)
+    {
+        const int l = c.second;
+        LevelLists& LL = D.lists[l];
+        const int ns = (int)D.slot_el[l].n;
+        DevBuf<long long> sz;
+        sz.alloc((size_t)ns * 8);
+        if (!upward_tc_image_sizes(lo_, LL.fe_list, LL.fe_pad, LL.up_pad, ns, sz.p))
+            return; // no tensor-core kernel for this order shape
+        const std::vector<long long> hs = sz.download();
+        std::vector<long long> off(hs.size());
+        long long tot = 0;
+        for (size_t i = 0; i < hs.size(); i++)
+        {
+            off[i] = tot;
+            tot += hs[i];
+        }
+        if (tot == 0 || used + tot > UPTC_IMG_BUDGET)
+            continue;
+        D.tc_img_off[l].upload(off);
+        D.tc_img[l].alloc((size_t)tot);
+        upward_tc_image_fill(lo_, LL.fe_list, LL.fe_pad, LL.geo32, LL.up_pad, ns,
+                             D.tc_img_off[l].p, D.tc_img[l].p);
+        LL.tc_img = D.tc_img[l].p;
+        LL.tc_img_off = D.tc_img_off[l].p;
+        used += tot;
+    }
+}
+
 void Operator::ensure_upward_tuned(int planes, const BatchPtrs* bp, void* stream)
 {
     DeviceState& D = *dev_;
@@ -1838,6 +1916,8 @@ void Operator::set_batch_far(BatchPtrs& bp)
 void Operator::set_batch_tc(BatchPtrs& bp, void* stream)
 {
     DeviceState& D = *dev_;
+    if (!bp.kp_plane)
+        ensure_tc_images();
     const int planes = bp.groups * BATCH_NB;
     ensure_tc_tiles(planes);
     const int L = (int)lv_.size();
@@ -2127,6 +2207,11 @@ void Operator::ensure_variant_tables(int vkind)
     D.vgeo64.resize(L);
     D.vgeo32.resize(L);
     D.vlists = D.lists;
+    for (auto& VL : D.vlists) // the images hold the base kernel's centre-shift factors
+    {
+        VL.tc_img = nullptr;
+        VL.tc_img_off = nullptr;
+    }
     for (int l = 0; l + 1 < L; l++)
     {
         const LevelLists& LL = D.lists[l];
@@ -2179,7 +2264,10 @@ void Operator::launch_mult(const void* d_w, void* d_u, void* stream, bool timed,
     if (vkind >= 0)
         ensure_variant_tables(vkind);
     if (vkind < 0 && precision_ == PREC_MIXED)
+    {
+        ensure_tc_images();
         ensure_upward_tuned(1, nullptr, stream);
+    }
     MultPtrs m;
     fill_mult_ptrs(m, vkind >= 0);
     EventHooks log(D, st);
@@ -2796,6 +2884,10 @@ std::string Operator::stats_json() const
       << (dev_->fp_group.n * sizeof(FarGroup) + dev_->fp_rec.n * sizeof(FarPlanRec) +
           dev_->fp_slot.n * sizeof(int) + dev_->fp_chunk.n * sizeof(FarChunk))
       << ",\"slots_per_group\":" << dev_->fp_nslot << ",\"overflow_share_at_few_slots\":" << dev_->fp_ovf_few << ",\"build_ms\":" << dev_->fp_ms << "}";
+    o << ",\"upward_images_bytes\":[";
+    for (int l = 0; l < (int)lv_.size(); l++)
+        o << (l ? "," : "") << (l < (int)dev_->tc_img.size() ? dev_->tc_img[l].n : 0);
+    o << "]";
     o << ",\"upward_path\":" << up_path_ << ",\"upward_tuner\":{";
     {
         bool first = true;

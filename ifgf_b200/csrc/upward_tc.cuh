@@ -41,7 +41,10 @@
 //   4-7   epilogue: read D, sum the hi / lo lanes, form the complex value,
 //         multiply by the centre-shift factor and add it into the cone's
 //         node accumulators (shared memory, FP32)
-//   8-11  B producers: the basis rows of a chunk of <= 48 entries
+//   8-11  B producers: the basis rows of a chunk of <= 48 entries; with the
+//         level's basis images (upward_tc_image_fill) one elected thread of
+//         warp 8 copies the chunk's rows and entry data instead (two bulk
+//         copies completing the same barriers by byte count)
 //   12    loader: per run, the child fine cone of every row (looked up up
 //         to four runs ahead) and an L2 prefetch of its coefficient block
 //   13    lane 0 issues the MMAs (tcgen05.mma kind::tf32) and commits
@@ -283,10 +286,11 @@ __global__ void __launch_bounds__(UPTC_THREADS, 1) upward_tc_kernel(const __grid
         {
             unsigned cnt = 1;
             if ((b >= UTB_ROW_EMPTY && b < UTB_ROW_EMPTY + UPTC_ROW_STAGES) ||
-                b == UTB_A_FULL || b == UTB_A_FULL + 1 || b == UTB_B_FULL || b == UTB_B_FULL + 1 ||
-                b == UTB_D_EMPTY || b == UTB_D_EMPTY + 1 || b == UTB_META_FULL ||
-                b == UTB_META_FULL + 1)
+                b == UTB_A_FULL || b == UTB_A_FULL + 1 || b == UTB_D_EMPTY || b == UTB_D_EMPTY + 1)
                 cnt = 4;
+            if (b == UTB_B_FULL || b == UTB_B_FULL + 1 || b == UTB_META_FULL ||
+                b == UTB_META_FULL + 1)
+                cnt = a.tc_img ? 1 : 4; // one bulk-copy issuer, or four producer warps
             tc::mbar_init(tc::smem_u32(bars + b), cnt);
         }
         tc::mbar_init_fence();
@@ -456,6 +460,56 @@ __global__ void __launch_bounds__(UPTC_THREADS, 1) upward_tc_kernel(const __grid
         }
         if (!ok && lane == 0)
             atomicOr(a.tc_status, 1u);
+    }
+    else if (warp >= 8 && warp < 12 && a.tc_img)
+    {
+        // ---------------- B operand and entry data from the basis images ----------------
+        // the walk of the MMA issuer; per chunk, once its stage is free, one
+        // lane copies the record (entry data, then the B rows) of the image
+        if (warp == 8)
+        {
+            int Cn = 0;
+            for (int o = 0; o < 8 && ok; o++)
+            {
+                if (!used[o])
+                    continue;
+                long long pos = a.tc_img_off[(size_t)slot * 8 + o];
+                for (int r = 0; r < row_n[o] && ok; r++)
+                {
+                    int ce, g0, g1;
+                    run_info(o, r, ce, g0, g1);
+                    for (int cg = g0; cg < g1; cg += GMAX, Cn++)
+                    {
+                        const int nent = UPGEO_RUN * min(GMAX, g1 - cg);
+                        const int N = (nent + 15) & ~15;
+                        const int bs = Cn & 1;
+                        if (Cn >= 2 &&
+                            (!tc::mbar_wait(bar(UTB_B_EMPTY + bs), ((Cn >> 1) - 1) & 1,
+                                            UPTC_WAIT_NS) ||
+                             !tc::mbar_wait(bar(UTB_D_EMPTY + bs), ((Cn >> 1) - 1) & 1,
+                                            UPTC_WAIT_NS)))
+                        {
+                            ok = false;
+                            break;
+                        }
+                        if (tc::elect_one())
+                        {
+                            const unsigned mbytes = 16u * N, bbytes = 8u * N * K;
+                            tc::mbar_arrive_expect_tx(bar(UTB_META_FULL + bs), mbytes);
+                            tc::bulk_g2s(tc::smem_u32(meta + bs * UPTC_NMAX), a.tc_img + pos, mbytes,
+                                         bar(UTB_META_FULL + bs));
+                            tc::mbar_arrive_expect_tx(bar(UTB_B_FULL + bs), bbytes);
+                            tc::bulk_g2s(tc::smem_u32(Bs + (size_t)bs * (S::B_BYTES / 4)),
+                                         a.tc_img + pos + mbytes, bbytes, bar(UTB_B_FULL + bs));
+                        }
+                        __syncwarp();
+                        pos += (long long)N * (16 + 8 * K);
+                    }
+                }
+            }
+            if (!ok && lane == 0)
+                atomicOr(a.tc_status, 1u);
+        }
     }
     else if (warp >= 8 && warp < 12)
     {
@@ -757,6 +811,75 @@ __global__ void __launch_bounds__(UPTC_THREADS, 1) upward_tc_kernel(const __grid
     }
     if (warp == 13)
         tc::tmem_dealloc(tbase, UPTC_TM_COLS);
+}
+
+// Basis images of one level (upward_tc_image_sizes / _fill, mult.hpp): one
+// CTA per (slot, octant) row, walking its runs and chunks as the kernel does;
+// per chunk of nent entries (N = nent rounded up to 16) the record is the
+// entry data (N x int4: node, centre-shift factor) followed by the B stage
+// image (2 N x K floats: TF32 high parts of the basis rows, then low parts,
+// in the K-major core-matrix layout), exactly what the B producers would
+// write to shared memory.  sizes != null: only the row's bytes.
+template <int N0, int N1, int N2>
+__global__ void __launch_bounds__(128)
+    uptc_image_kernel(const int2* __restrict__ fe_list, int fe_pad,
+                      const UpGeo32* __restrict__ geo32, int P_pad,
+                      const long long* __restrict__ off, unsigned char* img, long long* sizes)
+{
+    using S = UpTcShape<N0, N1, N2>;
+    constexpr int K = S::K;
+    constexpr int GMAX = UPTC_NMAX / UPGEO_RUN;
+    const int so = blockIdx.x, o = so & 7;
+    const size_t slot = (size_t)(so >> 3);
+    const int FL = fe_pad + 1, ngroups = P_pad / UPGEO_RUN;
+    const int2* fl = fe_list + (size_t)so * FL;
+    int nrun = fe_pad, rgroups = ngroups;
+    for (int r = 0; r < FL; r++)
+    {
+        const int2 f = fl[r];
+        if (f.x < 0 && f.y >= 0)
+        {
+            nrun = r;
+            rgroups = f.y;
+            break;
+        }
+    }
+    long long pos = sizes ? 0 : off[so];
+    const int half = threadIdx.x >> 6, e = threadIdx.x & 63;
+    for (int r = 0; r < nrun; r++)
+    {
+        const int g0 = fl[r].y, g1 = r + 1 < nrun ? fl[r + 1].y : rgroups;
+        for (int cg = g0; cg < g1; cg += GMAX)
+        {
+            const int nent = UPGEO_RUN * min(GMAX, g1 - cg);
+            const int N = (nent + 15) & ~15;
+            if (!sizes && e < N)
+            {
+                UpGeo32 g;
+                g.node = -1;
+                g.loc[0] = g.loc[1] = g.loc[2] = 0.f;
+                g.tr = g.ti = 0.f;
+                if (e < nent)
+                    g = geo32[(slot * 8 + o) * P_pad + (size_t)(e % UPGEO_RUN) * ngroups + cg +
+                              e / UPGEO_RUN];
+                const int node = e < nent ? g.node : -1;
+                int4* meta = reinterpret_cast<int4*>(img + pos);
+                float* B = reinterpret_cast<float*>(img + pos + 16 * N);
+                float* bh = B + (size_t)(e >> 3) * (S::SBO / 4) + (e & 7) * 4;
+                float* bl = B + (size_t)((N + e) >> 3) * (S::SBO / 4) + ((N + e) & 7) * 4;
+                if (half == 0)
+                {
+                    uptc_basis_half<N0, N1, N2, 0>(node >= 0, g.loc[0], g.loc[1], g.loc[2], bh, bl);
+                    meta[e] = make_int4(node, __float_as_int(g.tr), __float_as_int(g.ti), 0);
+                }
+                else
+                    uptc_basis_half<N0, N1, N2, 1>(node >= 0, g.loc[0], g.loc[1], g.loc[2], bh, bl);
+            }
+            pos += (long long)N * (16 + 8 * K);
+        }
+    }
+    if (sizes && threadIdx.x == 0)
+        sizes[so] = pos;
 }
 
 // Order shapes with a tensor-core upward kernel: the low orders of p = 8 and
