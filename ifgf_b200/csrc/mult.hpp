@@ -294,7 +294,8 @@ struct BatchPtrs
 // in the kernel's shared-memory layout -- so that the kernel copies them
 // instead of computing them in every tile of the slot.
 // upward_tc_image_sizes writes the bytes of every row (nslots x 8 entries);
-// upward_tc_image_fill writes the images at the given byte offsets.
+// upward_tc_image_fill writes the images at the given byte offsets (with
+// meta_only, just the entry data: after the wavenumber changed).
 // Both synchronise the device.  False: no tensor-core kernel for lo.
 // Levels get images when their slots average at least UPTC_IMG_MIN_CONES
 // cones (row tiles reusing each image), up to UPTC_IMG_BUDGET bytes in all.
@@ -303,7 +304,8 @@ constexpr long long UPTC_IMG_BUDGET = 8ll << 30;
 bool upward_tc_image_sizes(const int* lo, const int2* fe_list, int fe_pad, int up_pad, int nslots,
                            long long* d_sizes);
 bool upward_tc_image_fill(const int* lo, const int2* fe_list, int fe_pad, const UpGeo32* geo32,
-                          int up_pad, int nslots, const long long* d_off, unsigned char* img);
+                          int up_pad, int nslots, const long long* d_off, unsigned char* img,
+                          bool meta_only = false);
 
 // Enqueues the mixed matvec of bp.nrhs <= bp.groups * BATCH_NB right-hand
 // sides, one launch per stage and level for all of them; planes of a group

@@ -617,8 +617,15 @@ void Operator::set_wavenumber(double k_re, double k_im)
     }
     IFGF_CUDA(cudaDeviceSynchronize());
     D.vkind = -1; // variant (k-derivative) tables are rebuilt on next use
-    // the basis images hold the old centre-shift factors: rebuilt on next use
-    drop_tc_images();
+    // the basis images hold the old centre-shift factors: new entry data (the
+    // basis rows do not depend on the wavenumber)
+    for (int l = 0; l < (int)D.tc_img.size(); l++)
+        if (D.tc_img[l].n > 0)
+        {
+            const LevelLists& LL = D.lists[l];
+            upward_tc_image_fill(lo_, LL.fe_list, LL.fe_pad, LL.geo32, LL.up_pad,
+                                 (int)D.slot_el[l].n, D.tc_img_off[l].p, D.tc_img[l].p, true);
+        }
 }
 
 // Whether wavenumber k_re + i k_im gives every level the cone grids and
@@ -1634,21 +1641,6 @@ void Operator::fill_mult_ptrs(MultPtrs& m, bool variant) const
 // null: the single-plane buffers) and keeps the per-level choice.  It
 // synchronises `st` once; the buffers it ran on are rewritten by the matvec
 // that follows.
-void Operator::drop_tc_images()
-{
-    DeviceState& D = *dev_;
-    for (auto& b : D.tc_img)
-        b.release();
-    for (auto& b : D.tc_img_off)
-        b.release();
-    for (auto& LL : D.lists)
-    {
-        LL.tc_img = nullptr;
-        LL.tc_img_off = nullptr;
-    }
-    D.tc_img_ready = false;
-}
-
 void Operator::ensure_tc_images()
 {
     DeviceState& D = *dev_;

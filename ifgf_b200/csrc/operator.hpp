@@ -139,9 +139,8 @@ class Operator
     void set_batch_far(BatchPtrs& bp);
     void ensure_upward_tuned(int planes, const BatchPtrs* bp, void* stream);
     // basis images of the tensor-core upward transfer (built on first use of
-    // the mixed pipeline; dropped when the geometry tables change)
+    // the mixed pipeline; their entry data is rewritten by set_wavenumber)
     void ensure_tc_images();
-    void drop_tc_images();
     void setup_device(const double* normals);
     // vkind >= 0: run that kernel with the variant geometry tables
     void launch_mult(const void* d_w, void* d_u, void* stream, bool timed, int vkind = -1);

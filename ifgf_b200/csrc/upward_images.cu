@@ -9,12 +9,13 @@ namespace
 {
 template <int N0, int N1, int N2>
 void image_pass(const int2* fe_list, int fe_pad, const UpGeo32* geo32, int up_pad, int nslots,
-                const long long* off, unsigned char* img, long long* sizes)
+                const long long* off, unsigned char* img, long long* sizes, bool meta_only)
 {
     const unsigned rows = (unsigned)nslots * 8u;
     if (rows == 0)
         return;
-    uptc_image_kernel<N0, N1, N2><<<rows, 128>>>(fe_list, fe_pad, geo32, up_pad, off, img, sizes);
+    uptc_image_kernel<N0, N1, N2><<<rows, 128>>>(fe_list, fe_pad, geo32, up_pad, off, img, sizes,
+                                                 meta_only);
     IFGF_CHECK_LAUNCH();
     IFGF_CHECK(cudaDeviceSynchronize());
 }
@@ -40,16 +41,17 @@ bool upward_tc_image_sizes(const int* lo, const int2* fe_list, int fe_pad, int u
 {
     return by_shape(lo, [&](auto a, auto b) {
         image_pass<decltype(a)::value, decltype(b)::value, decltype(b)::value>(
-            fe_list, fe_pad, nullptr, up_pad, nslots, nullptr, nullptr, d_sizes);
+            fe_list, fe_pad, nullptr, up_pad, nslots, nullptr, nullptr, d_sizes, false);
     });
 }
 
 bool upward_tc_image_fill(const int* lo, const int2* fe_list, int fe_pad, const UpGeo32* geo32,
-                          int up_pad, int nslots, const long long* d_off, unsigned char* img)
+                          int up_pad, int nslots, const long long* d_off, unsigned char* img,
+                          bool meta_only)
 {
     return by_shape(lo, [&](auto a, auto b) {
         image_pass<decltype(a)::value, decltype(b)::value, decltype(b)::value>(
-            fe_list, fe_pad, geo32, up_pad, nslots, d_off, img, nullptr);
+            fe_list, fe_pad, geo32, up_pad, nslots, d_off, img, nullptr, meta_only);
     });
 }
 

@@ -819,12 +819,15 @@ __global__ void __launch_bounds__(UPTC_THREADS, 1) upward_tc_kernel(const __grid
 // entry data (N x int4: node, centre-shift factor) followed by the B stage
 // image (2 N x K floats: TF32 high parts of the basis rows, then low parts,
 // in the K-major core-matrix layout), exactly what the B producers would
-// write to shared memory.  sizes != null: only the row's bytes.
+// write to shared memory.  sizes != null: only the row's bytes.  meta_only:
+// only the entry data (the centre-shift factors follow the wavenumber, the
+// basis rows do not).
 template <int N0, int N1, int N2>
 __global__ void __launch_bounds__(128)
     uptc_image_kernel(const int2* __restrict__ fe_list, int fe_pad,
                       const UpGeo32* __restrict__ geo32, int P_pad,
-                      const long long* __restrict__ off, unsigned char* img, long long* sizes)
+                      const long long* __restrict__ off, unsigned char* img, long long* sizes,
+                      bool meta_only)
 {
     using S = UpTcShape<N0, N1, N2>;
     constexpr int K = S::K;
@@ -869,10 +872,12 @@ __global__ void __launch_bounds__(128)
                 float* bl = B + (size_t)((N + e) >> 3) * (S::SBO / 4) + ((N + e) & 7) * 4;
                 if (half == 0)
                 {
-                    uptc_basis_half<N0, N1, N2, 0>(node >= 0, g.loc[0], g.loc[1], g.loc[2], bh, bl);
+                    if (!meta_only)
+                        uptc_basis_half<N0, N1, N2, 0>(node >= 0, g.loc[0], g.loc[1], g.loc[2], bh,
+                                                       bl);
                     meta[e] = make_int4(node, __float_as_int(g.tr), __float_as_int(g.ti), 0);
                 }
-                else
+                else if (!meta_only)
                     uptc_basis_half<N0, N1, N2, 1>(node >= 0, g.loc[0], g.loc[1], g.loc[2], bh, bl);
             }
             pos += (long long)N * (16 + 8 * K);

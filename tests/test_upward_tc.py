@@ -147,3 +147,31 @@ def test_autotuner_records_a_choice_per_level_and_plane_count():
     g.set_upward_path("ffma")
     assert rel2(u1, g.mult(w)) <= TC_VS_FFMA
     assert rel2(ub, g.mult_batch(wb)) <= TC_VS_FFMA
+
+
+@pytest.mark.gpu
+def test_tensor_upward_basis_images_follow_the_wavenumber():
+    """The basis images of the tensor-core kernel (built once per level)
+    carry the centre-shift factors of the operator's wavenumber: after
+    set_wavenumber on the same cone grids the matvec equals a fresh
+    operator's at the new wavenumber."""
+    import ifgf_b200 as G
+
+    n = 60000
+    pts = W.sphere_points(n, seed=0)
+    w = W.densities(n, seed=1)
+    k1, k2 = 20.2, 20.6  # the same cone grids on every level
+    g = G.HelmholtzIfgfOperator(k1, 60, 9)
+    g.init(pts, pts)
+    g.set_precision("mixed")
+    g.set_upward_path("tensor")
+    g.mult(w)
+    assert sum(g.stats()["upward_images_bytes"]) > 0
+    g.set_wavenumber(k2)
+    assert g.stats()["far_plan"]["built"] in (0, 1)
+    u = g.mult(w)
+    f = G.HelmholtzIfgfOperator(k2, 60, 9)
+    f.init(pts, pts)
+    f.set_precision("mixed")
+    f.set_upward_path("tensor")
+    assert rel2(u, f.mult(w)) <= 1e-14, rel2(u, f.mult(w))
