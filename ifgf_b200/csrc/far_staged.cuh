@@ -113,11 +113,13 @@ template <int N0, int N1, int N2> struct ChebF2
         float a0[N0], a1[N1], a2[N2], b0[N0], b1[N1], b2[N2];
         basis(xa, a0, a1, a2);
         basis(xb, b0, b1, b2);
-        float aar = 0, aai = 0, bar = 0, bai = 0;
+        // T_0 = 1: every sum starts from its first term instead of adding
+        // it to zero (the same values; one instruction less per sum)
+        float aar, aai, bar, bai;
 #pragma unroll
         for (int k = 0; k < N2; k++)
         {
-            float abr = 0, abi = 0, bbr = 0, bbi = 0;
+            float abr, abi, bbr, bbi;
 #pragma unroll
             for (int j = 0; j < N1; j += CoefRows<N0, N1>::ROWS)
             {
@@ -126,25 +128,40 @@ template <int N0, int N1, int N2> struct ChebF2
 #pragma unroll
                 for (int jj = 0; jj < CoefRows<N0, N1>::ROWS; jj++)
                 {
-                    float acr = 0, aci = 0, bcr = 0, bci = 0;
+                    float acr = v[jj * N0].x, aci = v[jj * N0].y;
+                    float bcr = acr, bci = aci;
 #pragma unroll
-                    for (int i = 0; i < N0; i++)
+                    for (int i = 1; i < N0; i++)
                     {
                         acr = fmaf(v[jj * N0 + i].x, a0[i], acr);
                         aci = fmaf(v[jj * N0 + i].y, a0[i], aci);
                         bcr = fmaf(v[jj * N0 + i].x, b0[i], bcr);
                         bci = fmaf(v[jj * N0 + i].y, b0[i], bci);
                     }
-                    abr = fmaf(acr, a1[j + jj], abr);
-                    abi = fmaf(aci, a1[j + jj], abi);
-                    bbr = fmaf(bcr, b1[j + jj], bbr);
-                    bbi = fmaf(bci, b1[j + jj], bbi);
+                    if (j + jj == 0)
+                    {
+                        abr = acr, abi = aci, bbr = bcr, bbi = bci;
+                    }
+                    else
+                    {
+                        abr = fmaf(acr, a1[j + jj], abr);
+                        abi = fmaf(aci, a1[j + jj], abi);
+                        bbr = fmaf(bcr, b1[j + jj], bbr);
+                        bbi = fmaf(bci, b1[j + jj], bbi);
+                    }
                 }
             }
-            aar = fmaf(abr, a2[k], aar);
-            aai = fmaf(abi, a2[k], aai);
-            bar = fmaf(bbr, b2[k], bar);
-            bai = fmaf(bbi, b2[k], bai);
+            if (k == 0)
+            {
+                aar = abr, aai = abi, bar = bbr, bai = bbi;
+            }
+            else
+            {
+                aar = fmaf(abr, a2[k], aar);
+                aai = fmaf(abi, a2[k], aai);
+                bar = fmaf(bbr, b2[k], bar);
+                bai = fmaf(bbi, b2[k], bai);
+            }
         }
         va = {aar, aai};
         vb = {bar, bai};
@@ -440,10 +457,12 @@ __global__ void __launch_bounds__(FARB_THREADS, FARB_CTAS)
 // computed, so a group is: copy its records and slot blocks (cp.async), the
 // owners' box distances meanwhile, one barrier, the sums (two pairs of one
 // slot per work item, as in far_batch_kernel), one barrier, the owners'
-// factors and FP64 sums in box order, overlapping the next group's copies.  One CTA per chunk of up to 256
-// targets of a leaf and per group of NP planes.
-static_assert(FAR_PLAN_THREADS == FARB_THREADS && FAR_PLAN_PAD == FAR_PAD,
-              "the plan's layout is the far kernels'");
+// factors and FP64 sums in box order, overlapping the next group's copies.
+// (Prefetching the next group's blocks and records into L2 during this
+// group's copies measured slower.)  One CTA per chunk of up to 256 targets of
+// a leaf and per group of NP planes.
+static_assert(FAR_PLAN_THREADS == FARB_THREADS && FAR_PLAN_PAD % 2 == 0,
+              "the plan's owners are threads of 256, its work items pairs of one slot");
 template <int P_LO, int NP, int NSL> __host__ __device__ constexpr size_t far_plan_smem()
 {
     const size_t slots = (size_t)NSL * far_slot_stride<P_LO, NP>() * 8;
@@ -523,47 +542,50 @@ __global__ void __launch_bounds__(FARB_THREADS, far_plan_ctas(NSL, N0 * N1 * N2,
         auto items = [&](auto nh) {
             constexpr int NHX = decltype(nh)::value, RHX = NB / NHX;
             const int n_item = NHX * (n_two + n_one);
-            for (int w = threadIdx.x; w < n_item; w += FARB_THREADS)
+            // item w = h n_two + q (two pairs 2q, 2q + 1, planes from h RHX),
+            // then the one-pair items; q and h follow w without divisions
+            int w = threadIdx.x, q = w, h = 0;
+            while (h < NHX && q >= n_two)
+                q -= n_two, h++;
+            for (; h < NHX; w += FARB_THREADS)
             {
-                if (w < NHX * n_two)
-                {
-                    const int q = w % n_two, r0 = (w / n_two) * RHX;
-                    const FarPlanRec ra = frec[2 * q], rb = frec[2 * q + 1];
-                    const float la[3] = {__int_as_float(ra.l0), __int_as_float(ra.l1),
-                                         __int_as_float(ra.l2)};
-                    const float lb[3] = {__int_as_float(rb.l0), __int_as_float(rb.l1),
-                                         __int_as_float(rb.l2)};
-                    const int k = (ra.w >> 9) & 31;
-                    const int oa = min(ra.w & 511, FARB_THREADS),
-                              ob = min(rb.w & 511, FARB_THREADS);
+                const int r0 = h * RHX;
+                const FarPlanRec ra = frec[2 * q], rb = frec[2 * q + 1];
+                const float la[3] = {__int_as_float(ra.l0), __int_as_float(ra.l1),
+                                     __int_as_float(ra.l2)};
+                const float lb[3] = {__int_as_float(rb.l0), __int_as_float(rb.l1),
+                                     __int_as_float(rb.l2)};
+                const int k = (ra.w >> 9) & 31;
+                const int oa = min(ra.w & 511, FARB_THREADS), ob = min(rb.w & 511, FARB_THREADS);
 #pragma unroll
-                    for (int rr = 0; rr < RHX; rr++)
-                    {
-                        cplx<float> va, vb;
-                        ChebF2<N0, N1, N2>::eval(far_sh + (size_t)k * SS + (r0 + rr) * P_LO, la,
-                                                 lb, va, vb);
-                        fres[r0 + rr][oa] = make_float2(va.re, va.im);
-                        fres[r0 + rr][ob] = make_float2(vb.re, vb.im);
-                    }
+                for (int rr = 0; rr < RHX; rr++)
+                {
+                    cplx<float> va, vb;
+                    ChebF2<N0, N1, N2>::eval(far_sh + (size_t)k * SS + (r0 + rr) * P_LO, la, lb,
+                                             va, vb);
+                    fres[r0 + rr][oa] = make_float2(va.re, va.im);
+                    fres[r0 + rr][ob] = make_float2(vb.re, vb.im);
                 }
-                else
-                {
-                    const int w1 = w - NHX * n_two;
-                    const int j = w1 % n_one, r0 = (w1 / n_one) * RHX;
-                    const FarPlanRec rc = frec[G.nslotted + j];
-                    const float l3[3] = {__int_as_float(rc.l0), __int_as_float(rc.l1),
-                                         __int_as_float(rc.l2)};
-                    const int cone = bp.fp_slot[G.slot + G.nslot + j];
-                    const int o = min(rc.w & 511, FARB_THREADS);
+                q += FARB_THREADS;
+                while (h < NHX && q >= n_two)
+                    q -= n_two, h++;
+            }
+            for (; w < n_item; w += FARB_THREADS)
+            {
+                const int w1 = w - NHX * n_two;
+                const int j = w1 % n_one, r0 = (w1 / n_one) * RHX;
+                const FarPlanRec rc = frec[G.nslotted + j];
+                const float l3[3] = {__int_as_float(rc.l0), __int_as_float(rc.l1),
+                                     __int_as_float(rc.l2)};
+                const int cone = bp.fp_slot[G.slot + G.nslot + j];
+                const int o = min(rc.w & 511, FARB_THREADS);
 #pragma unroll
-                    for (int rr = 0; rr < RHX; rr++)
-                    {
-                        const cplx<float> v = ChebF<N0, N1, N2>::eval(
-                            bp.fcoef + (size_t)(pb + r0 + rr) * bp.fc_plane +
-                                (size_t)cone * P_LO,
-                            l3, a.lo);
-                        fres[r0 + rr][o] = make_float2(v.re, v.im);
-                    }
+                for (int rr = 0; rr < RHX; rr++)
+                {
+                    const cplx<float> v = ChebF<N0, N1, N2>::eval(
+                        bp.fcoef + (size_t)(pb + r0 + rr) * bp.fc_plane + (size_t)cone * P_LO, l3,
+                        a.lo);
+                    fres[r0 + rr][o] = make_float2(v.re, v.im);
                 }
             }
         };

@@ -199,7 +199,11 @@ constexpr int BATCH_NB = 4;
 // each target-leaf chunk in groups of S consecutive far boxes (one pair per
 // thread of a 256-thread CTA, thread = target + (box - first box) x targets),
 // each group's distinct fine cones in slots (the 24 with the smallest ids)
-// and its pairs as records in slot order, every slot's run padded to 8.
+// and its pairs as records in slot order, every slot's run padded to
+// FAR_PLAN_PAD positions (4: a quad of evaluating lanes takes 8, so about
+// half the quads of a slot's last positions straddle two slots and read two
+// blocks -- measured cheaper than padding to 8, which evaluated some 30 %
+// padding positions, or to 2).
 struct FarChunk // up to 256 targets of one target leaf
 {
     long long g0, g1; // its groups
@@ -227,7 +231,7 @@ struct __align__(16) FarPlanRec
 // records then read global memory
 constexpr int FAR_PLAN_SLOTS = 24;
 constexpr int FAR_PLAN_SLOTS_FEW = 16;
-constexpr int FAR_PLAN_THREADS = 256, FAR_PLAN_PAD = 8;
+constexpr int FAR_PLAN_THREADS = 256, FAR_PLAN_PAD = 4;
 // record positions of a group with nsl slots (each slot's run padded)
 __host__ __device__ constexpr int far_plan_pos(int nsl)
 {

@@ -192,7 +192,7 @@ __global__ void mark_far_kernel(LevelGeom G, TreeArgs T, const int* __restrict__
 // of the far kernels), the distinct cones in a hash table of twice the pairs
 // (never full, so every cone is in it), slots for the nslot smallest cone
 // ids, and the records in slot order, each slot's run padded
-// to 8 positions; pairs of the other cones go last, with their cone ids
+// to FAR_PLAN_PAD positions; pairs of the other cones go last, with their cone ids
 // after the group's slot list.  Every count depends only on the set of cones
 // of the group, not on the order of the atomics, so the two passes agree:
 // FILL = false counts the groups, records and slot-list entries of every
@@ -322,7 +322,7 @@ __global__ void __launch_bounds__(256) far_plan_build_kernel(FarBuildArgs b)
             __syncthreads(); // slot order complete
             const int ns = min(nd, NS);
             const int ck = lane < ns ? scnt[lane] : 0;
-            const int pk = (ck + 7) & ~7;
+            const int pk = (ck + FAR_PLAN_PAD - 1) & ~(FAR_PLAN_PAD - 1);
             int incl = pk;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1)
