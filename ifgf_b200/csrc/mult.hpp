@@ -198,7 +198,7 @@ constexpr int BATCH_NB = 4;
 // every batched or multi-wavenumber matvec): the (target, far box) pairs of
 // each target-leaf chunk in groups of S consecutive far boxes (one pair per
 // thread of a 256-thread CTA, thread = target + (box - first box) x targets),
-// each group's distinct fine cones in slots (the 24 with the smallest ids)
+// each group's distinct fine cones in slots (the 24 with the most pairs)
 // and its pairs as records in slot order, every slot's run padded to
 // FAR_PLAN_PAD positions (4: a quad of evaluating lanes takes 8, so about
 // half the quads of a slot's last positions straddle two slots and read two
@@ -227,7 +227,7 @@ struct __align__(16) FarPlanRec
     int l0, l1, l2, w;
 };
 // slots per group of a plan: FAR_PLAN_SLOTS, or FAR_PLAN_SLOTS_FEW where
-// the fewer slots let more far CTAs reside per SM and at most 10 % of the
+// the fewer slots let more far CTAs reside per SM and at most 5 % of the
 // records then read global memory
 constexpr int FAR_PLAN_SLOTS = 24;
 constexpr int FAR_PLAN_SLOTS_FEW = 16;

@@ -190,8 +190,9 @@ __global__ void mark_far_kernel(LevelGeom G, TreeArgs T, const int* __restrict__
 // leaf's far list (evaluateFromInterp's pairs, ifgfoperator.hpp:1736-1891).
 // Per group: the fine cone and local coordinates of every pair (the lookup
 // of the far kernels), the distinct cones in a hash table of twice the pairs
-// (never full, so every cone is in it), slots for the nslot smallest cone
-// ids, and the records in slot order, each slot's run padded
+// (never full, so every cone is in it), slots for the nslot cones with the
+// most pairs (ties: smaller id first), and the records in slot order, each
+// slot's run padded
 // to FAR_PLAN_PAD positions; pairs of the other cones go last, with their cone ids
 // after the group's slot list.  Every count depends only on the set of cones
 // of the group, not on the order of the atomics, so the two passes agree:
@@ -308,15 +309,20 @@ __global__ void __launch_bounds__(256) far_plan_build_kernel(FarBuildArgs b)
             const int nd = ndist;
             if (threadIdx.x < nd)
             {
-                const int key = klist[threadIdx.x];
+                // rank by pairs (most first), then cone id: the slots hold the
+                // most-used cones, so the fewest pairs read global memory
+                const int key = klist[threadIdx.x], kc = hcnt[kent[threadIdx.x]];
                 int r = 0;
                 for (int u = 0; u < nd; u++)
-                    r += klist[u] < key ? 1 : 0;
+                {
+                    const int cu = hcnt[kent[u]];
+                    r += cu > kc || (cu == kc && klist[u] < key) ? 1 : 0;
+                }
                 hrank[kent[threadIdx.x]] = r;
                 if (r < NS)
                 {
                     sgf[r] = key;
-                    scnt[r] = hcnt[kent[threadIdx.x]];
+                    scnt[r] = kc;
                 }
             }
             __syncthreads(); // slot order complete
@@ -1807,9 +1813,10 @@ void Operator::ensure_far_plan()
     b.n_slot = n_slot.p;
     b.n_ovf = n_ovf.p;
     // the smaller slot count where it lets more far CTAs reside per SM and at
-    // most 10 % of the records would overflow it and read global memory
-    // (measured at p = 9: 16 slots and three CTAs 4.5 % faster at N = 1e6,
-    // k = 100, with 4.6 % overflowing; 10 % slower at N = 2e5 with 15.7 %)
+    // most 5 % of the records would overflow it and read global memory
+    // (measured at p = 9, slots holding the most-used cones: 16 slots and
+    // three CTAs faster at N = 1e6, k = 100, with 2.2 % overflowing; 4 %
+    // slower at N = 2e5 with 6.4 %)
     auto count = [&](int nslot) {
         b.nslot = nslot;
         far_plan_build_kernel<false><<<nc, 256>>>(b);
@@ -1829,7 +1836,7 @@ void Operator::ensure_far_plan()
         const int p_lo = lo_[0] * lo_[1] * lo_[2];
         const bool more_ctas = far_plan_ctas(FAR_PLAN_SLOTS_FEW, p_lo, BATCH_NB) >
                                far_plan_ctas(FAR_PLAN_SLOTS, p_lo, BATCH_NB);
-        if (!more_ctas || o * 10 > r)
+        if (!more_ctas || o * 20 > r)
             count(FAR_PLAN_SLOTS);
     }
     const std::vector<long long> hg = n_group.download(), hr = n_rec.download(),
