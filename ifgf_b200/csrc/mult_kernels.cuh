@@ -1733,11 +1733,19 @@ __host__ __device__ constexpr int c2f_row_stride()
     return s;
 }
 
+// stage 2 of the fixed coarse-to-fine kernel: threads per fine column
+// block j0 (its L0 x H2 row vectors, whole warps, so that a warp works for
+// one j0 only)
+template <int H2, int L0> __host__ __device__ constexpr int c2f_stage2_group()
+{
+    return (L0 * H2 + 31) / 32 * 32;
+}
+
 // one thread per row vector of the widest of the three stages
 template <int H0, int H1, int H2, int L0, int L1, int L2, int F>
 constexpr int c2f_fixed_threads()
 {
-    constexpr int s1 = H1 * H2, s2 = F * L0 * H2, s3 = F * L0 * F * L1;
+    constexpr int s1 = H1 * H2, s2 = F * c2f_stage2_group<H2, L0>(), s3 = F * L0 * F * L1;
     constexpr int m = s1 > s2 ? (s1 > s3 ? s1 : s3) : (s2 > s3 ? s2 : s3);
     return (m + 31) / 32 * 32;
 }
@@ -1750,8 +1758,12 @@ constexpr int c2f_fixed_threads()
 //   stage 2 (thread = (i0, m2)):  Y2[m2][i0 + F0 i1] = sum_m A1[i1][m] Y1[i0][m][m2]
 //   stage 3 (thread = i0 + F0 i1): C[j2 L2 + i2] = sum_m A2[j2 L2 + i2][m] Y2[m][.]
 // Stage 3 writes the coefficients of every active sub-cone straight to
-// global memory.  T is the working precision (double, or float in the mixed
-// pipeline).
+// global memory.  Warps follow the sub-cones: a stage-2 warp works for one
+// fine column block j0 and skips the row blocks j1 whose sub-cones (j0, j1,
+// j2) are all inactive; stage-3 threads go sub-cone by sub-cone (L0 L1 each),
+// so that a warp spans about two sub-cones, skips the j2 where they are
+// inactive and writes each active one's rows as contiguous runs.  T is the
+// working precision (double, or float in the mixed pipeline).
 template <int H0, int H1, int H2, int L0, int L1, int L2, int F, typename T>
 __global__ void __launch_bounds__(c2f_fixed_threads<H0, H1, H2, L0, L1, L2, F>())
     coarse_to_fine_fixed_kernel(C2FArgs a, const C2FMats<H0, H1, H2, L0, L1, L2, F, T> M)
@@ -1799,35 +1811,48 @@ __global__ void __launch_bounds__(c2f_fixed_threads<H0, H1, H2, L0, L1, L2, F>()
         }
     }
     __syncthreads();
-    if (t < F0 * H2)
+    constexpr int G2 = c2f_stage2_group<H2, L0>();
+    if (t < F * G2 && t % G2 < L0 * H2)
     {
-        const int i0 = t % F0, m2 = t / F0;
+        const int j0 = t / G2, u = t % G2;
+        const int i0 = j0 * L0 + u % L0, m2 = u / L0;
         V x[H1];
 #pragma unroll
         for (int m = 0; m < H1; m++)
             x[m] = Y1[i0 + F0 * (m + H1 * m2)];
 #pragma unroll
-        for (int i1 = 0; i1 < F1; i1++)
+        for (int j1 = 0; j1 < F; j1++)
         {
-            T re = 0, im = 0;
+            bool used = false;
 #pragma unroll
-            for (int m = 0; m < H1; m++)
+            for (int j2 = 0; j2 < F; j2++)
+                used |= gsub[j0 + F * (j1 + F * j2)] >= 0;
+            if (!used)
+                continue; // no active sub-cone reads these rows
+#pragma unroll
+            for (int i1 = j1 * L1; i1 < (j1 + 1) * L1; i1++)
             {
-                re = fma(M.a1[i1 * H1 + m], x[m].x, re);
-                im = fma(M.a1[i1 * H1 + m], x[m].y, im);
+                T re = 0, im = 0;
+#pragma unroll
+                for (int m = 0; m < H1; m++)
+                {
+                    re = fma(M.a1[i1 * H1 + m], x[m].x, re);
+                    im = fma(M.a1[i1 * H1 + m], x[m].y, im);
+                }
+                Y2[i0 + F0 * i1 + S2 * m2] = V{re, im};
             }
-            Y2[i0 + F0 * i1 + S2 * m2] = V{re, im};
         }
     }
     __syncthreads();
     if (t < F0 * F1)
     {
-        const int i0f = t % F0, i1f = t / F0;
-        const int j0 = i0f / L0, i0 = i0f % L0, j1 = i1f / L1, i1 = i1f % L1;
+        const int q = t % (L0 * L1), sc = t / (L0 * L1);
+        const int i0 = q % L0, i1 = q / L0, j0 = sc % F, j1 = sc / F;
+        const int i0f = j0 * L0 + i0, i1f = j1 * L1 + i1;
         V x[H2];
 #pragma unroll
         for (int m = 0; m < H2; m++)
-            x[m] = Y2[t + S2 * m];
+            x[m] = Y2[i0f + F0 * i1f + S2 * m];
         V* fco = reinterpret_cast<V*>(a.fcoef) + blockIdx.y * a.fc_plane;
 #pragma unroll
         for (int j2 = 0; j2 < F; j2++)
