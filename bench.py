@@ -60,7 +60,7 @@ REF_BUDGET_S = 100.0
 # (profiles/launches_bench_1e6_mixed_batched.md)
 UPWARD_FFMA_DRAM_B = 19.4
 UPWARD_TC_DRAM_B = 22.1
-FAR_DRAM_B = 26.9
+FAR_DRAM_B = 26.6
 
 
 def parse():
