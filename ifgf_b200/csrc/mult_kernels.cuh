@@ -1762,9 +1762,12 @@ constexpr int c2f_fixed_threads()
 // fine column block j0 and skips the row blocks j1 whose sub-cones (j0, j1,
 // j2) are all inactive; stage-3 threads go sub-cone by sub-cone (L0 L1 each),
 // so that a warp spans about two sub-cones, skips the j2 where they are
-// inactive and writes each active one's rows as contiguous runs.  T is the
-// working precision (double, or float in the mixed pipeline).
-template <int H0, int H1, int H2, int L0, int L1, int L2, int F, typename T>
+// inactive and writes each active one's rows as contiguous runs.  NPL
+// planes per CTA (blockIdx.y: planes NPL y ...): each matrix constant, index
+// and barrier then serves NPL row vectors (2 for FP32 batches: 3.15 -> 3.03
+// ms per batched matvec at N = 1e6).  T is the working precision (double,
+// or float in the mixed pipeline).
+template <int H0, int H1, int H2, int L0, int L1, int L2, int F, typename T, int NPL>
 __global__ void __launch_bounds__(c2f_fixed_threads<H0, H1, H2, L0, L1, L2, F>())
     coarse_to_fine_fixed_kernel(C2FArgs a, const C2FMats<H0, H1, H2, L0, L1, L2, F, T> M)
 {
@@ -1772,13 +1775,15 @@ __global__ void __launch_bounds__(c2f_fixed_threads<H0, H1, H2, L0, L1, L2, F>()
     constexpr int F0 = F * L0, F1 = F * L1;
     constexpr int P_HI = H0 * H1 * H2, P_LO = L0 * L1 * L2;
     constexpr int S2 = c2f_row_stride<F0, F1>();
+    constexpr int Y1N = F0 * H1 * H2, YN = Y1N + S2 * H2; // elements per plane
     extern __shared__ __align__(16) unsigned char c2f_raw[];
-    V* Y1 = reinterpret_cast<V*>(c2f_raw); // [m2][m1][i0], i0 fastest
-    V* Y2 = Y1 + F0 * H1 * H2;             // [m2][S2]
+    // plane p: Y1 at p YN ([m2][m1][i0], i0 fastest), Y2 at p YN + Y1N ([m2][S2])
+    V* Y = reinterpret_cast<V*>(c2f_raw);
     __shared__ int gsub[F * F * F];
     const int c = a.idx ? a.idx[blockIdx.x] : (int)blockIdx.x;
     const int t = threadIdx.x;
     const int box = a.cc_box[c], el = a.cc_el[c];
+    const int p0 = blockIdx.y * NPL; // first plane of the CTA
     if (t < F * F * F)
     {
         const int nc0 = a.G.nc[0], nc1 = a.G.nc[1];
@@ -1791,23 +1796,31 @@ __global__ void __launch_bounds__(c2f_fixed_threads<H0, H1, H2, L0, L1, L2, F>()
     }
     if (t < H1 * H2)
     {
-        const V* src = reinterpret_cast<const V*>(a.cvals) + blockIdx.y * a.cv_plane +
-                       (size_t)c * P_HI + H0 * t;
-        V x[H0];
+        V x[NPL][H0];
 #pragma unroll
-        for (int m = 0; m < H0; m++)
-            x[m] = src[m];
+        for (int p = 0; p < NPL; p++)
+        {
+            const V* src = reinterpret_cast<const V*>(a.cvals) + (p0 + p) * a.cv_plane +
+                           (size_t)c * P_HI + H0 * t;
+#pragma unroll
+            for (int m = 0; m < H0; m++)
+                x[p][m] = src[m];
+        }
 #pragma unroll
         for (int i0 = 0; i0 < F0; i0++)
         {
-            T re = 0, im = 0;
 #pragma unroll
-            for (int m = 0; m < H0; m++)
+            for (int p = 0; p < NPL; p++)
             {
-                re = fma(M.a0[i0 * H0 + m], x[m].x, re);
-                im = fma(M.a0[i0 * H0 + m], x[m].y, im);
+                T re = 0, im = 0;
+#pragma unroll
+                for (int m = 0; m < H0; m++)
+                {
+                    re = fma(M.a0[i0 * H0 + m], x[p][m].x, re);
+                    im = fma(M.a0[i0 * H0 + m], x[p][m].y, im);
+                }
+                Y[p * YN + i0 + F0 * t] = V{re, im};
             }
-            Y1[i0 + F0 * t] = V{re, im};
         }
     }
     __syncthreads();
@@ -1816,10 +1829,12 @@ __global__ void __launch_bounds__(c2f_fixed_threads<H0, H1, H2, L0, L1, L2, F>()
     {
         const int j0 = t / G2, u = t % G2;
         const int i0 = j0 * L0 + u % L0, m2 = u / L0;
-        V x[H1];
+        V x[NPL][H1];
 #pragma unroll
-        for (int m = 0; m < H1; m++)
-            x[m] = Y1[i0 + F0 * (m + H1 * m2)];
+        for (int p = 0; p < NPL; p++)
+#pragma unroll
+            for (int m = 0; m < H1; m++)
+                x[p][m] = Y[p * YN + i0 + F0 * (m + H1 * m2)];
 #pragma unroll
         for (int j1 = 0; j1 < F; j1++)
         {
@@ -1832,14 +1847,18 @@ __global__ void __launch_bounds__(c2f_fixed_threads<H0, H1, H2, L0, L1, L2, F>()
 #pragma unroll
             for (int i1 = j1 * L1; i1 < (j1 + 1) * L1; i1++)
             {
-                T re = 0, im = 0;
 #pragma unroll
-                for (int m = 0; m < H1; m++)
+                for (int p = 0; p < NPL; p++)
                 {
-                    re = fma(M.a1[i1 * H1 + m], x[m].x, re);
-                    im = fma(M.a1[i1 * H1 + m], x[m].y, im);
+                    T re = 0, im = 0;
+#pragma unroll
+                    for (int m = 0; m < H1; m++)
+                    {
+                        re = fma(M.a1[i1 * H1 + m], x[p][m].x, re);
+                        im = fma(M.a1[i1 * H1 + m], x[p][m].y, im);
+                    }
+                    Y[p * YN + Y1N + i0 + F0 * i1 + S2 * m2] = V{re, im};
                 }
-                Y2[i0 + F0 * i1 + S2 * m2] = V{re, im};
             }
         }
     }
@@ -1849,39 +1868,44 @@ __global__ void __launch_bounds__(c2f_fixed_threads<H0, H1, H2, L0, L1, L2, F>()
         const int q = t % (L0 * L1), sc = t / (L0 * L1);
         const int i0 = q % L0, i1 = q / L0, j0 = sc % F, j1 = sc / F;
         const int i0f = j0 * L0 + i0, i1f = j1 * L1 + i1;
-        V x[H2];
+        V x[NPL][H2];
 #pragma unroll
-        for (int m = 0; m < H2; m++)
-            x[m] = Y2[i0f + F0 * i1f + S2 * m];
-        V* fco = reinterpret_cast<V*>(a.fcoef) + blockIdx.y * a.fc_plane;
+        for (int p = 0; p < NPL; p++)
+#pragma unroll
+            for (int m = 0; m < H2; m++)
+                x[p][m] = Y[p * YN + Y1N + i0f + F0 * i1f + S2 * m];
 #pragma unroll
         for (int j2 = 0; j2 < F; j2++)
         {
             const int gf = gsub[j0 + F * (j1 + F * j2)];
             if (gf < 0)
                 continue;
-            V* dst = fco + (size_t)gf * P_LO + i0 + L0 * i1;
 #pragma unroll
             for (int i2 = 0; i2 < L2; i2++)
             {
-                T re = 0, im = 0;
 #pragma unroll
-                for (int m = 0; m < H2; m++)
+                for (int p = 0; p < NPL; p++)
                 {
-                    re = fma(M.a2[(j2 * L2 + i2) * H2 + m], x[m].x, re);
-                    im = fma(M.a2[(j2 * L2 + i2) * H2 + m], x[m].y, im);
+                    T re = 0, im = 0;
+#pragma unroll
+                    for (int m = 0; m < H2; m++)
+                    {
+                        re = fma(M.a2[(j2 * L2 + i2) * H2 + m], x[p][m].x, re);
+                        im = fma(M.a2[(j2 * L2 + i2) * H2 + m], x[p][m].y, im);
+                    }
+                    V* fco = reinterpret_cast<V*>(a.fcoef) + (p0 + p) * a.fc_plane;
+                    fco[(size_t)gf * P_LO + i0 + L0 * i1 + L0 * L1 * i2] = V{re, im};
                 }
-                dst[L0 * L1 * i2] = V{re, im};
             }
         }
     }
 }
 
 template <int H0, int H1, int H2, int L0, int L1, int L2, int F, typename T>
-constexpr size_t c2f_fixed_smem()
+constexpr size_t c2f_fixed_smem(int npl = 1)
 {
     constexpr int F0 = F * L0, F1 = F * L1;
-    return (size_t)(F0 * H1 * H2 + c2f_row_stride<F0, F1>() * H2) * 2 * sizeof(T);
+    return (size_t)npl * (F0 * H1 * H2 + c2f_row_stride<F0, F1>() * H2) * 2 * sizeof(T);
 }
 
 // Launches the fixed-size coarse-to-fine kernel when (hi, lo, f) is one of the
@@ -1905,11 +1929,16 @@ static bool launch_c2f_fixed(const C2FArgs& fa, const double* A_host, unsigned g
         static_assert(sizeof(mats) == NA * sizeof(T), "matrix block layout");                  \
         for (int i = 0; i < NA; i++)                                                           \
             dst[i] = (T)A_host[i];                                                             \
-        constexpr size_t sm = c2f_fixed_smem<A, B, C, D, E, G, F, T>();                        \
-        auto kern = coarse_to_fine_fixed_kernel<A, B, C, D, E, G, F, T>;                       \
+        /* FP32: two planes per CTA share every matrix constant and index */                  \
+        constexpr int NPL = std::is_same<T, float>::value ? 2 : 1;                             \
+        const int npl = planes % NPL == 0 ? NPL : 1;                                           \
+        const size_t sm = c2f_fixed_smem<A, B, C, D, E, G, F, T>(npl);                         \
+        auto kern = npl == 2 ? coarse_to_fine_fixed_kernel<A, B, C, D, E, G, F, T, NPL>        \
+                             : coarse_to_fine_fixed_kernel<A, B, C, D, E, G, F, T, 1>;         \
         if (sm > 48 * 1024)                                                                    \
             cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);  \
-        kern<<<dim3(grid, planes), c2f_fixed_threads<A, B, C, D, E, G, F>(), sm, st>>>(fa, mats); \
+        kern<<<dim3(grid, planes / npl), c2f_fixed_threads<A, B, C, D, E, G, F>(), sm, st>>>(  \
+            fa, mats);                                                                         \
         return true;                                                                           \
     }
 #define IFGF_C2F_CASE(A, B, C, D, E, G)                                                       \
