@@ -45,28 +45,51 @@ static __global__ void permute_batch_kernel(const double* __restrict__ in, int r
 // Leaf sampling of a plane group (blockIdx.z): the factored kernel at a
 // (node, source) pair is evaluated once with unit density and applied to
 // every plane's density (the kernels are linear in the density); with MK once
-// per plane, at its wavenumber.
+// per plane, at its wavenumber.  Each thread takes LEAF_NPT nodes, and a
+// source's data (relative position and squared distance as one float4, the
+// planes' densities as two) are read from shared memory once for all of
+// them.
+constexpr int LEAF_NPT = 4;
+inline int leaf_batch_threads(int P_hi)
+{
+    int t = (P_hi + LEAF_NPT - 1) / LEAF_NPT;
+    t = (t + 31) / 32 * 32;
+    return t < 32 ? 32 : (t > NODE_THREADS ? NODE_THREADS : t);
+}
+inline int leaf_batch_chunks(int P_hi)
+{
+    const int per = LEAF_NPT * leaf_batch_threads(P_hi);
+    return (P_hi + per - 1) / per;
+}
+// dynamic shared memory: per source slot a float4, BATCH_NB float2 and the
+// normal's three floats
+inline size_t leaf_batch_smem(int nt)
+{
+    return (size_t)nt * (sizeof(float4) + BATCH_NB * sizeof(float2) + 3 * sizeof(float));
+}
+
 template <int KIND, bool MK>
 __global__ void __launch_bounds__(NODE_THREADS) leaf_sample_batch_kernel(LeafArgs a, BatchPtrs bp)
 {
     using P = PluginF<KIND>;
-    constexpr int NB = BATCH_NB;
-    extern __shared__ float smb[];
+    constexpr int NB = BATCH_NB, NPQ = LEAF_NPT;
+    static_assert(NB % 2 == 0, "the planes' densities are read as float4 pairs");
+    extern __shared__ __align__(16) float4 leaf_sm4[];
     __shared__ KParams kps[MK ? NB : 1];
     const int pb = blockIdx.z * NB; // first plane of the group
     if constexpr (MK)
         if (threadIdx.x < NB)
             kps[threadIdx.x] = bp.kp_plane[pb + threadIdx.x]; // read after the chunk barriers
     const int c = a.idx[blockIdx.x];
-    const int node0 = blockIdx.y * NPT * blockDim.x;
+    const int node0 = blockIdx.y * NPQ * blockDim.x;
     const int box = a.cc_box[c], el = a.cc_el[c];
     const double xc[3] = {a.T.box_c[3 * box], a.T.box_c[3 * box + 1], a.T.box_c[3 * box + 2]};
     const double H = a.T.box_H[box];
-    float b[NPT][3], dc[NPT];
-    bool live[NPT];
-    cplx<float> acc[NPT][NB];
+    float b[NPQ][3], dc[NPQ];
+    bool live[NPQ];
+    cplx<float> acc[NPQ][NB];
 #pragma unroll
-    for (int q = 0; q < NPT; q++)
+    for (int q = 0; q < NPQ; q++)
     {
         const int n = node0 + threadIdx.x + q * blockDim.x;
 #pragma unroll
@@ -87,14 +110,11 @@ __global__ void __launch_bounds__(NODE_THREADS) leaf_sample_batch_kernel(LeafArg
         }
     }
     const int nt = blockDim.x;
-    float* ax = smb;
-    float* ay = ax + nt;
-    float* az = ay + nt;
-    float* aa = az + nt;
-    float* n0 = aa + nt;
+    float4* sa = leaf_sm4;                                 // [nt] (x, y, z, |.|^2)
+    float4* sw = sa + nt;                                  // [nt][NB / 2] densities
+    float* n0 = reinterpret_cast<float*>(sw + nt * NB / 2); // [nt] x 3 normals
     float* n1 = n0 + nt;
     float* n2 = n1 + nt;
-    float2* wv = reinterpret_cast<float2*>(n2 + nt); // [NB][nt]
     const int f = a.T.box_first[box], l = a.T.box_last[box];
     for (int cs = f; cs < l; cs += nt)
     {
@@ -104,13 +124,15 @@ __global__ void __launch_bounds__(NODE_THREADS) leaf_sample_batch_kernel(LeafArg
         {
             const int i = cs + threadIdx.x;
             const double a0 = a.S.sx[i] - xc[0], a1 = a.S.sy[i] - xc[1], a2 = a.S.sz[i] - xc[2];
-            ax[threadIdx.x] = (float)a0;
-            ay[threadIdx.x] = (float)a1;
-            az[threadIdx.x] = (float)a2;
-            aa[threadIdx.x] = (float)(a0 * a0 + a1 * a1 + a2 * a2);
+            sa[threadIdx.x] =
+                make_float4((float)a0, (float)a1, (float)a2, (float)(a0 * a0 + a1 * a1 + a2 * a2));
 #pragma unroll
-            for (int r = 0; r < NB; r++)
-                wv[r * nt + threadIdx.x] = bp.w[(size_t)(pb + r) * bp.n_src + i];
+            for (int r = 0; r < NB; r += 2)
+            {
+                const float2 u = bp.w[(size_t)(pb + r) * bp.n_src + i];
+                const float2 v = bp.w[(size_t)(pb + r + 1) * bp.n_src + i];
+                sw[threadIdx.x * (NB / 2) + r / 2] = make_float4(u.x, u.y, v.x, v.y);
+            }
             if (P::needs_normals)
             {
                 n0[threadIdx.x] = (float)a.S.nx[i];
@@ -124,16 +146,21 @@ __global__ void __launch_bounds__(NODE_THREADS) leaf_sample_batch_kernel(LeafArg
         // runs over the sources in order)
         for (int i = 0; i < cnt; i++)
         {
-            const float av[3] = {ax[i], ay[i], az[i]};
-            const float aai = aa[i];
+            const float4 s4 = sa[i];
+            const float av[3] = {s4.x, s4.y, s4.z};
+            const float aai = s4.w;
             const float nv[3] = {P::needs_normals ? n0[i] : 0.f, P::needs_normals ? n1[i] : 0.f,
                                  P::needs_normals ? n2[i] : 0.f};
             float2 wr[NB];
 #pragma unroll
-            for (int r = 0; r < NB; r++)
-                wr[r] = wv[r * nt + i];
+            for (int r = 0; r < NB; r += 2)
+            {
+                const float4 u = sw[i * (NB / 2) + r / 2];
+                wr[r] = make_float2(u.x, u.y);
+                wr[r + 1] = make_float2(u.z, u.w);
+            }
 #pragma unroll
-            for (int q = 0; q < NPT; q++)
+            for (int q = 0; q < NPQ; q++)
             {
                 if (!live[q])
                     continue;
@@ -162,7 +189,7 @@ __global__ void __launch_bounds__(NODE_THREADS) leaf_sample_batch_kernel(LeafArg
         }
     }
 #pragma unroll
-    for (int q = 0; q < NPT; q++)
+    for (int q = 0; q < NPQ; q++)
     {
         const int n = node0 + threadIdx.x + q * blockDim.x;
         if (n < a.P_hi)
@@ -401,8 +428,8 @@ static int run_mult_batch(const MultPtrs& m, const BatchPtrs& bp, const void* d_
                 IFGF_CHECK(cudaEventRecord(m.ev_join, m.side));
             launches++;
         }
-        const int nthr = node_threads(m.P_hi);
-        const int nchk = node_chunks(m.P_hi);
+        const int nthr = leaf_batch_threads(m.P_hi);
+        const int nchk = leaf_batch_chunks(m.P_hi);
         for (int l = m.L - 1; l >= 0; l--)
         {
             const LevelGeom& G = m.lv_host[l];
@@ -416,8 +443,7 @@ static int run_mult_batch(const MultPtrs& m, const BatchPtrs& bp, const void* d_
                 if (hk)
                     hk->begin(PROF_COARSE, l);
                 leaf_sample_batch_kernel<KIND, MK>
-                    <<<dim3(LL.n_leaf, nchk, bp.groups), nthr,
-                       (7 * nthr + 2 * BATCH_NB * nthr) * sizeof(float), st>>>(la, bp);
+                    <<<dim3(LL.n_leaf, nchk, bp.groups), nthr, leaf_batch_smem(nthr), st>>>(la, bp);
                 IFGF_CHECK_LAUNCH();
                 if (hk)
                     hk->end();
