@@ -48,7 +48,8 @@ static __global__ void permute_batch_kernel(const double* __restrict__ in, int r
 // per plane, at its wavenumber.  Each thread takes LEAF_NPT nodes, and a
 // source's data (relative position and squared distance as one float4, the
 // planes' densities as two) are read from shared memory once for all of
-// them.
+// them (measured per batched matvec at N = 1e6, p = 9: 2 nodes 3.23 ms, 3
+// nodes 3.17, 4 nodes 3.06, 6 nodes 3.88).
 constexpr int LEAF_NPT = 4;
 inline int leaf_batch_threads(int P_hi)
 {
