@@ -1361,8 +1361,11 @@ constexpr int UPS_THREADS = 64;
 // 16-byte chunks).
 // MK: every plane (blockIdx.y) has its own wavenumber; the centre-shift
 // factor is formed from the distance table per plane.
+// At least 8 CTAs per SM (128 registers; measured at N = 1e6, p = 9: levels
+// 2 and 3 of the batched matvec 0.79 + 3.45 ms with 8 or 7, 0.86 + 3.71 with
+// 10 (96 registers, more spills), 0.85 + 3.66 with 6, 0.93 + 4.09 with 12).
 template <int KIND, int N0, int N1, int N2, bool MK = false>
-__global__ void __launch_bounds__(UPS_THREADS, 10) upward_staged_kernel(UpArgs a)
+__global__ void __launch_bounds__(UPS_THREADS, 8) upward_staged_kernel(UpArgs a)
 {
     constexpr int R = UPGEO_RUN;
     constexpr int P_LO = N0 * N1 * N2;

@@ -88,9 +88,14 @@ def test_batch_planes_follow_a_reinitialised_tree():
     fresh = make_gpu_op("helmholtz", leaf=50, order=8, k=60.0)
     fresh.init(pts, pts)
     fresh.set_precision("mixed")
-    ug, uf = g.mult_batch(w), fresh.mult_batch(w)
-    for b in range(5):
-        assert rel2(ug[b], uf[b]) <= 1e-14, b
+    # the same upward kernel in both (each operator's autotuner times its own
+    # launches and may pick the other kernel on a near tie)
+    for path in ("ffma", "tensor"):
+        g.set_upward_path(path)
+        fresh.set_upward_path(path)
+        ug, uf = g.mult_batch(w), fresh.mult_batch(w)
+        for b in range(5):
+            assert rel2(ug[b], uf[b]) <= 1e-14, (path, b)
 
 
 @pytest.mark.gpu

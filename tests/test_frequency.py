@@ -58,11 +58,17 @@ def test_wavenumber_change_with_new_grids_reinitialises():
     fresh = G.HelmholtzIfgfOperator(60.0, 64, 8)
     fresh.init(pts, pts)
     assert rel2(op.mult(w), fresh.mult(w)) <= 1e-14
-    # mixed precision and batched right-hand sides follow the new wavenumber
+    # mixed precision and batched right-hand sides follow the new wavenumber,
+    # on either upward kernel (pinned: the autotuner of each operator times
+    # its own launches, and two near-equal timings may pick different
+    # kernels, whose FP32 results differ in rounding)
     op.set_precision("mixed")
     fresh.set_precision("mixed")
     wb = np.stack([w, W.densities(n, seed=2)])
-    assert rel2(op.mult_batch(wb), fresh.mult_batch(wb)) <= 1e-14
+    for path in ("ffma", "tensor"):
+        op.set_upward_path(path)
+        fresh.set_upward_path(path)
+        assert rel2(op.mult_batch(wb), fresh.mult_batch(wb)) <= 1e-14, path
 
 
 @pytest.mark.gpu

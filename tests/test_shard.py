@@ -219,6 +219,9 @@ def test_plane_parallel_and_sharded_batches_on_one_gpu():
         full = make_gpu_op("helmholtz", leaf=50, order=8)
         full.init(pts, pts)
         full.set_precision("mixed")
+        # one upward kernel for both operators (each one's autotuner times its
+        # own launches and may pick the other kernel on a near tie)
+        full.set_upward_path("ffma")
         uf = full.mult_batch(w)
         dw = torch.from_numpy(w).cuda()
         du = torch.zeros_like(dw)
@@ -229,6 +232,7 @@ def test_plane_parallel_and_sharded_batches_on_one_gpu():
         up = du.cpu().numpy()
         sh = ShardedOperator(make_gpu_op("helmholtz", leaf=50, order=8), pts, pts)
         sh.op.set_precision("mixed")
+        sh.op.set_upward_path("ffma")
         ds = torch.zeros_like(dw)
         sh.mult_batch_device(dw, ds)
         torch.cuda.synchronize()
