@@ -58,9 +58,9 @@ REF_BUDGET_S = 100.0
 # per (target, far box) pair; from the full-size launch list with
 # dram__bytes_read.sum + dram__bytes_write.sum
 # (profiles/launches_bench_1e6_mixed_batched.md)
-UPWARD_FFMA_DRAM_B = 19.4
-UPWARD_TC_DRAM_B = 22.1
-FAR_DRAM_B = 26.6
+UPWARD_FFMA_DRAM_B = 19.3
+UPWARD_TC_DRAM_B = 22.2
+FAR_DRAM_B = 26.7
 
 
 def parse():
