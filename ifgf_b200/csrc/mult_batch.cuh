@@ -51,15 +51,19 @@ static __global__ void permute_batch_kernel(const double* __restrict__ in, int r
 // them (measured per batched matvec at N = 1e6, p = 9: 2 nodes 3.23 ms, 3
 // nodes 3.17, 4 nodes 3.06, 6 nodes 3.88).
 constexpr int LEAF_NPT = 4;
-inline int leaf_batch_threads(int P_hi)
+// with MK every (node, plane) pair has its own kernel evaluation, so more
+// nodes per thread save no evaluations: two, at fewer registers (the
+// 64-wavenumber CQ batch at N = 1e5: 61.8 ms, 66.6 with four)
+__host__ __device__ constexpr int leaf_npt(bool mk) { return mk ? 2 : LEAF_NPT; }
+inline int leaf_batch_threads(int P_hi, int npt)
 {
-    int t = (P_hi + LEAF_NPT - 1) / LEAF_NPT;
+    int t = (P_hi + npt - 1) / npt;
     t = (t + 31) / 32 * 32;
     return t < 32 ? 32 : (t > NODE_THREADS ? NODE_THREADS : t);
 }
-inline int leaf_batch_chunks(int P_hi)
+inline int leaf_batch_chunks(int P_hi, int npt)
 {
-    const int per = LEAF_NPT * leaf_batch_threads(P_hi);
+    const int per = npt * leaf_batch_threads(P_hi, npt);
     return (P_hi + per - 1) / per;
 }
 // dynamic shared memory: per source slot a float4, BATCH_NB float2 and the
@@ -73,7 +77,7 @@ template <int KIND, bool MK>
 __global__ void __launch_bounds__(NODE_THREADS) leaf_sample_batch_kernel(LeafArgs a, BatchPtrs bp)
 {
     using P = PluginF<KIND>;
-    constexpr int NB = BATCH_NB, NPQ = LEAF_NPT;
+    constexpr int NB = BATCH_NB, NPQ = leaf_npt(MK);
     static_assert(NB % 2 == 0, "the planes' densities are read as float4 pairs");
     extern __shared__ __align__(16) float4 leaf_sm4[];
     __shared__ KParams kps[MK ? NB : 1];
@@ -429,8 +433,8 @@ static int run_mult_batch(const MultPtrs& m, const BatchPtrs& bp, const void* d_
                 IFGF_CHECK(cudaEventRecord(m.ev_join, m.side));
             launches++;
         }
-        const int nthr = leaf_batch_threads(m.P_hi);
-        const int nchk = leaf_batch_chunks(m.P_hi);
+        const int nthr = leaf_batch_threads(m.P_hi, leaf_npt(MK));
+        const int nchk = leaf_batch_chunks(m.P_hi, leaf_npt(MK));
         for (int l = m.L - 1; l >= 0; l--)
         {
             const LevelGeom& G = m.lv_host[l];
