@@ -226,10 +226,11 @@ struct __align__(16) FarPlanRec
 {
     int l0, l1, l2, w;
 };
-// slots per group of a plan: FAR_PLAN_SLOTS, or FAR_PLAN_SLOTS_FEW where
-// the fewer slots let more far CTAs reside per SM and at most 5 % of the
-// records then read global memory
+// slots per group of a plan: FAR_PLAN_SLOTS, or the larger of
+// FAR_PLAN_SLOTS_MID and FAR_PLAN_SLOTS_FEW that lets more far CTAs reside
+// per SM, where at most 3 % of the records then read global memory
 constexpr int FAR_PLAN_SLOTS = 24;
+constexpr int FAR_PLAN_SLOTS_MID = 18;
 constexpr int FAR_PLAN_SLOTS_FEW = 16;
 constexpr int FAR_PLAN_THREADS = 256, FAR_PLAN_PAD = 4;
 // record positions of a group with nsl slots (each slot's run padded)

@@ -560,6 +560,8 @@ static int run_mult_batch(const MultPtrs& m, const BatchPtrs& bp, const void* d_
                 };
                 if (bp.fp_nslot <= FAR_PLAN_SLOTS_FEW)
                     IFGF_CHECK(launch_plan(std::integral_constant<int, FAR_PLAN_SLOTS_FEW>{}));
+                else if (bp.fp_nslot <= FAR_PLAN_SLOTS_MID)
+                    IFGF_CHECK(launch_plan(std::integral_constant<int, FAR_PLAN_SLOTS_MID>{}));
                 else
                     IFGF_CHECK(launch_plan(std::integral_constant<int, FAR_PLAN_SLOTS>{}));
             }

@@ -70,7 +70,7 @@ struct DeviceState
     DevBuf<int> fp_slot;
     int fp_nchunk = 0;
     int fp_nslot = 0;
-    double fp_ovf_few = 0; // share of the records beyond FAR_PLAN_SLOTS_FEW slots
+    double fp_ovf_few = 0; // share of the records beyond the smaller slot count tried
     bool fp_ready = false;
     double fp_ms = 0;
     DevBuf<double2> w, cvals, fcoef, unear;
@@ -1812,19 +1812,29 @@ void Operator::ensure_far_plan()
     b.n_rec = n_rec.p;
     b.n_slot = n_slot.p;
     b.n_ovf = n_ovf.p;
-    // the smaller slot count where it lets more far CTAs reside per SM and at
-    // most 5 % of the records would overflow it and read global memory
-    // (measured at p = 9, slots holding the most-used cones: 16 slots and
-    // three CTAs faster at N = 1e6, k = 100, with 2.2 % overflowing; 4 %
-    // slower at N = 2e5 with 6.4 %)
+    // a smaller slot count where it lets more far CTAs reside per SM and at
+    // most 3 % of the records would overflow it and read global memory
+    // (measured at p = 9, slots holding the most-used cones: at N = 1e6,
+    // k = 100, 16 slots and three CTAs faster than 24 with 2.2 %
+    // overflowing, 18 faster still with 1.7 %; at N = 2e5 16 slots 4 %
+    // slower with 6.4 %, 18 slots 2.6 % slower)
     auto count = [&](int nslot) {
         b.nslot = nslot;
         far_plan_build_kernel<false><<<nc, 256>>>(b);
         IFGF_CUDA(cudaGetLastError());
         IFGF_CUDA(cudaDeviceSynchronize());
     };
-    count(FAR_PLAN_SLOTS_FEW);
     {
+        // the larger of the two smaller slot counts that still gives more
+        // CTAs per SM than FAR_PLAN_SLOTS (fewer records overflow with more
+        // slots); FAR_PLAN_SLOTS where neither does
+        const int p_lo = lo_[0] * lo_[1] * lo_[2];
+        const int full = far_plan_ctas(FAR_PLAN_SLOTS, p_lo, BATCH_NB);
+        const int few = far_plan_ctas(FAR_PLAN_SLOTS_MID, p_lo, BATCH_NB) > full ? FAR_PLAN_SLOTS_MID
+                        : far_plan_ctas(FAR_PLAN_SLOTS_FEW, p_lo, BATCH_NB) > full
+                            ? FAR_PLAN_SLOTS_FEW
+                            : FAR_PLAN_SLOTS;
+        count(few);
         const std::vector<long long> ho = n_ovf.download(), hr0 = n_rec.download();
         long long o = 0, r = 0;
         for (int c = 0; c < nc; c++)
@@ -1833,10 +1843,7 @@ void Operator::ensure_far_plan()
             r += hr0[c];
         }
         D.fp_ovf_few = r > 0 ? (double)o / (double)r : 0.0;
-        const int p_lo = lo_[0] * lo_[1] * lo_[2];
-        const bool more_ctas = far_plan_ctas(FAR_PLAN_SLOTS_FEW, p_lo, BATCH_NB) >
-                               far_plan_ctas(FAR_PLAN_SLOTS, p_lo, BATCH_NB);
-        if (!more_ctas || o * 20 > r)
+        if (few != FAR_PLAN_SLOTS && o * 100 > 3 * r)
             count(FAR_PLAN_SLOTS);
     }
     const std::vector<long long> hg = n_group.download(), hr = n_rec.download(),
